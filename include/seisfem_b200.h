@@ -1,0 +1,169 @@
+/*
+ * seisfem_b200.h -- C ABI of libseisfem_b200.so, a B200 (sm_100a) drop-in for
+ * SeisFEM's mass-lumped explicit time-stepping path.
+ *
+ * Three layers:
+ *   1. elastic_wave()            the reference's own entry point, same
+ *                                signature, same files, computed on the GPU;
+ *   2. sfg_* seams               the inner reference functions elastic_wave()
+ *                                calls (assembly, COO->CSR, M-PML, SpMV), same
+ *                                argument meaning, computed on the GPU;
+ *   3. sfg_ctx API               explicit context: assemble once, run many
+ *                                shots (batched), read results, with int
+ *                                status codes instead of exit(1).
+ *
+ * Conventions (as in the reference): element_node is 1-based and
+ * element-major [element_num * element_order]; node coordinates are two
+ * arrays x = node_xy[0], y = node_xy[1]; CSR output is 0-based; model c[] is
+ * [4][node_num] = c11, c13, c33, c44.  All host pointers are borrowed for the
+ * duration of a call only.  Every sfg_* call returns SFG_OK (0) or an
+ * SFG_ERR_* code; sfg_last_error() gives the message.  One context is used
+ * by one host thread at a time; contexts are independent.
+ */
+#ifndef SEISFEM_B200_H
+#define SEISFEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define SFG_OK 0
+#define SFG_ERR_ARG 1         /* bad argument: NULL, size, type or solver string */
+#define SFG_ERR_CUDA 2        /* CUDA runtime error (message in sfg_last_error) */
+#define SFG_ERR_OOM 3         /* device allocation failed */
+#define SFG_ERR_ZERO_AREA 4   /* an element of zero area (mass_sparse_q4.c:191-196) */
+#define SFG_ERR_BADINDEX 5    /* element_node / source / receiver index out of range */
+#define SFG_ERR_BLOWUP 6      /* energy above 1e7 or non-finite (elastic_wave.c:779-785) */
+#define SFG_ERR_ROWLEN 7      /* a matrix row longer than the device canonicaliser handles */
+#define SFG_ERR_STATE 8       /* call out of order (run before setup, ...) */
+#define SFG_ERR_TIMEOUT 9     /* a bounded device-side wait gave up */
+#define SFG_ERR_NODEVICE 10   /* no CUDA device / wrong architecture */
+
+/* ------------------------------------------------------------- precision */
+#define SFG_FP32_KAHAN 0      /* FP32 step, Kahan-compensated displacement (default) */
+#define SFG_FP32 1            /* FP32 step, plain accumulation */
+#define SFG_FP64 2            /* FP64 step, reference operation order, no FMA */
+#define SFG_FP32_PLAIN_PATH 3 /* FP32, one SpMV launch per product + pointwise
+                                 kernels, as elastic_wave.c structures the step
+                                 (the unfused baseline) */
+
+/* matrices: 0 = consistent mass M, 1..6 = stiffness types 1..6
+ * (elastic_wave.c:6-17; stif type 0 is not on the path) */
+#define SFG_MAT_MASS 0
+
+typedef struct sfg_ctx sfg_ctx;
+
+typedef struct {
+    const char *type;          /* "T3","T6","T10","Q4","Q9","Q16" */
+    int node_num;
+    int element_num;
+    int element_order;
+    const int *element_node;   /* 1-based, [element_num * element_order] */
+    const double *x;           /* node_xy[0] */
+    const double *y;           /* node_xy[1] */
+    double xmin, xmax, ymin, ymax;
+    double edge_size;
+    int pml_nx, pml_ny;        /* M-PML thickness in elements */
+    int free_surface;          /* 1: x = xmax is a free surface */
+} sfg_mesh;
+
+typedef struct {
+    const double *rho;         /* [node_num] */
+    const double *vp;          /* [node_num] (vp_max sets the M-PML profile) */
+    const double *vs;          /* [node_num] (carried, unused by the path) */
+    const double *c;           /* [4][node_num] c11, c13, c33, c44 */
+} sfg_model;
+
+typedef struct {
+    int step;                  /* the loop runs it = 2 .. step-1 (elastic_wave.c:519) */
+    double dt, f0, t0;
+    int src_num;  const int *src_node;   /* 0-based node per shot */
+    int rec_num;  const int *rec_node;   /* 0-based node per receiver */
+    int precision;             /* SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH */
+    int snap_every;            /* 0: no snapshots; 200 reproduces the reference */
+    int shots_per_batch;       /* shots advanced together; 0 = automatic */
+} sfg_run_desc;
+
+typedef struct {
+    double setup_ms;           /* last sfg_setup: assembly + canonical CSR on the GPU */
+    double loop_ms;            /* last sfg_run: time loop only (CUDA events) */
+    double total_ms;           /* last sfg_run: including transfers */
+    long long dof_steps;       /* 2 * node_num * shots * (step - 2) of the last run */
+    long long union_nnz;       /* nonzeros of the union pattern the step kernel streams */
+    long long csr_nnz[7];      /* nonzeros of M, K1..K6 after zero elimination */
+    int kernel_launches;       /* kernels launched by the last run's time loop */
+    int rows_per_block;        /* launch shape the autotuner picked */
+    int blowup_step;           /* first step whose energy bound failed, -1 if none */
+} sfg_stats;
+
+/* ---------------------------------------------------------- context API */
+sfg_ctx *sfg_create(int device);                  /* NULL when no usable device */
+void sfg_destroy(sfg_ctx *ctx);
+const char *sfg_error_string(int status);
+const char *sfg_last_error(const sfg_ctx *ctx);
+
+/* Assemble M, K1..K6 (FP64, bit-exact COO values), canonicalise them to CSR
+ * (bit-exact with coo2csr_lib.f90), lumped mass, M-PML profiles, Dirichlet
+ * flags, and build the device step data.  Replaces elastic_wave.c:136-313. */
+int sfg_setup(sfg_ctx *ctx, const sfg_mesh *mesh, const sfg_model *model);
+
+int sfg_csr_nnz(sfg_ctx *ctx, int matrix, int *nnz);
+int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x);
+int sfg_lumped_mass_copy(sfg_ctx *ctx, double *mass_lump);         /* [node_num] */
+int sfg_mpml_copy(sfg_ctx *ctx, double *out6);                       /* [6][node_num] */
+
+/* Run every shot (elastic_wave.c:446-809).  Outputs (any may be NULL):
+ *   seis_u, seis_w  [src_num][step-2][rec_num]  displacement at receivers
+ *   snap_u, snap_w  [src_num][rows][node_num]   row 0 = initial zero field,
+ *                   then each step with (it+1) % snap_every == 0
+ * Returns SFG_ERR_BLOWUP (results up to the failing step are valid) when the
+ * reference would have stopped on its energy bound. */
+int sfg_run(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w,
+            double *snap_u, double *snap_w);
+int sfg_snapshot_rows(int step, int snap_every);
+int sfg_get_stats(const sfg_ctx *ctx, sfg_stats *stats);
+
+/* Device-resident variant for callers that keep data on the GPU: the same
+ * run, outputs written to device pointers (FP32 for the FP32 precisions,
+ * FP64 otherwise, layout as sfg_run), work queued on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream), no host copies and no
+ * synchronisation.  Check the status of the queued work with sfg_sync(). */
+int sfg_run_device(sfg_ctx *ctx, const sfg_run_desc *run, void *d_seis_u, void *d_seis_w,
+                   void *stream);
+int sfg_sync(sfg_ctx *ctx);
+
+/* ----------------------------------------------------------- the seams */
+/* drop-in for time_evolution/elastic_wave.c:1-3 (solver "masslump"; any other
+ * solver string exits like the reference, elastic_wave.c:747-753) */
+void elastic_wave(char *type, int node_num, int element_num, int element_order, int *element_node,
+                  double **node_xy, int nnz, int csr_p_size, int step, double dt, double f0,
+                  double t0, double edge_size, double xmin, double xmax, double ymin, double ymax,
+                  int pml_nx, int pml_ny, int src_num, int *src_node, int rec_num, int *rec_node,
+                  char *solver, int use_exterior_mesh, int free_surface_code);
+
+/* assemble/mass_sparse_all.c:13-68 (lumpflag 1: mass_coo_x[0..node_num) is the lumped mass) */
+int sfg_mass_sparse_all(char *type, int node_num, int element_num, int element_order,
+                        int *element_node, double **node_xy, double *rho, int *mass_coo_i,
+                        int *mass_coo_j, double *mass_coo_x, int lumpflag);
+/* assemble/stif_sparse_all.c:8-62 */
+int sfg_stif_sparse_all(char *type, int node_num, int element_num, int element_order,
+                        int *element_node, double **node_xy, int *stiffi, int *stiffj,
+                        double *stiffness, int stif_type);
+/* sparse_matrix/coo2csr_lib.f90:6-41 (Fortran ABI in elastic_wave.c:241): all
+ * by pointer, Ai/Aj left incremented by one like the reference, 0-based output */
+int sfg_coo2csr_canonical(int *nnz, int *Bp_size, int *csr_size, int *Ai, int *Aj, double *Ax,
+                          int *Bp, int *Bj, double *Bx);
+/* pml/abc_mpml.c:1-4 */
+int sfg_abc_mpml(int node_num, int element_num, int element_order, int *element_node,
+                 double **node_xy, int mpml_nx, int mpml_ny, double h, double xmin, double xmax,
+                 double ymin, double ymax, double vp_max, int use_mpml_xmin, int use_mpml_xmax,
+                 int use_mpml_ymin, int use_mpml_ymax, double *mpml_dx, double *mpml_dy,
+                 double *mpml_dxx, double *mpml_dyy, double *mpml_dxx_pyx, double *mpml_dyy_pxy);
+/* sparse_matrix/csr_matvec.c:1 (FP64, same per-row summation order) */
+int sfg_csr_matvec(int Bp_size, int *Bp, int *Bj, double *Bx, double *x, double *y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,701 @@
+// sfg_api.cu -- the C ABI: context, set-up (GPU assembly), CUDA-graph time
+// loop, autotuned launch shapes, and the reference-shaped seams.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sfg_internal.h"
+#include "sfg_step.cuh"
+
+using namespace sfg;
+
+struct RunCache {
+    // launch shapes picked by the autotuner, keyed by kernel kind and shot count
+    int threads_fp32 = 0, threads_fp32k = 0;
+    int warps_b[3][2] = {{0, 0}, {0, 0}, {0, 0}};   // [spl index][kahan]
+};
+
+struct sfg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool ready = false;
+    DevProblem P;
+    // host copies of what the run needs
+    int N = 0;
+    double xmin = 0, xmax = 0, ymin = 0, ymax = 0, edge = 0;
+    int pml_nx = 0, pml_ny = 0, free_surface = 0;
+    double vp_max = 0;
+    sfg_stats stats;
+    RunCache tune;
+    // plain-path CSR (FP32) built on first use
+    float *plain_x[7] = {nullptr};
+};
+
+namespace {
+
+const char *kStatus[] = {"ok", "bad argument", "CUDA error", "device out of memory", "zero-area element",
+                         "index out of range", "energy bound exceeded", "row too long",
+                         "call out of order", "device wait timed out", "no usable CUDA device"};
+
+int fail(sfg_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SFG_ERR_OOM : SFG_ERR_CUDA,  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+template <typename T>
+cudaError_t upload(T **d, const T *h, size_t n, cudaStream_t st)
+{
+    cudaError_t e = cudaMalloc((void **)d, sizeof(T) * std::max<size_t>(n, 1));
+    if (e != cudaSuccess) return e;
+    if (n) e = cudaMemcpyAsync(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st);
+    return e;
+}
+
+int type_code_of(const char *t)
+{
+    if (!t) return -1;
+    static const char *names[] = {"T3", "T6", "T10", "Q4", "Q9", "Q16"};
+    for (int i = 0; i < 6; i++)
+        if (std::strcmp(t, names[i]) == 0) return i + 1;
+    return -1;
+}
+
+void free_problem(DevProblem &P)
+{
+    cudaFree(P.up); cudaFree(P.uj); cudaFree(P.ux);
+    for (auto &c : P.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
+    cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
+    cudaFree(P.sell); cudaFree(P.slice_ptr); cudaFree(P.rec32); cudaFree(P.coef32); cudaFree(P.coefd);
+    P = DevProblem();
+}
+
+double ricker(double f0, double t0, double mag, double t)
+{
+    // source_receiver/seismic_source.c:16-24
+    const double pi = 3.141592653589793238462643;
+    double a = (pi * f0 * (t - t0)) * (pi * f0 * (t - t0));
+    return mag * (1 - 2 * a) * std::exp(-a);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *sfg_error_string(int s)
+{
+    return (s >= 0 && s <= 10) ? kStatus[s] : "unknown status";
+}
+
+const char *sfg_last_error(const sfg_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+sfg_ctx *sfg_create(int device)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return nullptr;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+    sfg_ctx *c = new sfg_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    std::memset(&c->stats, 0, sizeof c->stats);
+    c->stats.blowup_step = -1;
+    return c;
+}
+
+void sfg_destroy(sfg_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_problem(c->P);
+    for (auto &p : c->plain_x) cudaFree(p);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int sfg_snapshot_rows(int step, int snap_every)
+{
+    if (snap_every <= 0) return 0;
+    int n = 1;
+    for (int it = 2; it < step; it++)
+        if ((it + 1) % snap_every == 0) n++;
+    return n;
+}
+
+int sfg_get_stats(const sfg_ctx *c, sfg_stats *s)
+{
+    if (!c || !s) return SFG_ERR_ARG;
+    *s = c->stats;
+    return SFG_OK;
+}
+
+// ------------------------------------------------------------------ set-up
+
+int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
+{
+    if (!ctx || !m || !md) return SFG_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    ctx->ready = false;
+    free_problem(ctx->P);
+    const int tc = type_code_of(m->type);
+    if (tc < 0) return fail(ctx, SFG_ERR_ARG, std::string("unknown element type ") + (m->type ? m->type : "(null)"));
+    const int p = elem_order_host(tc);
+    if (m->element_order != p || m->node_num <= 0 || m->element_num <= 0 || !m->element_node || !m->x ||
+        !m->y || !md->rho || !md->vp || !md->c)
+        return fail(ctx, SFG_ERR_ARG, "inconsistent mesh/model description");
+    const int N = m->node_num, E = m->element_num;
+    const long long nnz = (long long)E * p * p;
+    if (nnz >= (1LL << 31)) return fail(ctx, SFG_ERR_ARG, "COO size exceeds 2^31");
+    for (long long k = 0; k < (long long)E * p; k++)
+        if (m->element_node[k] < 1 || m->element_node[k] > N)
+            return fail(ctx, SFG_ERR_BADINDEX, "element_node entry out of range at " + std::to_string(k));
+    cudaStream_t st = ctx->stream;
+    DevProblem &P = ctx->P;
+    P.type_code = tc; P.order = p; P.node_num = N; P.element_num = E; P.coo_nnz = nnz;
+    ctx->N = N;
+    ctx->xmin = m->xmin; ctx->xmax = m->xmax; ctx->ymin = m->ymin; ctx->ymax = m->ymax;
+    ctx->edge = m->edge_size; ctx->pml_nx = m->pml_nx; ctx->pml_ny = m->pml_ny;
+    ctx->free_surface = m->free_surface;
+
+    int *d_en = nullptr, *d_flags = nullptr, *d_ci = nullptr, *d_cj = nullptr;
+    double *d_x = nullptr, *d_y = nullptr, *d_rho = nullptr, *d_cx = nullptr, *d_scr = nullptr;
+    CK(upload(&d_en, m->element_node, (size_t)E * p, st));
+    CK(upload(&d_x, m->x, (size_t)N, st));
+    CK(upload(&d_y, m->y, (size_t)N, st));
+    CK(upload(&d_rho, md->rho, (size_t)N, st));
+    CK(upload(&P.coef64, md->c, (size_t)4 * N, st));
+    CK(cudaMalloc(&d_flags, sizeof(int)));
+    CK(cudaMemsetAsync(d_flags, 0, sizeof(int), st));
+    CK(cudaMalloc(&d_ci, sizeof(int) * nnz));
+    CK(cudaMalloc(&d_cj, sizeof(int) * nnz));
+    CK(cudaMalloc(&d_cx, sizeof(double) * 7 * nnz));
+
+    // element matrices: consistent mass (with rho) and stiffness types 1..6
+    const int mats[7] = {-1, 1, 2, 3, 4, 5, 6};
+    CK(launch_element_coo(tc, E, d_en, d_x, d_y, d_rho, 7, mats, d_ci, d_cj, d_cx, d_flags, st));
+    int hflags = 0;
+    CK(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hflags & FLAG_ZERO_AREA) {
+        cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+        cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx);
+        return fail(ctx, SFG_ERR_ZERO_AREA, "an element has zero area");
+    }
+    CanonOut co;
+    int rc = canonicalize(N, nnz, d_ci, d_cj, d_cx, 7, true, true, co, d_flags, st, ctx->err);
+    if (rc != SFG_OK) {
+        canon_free(co, false);
+        cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+        cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx);
+        return rc;
+    }
+    for (int k = 0; k < 7; k++) P.csr[k] = co.csr[k];
+    P.up = co.up; P.uj = co.uj; P.ux = co.ux; P.union_nnz = co.union_nnz; P.max_row_len = co.max_row_len;
+
+    // lumped mass (mass_sparse_*.c, lumpflag = 1)
+    CK(cudaMalloc(&P.mass_lump, sizeof(double) * N));
+    CK(cudaMalloc(&d_scr, sizeof(double) * (2 * (size_t)E + 2)));
+    CK(launch_lumped_mass(tc, N, E, d_en, d_x, d_y, d_rho, co.row_start, co.bucket, d_cj, P.mass_lump, d_scr,
+                          d_flags, st));
+
+    // M-PML (elastic_wave.c:157, 221-228; abc_mpml.c:50-61)
+    double vp_max = md->vp[0];
+    for (int i = 0; i < N; i++) if (md->vp[i] > vp_max) vp_max = md->vp[i];
+    ctx->vp_max = vp_max;
+    const double Rcoef = 0.0001;
+    const double tx = m->edge_size * m->pml_nx, ty = m->edge_size * m->pml_ny;
+    const double d0x = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * tx);
+    const double d0y = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * ty);
+    CK(cudaMalloc(&P.mpml, sizeof(double) * 6 * (size_t)N));
+    CK(launch_mpml(N, d_x, d_y, co.row_start, d0x, d0y, tx, ty, m->xmin + tx, m->xmax - tx, m->ymin + ty,
+                   m->ymax - ty, 1, 1 - m->free_surface, 1, 1, P.mpml, st));
+
+    // Dirichlet flags (elastic_wave.c:136-155)
+    std::vector<unsigned char> dir(N, 0);
+    const double es = m->edge_size;
+    for (int i = 0; i < N; i++) {
+        const double X = m->x[i], Y = m->y[i];
+        bool d = (X <= m->xmin + es / 4.0) || (Y <= m->ymin + es / 4.0) || (Y >= m->ymax - es / 4.0);
+        if (m->free_surface == 0) d = d || (X >= m->xmax - es / 4.0);
+        dir[i] = d ? 1 : 0;
+    }
+    CK(upload(&P.dirichlet, dir.data(), (size_t)N, st));
+
+    // step data: coefficients, SELL-32 slices (single shot), row records (batched)
+    CK(build_coef(N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, st));
+    CK(build_sell32(N, P.up, P.uj, P.ux, P.union_nnz, &P.sell, &P.slice_ptr, &P.sell_slots, st));
+    CK(build_rec32(N, P.up, P.uj, P.ux, P.union_nnz, &P.rec32, st));
+    CK(cudaStreamSynchronize(st));
+    canon_free(co, true);
+    cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+    cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx); cudaFree(d_scr);
+    for (auto &px : ctx->plain_x) { cudaFree(px); px = nullptr; }
+    ctx->tune = RunCache();
+    ctx->ready = true;
+    ctx->stats.union_nnz = P.union_nnz;
+    for (int k = 0; k < 7; k++) ctx->stats.csr_nnz[k] = P.csr[k].nnz;
+    ctx->stats.setup_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SFG_OK;
+}
+
+int sfg_csr_nnz(sfg_ctx *ctx, int matrix, int *nnz)
+{
+    if (!ctx || !nnz || matrix < 0 || matrix > 6) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    *nnz = (int)ctx->P.csr[matrix].nnz;
+    return SFG_OK;
+}
+
+int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x)
+{
+    if (!ctx || matrix < 0 || matrix > 6) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    CK(cudaSetDevice(ctx->device));
+    const DevCsr &c = ctx->P.csr[matrix];
+    if (p) CK(cudaMemcpy(p, c.p, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
+    if (j && c.nnz) CK(cudaMemcpy(j, c.j, sizeof(int) * c.nnz, cudaMemcpyDeviceToHost));
+    if (x && c.nnz) CK(cudaMemcpy(x, c.x, sizeof(double) * c.nnz, cudaMemcpyDeviceToHost));
+    return SFG_OK;
+}
+
+int sfg_lumped_mass_copy(sfg_ctx *ctx, double *out)
+{
+    if (!ctx || !out) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpy(out, ctx->P.mass_lump, sizeof(double) * ctx->N, cudaMemcpyDeviceToHost));
+    return SFG_OK;
+}
+
+int sfg_mpml_copy(sfg_ctx *ctx, double *out6)
+{
+    if (!ctx || !out6) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpy(out6, ctx->P.mpml, sizeof(double) * 6 * (size_t)ctx->N, cudaMemcpyDeviceToHost));
+    return SFG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- time loop
+
+namespace {
+
+struct LoopPlan {
+    int kind;            // SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH
+    int S;               // shots advanced together (1, 32, 64, 128)
+    int spl;             // shots per lane (batched)
+    int threads;         // single-shot launch shape
+    int warps;           // batched launch shape
+};
+
+// Device buffers of one batch.
+struct BatchBufs {
+    void *G[2] = {nullptr, nullptr}, *Pv[2] = {nullptr, nullptr};
+    size_t gbytes = 0, pbytes = 0;
+    int *src = nullptr;
+    int *rec = nullptr;
+    double *amp = nullptr;
+    double *seis_u = nullptr, *seis_w = nullptr;
+    double *snap_u = nullptr, *snap_w = nullptr;
+    double *energy = nullptr;
+    // unfused path
+    float *pst = nullptr, *peq = nullptr, *prhs = nullptr, *panew = nullptr;
+};
+
+void free_bufs(BatchBufs &b)
+{
+    for (int k = 0; k < 2; k++) { cudaFree(b.G[k]); cudaFree(b.Pv[k]); }
+    cudaFree(b.src); cudaFree(b.rec); cudaFree(b.amp); cudaFree(b.seis_u); cudaFree(b.seis_w);
+    cudaFree(b.snap_u); cudaFree(b.snap_w); cudaFree(b.energy);
+    cudaFree(b.pst); cudaFree(b.peq); cudaFree(b.prhs); cudaFree(b.panew);
+    b = BatchBufs();
+}
+
+// Queue the whole time loop of one batch on `st` (captured into a graph by
+// the caller).  Returns the number of kernels queued, or -1 on a launch error.
+int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b, int snap_every,
+               int nsnap, int steps_to_run, cudaStream_t st)
+{
+    const DevProblem &P = ctx->P;
+    const int N = P.node_num, S = pl.S, R = run->rec_num, rows = run->step - 2;
+    int launches = 0;
+    StepCommon c;
+    c.n = N; c.dt = run->dt; c.amp = b.amp;
+    const double pi_af = 3.1415926535898;                 // elastic_wave.c:66-67
+    c.sin_af = std::sin(90.0 * pi_af / 180.0);
+    c.cos_af = std::cos(90.0 * pi_af / 180.0);
+    c.src = b.src; c.nshot = S; c.rec = b.rec; c.nrec = R; c.seis_rows = rows;
+    c.seis_u = b.seis_u; c.seis_w = b.seis_w; c.energy = b.energy; c.nsteps = run->step;
+    int cur = 0, srow = 1;
+    const int last = 2 + steps_to_run;   // exclusive
+    if (pl.kind == SFG_FP32_PLAIN_PATH) {
+        Plain32 a;
+        a.c = c;
+        for (int k = 0; k < 7; k++) a.m[k] = {P.csr[k].p, P.csr[k].j, ctx->plain_x[k]};
+        a.coef = P.coef32; a.st = b.pst; a.eq = b.peq; a.rhs = b.prhs; a.anew = b.panew;
+        for (int it = 2; it < last; it++) {
+            a.c.it = it;
+            a.c.seis_row = it - 2;
+            if (launch_plain_step(a, 256, st, &launches) != cudaSuccess) return -1;
+            if (nsnap > 0 && (it + 1) % snap_every == 0 && srow < nsnap) {
+                // U, W planes of the unfused state are FP32; snapshots go through
+                // the FP64 buffers with a tiny copy kernel-free path: skip here
+                srow++;
+            }
+        }
+        return launches;
+    }
+    for (int it = 2; it < last; it++) {
+        c.it = it;
+        c.seis_row = it >= 3 ? it - 3 : -1;
+        const int nxt = cur ^ 1;
+        cudaError_t e;
+        if (pl.kind == SFG_FP64) {
+            Step64 a;
+            a.c = c; a.up = P.up; a.uj = P.uj; a.ux = P.ux; a.nnz = P.union_nnz; a.coef = P.coefd;
+            a.Gin = (const double *)b.G[cur]; a.Gout = (double *)b.G[nxt];
+            a.Pin = (const double *)b.Pv[cur]; a.Pout = (double *)b.Pv[nxt];
+            e = launch_step64(a, pl.threads, st);
+        } else {
+            Step32 a;
+            a.c = c; a.sell = P.sell; a.slice_ptr = P.slice_ptr; a.rec32 = P.rec32; a.up = P.up;
+            a.coef = P.coef32;
+            a.Gin = (const float *)b.G[cur]; a.Gout = (float *)b.G[nxt];
+            a.Pin = (const float *)b.Pv[cur]; a.Pout = (float *)b.Pv[nxt];
+            const bool kahan = pl.kind == SFG_FP32_KAHAN;
+            e = S == 1 ? launch_step32(a, kahan, pl.threads, st)
+                       : launch_step32_batched(a, kahan, pl.spl, pl.warps, st);
+        }
+        if (e != cudaSuccess) return -1;
+        launches++;
+        cur = nxt;
+        if (nsnap > 0 && (it + 1) % snap_every == 0 && srow < nsnap) {
+            const size_t off = (size_t)srow * N;
+            if (pl.kind == SFG_FP64)
+                e = launch_snapshot64((const double *)b.G[cur], N, b.snap_u + off, b.snap_w + off, st);
+            else
+                e = launch_snapshot32((const float *)b.G[cur], (const float *)b.Pv[cur], N, S, b.snap_u + off,
+                                      b.snap_w + off, (long long)nsnap * N, st);
+            if (e != cudaSuccess) return -1;
+            launches++;
+            srow++;
+        }
+    }
+    // the last state's receiver row
+    c.it = last - 1;
+    c.seis_row = last - 3;
+    cudaError_t e = pl.kind == SFG_FP64 ? launch_gather64(c, (const double *)b.G[cur], S, st)
+                                        : launch_gather32(c, (const float *)b.G[cur], (const float *)b.Pv[cur], S, st);
+    if (e != cudaSuccess) return -1;
+    launches++;
+    return launches;
+}
+
+int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int nsnap, BatchBufs &b)
+{
+    const int N = ctx->N, S = pl.S, R = run->rec_num, rows = run->step - 2;
+    const size_t esz = pl.kind == SFG_FP64 ? sizeof(double) : sizeof(float);
+    b.gbytes = (size_t)N * GREC * S * esz;
+    b.pbytes = (size_t)N * PREC * S * esz;
+    cudaStream_t st = ctx->stream;
+    if (pl.kind == SFG_FP32_PLAIN_PATH) {
+        CK(cudaMalloc(&b.pst, sizeof(float) * 36 * (size_t)N));
+        CK(cudaMalloc(&b.peq, sizeof(float) * 22 * (size_t)N));
+        CK(cudaMalloc(&b.prhs, sizeof(float) * 14 * (size_t)N));
+        CK(cudaMalloc(&b.panew, sizeof(float) * 6 * (size_t)N));
+    } else {
+        for (int k = 0; k < 2; k++) {
+            CK(cudaMalloc(&b.G[k], b.gbytes));
+            CK(cudaMalloc(&b.Pv[k], b.pbytes));
+        }
+    }
+    CK(cudaMalloc(&b.src, sizeof(int) * S));
+    CK(cudaMalloc(&b.rec, sizeof(int) * std::max(R, 1)));
+    if (R) CK(cudaMemcpyAsync(b.rec, run->rec_node, sizeof(int) * R, cudaMemcpyHostToDevice, st));
+    std::vector<double> amp(run->step, 0.0);
+    for (int it = 0; it < run->step; it++) amp[it] = ricker(run->f0, run->t0, 1.0e10, (it + 1) * run->dt);
+    CK(upload(&b.amp, amp.data(), amp.size(), st));
+    CK(cudaMalloc(&b.seis_u, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
+    CK(cudaMalloc(&b.seis_w, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
+    if (nsnap > 0) {
+        CK(cudaMalloc(&b.snap_u, sizeof(double) * (size_t)S * nsnap * N));
+        CK(cudaMalloc(&b.snap_w, sizeof(double) * (size_t)S * nsnap * N));
+    }
+    CK(cudaMalloc(&b.energy, sizeof(double) * (size_t)S * run->step * 2));
+    CK(cudaStreamSynchronize(st));
+    return SFG_OK;
+}
+
+int reset_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int nsnap, BatchBufs &b,
+               const int *src_nodes, int nshot)
+{
+    cudaStream_t st = ctx->stream;
+    const int N = ctx->N, S = pl.S;
+    if (pl.kind == SFG_FP32_PLAIN_PATH) {
+        CK(cudaMemsetAsync(b.pst, 0, sizeof(float) * 36 * (size_t)N, st));
+        CK(cudaMemsetAsync(b.panew, 0, sizeof(float) * 6 * (size_t)N, st));
+    } else {
+        for (int k = 0; k < 2; k++) {
+            CK(cudaMemsetAsync(b.G[k], 0, b.gbytes, st));
+            CK(cudaMemsetAsync(b.Pv[k], 0, b.pbytes, st));
+        }
+    }
+    std::vector<int> src(S, -1);
+    for (int s = 0; s < nshot; s++) src[s] = src_nodes[s];
+    CK(cudaMemcpyAsync(b.src, src.data(), sizeof(int) * S, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(b.energy, 0, sizeof(double) * (size_t)S * run->step * 2, st));
+    if (nsnap > 0) {
+        CK(cudaMemsetAsync(b.snap_u, 0, sizeof(double) * (size_t)S * nsnap * N, st));
+        CK(cudaMemsetAsync(b.snap_w, 0, sizeof(double) * (size_t)S * nsnap * N, st));
+    }
+    return SFG_OK;
+}
+
+// Time a few steps of each candidate launch shape and keep the fastest
+// (state is reset afterwards by the caller).
+int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
+{
+    if (pl.kind == SFG_FP64 || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
+    const bool kahan = pl.kind == SFG_FP32_KAHAN;
+    int *slot;
+    std::vector<int> cand;
+    if (pl.S == 1) {
+        slot = kahan ? &ctx->tune.threads_fp32k : &ctx->tune.threads_fp32;
+        cand = {64, 128, 256};
+    } else {
+        int si = pl.spl == 1 ? 0 : (pl.spl == 2 ? 1 : 2);
+        slot = &ctx->tune.warps_b[si][kahan ? 1 : 0];
+        cand = {2, 4, 8};
+    }
+    if (*slot > 0) {
+        if (pl.S == 1) pl.threads = *slot; else pl.warps = *slot;
+        return SFG_OK;
+    }
+    cudaStream_t st = ctx->stream;
+    sfg_run_desc r2 = *run;
+    const int probe = std::min(12, run->step - 2);
+    r2.step = probe + 2;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int pick = cand[0];
+    for (int cnd : cand) {
+        LoopPlan q = pl;
+        if (pl.S == 1) q.threads = cnd; else q.warps = cnd;
+        if (queue_loop(ctx, q, &r2, b, 0, 0, 2, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune warm-up");
+        CK(cudaEventRecord(e0, st));
+        if (queue_loop(ctx, q, &r2, b, 0, 0, probe, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune launch");
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; pick = cnd; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *slot = pick;
+    if (pl.S == 1) pl.threads = pick; else pl.warps = pick;
+    return SFG_OK;
+}
+
+int ensure_plain_matrices(sfg_ctx *ctx)
+{
+    if (ctx->plain_x[0]) return SFG_OK;
+    for (int k = 0; k < 7; k++) {
+        const DevCsr &c = ctx->P.csr[k];
+        std::vector<double> h(std::max<long long>(c.nnz, 1));
+        std::vector<float> f(h.size());
+        if (c.nnz) CK(cudaMemcpy(h.data(), c.x, sizeof(double) * c.nnz, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < h.size(); i++) f[i] = (float)h[i];
+        CK(cudaMalloc(&ctx->plain_x[k], sizeof(float) * f.size()));
+        CK(cudaMemcpy(ctx->plain_x[k], f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+    }
+    return SFG_OK;
+}
+
+int run_impl(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
+             double *snap_w, bool host_out, cudaStream_t user_stream)
+{
+    if (!ctx || !run) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    const int N = ctx->N;
+    if (run->step < 3 || run->dt <= 0 || run->src_num < 1 || run->rec_num < 0 || !run->src_node ||
+        (run->rec_num > 0 && !run->rec_node))
+        return fail(ctx, SFG_ERR_ARG, "bad run description");
+    for (int s = 0; s < run->src_num; s++)
+        if (run->src_node[s] < 0 || run->src_node[s] >= N)
+            return fail(ctx, SFG_ERR_BADINDEX, "source node out of range (node_location miss gives -1)");
+    for (int r = 0; r < run->rec_num; r++)
+        if (run->rec_node[r] < 0 || run->rec_node[r] >= N)
+            return fail(ctx, SFG_ERR_BADINDEX, "receiver node out of range (node_location miss gives -1)");
+    if (run->precision < 0 || run->precision > 3) return fail(ctx, SFG_ERR_ARG, "bad precision");
+    CK(cudaSetDevice(ctx->device));
+    auto t_all = std::chrono::steady_clock::now();
+    LoopPlan pl;
+    pl.kind = run->precision;
+    pl.S = 1; pl.spl = 1; pl.threads = 128; pl.warps = 4;
+    const bool fp32 = pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN;
+    int spb = run->shots_per_batch;
+    if (fp32) {
+        if (spb <= 0) spb = run->src_num >= 64 ? 64 : (run->src_num >= 16 ? 32 : 1);
+        if (spb != 1 && spb != 32 && spb != 64 && spb != 128)
+            return fail(ctx, SFG_ERR_ARG, "shots_per_batch must be 1, 32, 64 or 128");
+        pl.S = spb;
+        pl.spl = spb / 32 > 0 ? spb / 32 : 1;
+    }
+    if (pl.kind == SFG_FP32_PLAIN_PATH) {
+        int rc = ensure_plain_matrices(ctx);
+        if (rc) return rc;
+    }
+    const int snap_every = run->snap_every;
+    const int nsnap = sfg_snapshot_rows(run->step, snap_every);
+    const int rows = run->step - 2, R = run->rec_num;
+    BatchBufs b;
+    int rc = alloc_bufs(ctx, pl, run, nsnap, b);
+    if (rc) { free_bufs(b); return rc; }
+    cudaStream_t st = ctx->stream;
+    rc = reset_bufs(ctx, pl, run, nsnap, b, run->src_node, std::min(pl.S, run->src_num));
+    if (rc == SFG_OK) rc = autotune(ctx, pl, run, b);
+    if (rc) { free_bufs(b); return rc; }
+    ctx->stats.rows_per_block = pl.S == 1 ? pl.threads : pl.warps;
+
+    // capture the whole loop once; relaunch it per batch
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+    {
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { free_bufs(b); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
+        launches = queue_loop(ctx, pl, run, b, snap_every, nsnap, rows, st);
+        e = cudaStreamEndCapture(st, &graph);
+        if (launches < 0 || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            free_bufs(b);
+            return fail(ctx, SFG_ERR_CUDA, "graph capture failed");
+        }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            free_bufs(b);
+            return fail(ctx, SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double loop_ms = 0.0;
+    int status = SFG_OK;
+    ctx->stats.blowup_step = -1;
+    std::vector<double> energy;
+    for (int s0 = 0; s0 < run->src_num && status != SFG_ERR_CUDA; s0 += pl.S) {
+        const int ns = std::min(pl.S, run->src_num - s0);
+        rc = reset_bufs(ctx, pl, run, nsnap, b, run->src_node + s0, ns);
+        if (rc) { status = rc; break; }
+        cudaEventRecord(e0, st);
+        cudaError_t e = cudaGraphLaunch(exec, st);
+        cudaEventRecord(e1, st);
+        if (e != cudaSuccess) { status = fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); break; }
+        if (!host_out) {
+            // device variant: copy seismograms to the caller's device buffers
+            if (seis_u) cudaMemcpyAsync(seis_u + (size_t)s0 * rows * R, b.seis_u, sizeof(double) * ns * rows * R,
+                                        cudaMemcpyDeviceToDevice, user_stream ? user_stream : st);
+            if (seis_w) cudaMemcpyAsync(seis_w + (size_t)s0 * rows * R, b.seis_w, sizeof(double) * ns * rows * R,
+                                        cudaMemcpyDeviceToDevice, user_stream ? user_stream : st);
+        }
+        e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { status = fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        loop_ms += ms;
+        if (host_out) {
+            if (seis_u && R) CK(cudaMemcpy(seis_u + (size_t)s0 * rows * R, b.seis_u, sizeof(double) * ns * rows * R, cudaMemcpyDeviceToHost));
+            if (seis_w && R) CK(cudaMemcpy(seis_w + (size_t)s0 * rows * R, b.seis_w, sizeof(double) * ns * rows * R, cudaMemcpyDeviceToHost));
+            if (nsnap > 0 && snap_u) CK(cudaMemcpy(snap_u + (size_t)s0 * nsnap * N, b.snap_u, sizeof(double) * ns * nsnap * N, cudaMemcpyDeviceToHost));
+            if (nsnap > 0 && snap_w) CK(cudaMemcpy(snap_w + (size_t)s0 * nsnap * N, b.snap_w, sizeof(double) * ns * nsnap * N, cudaMemcpyDeviceToHost));
+        }
+        // energy bound (elastic_wave.c:777-785): first failing step
+        energy.resize((size_t)pl.S * run->step * 2);
+        CK(cudaMemcpy(energy.data(), b.energy, sizeof(double) * energy.size(), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < ns && pl.kind != SFG_FP32_PLAIN_PATH; s++) {
+            const double *en = energy.data() + (pl.S == 1 ? 0 : (size_t)s * run->step * 2);
+            for (int it = 2; it < run->step; it++) {
+                const double a = en[2 * it], c = en[2 * it + 1];
+                if (!(a <= 10e6) || !(c <= 10e6)) {
+                    if (ctx->stats.blowup_step < 0 || it < ctx->stats.blowup_step) ctx->stats.blowup_step = it;
+                    status = SFG_ERR_BLOWUP;
+                    break;
+                }
+            }
+        }
+        if (pl.kind == SFG_FP32_PLAIN_PATH) {
+            for (int it = 2; it < run->step; it++) {
+                const double a = energy[2 * it], c = energy[2 * it + 1];
+                if (!(a <= 10e6) || !(c <= 10e6)) { ctx->stats.blowup_step = it; status = SFG_ERR_BLOWUP; break; }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    free_bufs(b);
+    ctx->stats.loop_ms = loop_ms;
+    ctx->stats.dof_steps = 2LL * N * run->src_num * (long long)(run->step - 2);
+    ctx->stats.kernel_launches = launches;
+    ctx->stats.total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_all).count();
+    if (status == SFG_ERR_BLOWUP) ctx->err = "energy exceeds maximum value at step " + std::to_string(ctx->stats.blowup_step);
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfg_run(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
+            double *snap_w)
+{
+    return run_impl(ctx, run, seis_u, seis_w, snap_u, snap_w, true, nullptr);
+}
+
+int sfg_run_device(sfg_ctx *ctx, const sfg_run_desc *run, void *d_seis_u, void *d_seis_w, void *stream)
+{
+    return run_impl(ctx, run, (double *)d_seis_u, (double *)d_seis_w, nullptr, nullptr, false,
+                    (cudaStream_t)stream);
+}
+
+int sfg_sync(sfg_ctx *ctx)
+{
+    if (!ctx) return SFG_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaDeviceSynchronize());
+    return SFG_OK;
+}
+
+}  // extern "C"

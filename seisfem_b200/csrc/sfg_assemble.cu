@@ -1,0 +1,642 @@
+// sfg_assemble.cu -- FP64 element assembly, lumped mass, M-PML profiles and
+// COO -> canonical CSR on the GPU.
+//
+// Compiled with -fmad=false: no multiply-add contraction, so every FP64
+// value reproduces the reference's scalar C loops bit for bit
+// (assemble/*_sparse_*.c, pml/abc_mpml.c, sparse_matrix/coo2csr_lib.f90).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+
+#include "sfg_elem.cuh"
+#include "sfg_internal.h"
+
+namespace sfg {
+
+// ------------------------------------------------------------------ scan
+
+namespace {
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long *sh, long long &total)
+{
+    // Hillis-Steele over one block (sh has blockDim.x entries)
+    int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int off = 1; off < blockDim.x; off <<= 1) {
+        long long a = t >= off ? sh[t - off] : 0;
+        __syncthreads();
+        sh[t] += a;
+        __syncthreads();
+    }
+    total = sh[blockDim.x - 1];
+    long long incl = sh[t];
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void scan_tile_sums(const int *in, int n, long long *tile_sum)
+{
+    __shared__ long long sh[SCAN_THREADS];
+    long long base = (long long)blockIdx.x * SCAN_TILE;
+    long long s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        long long i = base + (long long)k * SCAN_THREADS + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    long long tot;
+    block_exclusive_scan(s, sh, tot);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
+}
+
+__global__ void scan_tile_offsets(long long *tile_sum, int ntiles)
+{
+    // one block: exclusive scan of the tile sums, in chunks of blockDim
+    __shared__ long long sh[SCAN_THREADS];
+    long long carry = 0;
+    for (int base = 0; base < ntiles; base += SCAN_THREADS) {
+        int i = base + threadIdx.x;
+        long long v = i < ntiles ? tile_sum[i] : 0;
+        long long tot;
+        long long ex = block_exclusive_scan(v, sh, tot);
+        if (i < ntiles) tile_sum[i] = carry + ex;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tile_sum[ntiles] = carry;
+}
+
+__global__ void scan_tiles(const int *in, int *out, int n, const long long *tile_off)
+{
+    // each thread owns SCAN_ITEMS consecutive items of the tile
+    __shared__ long long sh[SCAN_THREADS];
+    long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    long long s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        long long i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        s += v[k];
+    }
+    long long tot;
+    long long ex = block_exclusive_scan(s, sh, tot) + tile_off[blockIdx.x];
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        long long i = base + k;
+        if (i < n) out[i] = (int)ex;
+        ex += v[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (int)tile_off[gridDim.x];
+}
+}  // namespace
+
+// out[0..n] = exclusive prefix sums of in[0..n), out[n] = total.
+cudaError_t exclusive_scan_int(const int *d_in, int *d_out, int n, cudaStream_t st)
+{
+    int ntiles = std::max(1, (n + SCAN_TILE - 1) / SCAN_TILE);
+    long long *tile = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&tile, sizeof(long long) * (ntiles + 1), st);
+    if (e != cudaSuccess) return e;
+    scan_tile_sums<<<ntiles, SCAN_THREADS, 0, st>>>(d_in, n, tile);
+    scan_tile_offsets<<<1, SCAN_THREADS, 0, st>>>(tile, ntiles);
+    scan_tiles<<<ntiles, SCAN_THREADS, 0, st>>>(d_in, d_out, n, tile);
+    e = cudaGetLastError();
+    cudaFreeAsync(tile, st);
+    return e;
+}
+
+// ------------------------------------------------------- element matrices
+
+struct MatList { int m[8]; };   // -1: consistent mass (rho), 0..6: stiffness type
+
+// One thread per COO entry (e, iq, jq): integrates the requested matrices in
+// the reference's quadrature order (mass_sparse_q4.c:199-256,
+// stiffness_sparse_q4.c:202-271) and writes entry e*p*p + iq*p + jq.
+__global__ void element_coo_kernel(int tc, int p, long long nnz, const int *__restrict__ en,
+                                   const double *__restrict__ x, const double *__restrict__ y,
+                                   const double *__restrict__ rho, int nmat, MatList ml,
+                                   int *__restrict__ ci, int *__restrict__ cj,
+                                   double *__restrict__ cx, int *flags)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nnz) return;
+    int pp = p * p;
+    int e = (int)(t / pp);
+    int rem = (int)(t - (long long)e * pp);
+    int iq = rem / p, jq = rem - iq * p;
+    const int *enE = en + (long long)e * p;
+    ElemGeom g;
+    elem_geom(tc, enE, x, y, g);
+    if (g.area == 0.0 && rem == 0) atomicOr(flags, FLAG_ZERO_AREA);
+    int ip = enE[iq] - 1, jp = enE[jq] - 1;
+    double rho_ip = rho ? rho[ip] : 0.0;
+    double acc[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = 0.0;
+    int nq = quad_count(tc);
+    for (int q = 0; q < nq; q++) {
+        double r, s, w;
+        quad_point(tc, q, r, s, w);
+        double drdx, drdy, dsdx, dsdy;
+        map_point(tc, g, r, s, drdx, drdy, dsdx, dsdy);
+        double sv[16], sdr[16], sds[16];
+        shape_eval(tc, r, s, sv, sdr, sds);
+        double phi_i = sv[iq], phi_j = sv[jq];
+        double dxi = sdr[iq] * drdx + sds[iq] * dsdx;
+        double dyi = sdr[iq] * drdy + sds[iq] * dsdy;
+        double dxj = sdr[jq] * drdx + sds[jq] * dsdx;
+        double dyj = sdr[jq] * drdy + sds[jq] * dsdy;
+        double aw = g.area * w;
+        for (int m = 0; m < nmat; m++) {
+            double term;
+            switch (ml.m[m]) {
+            case -1: term = aw * rho_ip * phi_i * phi_j; break;
+            case 0: term = aw * (dxi * dxj + dyi * dyj); break;
+            case 1: term = aw * (dxi * dxj); break;
+            case 2: term = aw * (dyi * dyj); break;
+            case 3: term = aw * (dxi * dyj); break;
+            case 4: term = aw * (dyi * dxj); break;
+            case 5: term = aw * (phi_i * dxj); break;
+            default: term = aw * (phi_i * dyj); break;
+            }
+            acc[m] = acc[m] + term;
+        }
+    }
+    if (ci) ci[t] = ip;
+    if (cj) cj[t] = jp;
+    for (int m = 0; m < nmat; m++) cx[(long long)m * nnz + t] = acc[m];
+}
+
+cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x, const double *d_y,
+                               const double *d_rho, int nmat, const int *mats, int *d_ci, int *d_cj,
+                               double *d_cx, int *d_flags, cudaStream_t st)
+{
+    int p = elem_order(tc);
+    long long nnz = (long long)E * p * p;
+    MatList ml;
+    for (int m = 0; m < 8; m++) ml.m[m] = m < nmat ? mats[m] : 0;
+    int threads = 128;
+    long long blocks = (nnz + threads - 1) / threads;
+    if (blocks > 0)
+        element_coo_kernel<<<(unsigned)blocks, threads, 0, st>>>(tc, p, nnz, d_en, d_x, d_y, d_rho, nmat,
+                                                                  ml, d_ci, d_cj, d_cx, d_flags);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ lumped mass
+
+// Per element: the sums of all mass terms and of the diagonal terms, each in
+// the element's own (quad, iq, jq) order (mass_sparse_q4.c:238-246).
+__global__ void element_mass_sums(int tc, int p, int E, const int *__restrict__ en,
+                                  const double *__restrict__ x, const double *__restrict__ y,
+                                  const double *__restrict__ rho, double *__restrict__ part)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int *enE = en + (long long)e * p;
+    ElemGeom g;
+    elem_geom(tc, enE, x, y, g);
+    double ms = 0.0, ds = 0.0;
+    int nq = quad_count(tc);
+    for (int q = 0; q < nq; q++) {
+        double r, s, w;
+        quad_point(tc, q, r, s, w);
+        double sv[16], sdr[16], sds[16];
+        shape_eval(tc, r, s, sv, sdr, sds);
+        double aw = g.area * w;
+        for (int iq = 0; iq < p; iq++) {
+            int ip = enE[iq] - 1;
+            double a = aw * rho[ip];
+            for (int jq = 0; jq < p; jq++) {
+                double term = a * sv[iq] * sv[jq];
+                ms = ms + term;
+                if (enE[jq] - 1 == ip) ds = ds + term;
+            }
+        }
+    }
+    part[2 * (long long)e] = ms;
+    part[2 * (long long)e + 1] = ds;
+}
+
+// Deterministic reduction of the per-element sums: fixed chunking per
+// thread, then a fixed-shape tree (one block).
+__global__ void reduce_pairs(const double *__restrict__ part, int E, double *out2)
+{
+    __shared__ double sm[1024], sd[1024];
+    int t = threadIdx.x;
+    long long chunk = ((long long)E + blockDim.x - 1) / blockDim.x;
+    long long a = t * chunk, b = min((long long)E, a + chunk);
+    double ms = 0.0, ds = 0.0;
+    for (long long e = a; e < b; e++) { ms = ms + part[2 * e]; ds = ds + part[2 * e + 1]; }
+    sm[t] = ms;
+    sd[t] = ds;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (t < off) { sm[t] = sm[t] + sm[t + off]; sd[t] = sd[t] + sd[t + off]; }
+        __syncthreads();
+    }
+    if (t == 0) { out2[0] = sm[0]; out2[1] = sd[0]; }
+}
+
+// Per node: the diagonal mass terms in (element, quad) order; the node's COO
+// row lists its entries in ascending COO index, i.e. by element.
+__global__ void node_lumped_mass(int tc, int p, int N, const int *__restrict__ en,
+                                 const double *__restrict__ x, const double *__restrict__ y,
+                                 const double *__restrict__ rho, const int *__restrict__ row_start,
+                                 const int *__restrict__ bucket, const int *__restrict__ cj,
+                                 const double *__restrict__ sums, double *__restrict__ mass)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    int pp = p * p;
+    double m = 0.0;
+    int nq = quad_count(tc);
+    for (int k = row_start[r]; k < row_start[r + 1]; k++) {
+        int c = bucket[k];
+        if (cj[c] != r) continue;
+        int e = c / pp, rem = c - e * pp, iq = rem / p, jq = rem - iq * p;
+        const int *enE = en + (long long)e * p;
+        ElemGeom g;
+        elem_geom(tc, enE, x, y, g);
+        for (int q = 0; q < nq; q++) {
+            double rr, ss, w;
+            quad_point(tc, q, rr, ss, w);
+            double sv[16], sdr[16], sds[16];
+            shape_eval(tc, rr, ss, sv, sdr, sds);
+            m = m + g.area * w * rho[r] * sv[iq] * sv[jq];
+        }
+    }
+    // mass_sparse_q4.c:259-263
+    mass[r] = m * sums[0] / sums[1];
+}
+
+cudaError_t launch_lumped_mass(int tc, int N, int E, const int *d_en, const double *d_x,
+                               const double *d_y, const double *d_rho, const int *d_row_start,
+                               const int *d_bucket, const int *d_cj, double *d_mass,
+                               double *d_scratch, int *d_flags, cudaStream_t st)
+{
+    (void)d_flags;
+    int p = elem_order(tc);
+    element_mass_sums<<<(E + 127) / 128, 128, 0, st>>>(tc, p, E, d_en, d_x, d_y, d_rho, d_scratch);
+    double *sums = d_scratch + 2 * (size_t)E;
+    reduce_pairs<<<1, 1024, 0, st>>>(d_scratch, E, sums);
+    node_lumped_mass<<<(N + 127) / 128, 128, 0, st>>>(tc, p, N, d_en, d_x, d_y, d_rho, d_row_start,
+                                                       d_bucket, d_cj, sums, d_mass);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ M-PML
+
+// One thread per node, region tests in the reference's order
+// (pml/abc_mpml.c:73-199).  d0x/d0y come from the host (log10 of the host
+// library, abc_mpml.c:60-61).  Nodes that no element references keep 0.
+__global__ void mpml_kernel(int N, const double *__restrict__ xa, const double *__restrict__ ya,
+                            const int *__restrict__ row_start, double d0x, double d0y, double tx,
+                            double ty, double x0, double x1, double y0, double y1, int uxmin,
+                            int uxmax, int uymin, int uymax, double *__restrict__ out)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const double pxy = 0.15, pyx = 0.15;
+    double vdx = 0.0, vdy = 0.0, vdxx = 0.0, vdyy = 0.0;
+    if (row_start == nullptr || row_start[p + 1] > row_start[p]) {
+        double X = xa[p], Y = ya[p];
+        if (X <= x0 && Y >= y0 && Y <= y1 && uxmin == 1) {
+            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
+            vdy = pyx * vdx;
+            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
+            vdyy = 0.0;
+        } else if (X >= x1 && Y >= y0 && Y <= y1 && uxmax == 1) {
+            vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx);
+            vdy = pyx * vdx;
+            vdxx = d0x * 2 * (X - x1) / (tx * tx);
+            vdyy = 0.0;
+        } else if (Y <= y0 && X >= x0 && X <= x1 && uymin == 1) {
+            vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+            vdx = pxy * vdy;
+            vdxx = 0.0;
+            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
+        } else if (Y >= y1 && X >= x0 && X <= x1 && uymax == 1) {
+            vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+            vdx = pxy * vdy;
+            vdxx = 0.0;
+            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
+        } else if (X <= x0 && Y <= y0 && (uxmin == 1 || uymin == 1)) {
+            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx) + pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+            vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty) + pyx * d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
+            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
+            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
+        } else if (X <= x0 && Y >= y1 && (uxmin == 1 || uymax == 1)) {
+            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx) + pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+            vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty) + pyx * d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
+            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
+            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
+        } else if (X >= x1 && Y <= y0 && (uxmax == 1 || uymin == 1)) {
+            if (uymax == 1) {   // the reference tests ymax here (abc_mpml.c:147)
+                vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx) + pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+                vdxx = d0x * 2 * (X - x1) / (tx * tx);
+                vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty) + pyx * d0x * ((X - x1) / tx) * ((X - x1) / tx);
+            } else {
+                vdx = pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+                vdxx = 0.0;
+                vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+            }
+            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
+        } else if (X >= x1 && Y >= y1 && (uxmax == 1 || uymax == 1)) {
+            if (uymax == 1) {
+                vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx) + pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+                vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty) + pyx * d0x * ((X - x1) / tx) * ((X - x1) / tx);
+                vdxx = d0x * 2 * (X - x1) / (tx * tx);
+            } else {
+                vdx = pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+                vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+                vdxx = 0.0;
+            }
+            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
+        }
+    }
+    out[p] = vdx;
+    out[(size_t)N + p] = vdy;
+    out[2 * (size_t)N + p] = vdxx;
+    out[3 * (size_t)N + p] = vdyy;
+    out[4 * (size_t)N + p] = pyx * vdxx;
+    out[5 * (size_t)N + p] = pxy * vdyy;
+}
+
+cudaError_t launch_mpml(int N, const double *d_x, const double *d_y, const int *d_row_start,
+                        double d0x, double d0y, double tx, double ty, double x0, double x1,
+                        double y0, double y1, int uxmin, int uxmax, int uymin, int uymax,
+                        double *d_out6, cudaStream_t st)
+{
+    mpml_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, d_x, d_y, d_row_start, d0x, d0y, tx, ty, x0, x1, y0,
+                                                  y1, uxmin, uxmax, uymin, uymax, d_out6);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------- COO -> CSR rows
+
+__global__ void row_count_kernel(const int *__restrict__ ci, long long nnz, int N, int *cnt, int *flags)
+{
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    int r = ci[k];
+    if (r < 0 || r >= N) { atomicOr(flags, FLAG_BADINDEX); return; }
+    atomicAdd(&cnt[r], 1);
+}
+
+__global__ void row_fill_kernel(const int *__restrict__ ci, long long nnz, int N,
+                                const int *__restrict__ row_start, int *cursor, int *bucket)
+{
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    int r = ci[k];
+    if (r < 0 || r >= N) return;
+    int pos = atomicAdd(&cursor[r], 1);
+    bucket[row_start[r] + pos] = (int)k;
+}
+
+// selection sort with Fortran minloc semantics (coo2csr_lib.f90:256-267)
+__device__ void interchange_sort_dev(int *v, int *m, int n)
+{
+    for (int i = 0; i < n - 1; i++) {
+        int best = i, bv = v[i];
+        for (int k = i + 1; k < n; k++) {
+            int vk = v[k];
+            if (vk < bv) { best = k; bv = vk; }
+        }
+        if (best != i) {
+            int t = v[i]; v[i] = v[best]; v[best] = t;
+            t = m[i]; m[i] = m[best]; m[best] = t;
+        }
+    }
+}
+
+// iargsort_quicksort (coo2csr_lib.f90:191-246) on vec/map[0..n); returns
+// false when its explicit stack or a scan would leave the segment.
+__device__ bool iargsort_dev(int *vec, int *map, int n)
+{
+    constexpr int LEVELS = 64, SMALL = 20;
+    int lb[LEVELS + 1], ub[LEVELS + 1];
+    if (n <= 0) return true;
+    int sp = 0;
+    lb[0] = 0;
+    ub[0] = n - 1;
+    while (sp >= 0) {
+        int left = lb[sp], right = ub[sp];
+        if (right - left < SMALL) {
+            if (left < right) interchange_sort_dev(vec + left, map + left, right - left + 1);
+            sp--;
+            continue;
+        }
+        int lo = left, hi = right;
+        int pivot = (vec[left] + vec[right]) / 2;
+        left--;
+        right++;
+        for (;;) {
+            do { left++; } while (left <= hi && vec[left] < pivot);
+            do { right--; } while (right >= lo && vec[right] > pivot);
+            if (left > hi || right < lo) return false;
+            if (left < right) {
+                int t = vec[left]; vec[left] = vec[right]; vec[right] = t;
+                t = map[left]; map[left] = map[right]; map[right] = t;
+            } else if (left == right) {
+                if (left == lb[sp]) left++; else right--;
+                break;
+            } else {
+                break;
+            }
+        }
+        if (sp + 1 > LEVELS) return false;
+        ub[sp + 1] = ub[sp];
+        lb[sp + 1] = left;
+        ub[sp] = right;
+        sp++;
+    }
+    return true;
+}
+
+// Pass 1 per row: restore COO order inside the row (the bucket was filled
+// with atomics), replay the Fortran sort, and count the union entries and
+// the surviving (nonzero-sum) entries of each value stream.
+__global__ void canon_pass1(int N, int nv, long long nnz, const int *__restrict__ row_start,
+                            int *__restrict__ bucket, const int *__restrict__ cj,
+                            const double *__restrict__ cx, int *__restrict__ vec,
+                            int *__restrict__ map, int *__restrict__ cnt_union,
+                            int *__restrict__ cnt_v, int *maxlen, int *flags)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    int r1 = row_start[r], r2 = row_start[r + 1], l = r2 - r1;
+    int *b = bucket + r1;
+    for (int i = 1; i < l; i++) {   // insertion sort of COO indices
+        int key = b[i], k = i - 1;
+        while (k >= 0 && b[k] > key) { b[k + 1] = b[k]; k--; }
+        b[k + 1] = key;
+    }
+    int *v = vec + r1, *m = map + r1;
+    for (int i = 0; i < l; i++) { v[i] = cj[b[i]] + 1; m[i] = i; }
+    if (!iargsort_dev(v, m, l)) { atomicOr(flags, FLAG_SORT_STACK); return; }
+    atomicMax(maxlen, l);
+    int nu = 0;
+    int nz[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int k = 0;
+    while (k < l) {
+        int col = v[k];
+        double xs[8];
+        for (int s = 0; s < nv; s++) xs[s] = cx[(long long)s * nnz + b[m[k]]];
+        k++;
+        while (k < l && v[k] == col) {
+            for (int s = 0; s < nv; s++) xs[s] = xs[s] + cx[(long long)s * nnz + b[m[k]]];
+            k++;
+        }
+        nu++;
+        for (int s = 0; s < nv; s++) nz[s] += (xs[s] != 0.0);
+    }
+    cnt_union[r] = nu;
+    for (int s = 0; s < nv; s++) cnt_v[(long long)s * N + r] = nz[s];
+}
+
+// Pass 2 per row: write the union pattern and every stream's canonical CSR.
+__global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict__ row_start,
+                            const int *__restrict__ bucket, const double *__restrict__ cx,
+                            const int *__restrict__ vec, const int *__restrict__ map,
+                            const int *__restrict__ up, int *__restrict__ uj, double *__restrict__ ux,
+                            long long union_nnz, int *const *__restrict__ vp_,
+                            int *const *__restrict__ vj_, double *const *__restrict__ vx_)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    int r1 = row_start[r], r2 = row_start[r + 1], l = r2 - r1;
+    const int *b = bucket + r1, *v = vec + r1, *m = map + r1;
+    long long uo = up ? up[r] : 0;
+    int vo[8];
+    for (int s = 0; s < nv; s++) vo[s] = vp_[s] ? vp_[s][r] : 0;
+    int k = 0;
+    while (k < l) {
+        int col = v[k];
+        double xs[8];
+        for (int s = 0; s < nv; s++) xs[s] = cx[(long long)s * nnz + b[m[k]]];
+        k++;
+        while (k < l && v[k] == col) {
+            for (int s = 0; s < nv; s++) xs[s] = xs[s] + cx[(long long)s * nnz + b[m[k]]];
+            k++;
+        }
+        if (uj) {
+            uj[uo] = col - 1;
+            for (int s = 0; s < nv; s++) ux[(long long)s * union_nnz + uo] = xs[s];
+            uo++;
+        }
+        for (int s = 0; s < nv; s++)
+            if (vj_[s] && xs[s] != 0.0) {
+                vj_[s][vo[s]] = col - 1;
+                vx_[s][vo[s]] = xs[s];
+                vo[s]++;
+            }
+    }
+}
+
+#define SFG_TRY(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) { err = cudaGetErrorString(e_); return SFG_ERR_CUDA; } \
+    } while (0)
+
+void canon_free(CanonOut &o, bool keep_csr)
+{
+    if (!keep_csr)
+        for (auto &c : o.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
+    cudaFree(o.row_start);
+    cudaFree(o.bucket);
+    o.row_start = nullptr;
+    o.bucket = nullptr;
+}
+
+int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const double *d_cx, int nv,
+                 bool want_union, bool want_csr, CanonOut &out, int *d_flags, cudaStream_t st,
+                 std::string &err)
+{
+    if (nv < 1 || nv > 8 || nnz >= (1LL << 31) || N < 0) { err = "canonicalize: bad sizes"; return SFG_ERR_ARG; }
+    int *cnt = nullptr, *cursor = nullptr, *vec = nullptr, *map = nullptr, *cu = nullptr,
+        *cv = nullptr, *maxlen = nullptr;
+    size_t nn = (size_t)std::max<long long>(nnz, 1);
+    SFG_TRY(cudaMalloc(&cnt, sizeof(int) * ((size_t)N + 1)));
+    SFG_TRY(cudaMalloc(&cursor, sizeof(int) * ((size_t)N + 1)));
+    SFG_TRY(cudaMalloc(&out.row_start, sizeof(int) * ((size_t)N + 1)));
+    SFG_TRY(cudaMalloc(&out.bucket, sizeof(int) * nn));
+    SFG_TRY(cudaMalloc(&vec, sizeof(int) * nn));
+    SFG_TRY(cudaMalloc(&map, sizeof(int) * nn));
+    SFG_TRY(cudaMalloc(&cu, sizeof(int) * ((size_t)N + 1)));
+    SFG_TRY(cudaMalloc(&cv, sizeof(int) * (size_t)nv * ((size_t)N + 1)));
+    SFG_TRY(cudaMalloc(&maxlen, sizeof(int)));
+    SFG_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(cudaMemsetAsync(cursor, 0, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(cudaMemsetAsync(maxlen, 0, sizeof(int), st));
+    int tb = 256;
+    unsigned gb = (unsigned)((nnz + tb - 1) / tb);
+    if (gb) row_count_kernel<<<gb, tb, 0, st>>>(d_ci, nnz, N, cnt, d_flags);
+    SFG_TRY(exclusive_scan_int(cnt, out.row_start, N, st));
+    if (gb) row_fill_kernel<<<gb, tb, 0, st>>>(d_ci, nnz, N, out.row_start, cursor, out.bucket);
+    unsigned gr = (unsigned)((N + 127) / 128);
+    if (gr)
+        canon_pass1<<<gr, 128, 0, st>>>(N, nv, nnz, out.row_start, out.bucket, d_cj, d_cx, vec, map, cu,
+                                        cv, maxlen, d_flags);
+    SFG_TRY(cudaGetLastError());
+    int hflags = 0;
+    SFG_TRY(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SFG_TRY(cudaMemcpyAsync(&out.max_row_len, maxlen, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SFG_TRY(cudaStreamSynchronize(st));
+    if (hflags & FLAG_BADINDEX) { err = "COO row index out of range"; return SFG_ERR_BADINDEX; }
+    if (hflags & FLAG_SORT_STACK) { err = "row too long for the device sorter"; return SFG_ERR_ROWLEN; }
+
+    // row pointers: union + each stream
+    int *h_ptrs[8] = {nullptr};
+    int *up = nullptr;
+    if (want_union) {
+        SFG_TRY(cudaMalloc(&up, sizeof(int) * ((size_t)N + 1)));
+        SFG_TRY(exclusive_scan_int(cu, up, N, st));
+        int tot = 0;
+        SFG_TRY(cudaMemcpyAsync(&tot, up + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SFG_TRY(cudaStreamSynchronize(st));
+        out.union_nnz = tot;
+        out.up = up;
+        SFG_TRY(cudaMalloc(&out.uj, sizeof(int) * std::max<size_t>(tot, 1)));
+        SFG_TRY(cudaMalloc(&out.ux, sizeof(double) * (size_t)nv * std::max<size_t>(tot, 1)));
+    }
+    int *dvp[8] = {nullptr}, *dvj[8] = {nullptr};
+    double *dvx[8] = {nullptr};
+    if (want_csr) {
+        for (int s = 0; s < nv; s++) {
+            DevCsr &c = out.csr[s];
+            SFG_TRY(cudaMalloc(&c.p, sizeof(int) * ((size_t)N + 1)));
+            SFG_TRY(exclusive_scan_int(cv + (size_t)s * N, c.p, N, st));
+            int tot = 0;
+            SFG_TRY(cudaMemcpyAsync(&tot, c.p + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+            SFG_TRY(cudaStreamSynchronize(st));
+            c.nnz = tot;
+            SFG_TRY(cudaMalloc(&c.j, sizeof(int) * std::max<size_t>(tot, 1)));
+            SFG_TRY(cudaMalloc(&c.x, sizeof(double) * std::max<size_t>(tot, 1)));
+            dvp[s] = c.p; dvj[s] = c.j; dvx[s] = c.x;
+        }
+    }
+    (void)h_ptrs;
+    int **d_tab = nullptr;
+    SFG_TRY(cudaMalloc(&d_tab, sizeof(void *) * 24));
+    void *htab[24];
+    for (int s = 0; s < 8; s++) { htab[s] = dvp[s]; htab[8 + s] = dvj[s]; htab[16 + s] = dvx[s]; }
+    SFG_TRY(cudaMemcpyAsync(d_tab, htab, sizeof(htab), cudaMemcpyHostToDevice, st));
+    if (gr)
+        canon_pass2<<<gr, 128, 0, st>>>(N, nv, nnz, out.row_start, out.bucket, d_cx, vec, map, out.up,
+                                        out.uj, out.ux, out.union_nnz, d_tab, d_tab + 8,
+                                        (double *const *)(d_tab + 16));
+    SFG_TRY(cudaGetLastError());
+    SFG_TRY(cudaStreamSynchronize(st));
+    cudaFree(d_tab);
+    cudaFree(cnt); cudaFree(cursor); cudaFree(vec); cudaFree(map); cudaFree(cu); cudaFree(cv);
+    cudaFree(maxlen);
+    return SFG_OK;
+}
+
+}  // namespace sfg

@@ -1,0 +1,112 @@
+// sfg_internal.h -- device data of one context and the launchers shared by
+// the CUDA translation units (assembly, canonical CSR, step kernels, API).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/seisfem_b200.h"
+
+namespace sfg {
+
+// Error flags raised by device code (bitwise OR into one int).
+enum DevFlag {
+    FLAG_ZERO_AREA = 1,
+    FLAG_ROWLEN = 2,
+    FLAG_BADINDEX = 4,
+    FLAG_SORT_STACK = 8,
+};
+
+// Device memory block with size, freed by the owner.
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+};
+
+// Canonical CSR (FP64) of one matrix on the device.
+struct DevCsr {
+    int *p = nullptr;
+    int *j = nullptr;
+    double *x = nullptr;
+    long long nnz = 0;
+};
+
+// Assembled problem on the device (owned by the context).
+struct DevProblem {
+    int type_code = 0, order = 0, node_num = 0, element_num = 0;
+    long long coo_nnz = 0;
+    // union pattern of M, K1..K6 (all distinct columns of every row), FP64
+    // values of the seven matrices at the union positions, [7][union_nnz]
+    int *up = nullptr;
+    int *uj = nullptr;
+    double *ux = nullptr;
+    long long union_nnz = 0;
+    int max_row_len = 0;
+    DevCsr csr[7];
+    double *mass_lump = nullptr;     // [N]
+    double *mpml = nullptr;          // [6][N]: dx, dy, dxx, dyy, dxx_pyx, dyy_pxy
+    double *coef64 = nullptr;        // [4][N] c11, c13, c33, c44
+    unsigned char *dirichlet = nullptr;  // [N]
+    // FP32 step data
+    float *sell = nullptr;           // SELL-32 slots: [slots][8][32], plane 0 = column (int bits)
+    int *slice_ptr = nullptr;        // [slices + 1]
+    long long sell_slots = 0;
+    float *rec32 = nullptr;          // row-major union records [union_nnz][8] (col bits + 7 values)
+    float *coef32 = nullptr;         // [N][12]
+    double *coefd = nullptr;         // [N][12] FP64 coefficients for the FP64 step
+};
+
+// ---- assembly (sfg_assemble.cu) ------------------------------------------
+// All launchers queue work on `st` and return a cudaError_t.
+cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x, const double *d_y,
+                               const double *d_rho, int nmat, const int *mats, int *d_ci, int *d_cj,
+                               double *d_cx, int *d_flags, cudaStream_t st);
+cudaError_t launch_lumped_mass(int tc, int N, int E, const int *d_en, const double *d_x,
+                               const double *d_y, const double *d_rho, const int *d_row_start,
+                               const int *d_bucket, const int *d_cj, double *d_mass,
+                               double *d_scratch, int *d_flags, cudaStream_t st);
+cudaError_t launch_mpml(int N, const double *d_x, const double *d_y, const int *d_row_start,
+                        double d0x, double d0y, double tx, double ty, double x0, double x1,
+                        double y0, double y1, int uxmin, int uxmax, int uymin, int uymax,
+                        double *d_out6, cudaStream_t st);
+
+// COO -> canonical CSR for nv value streams sharing one (i, j) pattern.
+// Produces, per value stream, the CSR bit-exact with coo2csr_lib.f90, and
+// optionally the union pattern with the nv values at each union entry.
+struct CanonOut {
+    DevCsr csr[8];
+    int *up = nullptr, *uj = nullptr;
+    double *ux = nullptr;   // [nv][union_nnz]
+    long long union_nnz = 0;
+    int max_row_len = 0;
+    int *row_start = nullptr;   // COO bucket offsets [N+1] (kept for the lumped mass)
+    int *bucket = nullptr;      // COO indices per row, ascending [nnz]
+};
+int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const double *d_cx, int nv,
+                 bool want_union, bool want_csr, CanonOut &out, int *d_flags, cudaStream_t st,
+                 std::string &err);
+void canon_free(CanonOut &o, bool keep_csr);
+
+cudaError_t exclusive_scan_int(const int *d_in, int *d_out, int n, cudaStream_t st);
+
+// ---- step data and kernels (sfg_step.cu) ---------------------------------
+int build_step_data(DevProblem &P, const double *d_c, double dt_unused, std::string &err,
+                    cudaStream_t st);
+
+struct RunBuffers;
+struct StepLaunch;
+
+}  // namespace sfg
+
+namespace sfg {
+// mesh/mesh_element_order.c:2-57 (host side)
+inline int elem_order_host(int tc)
+{
+    static const int order[7] = {-1, 3, 6, 10, 4, 9, 16};
+    return (tc >= 1 && tc <= 6) ? order[tc] : -1;
+}
+}  // namespace sfg

@@ -1,0 +1,42 @@
+"""Shared test set-up: import paths, the ``gpu`` marker, oracle fixtures."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) CUDA device")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def reference():
+    from oracle import Reference, LIBREF
+    if not os.path.exists(LIBREF):
+        pytest.skip("reference build (oracle/_ref) not present")
+    return Reference()
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    from seisfem_b200.api import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def rel_l2(a, b):
+    import numpy as np
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))

@@ -1,0 +1,125 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bars: CSR row pointers / columns and FP64 values bit-exact; FP64 time loop
+within 1e-12 rel-L2 (the lumped-mass normalisation is a parallel sum, so its
+last bits may differ); FP32 paths within 1e-4 rel-L2 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from seisfem_b200.problem import small_problem, structured_mesh, isotropic_model, Problem
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-4      # seismogram / snapshot rel-L2 vs the FP64 oracle
+FP64_TOL = 1e-12
+
+
+@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6"])
+def test_csr_bit_exact(ctx, oracle, etype):
+    p = small_problem(etype, n=9, step=10, pml=2, seed=3)
+    ctx.setup(p)
+    m = p.mesh
+    mats = [oracle.mass_coo(m, p.model.rho)] + [oracle.stif_coo(m, k) for k in range(1, 7)]
+    for k, coo in enumerate(mats):
+        Bp, Bj, Bx = oracle.coo2csr(m.node_num, *coo)
+        gp, gj, gx = ctx.csr(k)
+        assert np.array_equal(gp, Bp), (etype, k)
+        assert np.array_equal(gj, Bj), (etype, k)
+        assert np.array_equal(gx, Bx), (etype, k)
+
+
+@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6"])
+def test_lumped_mass_and_mpml(ctx, oracle, etype):
+    p = small_problem(etype, n=9, step=10, pml=2, seed=5)
+    ctx.setup(p)
+    m = p.mesh
+    lm = oracle.mass_lumped(m, p.model.rho)
+    assert np.max(np.abs(ctx.lumped_mass() - lm) / lm) < 1e-14
+    ref = oracle.abc_mpml(m, p.pml_nx, p.pml_ny, p.edge_size, (m.xmin, m.xmax, m.ymin, m.ymax),
+                          p.model.vp.max(), (1, 1, 1, 1))
+    assert np.array_equal(ctx.mpml(), ref)
+
+
+@pytest.mark.parametrize("etype,n,step,dt", [("Q4", 24, 260, 1e-3), ("Q9", 12, 260, 5e-4),
+                                             ("T3", 24, 260, 1e-3), ("T6", 12, 85, 2.5e-4)])
+def test_fp64_run_matches_oracle(ctx, oracle, etype, n, step, dt):
+    p = small_problem(etype, n=n, step=step, pml=4, seed=11, dt=dt)
+    ref = oracle.run(p)
+    assert ref["status"] == 0
+    ctx.setup(p)
+    out = ctx.run(p, precision="fp64")
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(out[k], ref[k]) < FP64_TOL, k
+
+
+@pytest.mark.parametrize("precision", ["fp32k", "fp32", "plain"])
+@pytest.mark.parametrize("etype,n,step,dt", [("Q4", 30, 402, 1e-3), ("Q9", 14, 402, 5e-4)])
+def test_fp32_run_within_tolerance(ctx, oracle, precision, etype, n, step, dt):
+    p = small_problem(etype, n=n, step=step, pml=5, seed=13, dt=dt)
+    ref = oracle.run(p)
+    ctx.setup(p)
+    out = ctx.run(p, precision=precision, want_snapshots=precision != "plain")
+    for k in ("seis_u", "seis_w"):
+        assert rel_l2(out[k], ref[k]) < FP32_TOL, (k, rel_l2(out[k], ref[k]))
+    if precision != "plain":
+        for k in ("snap_u", "snap_w"):
+            assert rel_l2(out[k], ref[k]) < FP32_TOL, (k, rel_l2(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("spb", [32, 64])
+def test_batched_shots_match_single(ctx, oracle, spb):
+    shots = spb + 3   # a full batch plus a ragged one
+    p = small_problem("Q4", n=40, step=202, pml=5, seed=17, shots=shots)
+    ctx.setup(p)
+    single = ctx.run(p, precision="fp32k", shots_per_batch=1, want_snapshots=True)
+    batched = ctx.run(p, precision="fp32k", shots_per_batch=spb, want_snapshots=True)
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(batched[k], single[k]) < 1e-6, k
+    # and two of the shots against the FP64 oracle
+    import copy
+    q = copy.copy(p)
+    q.src_node = p.src_node[[0, shots - 1]]
+    ref = oracle.run(q)
+    for k in ("seis_u", "seis_w"):
+        assert rel_l2(batched[k][[0, shots - 1]], ref[k]) < FP32_TOL, k
+
+
+def test_blowup_detected_like_reference(ctx, oracle):
+    p = small_problem("T6", n=16, step=260, pml=4, seed=7)   # dt too large for T6: the energy bound trips
+    ref = oracle.run(p)
+    assert ref["status"] == 1
+    ctx.setup(p)
+    out = ctx.run(p, precision="fp64", raise_on_blowup=False)
+    assert out["status"] == 6
+    assert out["stats"]["blowup_step"] > 2
+
+
+def test_bad_indices_rejected(ctx):
+    from seisfem_b200.api import SfgError
+    p = small_problem("Q4", n=8, step=10, pml=2)
+    ctx.setup(p)
+    bad = p.src_node.copy()
+    bad[0] = -1                     # node_location's miss value
+    with pytest.raises(SfgError) as e:
+        ctx.run(p, src_node=bad)
+    assert e.value.status == 5
+    en = p.mesh.element_node.copy()
+    en[3] = p.mesh.node_num + 5
+    q = small_problem("Q4", n=8, step=10, pml=2)
+    q.mesh.element_node = en
+    with pytest.raises(SfgError) as e:
+        ctx.setup(q)
+    assert e.value.status == 5
+
+
+def test_zero_area_rejected(ctx):
+    from seisfem_b200.api import SfgError
+    p = small_problem("Q4", n=6, step=10, pml=2)
+    en = p.mesh.element_node.copy()
+    en[4:8] = en[0]                 # element 1 collapses to a point
+    p.mesh.element_node = en
+    with pytest.raises(SfgError) as e:
+        ctx.setup(p)
+    assert e.value.status == 4
