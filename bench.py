@@ -1,0 +1,337 @@
+"""Benchmark of the mass-lumped explicit time loop (DOF-steps/s).
+
+One bench "step" is one complete simulation of the workload -- every time
+step of one shot (or one batch of shots) -- with the mesh, matrices and state
+resident in HBM.  Default workload: the Q9 400x400 layered model (641,601
+nodes, 1,283,202 DOF, 3000 time steps, M-PML 30), FP32 with compensated
+displacement.  With N ranks (torchrun, one GPU each) every rank advances its
+own shot (shots are independent; no collective inside the loop) and the
+job's value is all ranks' DOF-steps over the slowest rank's time.
+
+Printed JSON line: value (device-resident loop), e2e (the public C-ABI call
+with host buffers: GPU assembly + run + copies back), roofline of the fused
+step kernel, clocks, the CPU baseline (rank 0, N=1), launch counts.
+`--impl reference` times the reference's own CPU code (oracle/_ref, else the
+oracle port) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from seisfem_b200 import problem as P  # noqa: E402
+
+METRIC = "DOF-steps/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+
+
+def workload(name: str, rank: int = 0):
+    if name == "q9_400_layered":
+        p = P.config_2()
+    elif name == "q4_200_homog":
+        p = P.config_1()
+    elif name == "q4_400_grf_64shots":
+        p = P.config_3a()
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    if rank and len(p.src_node) == 1:
+        # each rank runs its own shot: the source moves one element per rank
+        m = p.mesh
+        x0, y0 = m.x[p.src_node[0]], m.y[p.src_node[0]]
+        p.src_node = P.locate(m, p.edge_size, [(x0, y0 + p.edge_size * rank)])
+    return p
+
+
+def clocks_start(path):
+    try:
+        f = open(path, "w")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=f, stderr=subprocess.DEVNULL), f
+    except Exception:
+        return None, None
+
+
+def clocks_stop(proc, f, path, device):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    f.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(device):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for n, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(prob_name: str, seconds_budget: float = 30.0) -> dict:
+    """The reference's own CPU loop (oracle/_ref) on this host's cores, on a
+    bounded sample: the full set-up plus a few time steps of the workload,
+    each step timed from the reference's end-of-step output."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    prob = workload(prob_name)
+    cores = os.cpu_count() or 1
+    nsteps = 8
+    prob.step = 2 + nsteps
+    if os.path.exists(O.LIBREF):
+        ref = O.Reference()
+        out = ref.run(prob, nthreads=cores, want_snapshots=False)
+        t = out["step_end_times"]
+        dts = np.diff(t)
+        per_step = float(np.median(dts)) if len(dts) else float("nan")
+        kind = "reference"
+        sample = (f"{prob.name}: reference elastic_wave() with step={prob.step} ({nsteps} time steps, "
+                  f"set-up {t[0] - (t[1] - t[0]) if len(t) > 1 else float('nan'):.1f} s excluded); "
+                  f"median of per-step times from its end-of-step seismogram writes")
+    else:
+        orc = O.Oracle()
+        out = orc.run(prob, nthreads=cores)
+        per_step = out["loop_seconds"] / nsteps
+        kind = "port"
+        sample = f"{prob.name}: oracle port, {nsteps} time steps, loop time only"
+    dof_steps = 2 * prob.mesh.node_num
+    return {"value": dof_steps / per_step, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample,
+            "seconds_per_step": per_step}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    prob = workload(args.workload)
+    cores = os.cpu_count() or 1
+    n = args.warmup + args.steps
+    prob.step = 2 + n
+    if os.path.exists(O.LIBREF):
+        out = O.Reference().run(prob, nthreads=cores, want_snapshots=False)
+        t = out["step_end_times"]
+        dts = np.diff(np.concatenate([[t[0] - (t[1] - t[0])], t])) if len(t) > 1 else np.array([np.nan])
+        timed = dts[args.warmup:args.warmup + args.steps]
+        kind = "reference"
+    else:
+        out = O.Oracle().run(prob, nthreads=cores)
+        timed = np.full(args.steps, out["loop_seconds"] / n)
+        kind = "port"
+    ms = float(np.sum(timed)) * 1e3
+    value = 2 * prob.mesh.node_num * args.steps / (ms / 1e3)
+    sample = (f"{prob.name}: {n} time steps of the reference elastic_wave() loop on {cores} host threads; "
+              f"bench step = one time step; the first {args.warmup} are warm-up")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": prob.name, "nodes": prob.mesh.node_num, "dof": prob.dof, "element": "Q9",
+                       "time_steps_per_bench_step": 1},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="q9_400_layered")
+    ap.add_argument("--precision", default="fp32k", choices=["fp32k", "fp32", "fp64", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from seisfem_b200.api import Context, Plan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = local
+    torch.cuda.set_device(dev)
+    prob = workload(args.workload, rank)
+    S = len(prob.src_node)
+    ctx = Context(dev)
+    ctx.setup(prob)
+    st = ctx.stats()
+    # a dedicated (non-default) stream: the plan's graph and the timing events
+    # are queued on the same stream
+    stream = torch.cuda.Stream(dev)
+    plan = Plan(ctx, prob, precision=args.precision, snap_every=200)
+    sh = stream.cuda_stream
+    assert sh != 0
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        plan.launch(0, sh)
+    torch.cuda.synchronize(dev)
+    plan.finish(0, stream=sh)      # energy bound check of the warm-up result
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"sfg_clocks_{rank}.csv")
+    proc, fh = clocks_start(clk_path)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.launch(0, sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = clocks_stop(proc, fh, clk_path, dev)
+    ms = e0.elapsed_time(e1)
+    res = plan.finish(0, stream=sh)
+    launches = plan.launches * args.steps
+    plan.close()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    dof_steps_rank = 2 * prob.mesh.node_num * S * (prob.step - 2)
+    value = dof_steps_rank * world * args.steps / (ms_max / 1e3)
+
+    # roofline: the fused step kernel alone (a plan without snapshot copies),
+    # average launch time = loop time / time steps, on the launching stream
+    plan2 = Plan(ctx, prob, precision=args.precision, snap_every=0)
+    for _ in range(2):
+        plan2.launch(0, sh)
+    torch.cuda.synchronize(dev)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.steps)
+    k0.record(stream)
+    for _ in range(reps):
+        plan2.launch(0, sh)
+    k1.record(stream)
+    torch.cuda.synchronize(dev)
+    kms = k0.elapsed_time(k1) / (reps * (prob.step - 2))
+    plan2.close()
+    b_step = step_bytes(ctx, prob, S)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = b_step / (kms * 1e-3) / 1e9
+    traffic = None
+    if os.path.exists(TRAFFIC_FILE):
+        tj = json.load(open(TRAFFIC_FILE)).get(f"{args.workload}:{args.precision}")
+        if tj:
+            traffic = tj.get("bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "step32_kernel (fused SpMV + RHS + solve + Newmark)",
+                "algorithmic_bytes_per_launch": b_step, "avg_launch_us": round(kms * 1e3, 3),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback"}
+
+    # e2e: public C-ABI call with host buffers (GPU assembly + run + outputs)
+    e2e = None
+    if not args.no_e2e:
+        m, md = prob.mesh, prob.model
+        h2d = sum(a.nbytes for a in (m.element_node, m.x, m.y, md.rho, md.vp, md.vs, md.c)) + 8 * S + 4 * len(prob.rec_node)
+        ns = ctx.L.sfg_snapshot_rows(prob.step, 200)
+        d2h = 2 * 8 * S * (prob.step - 2) * len(prob.rec_node) + 2 * 8 * S * ns * m.node_num
+        times = []
+        for k in range(1 + 2):
+            barrier()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            c2 = Context(dev)
+            c2.setup(prob)
+            c2.run(prob, precision=args.precision, snap_every=200)
+            torch.cuda.synchronize(dev)
+            times.append(time.perf_counter() - t0)
+            c2.close()
+        t_e2e = torch.tensor([statistics.median(times[1:])], dtype=torch.float64, device=f"cuda:{dev}")
+        if world > 1:
+            dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+        e2e = {"value": dof_steps_rank * world / float(t_e2e.item()), "unit": METRIC,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "seconds_per_step": float(t_e2e.item()),
+               "note": "one elastic_wave()-equivalent call per step: sfg_setup (GPU assembly from host arrays) + "
+                       "sfg_run (loop, seismograms and 200-step snapshots copied back)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64",
+                "data": "synthetic",
+                "config": {"workload": prob.name, "element": prob.mesh.type_name, "nodes": prob.mesh.node_num,
+                           "dof": prob.dof, "shots_per_rank": S, "time_steps": prob.step - 2,
+                           "precision": args.precision, "union_nnz": st["union_nnz"],
+                           "setup_ms": round(st["setup_ms"], 1),
+                           "l2": "per-step working set (matrix + state) > 126 MB L2; no flush needed",
+                           "parallelism": f"shots over {world} GPU(s)"},
+                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": launches,
+                "energy_status": int(res["status"])}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+def step_bytes(ctx, prob, S) -> int:
+    """Algorithmic bytes of one fused FP32 time step (all S shots):
+    matrix stream -- per union entry 4 B column + 4 B each of M, K1..K4, plus
+    K5, K6 on rows inside the M-PML (rows outside it multiply every K5/K6,
+    M*V and M*U_k product by a zero damping coefficient) -- plus the
+    state record read and written once per node and shot (24 + 10 floats)
+    and the per-node coefficient record (12 floats)."""
+    p, _ = ctx.union_pattern()
+    L = np.diff(p).astype(np.int64)
+    mp = ctx.mpml()
+    pml = np.any(mp[:4].astype(np.float32) != 0, axis=0)
+    N = prob.mesh.node_num
+    mat = int(L[pml].sum()) * 32 + int(L[~pml].sum()) * 24 + 4 * (N // 32 + 1)
+    state = N * S * (24 + 10) * 4 * 2
+    coef = N * 12 * 4
+    return int(mat + state + coef)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

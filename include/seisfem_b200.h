@@ -111,7 +111,15 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *mesh, const sfg_model *model);
 int sfg_csr_nnz(sfg_ctx *ctx, int matrix, int *nnz);
 int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x);
 int sfg_lumped_mass_copy(sfg_ctx *ctx, double *mass_lump);         /* [node_num] */
+/* the union sparsity pattern of M, K1..K6 that the step kernels stream
+ * (p: [node_num+1], j: [*nnz]; either may be NULL to query the size) */
+int sfg_union_copy(sfg_ctx *ctx, int *p, int *j, long long *nnz);
 int sfg_mpml_copy(sfg_ctx *ctx, double *out6);                       /* [6][node_num] */
+/* Replace the lumped mass used by the time loop (e.g. a caller's own
+ * lumping).  The reference's normalisation mass_sum/diag_sum
+ * (mass_sparse_q4.c:259-263) is a long sequential FP64 sum; sfg_setup forms
+ * it with a fixed-shape parallel sum, equal to ~1e-14 relative. */
+int sfg_lumped_mass_set(sfg_ctx *ctx, const double *mass_lump);     /* [node_num] */
 
 /* Run every shot (elastic_wave.c:446-809).  Outputs (any may be NULL):
  *   seis_u, seis_w  [src_num][step-2][rec_num]  displacement at receivers
@@ -124,13 +132,29 @@ int sfg_run(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_
 int sfg_snapshot_rows(int step, int snap_every);
 int sfg_get_stats(const sfg_ctx *ctx, sfg_stats *stats);
 
-/* Device-resident variant for callers that keep data on the GPU: the same
- * run, outputs written to device pointers (FP32 for the FP32 precisions,
- * FP64 otherwise, layout as sfg_run), work queued on `stream`
- * (a cudaStream_t; NULL = the legacy default stream), no host copies and no
- * synchronisation.  Check the status of the queued work with sfg_sync(). */
+/* Same run with the seismograms written to DEVICE pointers (FP64, layout as
+ * sfg_run) and the work queued on `stream` (a cudaStream_t; NULL = the
+ * context's stream).  Returns when the work is done. */
 int sfg_run_device(sfg_ctx *ctx, const sfg_run_desc *run, void *d_seis_u, void *d_seis_w,
                    void *stream);
+
+/* Prepared runs.  sfg_plan_create allocates one batch's device state, stages
+ * every batch's sources on the device, picks the launch shape (autotuner) and
+ * captures the whole time loop of a batch -- state reset, one fused kernel
+ * per step, snapshot copies, receiver gathers -- into a CUDA graph.
+ * sfg_plan_launch queues batch b (shots b*S .. b*S+S-1) on `stream`
+ * asynchronously; sfg_plan_finish waits for it, copies its outputs to the
+ * given host or device buffers (full [src_num]... layout as sfg_run; any may
+ * be NULL) and applies the energy bound.  A plan is bound to its context and
+ * to the context's current set-up. */
+typedef struct sfg_plan sfg_plan;
+int sfg_plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **plan);
+int sfg_plan_batches(const sfg_plan *plan);
+int sfg_plan_launches(const sfg_plan *plan);   /* kernels one batch launches */
+int sfg_plan_launch(sfg_plan *plan, int batch, void *stream);
+int sfg_plan_finish(sfg_plan *plan, int batch, double *seis_u, double *seis_w, double *snap_u,
+                    double *snap_w, void *stream);
+void sfg_plan_destroy(sfg_plan *plan);
 int sfg_sync(sfg_ctx *ctx);
 
 /* ----------------------------------------------------------- the seams */

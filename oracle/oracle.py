@@ -43,6 +43,7 @@ class _Problem(C.Structure):
         ("src_num", C.c_int), ("src_node", C.POINTER(C.c_int)),
         ("rec_num", C.c_int), ("rec_node", C.POINTER(C.c_int)),
         ("free_surface", C.c_int), ("snap_every", C.c_int), ("nthreads", C.c_int),
+        ("timing", C.POINTER(C.c_double)),
     ]
 
 
@@ -144,6 +145,7 @@ class Oracle:
             out["energy_u"] = np.zeros((S, step))
             out["energy_w"] = np.zeros((S, step))
         keep = [prob.model.c, prob.src_node, prob.rec_node]
+        timing = np.zeros(2)
         pb = _Problem(
             m.type_code, N, m.element_num, m.order, _ptr(m.element_node, C.c_int),
             _ptr(m.x, C.c_double), _ptr(m.y, C.c_double),
@@ -152,12 +154,13 @@ class Oracle:
             step, prob.dt, prob.f0, prob.t0, prob.edge_size,
             m.xmin, m.xmax, m.ymin, m.ymax, prob.pml_nx, prob.pml_ny,
             S, _ptr(prob.src_node, C.c_int), R, _ptr(prob.rec_node, C.c_int),
-            prob.free_surface, snap_every, nthreads)
+            prob.free_surface, snap_every, nthreads, _ptr(timing, C.c_double))
         ptrs = [out[k].ctypes.data for k in ("seis_u", "seis_w", "snap_u", "snap_w")]
         ptrs += [out["energy_u"].ctypes.data, out["energy_w"].ctypes.data] if energy else [None, None]
         rc = self.lib.sfo_elastic_run(C.byref(pb), *ptrs)
         del keep
         out["status"] = rc
+        out["setup_seconds"], out["loop_seconds"] = float(timing[0]), float(timing[1])
         return out
 
 
@@ -185,7 +188,8 @@ class Reference:
         L.sfr_elastic_wave.argtypes = ([C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, _i32p,
                                         _f64p, _f64p, C.c_int] + [C.c_double] * 8 + [C.c_int, C.c_int,
                                         C.c_int, _i32p, C.c_int, _i32p, C.c_char_p, C.c_int, C.c_int] +
-                                       [C.c_void_p] * 4 + [C.c_int, C.POINTER(C.c_double)])
+                                       [C.c_void_p] * 4 + [C.c_int, C.POINTER(C.c_double), C.c_void_p, C.c_int])
+        L.sfr_now.restype = C.c_double
 
     def mesh(self, type_name, nx, ny, xmin, xmax, ymin, ymax):
         N, E = C.c_int(), C.c_int()
@@ -229,15 +233,18 @@ class Reference:
                               pml_nx, pml_ny, h, *bounds, vp_max, *use, out)
         return out.reshape(6, mesh.node_num)
 
-    def run(self, prob, nthreads: int = 0, workdir: str | None = None):
+    def run(self, prob, nthreads: int = 0, workdir: str | None = None, want_snapshots: bool = True):
         """Run the reference elastic_wave() (solver masslump) through its
         exterior-model path: the model is written to
         mesh/velocity_and_density.txt with %.17g so it reads back exactly."""
         m = prob.mesh
         S, R, N, step = len(prob.src_node), len(prob.rec_node), m.node_num, prob.step
         ns = snapshot_rows(step, 200)
-        out = {"seis_u": np.zeros((S, step - 2, R)), "seis_w": np.zeros((S, step - 2, R)),
-               "snap_u": np.zeros((S, ns, N)), "snap_w": np.zeros((S, ns, N))}
+        out = {"seis_u": np.zeros((S, step - 2, R)), "seis_w": np.zeros((S, step - 2, R))}
+        if want_snapshots:
+            out["snap_u"] = np.zeros((S, ns, N))
+            out["snap_w"] = np.zeros((S, ns, N))
+        step_t = np.zeros(step)
         tmp = workdir or tempfile.mkdtemp(prefix="sfref_")
         os.makedirs(os.path.join(tmp, "mesh"), exist_ok=True)
         os.makedirs(os.path.join(tmp, "outputfile"), exist_ok=True)
@@ -246,14 +253,18 @@ class Reference:
             cols = np.stack([md.rho, md.vp, md.vs, md.c[0], md.c[1], md.c[2], md.c[3]], axis=1)
             f.write("".join(" ".join("%.17g" % v for v in row) + "\n" for row in cols))
         secs = C.c_double()
+        t_call = self.lib.sfr_now()
         rc = self.lib.sfr_elastic_wave(
             tmp.encode(), nthreads, m.type_name.encode(), N, m.element_num, m.order, m.element_node,
             m.x, m.y, step, prob.dt, prob.f0, prob.t0, prob.edge_size, m.xmin, m.xmax, m.ymin, m.ymax,
             prob.pml_nx, prob.pml_ny, S, np.ascontiguousarray(prob.src_node, np.int32), R,
             np.ascontiguousarray(prob.rec_node, np.int32), b"masslump", 1, prob.free_surface,
-            out["seis_u"].ctypes.data, out["seis_w"].ctypes.data, out["snap_u"].ctypes.data,
-            out["snap_w"].ctypes.data, ns, C.byref(secs))
+            out["seis_u"].ctypes.data, out["seis_w"].ctypes.data,
+            out["snap_u"].ctypes.data if want_snapshots else None,
+            out["snap_w"].ctypes.data if want_snapshots else None, ns, C.byref(secs), step_t.ctypes.data, step)
         out["status"] = rc
+        nst = int(np.count_nonzero(step_t))
+        out["step_end_times"] = step_t[:nst] - t_call     # seconds since the call began
         out["seconds"] = secs.value
         out["workdir"] = tmp
         return out

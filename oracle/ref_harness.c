@@ -46,6 +46,17 @@ static FILE *g_open[64];
 static int g_nopen;
 static jmp_buf g_jmp;
 static int g_in_run;
+/* per-step timestamps: the reference ends every time step by writing "\n"
+ * to seismogram_u_shot_k (elastic_wave.c:794) */
+static double *g_step_t;
+static long g_step_n, g_step_cap;
+
+static double now_s(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
 
 static FILE *sfr_fopen(const char *path, const char *mode)
 {
@@ -91,6 +102,8 @@ static int sfr_fprintf(FILE *f, const char *fmt, ...)
         }
     }
     va_end(ap2);
+    if (f && f == g_cap.fp[CAP_SU] && fmt[0] == '\n' && g_step_t && g_step_n < g_step_cap)
+        g_step_t[g_step_n++] = now_s();
     int n = vfprintf(f, fmt, ap);
     va_end(ap);
     return n;
@@ -234,14 +247,17 @@ int sfr_mesh_sizes(char *type, int nelemx, int nelemy, int *node_num, int *eleme
  * Captured FP64 outputs: seis_u/seis_w [src_num][step-2][rec_num],
  * snap_u/snap_w [src_num][snap_rows][node_num] (any may be NULL).
  * Returns 0, 1 on the energy bound, 3 on a non-masslump solver; *seconds
- * gets the wall time of the elastic_wave() call. */
+ * gets the wall time of the elastic_wave() call; step_times (may be NULL)
+ * gets the CLOCK_MONOTONIC time at the end of each time step of shot 1.
+ * sfr_now() reads the same clock. */
+double sfr_now(void) { return now_s(); }
 int sfr_elastic_wave(const char *workdir, int nthreads, char *type, int node_num, int element_num,
                      int order, int *element_node, double *x, double *y, int step, double dt,
                      double f0, double t0, double edge_size, double xmin, double xmax, double ymin,
                      double ymax, int pml_nx, int pml_ny, int src_num, int *src_node, int rec_num,
                      int *rec_node, char *solver, int use_exterior_mesh, int free_surface,
                      double *seis_u, double *seis_w, double *snap_u, double *snap_w, int snap_rows,
-                     double *seconds)
+                     double *seconds, double *step_times, int step_times_cap)
 {
     char cwd[4096];
     if (!getcwd(cwd, sizeof cwd)) return 2;
@@ -252,6 +268,9 @@ int sfr_elastic_wave(const char *workdir, int nthreads, char *type, int node_num
     g_cap.buf[CAP_PU] = snap_u; g_cap.per_shot[CAP_PU] = (long)snap_rows * node_num;
     g_cap.buf[CAP_PW] = snap_w; g_cap.per_shot[CAP_PW] = (long)snap_rows * node_num;
     if (nthreads > 0) omp_set_num_threads(nthreads);
+    g_step_t = step_times;
+    g_step_n = 0;
+    g_step_cap = step_times_cap;
     double *xy[2] = {x, y};
     struct timespec a, b;
     clock_gettime(CLOCK_MONOTONIC, &a);
@@ -263,6 +282,7 @@ int sfr_elastic_wave(const char *workdir, int nthreads, char *type, int node_num
                      xmin, xmax, ymin, ymax, pml_nx, pml_ny, src_num, src_node, rec_num, rec_node,
                      solver, use_exterior_mesh, free_surface);
     g_in_run = 0;
+    g_step_t = NULL;
     clock_gettime(CLOCK_MONOTONIC, &b);
     while (g_nopen > 0) fclose(g_open[--g_nopen]);
     memset(&g_cap, 0, sizeof g_cap);

@@ -95,6 +95,7 @@ typedef struct {
     int free_surface;
     int snap_every;
     int nthreads;           /* OpenMP threads, <=0: library default */
+    double *timing;         /* optional out: [0] set-up seconds, [1] time-loop seconds */
 } sfo_problem;
 
 int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,

@@ -58,8 +58,9 @@ _LIB = None
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "sfg_setup", "sfg_csr_nnz",
-           "sfg_csr_copy", "sfg_lumped_mass_copy", "sfg_mpml_copy", "sfg_run", "sfg_snapshot_rows",
-           "sfg_get_stats", "sfg_run_device", "sfg_sync", "elastic_wave", "sfg_mass_sparse_all",
+           "sfg_csr_copy", "sfg_lumped_mass_copy", "sfg_lumped_mass_set", "sfg_union_copy", "sfg_mpml_copy", "sfg_run", "sfg_snapshot_rows",
+           "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
+           "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec"]
 
 
@@ -83,9 +84,17 @@ def lib(path: str = LIBPATH):
     L.sfg_csr_copy.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.sfg_lumped_mass_copy.argtypes = [C.c_void_p, C.c_void_p]
     L.sfg_mpml_copy.argtypes = [C.c_void_p, C.c_void_p]
+    L.sfg_lumped_mass_set.argtypes = [C.c_void_p, C.c_void_p]
+    L.sfg_union_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]
     L.sfg_run.argtypes = [C.c_void_p, C.POINTER(RunDesc_)] + [C.c_void_p] * 4
     L.sfg_run_device.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.c_void_p, C.c_void_p, C.c_void_p]
     L.sfg_sync.argtypes = [C.c_void_p]
+    L.sfg_plan_create.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.POINTER(C.c_void_p)]
+    L.sfg_plan_batches.argtypes = [C.c_void_p]
+    L.sfg_plan_launches.argtypes = [C.c_void_p]
+    L.sfg_plan_launch.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.sfg_plan_finish.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 5
+    L.sfg_plan_destroy.argtypes = [C.c_void_p]
     L.sfg_snapshot_rows.argtypes = [C.c_int, C.c_int]
     L.sfg_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats_)]
     L.sfg_mass_sparse_all.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _i32p, C.c_void_p, _f64p,
@@ -159,6 +168,18 @@ class Context:
         self._check(self.L.sfg_lumped_mass_copy(self.ptr, m.ctypes.data))
         return m
 
+    def union_pattern(self):
+        n = C.c_longlong()
+        self._check(self.L.sfg_union_copy(self.ptr, None, None, C.byref(n)))
+        p = np.zeros(self.node_num + 1, np.int32)
+        j = np.zeros(max(n.value, 1), np.int32)
+        self._check(self.L.sfg_union_copy(self.ptr, p.ctypes.data, j.ctypes.data, C.byref(n)))
+        return p, j[:n.value]
+
+    def set_lumped_mass(self, m):
+        m = np.ascontiguousarray(m, np.float64)
+        self._check(self.L.sfg_lumped_mass_set(self.ptr, m.ctypes.data))
+
     def mpml(self):
         m = np.zeros(6 * self.node_num)
         self._check(self.L.sfg_mpml_copy(self.ptr, m.ctypes.data))
@@ -200,6 +221,55 @@ class Context:
                         PRECISIONS[precision], 0, shots_per_batch)
         self._check(self.L.sfg_run_device(self.ptr, C.byref(desc), d_seis_u, d_seis_w, stream or None))
         return self.stats()
+
+
+class Plan:
+    """A prepared run (sfg_plan_*): one CUDA-graph launch per batch of shots."""
+
+    def __init__(self, ctx: Context, prob: Problem, precision: str = "fp32k", snap_every: int = 0,
+                 shots_per_batch: int = 0, src_node=None):
+        self.ctx, self.L = ctx, ctx.L
+        self.src = np.ascontiguousarray(prob.src_node if src_node is None else src_node, np.int32)
+        self.rec = np.ascontiguousarray(prob.rec_node, np.int32)
+        self.step, self.N = prob.step, prob.mesh.node_num
+        self.desc = RunDesc_(prob.step, prob.dt, prob.f0, prob.t0, len(self.src), self.src.ctypes.data,
+                             len(self.rec), self.rec.ctypes.data, PRECISIONS[precision], snap_every, shots_per_batch)
+        h = C.c_void_p()
+        ctx._check(self.L.sfg_plan_create(ctx.ptr, C.byref(self.desc), C.byref(h)))
+        self.ptr = h
+        self.batches = self.L.sfg_plan_batches(h)
+        self.launches = self.L.sfg_plan_launches(h)
+        self.snap_rows = self.L.sfg_snapshot_rows(prob.step, snap_every) if snap_every else 0
+
+    def launch(self, batch: int = 0, stream: int = 0):
+        self.ctx._check(self.L.sfg_plan_launch(self.ptr, batch, stream or None))
+
+    def finish(self, batch: int = 0, out=None, stream: int = 0, raise_on_blowup: bool = True):
+        """Wait for `batch`, copy its outputs into `out` (dict of host arrays;
+        created when None) and apply the energy bound."""
+        S, R = len(self.src), len(self.rec)
+        if out is None:
+            out = {"seis_u": np.zeros((S, self.step - 2, R)), "seis_w": np.zeros((S, self.step - 2, R))}
+            if self.snap_rows:
+                out["snap_u"] = np.zeros((S, self.snap_rows, self.N))
+                out["snap_w"] = np.zeros((S, self.snap_rows, self.N))
+        ptr = lambda k: out[k].ctypes.data if k in out else None
+        rc = self.L.sfg_plan_finish(self.ptr, batch, ptr("seis_u"), ptr("seis_w"), ptr("snap_u"), ptr("snap_w"),
+                                    stream or None)
+        self.ctx._check(rc, allow=() if raise_on_blowup else (SFG_ERR_BLOWUP,))
+        out["status"] = rc
+        return out
+
+    def close(self):
+        if self.ptr:
+            self.L.sfg_plan_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def elastic_wave(prob: Problem, precision: str = "fp32k", device: int = 0, snap_every: int = 200):

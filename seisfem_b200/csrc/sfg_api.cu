@@ -298,6 +298,33 @@ int sfg_mpml_copy(sfg_ctx *ctx, double *out6)
     return SFG_OK;
 }
 
+int sfg_union_copy(sfg_ctx *ctx, int *p, int *j, long long *nnz)
+{
+    if (!ctx) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    CK(cudaSetDevice(ctx->device));
+    if (nnz) *nnz = ctx->P.union_nnz;
+    if (p) CK(cudaMemcpy(p, ctx->P.up, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
+    if (j && ctx->P.union_nnz) CK(cudaMemcpy(j, ctx->P.uj, sizeof(int) * ctx->P.union_nnz, cudaMemcpyDeviceToHost));
+    return SFG_OK;
+}
+
+int sfg_lumped_mass_set(sfg_ctx *ctx, const double *mass_lump)
+{
+    if (!ctx || !mass_lump) return SFG_ERR_ARG;
+    if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
+    CK(cudaSetDevice(ctx->device));
+    DevProblem &P = ctx->P;
+    CK(cudaMemcpy(P.mass_lump, mass_lump, sizeof(double) * ctx->N, cudaMemcpyHostToDevice));
+    cudaFree(P.coef32);
+    cudaFree(P.coefd);
+    P.coef32 = nullptr;
+    P.coefd = nullptr;
+    CK(build_coef(ctx->N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SFG_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------- time loop
@@ -419,8 +446,9 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
 {
     const int N = ctx->N, S = pl.S, R = run->rec_num, rows = run->step - 2;
     const size_t esz = pl.kind == SFG_FP64 ? sizeof(double) : sizeof(float);
-    b.gbytes = (size_t)N * GREC * S * esz;
-    b.pbytes = (size_t)N * PREC * S * esz;
+    const bool f64 = pl.kind == SFG_FP64;
+    b.gbytes = (size_t)N * (f64 ? GREC : G32) * S * esz;
+    b.pbytes = (size_t)N * (f64 ? PREC : P32) * S * esz;
     cudaStream_t st = ctx->stream;
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         CK(cudaMalloc(&b.pst, sizeof(float) * 36 * (size_t)N));
@@ -450,29 +478,24 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
     return SFG_OK;
 }
 
-int reset_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int nsnap, BatchBufs &b,
-               const int *src_nodes, int nshot)
+// Queue the reset of one batch's state (captured into the batch graph).
+cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBufs &b, cudaStream_t st)
 {
-    cudaStream_t st = ctx->stream;
-    const int N = ctx->N, S = pl.S;
+    const int S = pl.S;
+    cudaError_t e = cudaSuccess;
+    auto z = [&](void *p, size_t n) { if (e == cudaSuccess && p && n) e = cudaMemsetAsync(p, 0, n, st); };
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
-        CK(cudaMemsetAsync(b.pst, 0, sizeof(float) * 36 * (size_t)N, st));
-        CK(cudaMemsetAsync(b.panew, 0, sizeof(float) * 6 * (size_t)N, st));
+        z(b.pst, sizeof(float) * 36 * (size_t)N);
+        z(b.panew, sizeof(float) * 6 * (size_t)N);
     } else {
-        for (int k = 0; k < 2; k++) {
-            CK(cudaMemsetAsync(b.G[k], 0, b.gbytes, st));
-            CK(cudaMemsetAsync(b.Pv[k], 0, b.pbytes, st));
-        }
+        for (int k = 0; k < 2; k++) { z(b.G[k], b.gbytes); z(b.Pv[k], b.pbytes); }
     }
-    std::vector<int> src(S, -1);
-    for (int s = 0; s < nshot; s++) src[s] = src_nodes[s];
-    CK(cudaMemcpyAsync(b.src, src.data(), sizeof(int) * S, cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(b.energy, 0, sizeof(double) * (size_t)S * run->step * 2, st));
+    z(b.energy, sizeof(double) * (size_t)S * step * 2);
     if (nsnap > 0) {
-        CK(cudaMemsetAsync(b.snap_u, 0, sizeof(double) * (size_t)S * nsnap * N, st));
-        CK(cudaMemsetAsync(b.snap_w, 0, sizeof(double) * (size_t)S * nsnap * N, st));
+        z(b.snap_u, sizeof(double) * (size_t)S * nsnap * N);
+        z(b.snap_w, sizeof(double) * (size_t)S * nsnap * N);
     }
-    return SFG_OK;
+    return e;
 }
 
 // Time a few steps of each candidate launch shape and keep the fastest
@@ -538,10 +561,39 @@ int ensure_plain_matrices(sfg_ctx *ctx)
     return SFG_OK;
 }
 
-int run_impl(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
-             double *snap_w, bool host_out, cudaStream_t user_stream)
+}  // namespace
+
+// A prepared run: device buffers of one batch, every batch's sources staged on
+// the device, and the whole time loop of a batch (state reset included)
+// captured once into a CUDA graph.
+struct sfg_plan {
+    sfg_ctx *ctx = nullptr;
+    LoopPlan pl;
+    sfg_run_desc run;
+    std::vector<int> src, rec;
+    int nsnap = 0, nbatch = 0, launches = 0;
+    BatchBufs b;
+    int *d_src_all = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void plan_free(sfg_plan *p)
 {
-    if (!ctx || !run) return SFG_ERR_ARG;
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    free_bufs(p->b);
+    cudaFree(p->d_src_all);
+    delete p;
+}
+
+int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
+{
+    if (!ctx || !run || !out) return SFG_ERR_ARG;
+    *out = nullptr;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     const int N = ctx->N;
     if (run->step < 3 || run->dt <= 0 || run->src_num < 1 || run->rec_num < 0 || !run->src_node ||
@@ -555,121 +607,130 @@ int run_impl(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis
             return fail(ctx, SFG_ERR_BADINDEX, "receiver node out of range (node_location miss gives -1)");
     if (run->precision < 0 || run->precision > 3) return fail(ctx, SFG_ERR_ARG, "bad precision");
     CK(cudaSetDevice(ctx->device));
-    auto t_all = std::chrono::steady_clock::now();
-    LoopPlan pl;
+    sfg_plan *p = new sfg_plan();
+    p->ctx = ctx;
+    p->run = *run;
+    p->src.assign(run->src_node, run->src_node + run->src_num);
+    p->rec.assign(run->rec_node, run->rec_node + run->rec_num);
+    p->run.src_node = p->src.data();
+    p->run.rec_node = p->rec.data();
+    LoopPlan &pl = p->pl;
     pl.kind = run->precision;
     pl.S = 1; pl.spl = 1; pl.threads = 128; pl.warps = 4;
     const bool fp32 = pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN;
     int spb = run->shots_per_batch;
     if (fp32) {
         if (spb <= 0) spb = run->src_num >= 64 ? 64 : (run->src_num >= 16 ? 32 : 1);
-        if (spb != 1 && spb != 32 && spb != 64 && spb != 128)
+        if (spb != 1 && spb != 32 && spb != 64 && spb != 128) {
+            plan_free(p);
             return fail(ctx, SFG_ERR_ARG, "shots_per_batch must be 1, 32, 64 or 128");
+        }
         pl.S = spb;
-        pl.spl = spb / 32 > 0 ? spb / 32 : 1;
+        pl.spl = spb >= 32 ? spb / 32 : 1;
     }
-    if (pl.kind == SFG_FP32_PLAIN_PATH) {
-        int rc = ensure_plain_matrices(ctx);
-        if (rc) return rc;
-    }
-    const int snap_every = run->snap_every;
-    const int nsnap = sfg_snapshot_rows(run->step, snap_every);
-    const int rows = run->step - 2, R = run->rec_num;
-    BatchBufs b;
-    int rc = alloc_bufs(ctx, pl, run, nsnap, b);
-    if (rc) { free_bufs(b); return rc; }
+    int rc;
+    if (pl.kind == SFG_FP32_PLAIN_PATH && (rc = ensure_plain_matrices(ctx)) != SFG_OK) { plan_free(p); return rc; }
+    p->nsnap = sfg_snapshot_rows(run->step, run->snap_every);
+    p->nbatch = (run->src_num + pl.S - 1) / pl.S;
+    if ((rc = alloc_bufs(ctx, pl, &p->run, p->nsnap, p->b)) != SFG_OK) { plan_free(p); return rc; }
+    std::vector<int> staged((size_t)p->nbatch * pl.S, -1);
+    for (int s = 0; s < run->src_num; s++) staged[s] = run->src_node[s];
     cudaStream_t st = ctx->stream;
-    rc = reset_bufs(ctx, pl, run, nsnap, b, run->src_node, std::min(pl.S, run->src_num));
-    if (rc == SFG_OK) rc = autotune(ctx, pl, run, b);
-    if (rc) { free_bufs(b); return rc; }
+    cudaError_t e = upload(&p->d_src_all, staged.data(), staged.size(), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p->b.src, p->d_src_all, sizeof(int) * pl.S, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
+    if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
+    if ((rc = autotune(ctx, pl, &p->run, p->b)) != SFG_OK) { plan_free(p); return rc; }
     ctx->stats.rows_per_block = pl.S == 1 ? pl.threads : pl.warps;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
+    cudaError_t er = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
+    p->launches = er == cudaSuccess ? queue_loop(ctx, pl, &p->run, p->b, run->snap_every, p->nsnap, run->step - 2, st) : -1;
+    e = cudaStreamEndCapture(st, &p->graph);
+    if (p->launches < 0 || e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, "graph capture failed"); }
+    e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+    CK(cudaStreamSynchronize(st));
+    *out = p;
+    return SFG_OK;
+}
 
-    // capture the whole loop once; relaunch it per batch
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int launches = 0;
-    {
-        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) { free_bufs(b); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
-        launches = queue_loop(ctx, pl, run, b, snap_every, nsnap, rows, st);
-        e = cudaStreamEndCapture(st, &graph);
-        if (launches < 0 || e != cudaSuccess) {
-            if (graph) cudaGraphDestroy(graph);
-            free_bufs(b);
-            return fail(ctx, SFG_ERR_CUDA, "graph capture failed");
-        }
-        e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e != cudaSuccess) {
-            cudaGraphDestroy(graph);
-            free_bufs(b);
-            return fail(ctx, SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+int plan_launch(sfg_plan *p, int batch, cudaStream_t st)
+{
+    sfg_ctx *ctx = p->ctx;
+    if (batch < 0 || batch >= p->nbatch) return fail(ctx, SFG_ERR_ARG, "batch out of range");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(p->b.src, p->d_src_all + (size_t)batch * p->pl.S, sizeof(int) * p->pl.S,
+                       cudaMemcpyDeviceToDevice, st));
+    CK(cudaGraphLaunch(p->exec, st));
+    return SFG_OK;
+}
+
+// Wait for a launched batch, copy its outputs to the caller (host or device
+// pointers, shot-major at the batch's offset) and apply the energy bound.
+int plan_finish(sfg_plan *p, int batch, double *seis_u, double *seis_w, double *snap_u, double *snap_w,
+                cudaStream_t st, cudaMemcpyKind kind)
+{
+    sfg_ctx *ctx = p->ctx;
+    const int S = p->pl.S, N = ctx->N, R = p->run.rec_num, rows = p->run.step - 2, step = p->run.step;
+    const int s0 = batch * S, ns = std::min(S, p->run.src_num - s0);
+    CK(cudaStreamSynchronize(st));
+    const size_t seis_n = (size_t)ns * rows * R, snap_n = (size_t)ns * p->nsnap * N;
+    if (seis_u && R) CK(cudaMemcpy(seis_u + (size_t)s0 * rows * R, p->b.seis_u, sizeof(double) * seis_n, kind));
+    if (seis_w && R) CK(cudaMemcpy(seis_w + (size_t)s0 * rows * R, p->b.seis_w, sizeof(double) * seis_n, kind));
+    if (p->nsnap > 0 && snap_u) CK(cudaMemcpy(snap_u + (size_t)s0 * p->nsnap * N, p->b.snap_u, sizeof(double) * snap_n, kind));
+    if (p->nsnap > 0 && snap_w) CK(cudaMemcpy(snap_w + (size_t)s0 * p->nsnap * N, p->b.snap_w, sizeof(double) * snap_n, kind));
+    std::vector<double> en((size_t)S * step * 2);
+    CK(cudaMemcpy(en.data(), p->b.energy, sizeof(double) * en.size(), cudaMemcpyDeviceToHost));
+    int status = SFG_OK;
+    for (int s = 0; s < ns; s++) {
+        const double *e = en.data() + (size_t)s * step * 2;
+        for (int it = 2; it < step; it++) {
+            if (!(e[2 * it] <= 10e6) || !(e[2 * it + 1] <= 10e6)) {
+                if (ctx->stats.blowup_step < 0 || it < ctx->stats.blowup_step) ctx->stats.blowup_step = it;
+                status = SFG_ERR_BLOWUP;
+                break;
+            }
         }
     }
+    if (status == SFG_ERR_BLOWUP)
+        ctx->err = "energy exceeds maximum value at step " + std::to_string(ctx->stats.blowup_step);
+    return status;
+}
+
+int run_all(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
+            double *snap_w, cudaStream_t user, cudaMemcpyKind kind)
+{
+    auto t_all = std::chrono::steady_clock::now();
+    sfg_plan *p = nullptr;
+    int rc = plan_create(ctx, run, &p);
+    if (rc) return rc;
+    cudaStream_t st = user ? user : ctx->stream;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double loop_ms = 0.0;
     int status = SFG_OK;
     ctx->stats.blowup_step = -1;
-    std::vector<double> energy;
-    for (int s0 = 0; s0 < run->src_num && status != SFG_ERR_CUDA; s0 += pl.S) {
-        const int ns = std::min(pl.S, run->src_num - s0);
-        rc = reset_bufs(ctx, pl, run, nsnap, b, run->src_node + s0, ns);
-        if (rc) { status = rc; break; }
+    for (int bidx = 0; bidx < p->nbatch; bidx++) {
         cudaEventRecord(e0, st);
-        cudaError_t e = cudaGraphLaunch(exec, st);
+        rc = plan_launch(p, bidx, st);
         cudaEventRecord(e1, st);
-        if (e != cudaSuccess) { status = fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); break; }
-        if (!host_out) {
-            // device variant: copy seismograms to the caller's device buffers
-            if (seis_u) cudaMemcpyAsync(seis_u + (size_t)s0 * rows * R, b.seis_u, sizeof(double) * ns * rows * R,
-                                        cudaMemcpyDeviceToDevice, user_stream ? user_stream : st);
-            if (seis_w) cudaMemcpyAsync(seis_w + (size_t)s0 * rows * R, b.seis_w, sizeof(double) * ns * rows * R,
-                                        cudaMemcpyDeviceToDevice, user_stream ? user_stream : st);
-        }
-        e = cudaEventSynchronize(e1);
-        if (e != cudaSuccess) { status = fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); break; }
+        if (rc) { status = rc; break; }
+        rc = plan_finish(p, bidx, seis_u, seis_w, snap_u, snap_w, st, kind);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         loop_ms += ms;
-        if (host_out) {
-            if (seis_u && R) CK(cudaMemcpy(seis_u + (size_t)s0 * rows * R, b.seis_u, sizeof(double) * ns * rows * R, cudaMemcpyDeviceToHost));
-            if (seis_w && R) CK(cudaMemcpy(seis_w + (size_t)s0 * rows * R, b.seis_w, sizeof(double) * ns * rows * R, cudaMemcpyDeviceToHost));
-            if (nsnap > 0 && snap_u) CK(cudaMemcpy(snap_u + (size_t)s0 * nsnap * N, b.snap_u, sizeof(double) * ns * nsnap * N, cudaMemcpyDeviceToHost));
-            if (nsnap > 0 && snap_w) CK(cudaMemcpy(snap_w + (size_t)s0 * nsnap * N, b.snap_w, sizeof(double) * ns * nsnap * N, cudaMemcpyDeviceToHost));
-        }
-        // energy bound (elastic_wave.c:777-785): first failing step
-        energy.resize((size_t)pl.S * run->step * 2);
-        CK(cudaMemcpy(energy.data(), b.energy, sizeof(double) * energy.size(), cudaMemcpyDeviceToHost));
-        for (int s = 0; s < ns && pl.kind != SFG_FP32_PLAIN_PATH; s++) {
-            const double *en = energy.data() + (pl.S == 1 ? 0 : (size_t)s * run->step * 2);
-            for (int it = 2; it < run->step; it++) {
-                const double a = en[2 * it], c = en[2 * it + 1];
-                if (!(a <= 10e6) || !(c <= 10e6)) {
-                    if (ctx->stats.blowup_step < 0 || it < ctx->stats.blowup_step) ctx->stats.blowup_step = it;
-                    status = SFG_ERR_BLOWUP;
-                    break;
-                }
-            }
-        }
-        if (pl.kind == SFG_FP32_PLAIN_PATH) {
-            for (int it = 2; it < run->step; it++) {
-                const double a = energy[2 * it], c = energy[2 * it + 1];
-                if (!(a <= 10e6) || !(c <= 10e6)) { ctx->stats.blowup_step = it; status = SFG_ERR_BLOWUP; break; }
-            }
-        }
+        if (rc == SFG_ERR_BLOWUP) status = rc;
+        else if (rc) { status = rc; break; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    free_bufs(b);
     ctx->stats.loop_ms = loop_ms;
-    ctx->stats.dof_steps = 2LL * N * run->src_num * (long long)(run->step - 2);
-    ctx->stats.kernel_launches = launches;
-    ctx->stats.total_ms =
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_all).count();
-    if (status == SFG_ERR_BLOWUP) ctx->err = "energy exceeds maximum value at step " + std::to_string(ctx->stats.blowup_step);
+    ctx->stats.dof_steps = 2LL * ctx->N * run->src_num * (long long)(run->step - 2);
+    ctx->stats.kernel_launches = p->launches;
+    plan_free(p);
+    ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_all).count();
     return status;
 }
 
@@ -680,13 +741,43 @@ extern "C" {
 int sfg_run(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
             double *snap_w)
 {
-    return run_impl(ctx, run, seis_u, seis_w, snap_u, snap_w, true, nullptr);
+    if (!ctx) return SFG_ERR_ARG;
+    return run_all(ctx, run, seis_u, seis_w, snap_u, snap_w, nullptr, cudaMemcpyDefault);
 }
 
 int sfg_run_device(sfg_ctx *ctx, const sfg_run_desc *run, void *d_seis_u, void *d_seis_w, void *stream)
 {
-    return run_impl(ctx, run, (double *)d_seis_u, (double *)d_seis_w, nullptr, nullptr, false,
-                    (cudaStream_t)stream);
+    if (!ctx) return SFG_ERR_ARG;
+    return run_all(ctx, run, (double *)d_seis_u, (double *)d_seis_w, nullptr, nullptr, (cudaStream_t)stream,
+                   cudaMemcpyDefault);
+}
+
+int sfg_plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **plan) { return plan_create(ctx, run, plan); }
+
+int sfg_plan_batches(const sfg_plan *plan) { return plan ? plan->nbatch : 0; }
+
+int sfg_plan_launches(const sfg_plan *plan) { return plan ? plan->launches : 0; }
+
+int sfg_plan_launch(sfg_plan *plan, int batch, void *stream)
+{
+    if (!plan) return SFG_ERR_ARG;
+    return plan_launch(plan, batch, stream ? (cudaStream_t)stream : plan->ctx->stream);
+}
+
+int sfg_plan_finish(sfg_plan *plan, int batch, double *seis_u, double *seis_w, double *snap_u, double *snap_w,
+                    void *stream)
+{
+    if (!plan) return SFG_ERR_ARG;
+    return plan_finish(plan, batch, seis_u, seis_w, snap_u, snap_w,
+                       stream ? (cudaStream_t)stream : plan->ctx->stream, cudaMemcpyDefault);
+}
+
+void sfg_plan_destroy(sfg_plan *plan)
+{
+    if (!plan) return;
+    cudaSetDevice(plan->ctx->device);
+    cudaDeviceSynchronize();
+    plan_free(plan);
 }
 
 int sfg_sync(sfg_ctx *ctx)

@@ -48,9 +48,9 @@ __device__ __forceinline__ void block_energy(double *dst, double a, double b)
     }
 }
 
-// Receiver gather of a finished state into seismogram row `row`
-// (elastic_wave.c:787-795).  Displacement = sum over the three split fields
-// of (value - Kahan compensation), in FP64.
+// Receiver gather of a finished FP32 state into seismogram row `row`
+// (elastic_wave.c:787-795): displacement = sum over the three split fields
+// of (high + low FP32 part), formed in FP64.
 __device__ __forceinline__ void gather_one32(const StepCommon &c, const float *G, const float *P, int S,
                                              int t, int row)
 {
@@ -60,8 +60,8 @@ __device__ __forceinline__ void gather_one32(const StepCommon &c, const float *G
     double u = 0.0, w = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        u += (double)G[(node * GREC + k) * S + s] - (double)P[(node * PREC + 6 + k) * S + s];
-        w += (double)G[(node * GREC + 3 + k) * S + s] - (double)P[(node * PREC + 9 + k) * S + s];
+        u += (double)G[(node * G32 + 10 + k) * S + s] + (double)P[(node * P32 + 4 + k) * S + s];
+        w += (double)G[(node * G32 + 13 + k) * S + s] + (double)P[(node * P32 + 7 + k) * S + s];
     }
     size_t o = ((size_t)s * c.seis_rows + row) * c.nrec + r;
     c.seis_u[o] = u;
@@ -70,61 +70,126 @@ __device__ __forceinline__ void gather_one32(const StepCommon &c, const float *G
 
 // ------------------------------------------------ FP32 single-shot kernel
 
-struct Rhs32 {
-    float a[6];    // accelerations of U1 U2 U3 W1 W2 W3
-    float lx[4], ly[4];
+template <typename T>
+struct RhsT {
+    T a[6];          // accelerations of U1 U2 U3 W1 W2 W3
+    T lx[4], ly[4];  // new memory variables
 };
 
 // Right-hand sides (elastic_wave.c:585-591, 651-657) times 1/m_lump
-// (:709-722).  kU[k], kW[k] = K_{k+1} times U, W; m[0..19] = M times the
-// gathered record (U1..W3, V1..V6, Lx1..4, Ly1..4).
-__device__ __forceinline__ void rhs32(const float *kU, const float *kW, const float *m, float4 c0,
-                                      float4 c1, float4 c2, float dt, float src_u, float src_w, Rhs32 &o)
+// (:709-722), evaluated in T (FP64 for the compensated path) from the FP32
+// products: kU[k], kW[k] = K_{k+1} times U, W; m[0..19] = M times U1..W3,
+// V1..V6, Lx1..4, Ly1..4.
+template <typename T>
+__device__ __forceinline__ void rhs_eval(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
+                                         float4 c2, T dt, T src_u, T src_w, RhsT<T> &o)
 {
-    const float c11 = c0.x, c13 = c0.y, c33 = c0.z, c44 = c0.w;
-    const float dx = c1.x, dy = c1.y, dxx = c1.z, dyy = c1.w;
-    const float im = c2.x, dxxp = c2.y, dyyp = c2.z;
-    const float kx = 1.0f - dt * dx, ky = 1.0f - dt * dy;
-    o.a[0] = im * (-c11 * kU[0] - 2.0f * dx * m[6] - dx * dx * m[0] + m[12] + m[13] + src_u);
-    o.a[1] = im * (-c13 * kW[2] - c44 * kW[3] - (dx + dy) * m[7] - dx * dy * m[1]);
-    o.a[2] = im * (-c44 * kU[1] - 2.0f * dy * m[8] - dy * dy * m[2] + m[14] + m[15]);
-    o.lx[0] = im * (-dt * c11 * dxx * kU[4] + kx * m[12]);
-    o.lx[1] = im * (-dt * c44 * dyyp * kW[4] + ky * m[13]);
-    o.lx[2] = im * (-dt * c13 * dxxp * kW[5] + kx * m[14]);
-    o.lx[3] = im * (-dt * c44 * dyy * kU[5] + ky * m[15]);
-    o.a[3] = im * (-c44 * kW[0] - 2.0f * dx * m[9] - dx * dx * m[3] + m[16] + m[17] + src_w);
-    o.a[4] = im * (-c44 * kU[2] - c13 * kU[3] - (dx + dy) * m[10] - dx * dy * m[4]);
-    o.a[5] = im * (-c33 * kW[1] - 2.0f * dy * m[11] - dy * dy * m[5] + m[18] + m[19]);
-    o.ly[0] = im * (-dt * c44 * dxx * kW[4] + kx * m[16]);
-    o.ly[1] = im * (-dt * c13 * dyyp * kU[4] + ky * m[17]);
-    o.ly[2] = im * (-dt * c44 * dxxp * kU[5] + kx * m[18]);
-    o.ly[3] = im * (-dt * c33 * dyy * kW[5] + ky * m[19]);
+    const T c11 = c0.x, c13 = c0.y, c33 = c0.z, c44 = c0.w;
+    const T dx = c1.x, dy = c1.y, dxx = c1.z, dyy = c1.w;
+    const T im = c2.x, dxxp = c2.y, dyyp = c2.z;
+    const T kx = T(1) - dt * dx, ky = T(1) - dt * dy;
+    auto K = [&](const float *v, int k) { return T(v[k]); };
+    auto Mv = [&](int k) { return T(m[k]); };
+    o.a[0] = im * (-c11 * K(kU, 0) - T(2) * dx * Mv(6) - dx * dx * Mv(0) + Mv(12) + Mv(13) + src_u);
+    o.a[1] = im * (-c13 * K(kW, 2) - c44 * K(kW, 3) - (dx + dy) * Mv(7) - dx * dy * Mv(1));
+    o.a[2] = im * (-c44 * K(kU, 1) - T(2) * dy * Mv(8) - dy * dy * Mv(2) + Mv(14) + Mv(15));
+    o.lx[0] = im * (-dt * c11 * dxx * K(kU, 4) + kx * Mv(12));
+    o.lx[1] = im * (-dt * c44 * dyyp * K(kW, 4) + ky * Mv(13));
+    o.lx[2] = im * (-dt * c13 * dxxp * K(kW, 5) + kx * Mv(14));
+    o.lx[3] = im * (-dt * c44 * dyy * K(kU, 5) + ky * Mv(15));
+    o.a[3] = im * (-c44 * K(kW, 0) - T(2) * dx * Mv(9) - dx * dx * Mv(3) + Mv(16) + Mv(17) + src_w);
+    o.a[4] = im * (-c44 * K(kU, 2) - c13 * K(kU, 3) - (dx + dy) * Mv(10) - dx * dy * Mv(4));
+    o.a[5] = im * (-c33 * K(kW, 1) - T(2) * dy * Mv(11) - dy * dy * Mv(5) + Mv(18) + Mv(19));
+    o.ly[0] = im * (-dt * c44 * dxx * K(kW, 4) + kx * Mv(16));
+    o.ly[1] = im * (-dt * c13 * dyyp * K(kU, 4) + ky * Mv(17));
+    o.ly[2] = im * (-dt * c44 * dxxp * K(kU, 5) + kx * Mv(18));
+    o.ly[3] = im * (-dt * c33 * dyy * K(kW, 5) + ky * Mv(19));
 }
 
-// Newmark (alpha = 1, delta = 1.5; elastic_wave.c:97, 757-768) for one
-// split field, with optional Kahan compensation of the displacement sum.
-template <bool KAHAN>
-__device__ __forceinline__ void newmark32(float &U, float &V, float &A, float &C, float an, float dt, float dt2)
+// Newmark, alpha = 1, delta = 1.5 (elastic_wave.c:97, 757-768), for one split
+// field.  Compensated: the displacement is carried as an FP32 pair hi + lo,
+// updated in FP64 and split again, so the running sum keeps ~48 bits.
+__device__ __forceinline__ double newmark_comp(float &hi, float &lo, float &V, float &A, double an, double dt)
 {
-    float du = V * dt + (an - 0.5f * A) * dt2;
-    if (KAHAN) {
-        float y = du - C;
-        float t = U + y;
-        C = (t - U) - y;
-        U = t;
-    } else {
-        U = U + du;
-    }
+    const double Ad = A, Vd = V;
+    const double U = ((double)hi + (double)lo) + Vd * dt + (an - 0.5 * Ad) * (dt * dt);
+    hi = (float)U;
+    lo = (float)(U - (double)hi);
+    V = (float)(Vd + (1.5 * an - 0.5 * Ad) * dt);
+    A = (float)an;
+    return U;
+}
+
+__device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, float an, float dt)
+{
+    U = U + V * dt + (an - 0.5f * A) * (dt * dt);
     V = V + (1.5f * an - 0.5f * A) * dt;
     A = an;
+    return U;
 }
 
-template <bool KAHAN>
+// Finish one node: right-hand sides, lumped solve, Newmark, new records.
+// g[24] / p[10] are the node's own records (layout in sfg_step.cuh).
+template <bool COMP>
+__device__ __forceinline__ void finish_node(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
+                                            float4 c2, double dt, double src_u, double src_w, const float *g,
+                                            const float *p, float *go, float *po, double &uu, double &ww)
+{
+    float hi[6] = {g[10], g[11], g[12], g[13], g[14], g[15]};
+    float V[6] = {g[16], g[17], g[18], g[19], g[20], g[21]};
+    float A[6] = {g[22], g[23], p[0], p[1], p[2], p[3]};
+    float lo[6] = {p[4], p[5], p[6], p[7], p[8], p[9]};
+    float Lx[4], Ly[4];
+    double Ut[6];
+    if (COMP) {
+        RhsT<double> r;
+        rhs_eval<double>(kU, kW, m, c0, c1, c2, dt, src_u, src_w, r);
+#pragma unroll
+        for (int k = 0; k < 6; k++) Ut[k] = newmark_comp(hi[k], lo[k], V[k], A[k], r.a[k], dt);
+#pragma unroll
+        for (int k = 0; k < 4; k++) { Lx[k] = (float)r.lx[k]; Ly[k] = (float)r.ly[k]; }
+    } else {
+        RhsT<float> r;
+        rhs_eval<float>(kU, kW, m, c0, c1, c2, (float)dt, (float)src_u, (float)src_w, r);
+#pragma unroll
+        for (int k = 0; k < 6; k++) Ut[k] = newmark_plain(hi[k], V[k], A[k], r.a[k], (float)dt);
+#pragma unroll
+        for (int k = 0; k < 4; k++) { Lx[k] = r.lx[k]; Ly[k] = r.ly[k]; }
+    }
+    uu = (Ut[0] + Ut[1]) + Ut[2];
+    ww = (Ut[3] + Ut[4]) + Ut[5];
+    go[0] = (float)uu; go[1] = (float)ww;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { go[2 + k] = Lx[k]; go[6 + k] = Ly[k]; }
+#pragma unroll
+    for (int k = 0; k < 6; k++) { go[10 + k] = hi[k]; go[16 + k] = V[k]; }
+    go[22] = A[0]; go[23] = A[1];
+    po[0] = A[2]; po[1] = A[3]; po[2] = A[4]; po[3] = A[5];
+#pragma unroll
+    for (int k = 0; k < 6; k++) po[4 + k] = COMP ? lo[k] : 0.f;
+}
+
+__device__ __forceinline__ bool is_pml_row(float4 c1)
+{
+    return c1.x != 0.f || c1.y != 0.f || c1.z != 0.f || c1.w != 0.f;
+}
+
+// One thread per row over SELL-32 slices.  Rows outside the M-PML (their
+// dx, dy, dxx, dyy are 0) multiply every M*V, M*U_k, K5 and K6 product by 0,
+// so a warp whose rows are all interior streams only the column, M and
+// K1..K4 planes and gathers only U, W, Lx, Ly (the first 10 record values).
+template <bool COMP>
 __global__ void __launch_bounds__(256) step32_kernel(const Step32 a)
 {
     const StepCommon &c = a.c;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     gather_one32(c, a.Gin, a.Pin, 1, i, c.seis_row);
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
+    if (i < c.n) {
+        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
+        c0 = __ldg(cf); c1 = __ldg(cf + 1); c2 = __ldg(cf + 2);
+    }
+    const bool full = __any_sync(0xffffffffu, i < c.n && is_pml_row(c1));
     double eu = 0.0, ew = 0.0;
     if (i < c.n) {
         const int lane = i & 31, slice = i >> 5;
@@ -135,66 +200,69 @@ __global__ void __launch_bounds__(256) step32_kernel(const Step32 a)
         for (int k = 0; k < 20; k++) m[k] = 0.f;
         const int s0 = __ldg(a.slice_ptr + slice), s1 = __ldg(a.slice_ptr + slice + 1);
         const float *sd = a.sell + (size_t)s0 * 256 + lane;
-        const float4 *G4 = reinterpret_cast<const float4 *>(a.Gin);
+        if (full) {
 #pragma unroll 2
-        for (int g = s0; g < s1; ++g, sd += 256) {
-            const int j = __float_as_int(ldgf(sd));
-            const float vm = ldgf(sd + 32);
-            float kv[6];
+            for (int g = s0; g < s1; ++g, sd += 256) {
+                const int j = __float_as_int(ldgf(sd));
+                const float vm = ldgf(sd + 32);
+                float kv[6];
 #pragma unroll
-            for (int k = 0; k < 6; k++) kv[k] = ldgf(sd + 64 + 32 * k);
-            const float4 *gj = G4 + (size_t)j * 5;
-            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2), q3 = __ldg(gj + 3),
-                         q4 = __ldg(gj + 4);
-            const float u = q0.x + q0.y + q0.z;
-            const float w = q0.w + q1.x + q1.y;
+                for (int k = 0; k < 6; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                const float4 *gj = reinterpret_cast<const float4 *>(a.Gin + (size_t)j * G32);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2), q3 = __ldg(gj + 3),
+                             q4 = __ldg(gj + 4);
+                const float2 q5 = __ldg(reinterpret_cast<const float2 *>(gj + 5));
 #pragma unroll
-            for (int k = 0; k < 6; k++) { kU[k] += kv[k] * u; kW[k] += kv[k] * w; }
-            m[0] += vm * q0.x;  m[1] += vm * q0.y;  m[2] += vm * q0.z;  m[3] += vm * q0.w;
-            m[4] += vm * q1.x;  m[5] += vm * q1.y;  m[6] += vm * q1.z;  m[7] += vm * q1.w;
-            m[8] += vm * q2.x;  m[9] += vm * q2.y;  m[10] += vm * q2.z; m[11] += vm * q2.w;
-            m[12] += vm * q3.x; m[13] += vm * q3.y; m[14] += vm * q3.z; m[15] += vm * q3.w;
-            m[16] += vm * q4.x; m[17] += vm * q4.y; m[18] += vm * q4.z; m[19] += vm * q4.w;
+                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                m[0] += vm * q2.z;  m[1] += vm * q2.w;  m[2] += vm * q3.x;  m[3] += vm * q3.y;
+                m[4] += vm * q3.z;  m[5] += vm * q3.w;  m[6] += vm * q4.x;  m[7] += vm * q4.y;
+                m[8] += vm * q4.z;  m[9] += vm * q4.w;  m[10] += vm * q5.x; m[11] += vm * q5.y;
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
+        } else {
+#pragma unroll 2
+            for (int g = s0; g < s1; ++g, sd += 256) {
+                const int j = __float_as_int(ldgf(sd));
+                const float vm = ldgf(sd + 32);
+                float kv[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                const float4 *gj = reinterpret_cast<const float4 *>(a.Gin + (size_t)j * G32);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
+                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+#pragma unroll
+                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
         }
-        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
-        const float4 c0 = __ldg(cf), c1 = __ldg(cf + 1), c2 = __ldg(cf + 2);
-        const float dt = (float)c.dt;
-        float src_u = 0.f, src_w = 0.f;
+        double src_u = 0.0, src_w = 0.0;
         if (i == c.src[0]) {
             const double ps = c.amp[c.it];
-            src_u = (float)(ps * c.sin_af);
-            src_w = (float)(ps * c.cos_af);
+            src_u = ps * c.sin_af;
+            src_w = ps * c.cos_af;
         }
-        Rhs32 r;
-        rhs32(kU, kW, m, c0, c1, c2, dt, src_u, src_w, r);
-        const float4 *gi = G4 + (size_t)i * 5;
-        const float4 g0 = __ldg(gi), g1 = __ldg(gi + 1), g2 = __ldg(gi + 2);
-        const float4 *pi = reinterpret_cast<const float4 *>(a.Pin) + (size_t)i * 3;
-        const float4 p0 = __ldg(pi), p1 = __ldg(pi + 1), p2 = __ldg(pi + 2);
-        float U[6] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y};
-        float V[6] = {g1.z, g1.w, g2.x, g2.y, g2.z, g2.w};
-        float A[6] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y};
-        float C[6] = {p1.z, p1.w, p2.x, p2.y, p2.z, p2.w};
-        const float dt2 = dt * dt;
+        float g[G32], p[P32], go[G32], po[P32];
+        const float4 *gi = reinterpret_cast<const float4 *>(a.Gin + (size_t)i * G32);
 #pragma unroll
-        for (int k = 0; k < 6; k++) newmark32<KAHAN>(U[k], V[k], A[k], C[k], r.a[k], dt, dt2);
-        float4 *go = reinterpret_cast<float4 *>(a.Gout) + (size_t)i * 5;
-        go[0] = make_float4(U[0], U[1], U[2], U[3]);
-        go[1] = make_float4(U[4], U[5], V[0], V[1]);
-        go[2] = make_float4(V[2], V[3], V[4], V[5]);
-        go[3] = make_float4(r.lx[0], r.lx[1], r.lx[2], r.lx[3]);
-        go[4] = make_float4(r.ly[0], r.ly[1], r.ly[2], r.ly[3]);
-        float4 *po = reinterpret_cast<float4 *>(a.Pout) + (size_t)i * 3;
-        po[0] = make_float4(A[0], A[1], A[2], A[3]);
-        if (KAHAN) {
-            po[1] = make_float4(A[4], A[5], C[0], C[1]);
-            po[2] = make_float4(C[2], C[3], C[4], C[5]);
-        } else {
-            reinterpret_cast<float2 *>(po + 1)[0] = make_float2(A[4], A[5]);
+        for (int k = 0; k < 6; k++) {
+            const float4 v = __ldg(gi + k);
+            g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
         }
-        const float uu = U[0] + U[1] + U[2], ww = U[3] + U[4] + U[5];
-        eu = (double)uu * uu;
-        ew = (double)ww * ww;
+        const float2 *pi = reinterpret_cast<const float2 *>(a.Pin + (size_t)i * P32);
+#pragma unroll
+        for (int k = 0; k < 5; k++) { const float2 v = __ldg(pi + k); p[2 * k] = v.x; p[2 * k + 1] = v.y; }
+        double uu, ww;
+        finish_node<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, g, p, go, po, uu, ww);
+        float4 *gout = reinterpret_cast<float4 *>(a.Gout + (size_t)i * G32);
+#pragma unroll
+        for (int k = 0; k < 6; k++) gout[k] = make_float4(go[4 * k], go[4 * k + 1], go[4 * k + 2], go[4 * k + 3]);
+        float2 *pout = reinterpret_cast<float2 *>(a.Pout + (size_t)i * P32);
+#pragma unroll
+        for (int k = 0; k < 5; k++) pout[k] = make_float2(po[2 * k], po[2 * k + 1]);
+        eu = uu * uu;
+        ew = ww * ww;
     }
     block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
 }
@@ -219,11 +287,12 @@ template <> struct VecF<4> {
     __device__ __forceinline__ void store(float *p) const { *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]); }
 };
 
-// One warp per row, S = 32*SPL shots with the shot index innermost: every
+// One warp per row, S = 32*SPL shots with the shot index innermost: each
 // matrix entry is read once (a warp-uniform 32-byte record) and applied to
 // all S shots; each lane gathers SPL consecutive shots of a neighbour's
-// record with one vector load per value.
-template <bool KAHAN, int SPL>
+// record with one vector load per value.  Interior rows (row-uniform
+// decision) gather only U, W, Lx, Ly.
+template <bool COMP, int SPL>
 __global__ void __launch_bounds__(256) step32_batched_kernel(const Step32 a)
 {
     constexpr int S = 32 * SPL;
@@ -236,13 +305,15 @@ __global__ void __launch_bounds__(256) step32_batched_kernel(const Step32 a)
     int src[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
-    const float dt = (float)c.dt, dt2 = dt * dt;
     const double ps = c.amp[c.it];
-    const float src_u = (float)(ps * c.sin_af), src_w = (float)(ps * c.cos_af);
+    const double src_u = ps * c.sin_af, src_w = ps * c.cos_af;
     float eu[SPL], ew[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
     for (int i = gtid >> 5; i < c.n; i += warps_total) {
+        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
+        const float4 c0 = __ldg(cf), c1 = __ldg(cf + 1), c2 = __ldg(cf + 2);
+        const bool full = is_pml_row(c1);
         float kU[6][SPL], kW[6][SPL], m[20][SPL];
 #pragma unroll
         for (int k = 0; k < 6; k++)
@@ -254,68 +325,80 @@ __global__ void __launch_bounds__(256) step32_batched_kernel(const Step32 a)
             for (int q = 0; q < SPL; q++) m[k][q] = 0.f;
         const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
         const float4 *rec = reinterpret_cast<const float4 *>(a.rec32);
-        for (int e = e0; e < e1; e++) {
-            const float4 r0 = __ldg(rec + 2 * (size_t)e), r1 = __ldg(rec + 2 * (size_t)e + 1);
-            const int j = __float_as_int(r0.x);
-            const float vm = r0.y;
-            const float kv[6] = {r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-            const float *gj = a.Gin + (size_t)j * GREC * S + s_base;
-            VecF<SPL> x[20];
+        if (full) {
+            for (int e = e0; e < e1; e++) {
+                const float4 r0 = __ldg(rec + 2 * (size_t)e), r1 = __ldg(rec + 2 * (size_t)e + 1);
+                const int j = __float_as_int(r0.x);
+                const float vm = r0.y;
+                const float kv[6] = {r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+                const float *gj = a.Gin + (size_t)j * G32 * S + s_base;
+                VecF<SPL> x[22];
 #pragma unroll
-            for (int v = 0; v < 20; v++) x[v].load(gj + v * S);
+                for (int v = 0; v < 22; v++) x[v].load(gj + v * S);
 #pragma unroll
-            for (int q = 0; q < SPL; q++) {
-                const float u = x[0].v[q] + x[1].v[q] + x[2].v[q];
-                const float w = x[3].v[q] + x[4].v[q] + x[5].v[q];
+                for (int q = 0; q < SPL; q++) {
 #pragma unroll
-                for (int k = 0; k < 6; k++) { kU[k][q] += kv[k] * u; kW[k][q] += kv[k] * w; }
+                    for (int k = 0; k < 6; k++) { kU[k][q] += kv[k] * x[0].v[q]; kW[k][q] += kv[k] * x[1].v[q]; }
 #pragma unroll
-                for (int v = 0; v < 20; v++) m[v][q] += vm * x[v].v[q];
+                    for (int v = 0; v < 8; v++) m[12 + v][q] += vm * x[2 + v].v[q];
+#pragma unroll
+                    for (int v = 0; v < 12; v++) m[v][q] += vm * x[10 + v].v[q];
+                }
+            }
+        } else {
+            for (int e = e0; e < e1; e++) {
+                const float4 r0 = __ldg(rec + 2 * (size_t)e), r1 = __ldg(rec + 2 * (size_t)e + 1);
+                const int j = __float_as_int(r0.x);
+                const float vm = r0.y;
+                const float kv[4] = {r0.z, r0.w, r1.x, r1.y};
+                const float *gj = a.Gin + (size_t)j * G32 * S + s_base;
+                VecF<SPL> x[10];
+#pragma unroll
+                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
+#pragma unroll
+                for (int q = 0; q < SPL; q++) {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) { kU[k][q] += kv[k] * x[0].v[q]; kW[k][q] += kv[k] * x[1].v[q]; }
+#pragma unroll
+                    for (int v = 0; v < 8; v++) m[12 + v][q] += vm * x[2 + v].v[q];
+                }
             }
         }
-        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
-        const float4 c0 = __ldg(cf), c1 = __ldg(cf + 1), c2 = __ldg(cf + 2);
-        const float *gi = a.Gin + (size_t)i * GREC * S + s_base;
-        const float *pi = a.Pin + (size_t)i * PREC * S + s_base;
-        float *go = a.Gout + (size_t)i * GREC * S + s_base;
-        float *po = a.Pout + (size_t)i * PREC * S + s_base;
-        VecF<SPL> g[12], p[12];
+        const float *gi = a.Gin + (size_t)i * G32 * S + s_base;
+        const float *pi = a.Pin + (size_t)i * P32 * S + s_base;
+        float *gop = a.Gout + (size_t)i * G32 * S + s_base;
+        float *pop = a.Pout + (size_t)i * P32 * S + s_base;
+        VecF<SPL> gv[G32], pv[P32];
 #pragma unroll
-        for (int v = 0; v < 12; v++) g[v].load(gi + v * S);
+        for (int v = 0; v < G32; v++) gv[v].load(gi + v * S);
 #pragma unroll
-        for (int v = 0; v < 12; v++) if (KAHAN || v < 6) p[v].load(pi + v * S);
-        VecF<SPL> out[20], pout[12];
+        for (int v = 0; v < P32; v++) pv[v].load(pi + v * S);
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
-            float kUq[6], kWq[6], mq[20];
+            float kUq[6], kWq[6], mq[20], g[G32], p[P32], go[G32], po[P32];
 #pragma unroll
             for (int k = 0; k < 6; k++) { kUq[k] = kU[k][q]; kWq[k] = kW[k][q]; }
 #pragma unroll
             for (int v = 0; v < 20; v++) mq[v] = m[v][q];
+#pragma unroll
+            for (int v = 0; v < G32; v++) g[v] = gv[v].v[q];
+#pragma unroll
+            for (int v = 0; v < P32; v++) p[v] = pv[v].v[q];
             const bool is_src = (i == src[q]);
-            Rhs32 r;
-            rhs32(kUq, kWq, mq, c0, c1, c2, dt, is_src ? src_u : 0.f, is_src ? src_w : 0.f, r);
-            float uu = 0.f, ww = 0.f;
+            double uu, ww;
+            finish_node<COMP>(kUq, kWq, mq, c0, c1, c2, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, go,
+                              po, uu, ww);
 #pragma unroll
-            for (int k = 0; k < 6; k++) {
-                float U = g[k].v[q], V = g[6 + k].v[q], A = p[k].v[q];
-                float C = KAHAN ? p[6 + k].v[q] : 0.f;
-                newmark32<KAHAN>(U, V, A, C, r.a[k], dt, dt2);
-                out[k].v[q] = U;
-                out[6 + k].v[q] = V;
-                pout[k].v[q] = A;
-                pout[6 + k].v[q] = C;
-                if (k < 3) uu += U; else ww += U;
-            }
+            for (int v = 0; v < G32; v++) gv[v].v[q] = go[v];
 #pragma unroll
-            for (int k = 0; k < 4; k++) { out[12 + k].v[q] = r.lx[k]; out[16 + k].v[q] = r.ly[k]; }
-            eu[q] += uu * uu;
-            ew[q] += ww * ww;
+            for (int v = 0; v < P32; v++) pv[v].v[q] = po[v];
+            eu[q] += (float)(uu * uu);
+            ew[q] += (float)(ww * ww);
         }
 #pragma unroll
-        for (int v = 0; v < 20; v++) out[v].store(go + v * S);
+        for (int v = 0; v < G32; v++) gv[v].store(gop + v * S);
 #pragma unroll
-        for (int v = 0; v < 12; v++) if (KAHAN || v < 6) pout[v].store(po + v * S);
+        for (int v = 0; v < P32; v++) pv[v].store(pop + v * S);
     }
     // energy per shot: block reduction over warps, one atomic pair per shot
     if (c.energy) {
@@ -460,8 +543,8 @@ __global__ void snapshot32_kernel(const float *G, const float *P, int n, int S, 
     long long node = t / S;
     double u = 0.0, w = 0.0;
     for (int k = 0; k < 3; k++) {
-        u += (double)G[(node * GREC + k) * S + s] - (double)P[(node * PREC + 6 + k) * S + s];
-        w += (double)G[(node * GREC + 3 + k) * S + s] - (double)P[(node * PREC + 9 + k) * S + s];
+        u += (double)G[(node * G32 + 10 + k) * S + s] + (double)P[(node * P32 + 4 + k) * S + s];
+        w += (double)G[(node * G32 + 13 + k) * S + s] + (double)P[(node * P32 + 7 + k) * S + s];
     }
     su[s * shot_stride + node] = u;
     sw[s * shot_stride + node] = w;

@@ -1,12 +1,18 @@
 // sfg_step.cuh -- step-kernel argument blocks and launchers.
 //
-// State layout (per shot; all device, node-major so that one node's record
-// is contiguous):
-//   G[n][20]  values the neighbours gather: U1 U2 U3 W1 W2 W3 | V1..V6
-//             (U1t U2t U3t W1t W2t W3t) | Lx1..Lx4 | Ly1..Ly4
-//   P[n][12]  values only the node itself reads: A1..A6 (U1tt..W3tt) and
-//             C1..C6 (Kahan compensation of U1..W3)
-// Batched runs put the shot index innermost: G[n][20][S], P[n][12][S].
+// State layout (per shot; node-major so that one node's record is
+// contiguous).  FP32 paths:
+//   G[n][24]  the record neighbours gather, ordered so that rows outside the
+//             M-PML read only its first 10 values:
+//               0 U, 1 W (totals U1+U2+U3, W1+W2+W3, formed by the owner in
+//               FP64), 2..5 Lx1..Lx4, 6..9 Ly1..Ly4, 10..15 U1 U2 U3 W1 W2 W3
+//               (high FP32 part), 16..21 V1..V6 (U1t U2t U3t W1t W2t W3t),
+//               22..23 A1 A2 (U1tt U2tt)
+//   P[n][10]  values only the owner reads: 0..3 A3..A6 (U3tt W1tt W2tt
+//             W3tt), 4..9 low FP32 parts of U1..W3 (compensated precision;
+//             the displacement is hi + lo)
+// FP64 path: G[n][20] = U1..W3 | V1..V6 | Lx1..4 | Ly1..4, P[n][12] = A1..A6.
+// Batched runs put the shot index innermost: G[n][24][S], P[n][10][S].
 // G and P are double-buffered (ping-pong) so that a step never reads a value
 // it has already overwritten.
 #pragma once
@@ -15,8 +21,10 @@
 
 namespace sfg {
 
-constexpr int GREC = 20;   // gathered values per node
-constexpr int PREC = 12;   // private values per node
+constexpr int G32 = 24;    // FP32 gathered record
+constexpr int P32 = 10;    // FP32 private record
+constexpr int GREC = 20;   // FP64 gathered record
+constexpr int PREC = 12;   // FP64 private record
 constexpr int CREC = 12;   // coefficients per node
 
 // Coefficient record per node (FP32 and FP64 variants share the order):
