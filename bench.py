@@ -170,6 +170,8 @@ def main():
     ap.add_argument("--precision", default="fp32k", choices=["fp32k", "fp32", "fp64", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--compare-plain", action="store_true",
+                    help="also time the unfused path (one SpMV launch per product) on one shot")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -225,6 +227,7 @@ def main():
     ms = e0.elapsed_time(e1)
     res = plan.finish(0, stream=sh)
     launches = plan.launches * args.steps
+    st = ctx.stats()
     plan.close()
     ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
     if world > 1:
@@ -290,6 +293,26 @@ def main():
                "note": "one elastic_wave()-equivalent call per step: sfg_setup (GPU assembly from host arrays) + "
                        "sfg_run (loop, seismograms and 200-step snapshots copied back)"}
 
+    plain = None
+    if args.compare_plain:
+        one = np.ascontiguousarray(prob.src_node[:1])
+        pp = Plan(ctx, prob, precision="plain", snap_every=0, src_node=one)
+        pp.launch(0, sh)
+        torch.cuda.synchronize(dev)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        pp.launch(0, sh)
+        p1.record(stream)
+        torch.cuda.synchronize(dev)
+        pms = p0.elapsed_time(p1)
+        per_shot_plain = 2 * prob.mesh.node_num * (prob.step - 2) / (pms / 1e3)
+        per_shot_fused = value / (world * S)
+        plain = {"plain_single_shot_dof_steps_per_s": per_shot_plain, "plain_ms_per_shot": pms,
+                 "plain_launches_per_time_step": pp.launches / (prob.step - 2),
+                 "fused_per_shot_dof_steps_per_s": per_shot_fused,
+                 "ratio_batched_over_plain_per_shot_cost": value / (world * per_shot_plain)}
+        pp.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload)
@@ -307,6 +330,8 @@ def main():
                            "parallelism": f"shots over {world} GPU(s)"},
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches,
+                "launch_shape": st["rows_per_block"],
+                "vs_plain_path": plain,
                 "energy_status": int(res["status"])}
         print(json.dumps(line), flush=True)
     if world > 1:

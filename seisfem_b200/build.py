@@ -23,6 +23,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler"
 UNITS = {
     "sfg_assemble.cu": ["-fmad=false"],
     "sfg_step.cu": [],
+    "sfg_step32.cu": [],
     "sfg_api.cu": [],
     "sfg_seams.cu": ["-fmad=false"],
 }

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <numeric>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -12,6 +13,7 @@
 
 #include "sfg_internal.h"
 #include "sfg_step.cuh"
+#include "sfg_step32.cuh"
 
 using namespace sfg;
 
@@ -24,6 +26,8 @@ struct RunCache {
 struct sfg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;       // second branch of each step (class-Z kernel)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     bool ready = false;
     DevProblem P;
@@ -81,7 +85,9 @@ void free_problem(DevProblem &P)
     cudaFree(P.up); cudaFree(P.uj); cudaFree(P.ux);
     for (auto &c : P.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
     cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
-    cudaFree(P.sell); cudaFree(P.slice_ptr); cudaFree(P.rec32); cudaFree(P.coef32); cudaFree(P.coefd);
+    cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.perm); cudaFree(P.inv);
+    cudaFree(P.sellA); cudaFree(P.sellZ); cudaFree(P.sliceA); cudaFree(P.sliceZ); cudaFree(P.upp);
+    cudaFree(P.recp); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ);
     P = DevProblem();
 }
 
@@ -113,7 +119,10 @@ sfg_ctx *sfg_create(int device)
     if (cudaSetDevice(device) != cudaSuccess) return nullptr;
     sfg_ctx *c = new sfg_ctx();
     c->device = device;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         delete c;
         return nullptr;
     }
@@ -130,6 +139,9 @@ void sfg_destroy(sfg_ctx *c)
     free_problem(c->P);
     for (auto &p : c->plain_x) cudaFree(p);
     cudaStreamDestroy(c->stream);
+    cudaStreamDestroy(c->stream2);
+    cudaEventDestroy(c->ev_fork);
+    cudaEventDestroy(c->ev_join);
     delete c;
 }
 
@@ -244,8 +256,60 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
 
     // step data: coefficients, SELL-32 slices (single shot), row records (batched)
     CK(build_coef(N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, st));
-    CK(build_sell32(N, P.up, P.uj, P.ux, P.union_nnz, &P.sell, &P.slice_ptr, &P.sell_slots, st));
-    CK(build_rec32(N, P.up, P.uj, P.ux, P.union_nnz, &P.rec32, st));
+    // two-class numbering of the fused FP32 step (sfg_step32.cuh): class Z =
+    // rows inside the M-PML and every column they reference; class A = the
+    // rest.  Inside each class, windows of 2048 rows are ordered by (M-PML
+    // flag, decreasing length) so that 32-row SELL slices need no padding.
+    {
+        // the context stream is non-blocking: finish its work (M-PML profiles,
+        // union pattern) before the host reads the results
+        CK(cudaStreamSynchronize(st));
+        const long long nz_all = P.union_nnz;
+        std::vector<int> hup((size_t)N + 1), huj((size_t)std::max<long long>(nz_all, 1));
+        std::vector<double> hmp(4 * (size_t)N);
+        CK(cudaMemcpy(hup.data(), P.up, sizeof(int) * ((size_t)N + 1), cudaMemcpyDeviceToHost));
+        if (nz_all) CK(cudaMemcpy(huj.data(), P.uj, sizeof(int) * nz_all, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hmp.data(), P.mpml, sizeof(double) * 4 * (size_t)N, cudaMemcpyDeviceToHost));
+        std::vector<char> pml(N, 0), zone(N, 0);
+        for (int r = 0; r < N; r++)
+            for (int k = 0; k < 4; k++)
+                if ((float)hmp[(size_t)k * N + r] != 0.f) pml[r] = 1;
+        for (int r = 0; r < N; r++)
+            if (pml[r]) {
+                zone[r] = 1;
+                for (int e = hup[r]; e < hup[r + 1]; e++) zone[huj[e]] = 1;
+            }
+        std::vector<int> perm;
+        perm.reserve(N);
+        for (int r = 0; r < N; r++) if (!zone[r]) perm.push_back(r);
+        const int na = (int)perm.size();
+        for (int r = 0; r < N; r++) if (zone[r]) perm.push_back(r);
+        const int sigma = 2048;
+        auto len = [&](int r) { return hup[r + 1] - hup[r]; };
+        for (int c = 0; c < 2; c++) {
+            const int r0 = c == 0 ? 0 : na, r1 = c == 0 ? na : N;
+            for (int w0 = r0; w0 < r1; w0 += sigma) {
+                const int w1 = std::min(r1, w0 + sigma);
+                std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int a, int b) {
+                    if (pml[a] != pml[b]) return pml[a] < pml[b];
+                    return len(a) > len(b);
+                });
+            }
+        }
+        std::vector<int> inv(N), upp((size_t)N + 1, 0);
+        for (int r = 0; r < N; r++) inv[perm[r]] = r;
+        for (int r = 0; r < N; r++) upp[r + 1] = upp[r] + len(perm[r]);
+        CK(upload(&P.perm, perm.data(), (size_t)N, st));
+        CK(upload(&P.inv, inv.data(), (size_t)N, st));
+        CK(upload(&P.upp, upp.data(), (size_t)N + 1, st));
+        P.h_inv = std::move(inv);
+        P.h_perm = std::move(perm);
+        P.na = na;
+    }
+    CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA, &P.slotsA, st));
+    CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ, &P.slotsZ, st));
+    CK(build_rec_perm(N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, P.upp, &P.recp, st));
+    CK(build_coef2(N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, st));
     CK(cudaStreamSynchronize(st));
     canon_free(co, true);
     cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
@@ -273,6 +337,7 @@ int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x)
     if (!ctx || matrix < 0 || matrix > 6) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
     const DevCsr &c = ctx->P.csr[matrix];
     if (p) CK(cudaMemcpy(p, c.p, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
     if (j && c.nnz) CK(cudaMemcpy(j, c.j, sizeof(int) * c.nnz, cudaMemcpyDeviceToHost));
@@ -285,6 +350,7 @@ int sfg_lumped_mass_copy(sfg_ctx *ctx, double *out)
     if (!ctx || !out) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(out, ctx->P.mass_lump, sizeof(double) * ctx->N, cudaMemcpyDeviceToHost));
     return SFG_OK;
 }
@@ -294,6 +360,7 @@ int sfg_mpml_copy(sfg_ctx *ctx, double *out6)
     if (!ctx || !out6) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(out6, ctx->P.mpml, sizeof(double) * 6 * (size_t)ctx->N, cudaMemcpyDeviceToHost));
     return SFG_OK;
 }
@@ -303,6 +370,7 @@ int sfg_union_copy(sfg_ctx *ctx, int *p, int *j, long long *nnz)
     if (!ctx) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
     if (nnz) *nnz = ctx->P.union_nnz;
     if (p) CK(cudaMemcpy(p, ctx->P.up, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
     if (j && ctx->P.union_nnz) CK(cudaMemcpy(j, ctx->P.uj, sizeof(int) * ctx->P.union_nnz, cudaMemcpyDeviceToHost));
@@ -315,12 +383,12 @@ int sfg_lumped_mass_set(sfg_ctx *ctx, const double *mass_lump)
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
     DevProblem &P = ctx->P;
+    CK(cudaStreamSynchronize(ctx->stream));   // no queued work may still read the old values
     CK(cudaMemcpy(P.mass_lump, mass_lump, sizeof(double) * ctx->N, cudaMemcpyHostToDevice));
-    cudaFree(P.coef32);
-    cudaFree(P.coefd);
-    P.coef32 = nullptr;
-    P.coefd = nullptr;
+    cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ);
+    P.coef32 = nullptr; P.coefd = nullptr; P.coefA = nullptr; P.imA = nullptr; P.coefZ = nullptr;
     CK(build_coef(ctx->N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, ctx->stream));
+    CK(build_coef2(ctx->N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return SFG_OK;
 }
@@ -335,14 +403,20 @@ struct LoopPlan {
     int kind;            // SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH
     int S;               // shots advanced together (1, 32, 64, 128)
     int spl;             // shots per lane (batched)
-    int threads;         // single-shot launch shape
+    int threads;         // single-shot launch shape (variant of launch_step32; FP64: threads)
     int warps;           // batched launch shape
 };
 
+// The fused FP32 kernels run in the two-class node numbering.
+bool permuted(const LoopPlan &pl) { return pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN; }
+
 // Device buffers of one batch.
 struct BatchBufs {
-    void *G[2] = {nullptr, nullptr}, *Pv[2] = {nullptr, nullptr};
+    void *G[2] = {nullptr, nullptr}, *Pv[2] = {nullptr, nullptr};   // FP64 path
     size_t gbytes = 0, pbytes = 0;
+    float *Gc[2] = {nullptr, nullptr}, *Pa[2] = {nullptr, nullptr};  // fused FP32 paths
+    float *Gs[2] = {nullptr, nullptr}, *Ps[2] = {nullptr, nullptr};
+    size_t gc_bytes = 0, pa_bytes = 0, gs_bytes = 0;
     int *src = nullptr;
     int *rec = nullptr;
     double *amp = nullptr;
@@ -355,7 +429,10 @@ struct BatchBufs {
 
 void free_bufs(BatchBufs &b)
 {
-    for (int k = 0; k < 2; k++) { cudaFree(b.G[k]); cudaFree(b.Pv[k]); }
+    for (int k = 0; k < 2; k++) {
+        cudaFree(b.G[k]); cudaFree(b.Pv[k]);
+        cudaFree(b.Gc[k]); cudaFree(b.Pa[k]); cudaFree(b.Gs[k]); cudaFree(b.Ps[k]);
+    }
     cudaFree(b.src); cudaFree(b.rec); cudaFree(b.amp); cudaFree(b.seis_u); cudaFree(b.seis_w);
     cudaFree(b.snap_u); cudaFree(b.snap_w); cudaFree(b.energy);
     cudaFree(b.pst); cudaFree(b.peq); cudaFree(b.prhs); cudaFree(b.panew);
@@ -407,26 +484,37 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             a.Gin = (const double *)b.G[cur]; a.Gout = (double *)b.G[nxt];
             a.Pin = (const double *)b.Pv[cur]; a.Pout = (double *)b.Pv[nxt];
             e = launch_step64(a, pl.threads, st);
+            if (e != cudaSuccess) return -1;
+            launches++;
         } else {
-            Step32 a;
-            a.c = c; a.sell = P.sell; a.slice_ptr = P.slice_ptr; a.rec32 = P.rec32; a.up = P.up;
-            a.coef = P.coef32;
-            a.Gin = (const float *)b.G[cur]; a.Gout = (float *)b.G[nxt];
-            a.Pin = (const float *)b.Pv[cur]; a.Pout = (float *)b.Pv[nxt];
-            const bool kahan = pl.kind == SFG_FP32_KAHAN;
-            e = S == 1 ? launch_step32(a, kahan, pl.threads, st)
-                       : launch_step32_batched(a, kahan, pl.spl, pl.warps, st);
+            Step2 a;
+            a.c = c; a.na = P.na;
+            a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
+            a.up = P.upp; a.rec = P.recp; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
+            a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
+            a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
+            const bool comp = pl.kind == SFG_FP32_KAHAN;
+            // fork: the class-Z kernel on the second stream, class A here; join
+            if (cudaEventRecord(ctx->ev_fork, st) != cudaSuccess) return -1;
+            if (cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0) != cudaSuccess) return -1;
+            e = S == 1 ? launch_stepZ(a, comp, pl.threads, ctx->stream2)
+                       : launch_stepZ_batched(a, comp, pl.spl, pl.warps, ctx->stream2);
+            if (e != cudaSuccess) return -1;
+            e = S == 1 ? launch_stepA(a, comp, pl.threads, st)
+                       : launch_stepA_batched(a, comp, pl.spl, pl.warps, st);
+            if (e != cudaSuccess) return -1;
+            if (cudaEventRecord(ctx->ev_join, ctx->stream2) != cudaSuccess) return -1;
+            if (cudaStreamWaitEvent(st, ctx->ev_join, 0) != cudaSuccess) return -1;
+            launches += (P.na > 0 || (c.seis_row >= 0 && c.nrec > 0)) + (P.na < N);
         }
-        if (e != cudaSuccess) return -1;
-        launches++;
         cur = nxt;
         if (nsnap > 0 && (it + 1) % snap_every == 0 && srow < nsnap) {
             const size_t off = (size_t)srow * N;
             if (pl.kind == SFG_FP64)
                 e = launch_snapshot64((const double *)b.G[cur], N, b.snap_u + off, b.snap_w + off, st);
             else
-                e = launch_snapshot32((const float *)b.G[cur], (const float *)b.Pv[cur], N, S, b.snap_u + off,
-                                      b.snap_w + off, (long long)nsnap * N, st);
+                e = launch_snapshot2({b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, N, P.na, S, P.perm, b.snap_u + off,
+                                     b.snap_w + off, (long long)nsnap * N, st);
             if (e != cudaSuccess) return -1;
             launches++;
             srow++;
@@ -435,8 +523,9 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
     // the last state's receiver row
     c.it = last - 1;
     c.seis_row = last - 3;
-    cudaError_t e = pl.kind == SFG_FP64 ? launch_gather64(c, (const double *)b.G[cur], S, st)
-                                        : launch_gather32(c, (const float *)b.G[cur], (const float *)b.Pv[cur], S, st);
+    cudaError_t e = pl.kind == SFG_FP64
+                        ? launch_gather64(c, (const double *)b.G[cur], S, st)
+                        : launch_gather2(c, P.na, {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, S, st);
     if (e != cudaSuccess) return -1;
     launches++;
     return launches;
@@ -446,24 +535,37 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
 {
     const int N = ctx->N, S = pl.S, R = run->rec_num, rows = run->step - 2;
     const size_t esz = pl.kind == SFG_FP64 ? sizeof(double) : sizeof(float);
-    const bool f64 = pl.kind == SFG_FP64;
-    b.gbytes = (size_t)N * (f64 ? GREC : G32) * S * esz;
-    b.pbytes = (size_t)N * (f64 ? PREC : P32) * S * esz;
+    b.gbytes = (size_t)N * GREC * S * esz;
+    b.pbytes = (size_t)N * PREC * S * esz;
+    const int na = ctx->P.na, nz = N - na;
+    b.gc_bytes = (size_t)N * GC * S * sizeof(float);
+    b.pa_bytes = (size_t)std::max(na, 1) * PA * S * sizeof(float);
+    b.gs_bytes = (size_t)std::max(nz, 1) * GS * S * sizeof(float);
     cudaStream_t st = ctx->stream;
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         CK(cudaMalloc(&b.pst, sizeof(float) * 36 * (size_t)N));
         CK(cudaMalloc(&b.peq, sizeof(float) * 22 * (size_t)N));
         CK(cudaMalloc(&b.prhs, sizeof(float) * 14 * (size_t)N));
         CK(cudaMalloc(&b.panew, sizeof(float) * 6 * (size_t)N));
-    } else {
+    } else if (pl.kind == SFG_FP64) {
         for (int k = 0; k < 2; k++) {
             CK(cudaMalloc(&b.G[k], b.gbytes));
             CK(cudaMalloc(&b.Pv[k], b.pbytes));
         }
+    } else {
+        for (int k = 0; k < 2; k++) {
+            CK(cudaMalloc(&b.Gc[k], b.gc_bytes));
+            CK(cudaMalloc(&b.Pa[k], b.pa_bytes));
+            CK(cudaMalloc(&b.Gs[k], b.gs_bytes));
+            CK(cudaMalloc(&b.Ps[k], b.gs_bytes));
+        }
     }
     CK(cudaMalloc(&b.src, sizeof(int) * S));
     CK(cudaMalloc(&b.rec, sizeof(int) * std::max(R, 1)));
-    if (R) CK(cudaMemcpyAsync(b.rec, run->rec_node, sizeof(int) * R, cudaMemcpyHostToDevice, st));
+    std::vector<int> rec(run->rec_node, run->rec_node + R);
+    if (permuted(pl))
+        for (int &r : rec) r = ctx->P.h_inv[r];
+    if (R) CK(cudaMemcpy(b.rec, rec.data(), sizeof(int) * R, cudaMemcpyHostToDevice));
     std::vector<double> amp(run->step, 0.0);
     for (int it = 0; it < run->step; it++) amp[it] = ricker(run->f0, run->t0, 1.0e10, (it + 1) * run->dt);
     CK(upload(&b.amp, amp.data(), amp.size(), st));
@@ -487,8 +589,12 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         z(b.pst, sizeof(float) * 36 * (size_t)N);
         z(b.panew, sizeof(float) * 6 * (size_t)N);
-    } else {
+    } else if (pl.kind == SFG_FP64) {
         for (int k = 0; k < 2; k++) { z(b.G[k], b.gbytes); z(b.Pv[k], b.pbytes); }
+    } else {
+        for (int k = 0; k < 2; k++) {
+            z(b.Gc[k], b.gc_bytes); z(b.Pa[k], b.pa_bytes); z(b.Gs[k], b.gs_bytes); z(b.Ps[k], b.gs_bytes);
+        }
     }
     z(b.energy, sizeof(double) * (size_t)S * step * 2);
     if (nsnap > 0) {
@@ -508,14 +614,14 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     std::vector<int> cand;
     if (pl.S == 1) {
         slot = kahan ? &ctx->tune.threads_fp32k : &ctx->tune.threads_fp32;
-        cand = {64, 128, 256};
+        for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
     } else {
         int si = pl.spl == 1 ? 0 : (pl.spl == 2 ? 1 : 2);
         slot = &ctx->tune.warps_b[si][kahan ? 1 : 0];
         cand = {2, 4, 8};
     }
-    if (*slot > 0) {
-        if (pl.S == 1) pl.threads = *slot; else pl.warps = *slot;
+    if (*slot > 0) {   // cached choice, stored + 1
+        if (pl.S == 1) pl.threads = *slot - 1; else pl.warps = *slot - 1;
         return SFG_OK;
     }
     cudaStream_t st = ctx->stream;
@@ -541,7 +647,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    *slot = pick;
+    *slot = pick + 1;
     if (pl.S == 1) pl.threads = pick; else pl.warps = pick;
     return SFG_OK;
 }
@@ -634,7 +740,8 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     p->nbatch = (run->src_num + pl.S - 1) / pl.S;
     if ((rc = alloc_bufs(ctx, pl, &p->run, p->nsnap, p->b)) != SFG_OK) { plan_free(p); return rc; }
     std::vector<int> staged((size_t)p->nbatch * pl.S, -1);
-    for (int s = 0; s < run->src_num; s++) staged[s] = run->src_node[s];
+    for (int s = 0; s < run->src_num; s++)
+        staged[s] = permuted(pl) ? ctx->P.h_inv[run->src_node[s]] : run->src_node[s];
     cudaStream_t st = ctx->stream;
     cudaError_t e = upload(&p->d_src_all, staged.data(), staged.size(), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->b.src, p->d_src_all, sizeof(int) * pl.S, cudaMemcpyDeviceToDevice, st);

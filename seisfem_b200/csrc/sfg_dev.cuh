@@ -1,0 +1,33 @@
+// sfg_dev.cuh -- small device helpers shared by the step kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sfg {
+
+// Block-wide sum of (a, b) into dst[0], dst[1] (one atomic pair per block).
+__device__ __forceinline__ void block_energy(double *dst, double a, double b)
+{
+    __shared__ double sa[32], sb[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sa[w] = a; sb[w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        a = l < nw ? sa[l] : 0.0;
+        b = l < nw ? sb[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0 && dst) { atomicAdd(dst, a); atomicAdd(dst + 1, b); }
+    }
+}
+
+}  // namespace sfg

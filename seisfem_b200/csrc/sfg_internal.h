@@ -51,12 +51,21 @@ struct DevProblem {
     double *mpml = nullptr;          // [6][N]: dx, dy, dxx, dyy, dxx_pyx, dyy_pxy
     double *coef64 = nullptr;        // [4][N] c11, c13, c33, c44
     unsigned char *dirichlet = nullptr;  // [N]
-    // FP32 step data
-    float *sell = nullptr;           // SELL-32 slots: [slots][8][32], plane 0 = column (int bits)
-    int *slice_ptr = nullptr;        // [slices + 1]
-    long long sell_slots = 0;
-    float *rec32 = nullptr;          // row-major union records [union_nnz][8] (col bits + 7 values)
-    float *coef32 = nullptr;         // [N][12]
+    // FP32 fused step data, in the two-class numbering of sfg_step32.cuh:
+    // row r' is mesh node perm[r'], node i is row inv[i]; rows [0, na) are
+    // class A (interior), [na, N) class Z (split zone)
+    float *coef32 = nullptr;         // [N][12], mesh order (unfused path)
+    int *perm = nullptr, *inv = nullptr;
+    std::vector<int> h_inv, h_perm;
+    int na = 0;
+    float *sellA = nullptr, *sellZ = nullptr;   // SELL-32 slots (6 / 8 planes of 32)
+    int *sliceA = nullptr, *sliceZ = nullptr;
+    long long slotsA = 0, slotsZ = 0;
+    int *upp = nullptr;              // permuted union row pointers
+    float *recp = nullptr;           // permuted row-major records [union_nnz][8]
+    float4 *coefA = nullptr;         // [na]
+    float *imA = nullptr;            // [na]
+    float *coefZ = nullptr;          // [N - na][12]
     double *coefd = nullptr;         // [N][12] FP64 coefficients for the FP64 step
 };
 

@@ -15,406 +15,13 @@
 #include <algorithm>
 
 #include "sfg_internal.h"
+#include "sfg_dev.cuh"
 #include "sfg_step.cuh"
 
 namespace sfg {
 
 namespace {
 
-__device__ __forceinline__ float ldgf(const float *p) { return __ldg(p); }
-
-// Block-wide sum of (a, b) into dst[0], dst[1] (one atomic pair per block).
-__device__ __forceinline__ void block_energy(double *dst, double a, double b)
-{
-    __shared__ double sa[32], sb[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { sa[w] = a; sb[w] = b; }
-    __syncthreads();
-    if (w == 0) {
-        int nw = (blockDim.x + 31) >> 5;
-        a = l < nw ? sa[l] : 0.0;
-        b = l < nw ? sb[l] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-        }
-        if (l == 0 && dst) { atomicAdd(dst, a); atomicAdd(dst + 1, b); }
-    }
-}
-
-// Receiver gather of a finished FP32 state into seismogram row `row`
-// (elastic_wave.c:787-795): displacement = sum over the three split fields
-// of (high + low FP32 part), formed in FP64.
-__device__ __forceinline__ void gather_one32(const StepCommon &c, const float *G, const float *P, int S,
-                                             int t, int row)
-{
-    if (row < 0 || t >= c.nrec * S) return;
-    int s = t / c.nrec, r = t - s * c.nrec;
-    long long node = c.rec[r];
-    double u = 0.0, w = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        u += (double)G[(node * G32 + 10 + k) * S + s] + (double)P[(node * P32 + 4 + k) * S + s];
-        w += (double)G[(node * G32 + 13 + k) * S + s] + (double)P[(node * P32 + 7 + k) * S + s];
-    }
-    size_t o = ((size_t)s * c.seis_rows + row) * c.nrec + r;
-    c.seis_u[o] = u;
-    c.seis_w[o] = w;
-}
-
-// ------------------------------------------------ FP32 single-shot kernel
-
-template <typename T>
-struct RhsT {
-    T a[6];          // accelerations of U1 U2 U3 W1 W2 W3
-    T lx[4], ly[4];  // new memory variables
-};
-
-// Right-hand sides (elastic_wave.c:585-591, 651-657) times 1/m_lump
-// (:709-722), evaluated in T (FP64 for the compensated path) from the FP32
-// products: kU[k], kW[k] = K_{k+1} times U, W; m[0..19] = M times U1..W3,
-// V1..V6, Lx1..4, Ly1..4.
-template <typename T>
-__device__ __forceinline__ void rhs_eval(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
-                                         float4 c2, T dt, T src_u, T src_w, RhsT<T> &o)
-{
-    const T c11 = c0.x, c13 = c0.y, c33 = c0.z, c44 = c0.w;
-    const T dx = c1.x, dy = c1.y, dxx = c1.z, dyy = c1.w;
-    const T im = c2.x, dxxp = c2.y, dyyp = c2.z;
-    const T kx = T(1) - dt * dx, ky = T(1) - dt * dy;
-    auto K = [&](const float *v, int k) { return T(v[k]); };
-    auto Mv = [&](int k) { return T(m[k]); };
-    o.a[0] = im * (-c11 * K(kU, 0) - T(2) * dx * Mv(6) - dx * dx * Mv(0) + Mv(12) + Mv(13) + src_u);
-    o.a[1] = im * (-c13 * K(kW, 2) - c44 * K(kW, 3) - (dx + dy) * Mv(7) - dx * dy * Mv(1));
-    o.a[2] = im * (-c44 * K(kU, 1) - T(2) * dy * Mv(8) - dy * dy * Mv(2) + Mv(14) + Mv(15));
-    o.lx[0] = im * (-dt * c11 * dxx * K(kU, 4) + kx * Mv(12));
-    o.lx[1] = im * (-dt * c44 * dyyp * K(kW, 4) + ky * Mv(13));
-    o.lx[2] = im * (-dt * c13 * dxxp * K(kW, 5) + kx * Mv(14));
-    o.lx[3] = im * (-dt * c44 * dyy * K(kU, 5) + ky * Mv(15));
-    o.a[3] = im * (-c44 * K(kW, 0) - T(2) * dx * Mv(9) - dx * dx * Mv(3) + Mv(16) + Mv(17) + src_w);
-    o.a[4] = im * (-c44 * K(kU, 2) - c13 * K(kU, 3) - (dx + dy) * Mv(10) - dx * dy * Mv(4));
-    o.a[5] = im * (-c33 * K(kW, 1) - T(2) * dy * Mv(11) - dy * dy * Mv(5) + Mv(18) + Mv(19));
-    o.ly[0] = im * (-dt * c44 * dxx * K(kW, 4) + kx * Mv(16));
-    o.ly[1] = im * (-dt * c13 * dyyp * K(kU, 4) + ky * Mv(17));
-    o.ly[2] = im * (-dt * c44 * dxxp * K(kU, 5) + kx * Mv(18));
-    o.ly[3] = im * (-dt * c33 * dyy * K(kW, 5) + ky * Mv(19));
-}
-
-// Newmark, alpha = 1, delta = 1.5 (elastic_wave.c:97, 757-768), for one split
-// field.  Compensated: the displacement is carried as an FP32 pair hi + lo,
-// updated in FP64 and split again, so the running sum keeps ~48 bits.
-__device__ __forceinline__ double newmark_comp(float &hi, float &lo, float &V, float &A, double an, double dt)
-{
-    const double Ad = A, Vd = V;
-    const double U = ((double)hi + (double)lo) + Vd * dt + (an - 0.5 * Ad) * (dt * dt);
-    hi = (float)U;
-    lo = (float)(U - (double)hi);
-    V = (float)(Vd + (1.5 * an - 0.5 * Ad) * dt);
-    A = (float)an;
-    return U;
-}
-
-__device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, float an, float dt)
-{
-    U = U + V * dt + (an - 0.5f * A) * (dt * dt);
-    V = V + (1.5f * an - 0.5f * A) * dt;
-    A = an;
-    return U;
-}
-
-// Finish one node: right-hand sides, lumped solve, Newmark, new records.
-// g[24] / p[10] are the node's own records (layout in sfg_step.cuh).
-template <bool COMP>
-__device__ __forceinline__ void finish_node(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
-                                            float4 c2, double dt, double src_u, double src_w, const float *g,
-                                            const float *p, float *go, float *po, double &uu, double &ww)
-{
-    float hi[6] = {g[10], g[11], g[12], g[13], g[14], g[15]};
-    float V[6] = {g[16], g[17], g[18], g[19], g[20], g[21]};
-    float A[6] = {g[22], g[23], p[0], p[1], p[2], p[3]};
-    float lo[6] = {p[4], p[5], p[6], p[7], p[8], p[9]};
-    float Lx[4], Ly[4];
-    double Ut[6];
-    if (COMP) {
-        RhsT<double> r;
-        rhs_eval<double>(kU, kW, m, c0, c1, c2, dt, src_u, src_w, r);
-#pragma unroll
-        for (int k = 0; k < 6; k++) Ut[k] = newmark_comp(hi[k], lo[k], V[k], A[k], r.a[k], dt);
-#pragma unroll
-        for (int k = 0; k < 4; k++) { Lx[k] = (float)r.lx[k]; Ly[k] = (float)r.ly[k]; }
-    } else {
-        RhsT<float> r;
-        rhs_eval<float>(kU, kW, m, c0, c1, c2, (float)dt, (float)src_u, (float)src_w, r);
-#pragma unroll
-        for (int k = 0; k < 6; k++) Ut[k] = newmark_plain(hi[k], V[k], A[k], r.a[k], (float)dt);
-#pragma unroll
-        for (int k = 0; k < 4; k++) { Lx[k] = r.lx[k]; Ly[k] = r.ly[k]; }
-    }
-    uu = (Ut[0] + Ut[1]) + Ut[2];
-    ww = (Ut[3] + Ut[4]) + Ut[5];
-    go[0] = (float)uu; go[1] = (float)ww;
-#pragma unroll
-    for (int k = 0; k < 4; k++) { go[2 + k] = Lx[k]; go[6 + k] = Ly[k]; }
-#pragma unroll
-    for (int k = 0; k < 6; k++) { go[10 + k] = hi[k]; go[16 + k] = V[k]; }
-    go[22] = A[0]; go[23] = A[1];
-    po[0] = A[2]; po[1] = A[3]; po[2] = A[4]; po[3] = A[5];
-#pragma unroll
-    for (int k = 0; k < 6; k++) po[4 + k] = COMP ? lo[k] : 0.f;
-}
-
-__device__ __forceinline__ bool is_pml_row(float4 c1)
-{
-    return c1.x != 0.f || c1.y != 0.f || c1.z != 0.f || c1.w != 0.f;
-}
-
-// One thread per row over SELL-32 slices.  Rows outside the M-PML (their
-// dx, dy, dxx, dyy are 0) multiply every M*V, M*U_k, K5 and K6 product by 0,
-// so a warp whose rows are all interior streams only the column, M and
-// K1..K4 planes and gathers only U, W, Lx, Ly (the first 10 record values).
-template <bool COMP>
-__global__ void __launch_bounds__(256) step32_kernel(const Step32 a)
-{
-    const StepCommon &c = a.c;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    gather_one32(c, a.Gin, a.Pin, 1, i, c.seis_row);
-    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
-    if (i < c.n) {
-        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
-        c0 = __ldg(cf); c1 = __ldg(cf + 1); c2 = __ldg(cf + 2);
-    }
-    const bool full = __any_sync(0xffffffffu, i < c.n && is_pml_row(c1));
-    double eu = 0.0, ew = 0.0;
-    if (i < c.n) {
-        const int lane = i & 31, slice = i >> 5;
-        float kU[6], kW[6], m[20];
-#pragma unroll
-        for (int k = 0; k < 6; k++) { kU[k] = 0.f; kW[k] = 0.f; }
-#pragma unroll
-        for (int k = 0; k < 20; k++) m[k] = 0.f;
-        const int s0 = __ldg(a.slice_ptr + slice), s1 = __ldg(a.slice_ptr + slice + 1);
-        const float *sd = a.sell + (size_t)s0 * 256 + lane;
-        if (full) {
-#pragma unroll 2
-            for (int g = s0; g < s1; ++g, sd += 256) {
-                const int j = __float_as_int(ldgf(sd));
-                const float vm = ldgf(sd + 32);
-                float kv[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) kv[k] = ldgf(sd + 64 + 32 * k);
-                const float4 *gj = reinterpret_cast<const float4 *>(a.Gin + (size_t)j * G32);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2), q3 = __ldg(gj + 3),
-                             q4 = __ldg(gj + 4);
-                const float2 q5 = __ldg(reinterpret_cast<const float2 *>(gj + 5));
-#pragma unroll
-                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
-                m[0] += vm * q2.z;  m[1] += vm * q2.w;  m[2] += vm * q3.x;  m[3] += vm * q3.y;
-                m[4] += vm * q3.z;  m[5] += vm * q3.w;  m[6] += vm * q4.x;  m[7] += vm * q4.y;
-                m[8] += vm * q4.z;  m[9] += vm * q4.w;  m[10] += vm * q5.x; m[11] += vm * q5.y;
-                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
-                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
-            }
-        } else {
-#pragma unroll 2
-            for (int g = s0; g < s1; ++g, sd += 256) {
-                const int j = __float_as_int(ldgf(sd));
-                const float vm = ldgf(sd + 32);
-                float kv[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
-                const float4 *gj = reinterpret_cast<const float4 *>(a.Gin + (size_t)j * G32);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
-                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
-#pragma unroll
-                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
-                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
-                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
-            }
-        }
-        double src_u = 0.0, src_w = 0.0;
-        if (i == c.src[0]) {
-            const double ps = c.amp[c.it];
-            src_u = ps * c.sin_af;
-            src_w = ps * c.cos_af;
-        }
-        float g[G32], p[P32], go[G32], po[P32];
-        const float4 *gi = reinterpret_cast<const float4 *>(a.Gin + (size_t)i * G32);
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            const float4 v = __ldg(gi + k);
-            g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
-        }
-        const float2 *pi = reinterpret_cast<const float2 *>(a.Pin + (size_t)i * P32);
-#pragma unroll
-        for (int k = 0; k < 5; k++) { const float2 v = __ldg(pi + k); p[2 * k] = v.x; p[2 * k + 1] = v.y; }
-        double uu, ww;
-        finish_node<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, g, p, go, po, uu, ww);
-        float4 *gout = reinterpret_cast<float4 *>(a.Gout + (size_t)i * G32);
-#pragma unroll
-        for (int k = 0; k < 6; k++) gout[k] = make_float4(go[4 * k], go[4 * k + 1], go[4 * k + 2], go[4 * k + 3]);
-        float2 *pout = reinterpret_cast<float2 *>(a.Pout + (size_t)i * P32);
-#pragma unroll
-        for (int k = 0; k < 5; k++) pout[k] = make_float2(po[2 * k], po[2 * k + 1]);
-        eu = uu * uu;
-        ew = ww * ww;
-    }
-    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
-}
-
-// ------------------------------------------------ FP32 batched kernel
-
-template <int SPL>
-struct VecF;
-template <> struct VecF<1> {
-    float v[1];
-    __device__ __forceinline__ void load(const float *p) { v[0] = __ldg(p); }
-    __device__ __forceinline__ void store(float *p) const { p[0] = v[0]; }
-};
-template <> struct VecF<2> {
-    float v[2];
-    __device__ __forceinline__ void load(const float *p) { float2 t = __ldg(reinterpret_cast<const float2 *>(p)); v[0] = t.x; v[1] = t.y; }
-    __device__ __forceinline__ void store(float *p) const { *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]); }
-};
-template <> struct VecF<4> {
-    float v[4];
-    __device__ __forceinline__ void load(const float *p) { float4 t = __ldg(reinterpret_cast<const float4 *>(p)); v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w; }
-    __device__ __forceinline__ void store(float *p) const { *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]); }
-};
-
-// One warp per row, S = 32*SPL shots with the shot index innermost: each
-// matrix entry is read once (a warp-uniform 32-byte record) and applied to
-// all S shots; each lane gathers SPL consecutive shots of a neighbour's
-// record with one vector load per value.  Interior rows (row-uniform
-// decision) gather only U, W, Lx, Ly.
-template <bool COMP, int SPL>
-__global__ void __launch_bounds__(256) step32_batched_kernel(const Step32 a)
-{
-    constexpr int S = 32 * SPL;
-    const StepCommon &c = a.c;
-    const int lane = threadIdx.x & 31;
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather_one32(c, a.Gin, a.Pin, S, t, c.seis_row);
-    const int warps_total = (gridDim.x * blockDim.x) >> 5;
-    const int s_base = lane * SPL;
-    int src[SPL];
-#pragma unroll
-    for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
-    const double ps = c.amp[c.it];
-    const double src_u = ps * c.sin_af, src_w = ps * c.cos_af;
-    float eu[SPL], ew[SPL];
-#pragma unroll
-    for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
-    for (int i = gtid >> 5; i < c.n; i += warps_total) {
-        const float4 *cf = reinterpret_cast<const float4 *>(a.coef) + (size_t)i * 3;
-        const float4 c0 = __ldg(cf), c1 = __ldg(cf + 1), c2 = __ldg(cf + 2);
-        const bool full = is_pml_row(c1);
-        float kU[6][SPL], kW[6][SPL], m[20][SPL];
-#pragma unroll
-        for (int k = 0; k < 6; k++)
-#pragma unroll
-            for (int q = 0; q < SPL; q++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
-#pragma unroll
-        for (int k = 0; k < 20; k++)
-#pragma unroll
-            for (int q = 0; q < SPL; q++) m[k][q] = 0.f;
-        const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
-        const float4 *rec = reinterpret_cast<const float4 *>(a.rec32);
-        if (full) {
-            for (int e = e0; e < e1; e++) {
-                const float4 r0 = __ldg(rec + 2 * (size_t)e), r1 = __ldg(rec + 2 * (size_t)e + 1);
-                const int j = __float_as_int(r0.x);
-                const float vm = r0.y;
-                const float kv[6] = {r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-                const float *gj = a.Gin + (size_t)j * G32 * S + s_base;
-                VecF<SPL> x[22];
-#pragma unroll
-                for (int v = 0; v < 22; v++) x[v].load(gj + v * S);
-#pragma unroll
-                for (int q = 0; q < SPL; q++) {
-#pragma unroll
-                    for (int k = 0; k < 6; k++) { kU[k][q] += kv[k] * x[0].v[q]; kW[k][q] += kv[k] * x[1].v[q]; }
-#pragma unroll
-                    for (int v = 0; v < 8; v++) m[12 + v][q] += vm * x[2 + v].v[q];
-#pragma unroll
-                    for (int v = 0; v < 12; v++) m[v][q] += vm * x[10 + v].v[q];
-                }
-            }
-        } else {
-            for (int e = e0; e < e1; e++) {
-                const float4 r0 = __ldg(rec + 2 * (size_t)e), r1 = __ldg(rec + 2 * (size_t)e + 1);
-                const int j = __float_as_int(r0.x);
-                const float vm = r0.y;
-                const float kv[4] = {r0.z, r0.w, r1.x, r1.y};
-                const float *gj = a.Gin + (size_t)j * G32 * S + s_base;
-                VecF<SPL> x[10];
-#pragma unroll
-                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
-#pragma unroll
-                for (int q = 0; q < SPL; q++) {
-#pragma unroll
-                    for (int k = 0; k < 4; k++) { kU[k][q] += kv[k] * x[0].v[q]; kW[k][q] += kv[k] * x[1].v[q]; }
-#pragma unroll
-                    for (int v = 0; v < 8; v++) m[12 + v][q] += vm * x[2 + v].v[q];
-                }
-            }
-        }
-        const float *gi = a.Gin + (size_t)i * G32 * S + s_base;
-        const float *pi = a.Pin + (size_t)i * P32 * S + s_base;
-        float *gop = a.Gout + (size_t)i * G32 * S + s_base;
-        float *pop = a.Pout + (size_t)i * P32 * S + s_base;
-        VecF<SPL> gv[G32], pv[P32];
-#pragma unroll
-        for (int v = 0; v < G32; v++) gv[v].load(gi + v * S);
-#pragma unroll
-        for (int v = 0; v < P32; v++) pv[v].load(pi + v * S);
-#pragma unroll
-        for (int q = 0; q < SPL; q++) {
-            float kUq[6], kWq[6], mq[20], g[G32], p[P32], go[G32], po[P32];
-#pragma unroll
-            for (int k = 0; k < 6; k++) { kUq[k] = kU[k][q]; kWq[k] = kW[k][q]; }
-#pragma unroll
-            for (int v = 0; v < 20; v++) mq[v] = m[v][q];
-#pragma unroll
-            for (int v = 0; v < G32; v++) g[v] = gv[v].v[q];
-#pragma unroll
-            for (int v = 0; v < P32; v++) p[v] = pv[v].v[q];
-            const bool is_src = (i == src[q]);
-            double uu, ww;
-            finish_node<COMP>(kUq, kWq, mq, c0, c1, c2, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, go,
-                              po, uu, ww);
-#pragma unroll
-            for (int v = 0; v < G32; v++) gv[v].v[q] = go[v];
-#pragma unroll
-            for (int v = 0; v < P32; v++) pv[v].v[q] = po[v];
-            eu[q] += (float)(uu * uu);
-            ew[q] += (float)(ww * ww);
-        }
-#pragma unroll
-        for (int v = 0; v < G32; v++) gv[v].store(gop + v * S);
-#pragma unroll
-        for (int v = 0; v < P32; v++) pv[v].store(pop + v * S);
-    }
-    // energy per shot: block reduction over warps, one atomic pair per shot
-    if (c.energy) {
-        __shared__ float se[8][2][32 * SPL];
-        const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-        for (int q = 0; q < SPL; q++) { se[w][0][s_base + q] = eu[q]; se[w][1][s_base + q] = ew[q]; }
-        __syncthreads();
-        for (int t = threadIdx.x; t < 2 * S; t += blockDim.x) {
-            int comp = t / S, s = t - comp * S;
-            double acc = 0.0;
-            for (int k = 0; k < nw; k++) acc += se[k][comp][s];
-            if (s < c.nshot) atomicAdd(c.energy + ((size_t)s * c.nsteps + c.it) * 2 + comp, acc);
-        }
-    }
-}
 
 // ------------------------------------------------------- FP64 kernel
 
@@ -517,12 +124,6 @@ __global__ void __launch_bounds__(128) step64_kernel(const Step64 a)
 
 // ------------------------------------------------ gathers, snapshots
 
-__global__ void gather32_kernel(const StepCommon c, const float *G, const float *P, int S)
-{
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    gather_one32(c, G, P, S, t, c.seis_row);
-}
-
 __global__ void gather64_kernel(const StepCommon c, const double *G)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -532,22 +133,6 @@ __global__ void gather64_kernel(const StepCommon c, const double *G)
     size_t o = (size_t)c.seis_row * c.nrec + i;
     c.seis_u[o] = __dadd_rn(__dadd_rn(g[0], g[1]), g[2]);
     c.seis_w[o] = __dadd_rn(__dadd_rn(g[3], g[4]), g[5]);
-}
-
-__global__ void snapshot32_kernel(const float *G, const float *P, int n, int S, double *su, double *sw,
-                                  long long shot_stride)
-{
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n * S) return;
-    int s = (int)(t % S);
-    long long node = t / S;
-    double u = 0.0, w = 0.0;
-    for (int k = 0; k < 3; k++) {
-        u += (double)G[(node * G32 + 10 + k) * S + s] + (double)P[(node * P32 + 4 + k) * S + s];
-        w += (double)G[(node * G32 + 13 + k) * S + s] + (double)P[(node * P32 + 7 + k) * S + s];
-    }
-    su[s * shot_stride + node] = u;
-    sw[s * shot_stride + node] = w;
 }
 
 __global__ void snapshot64_kernel(const double *G, int n, double *su, double *sw)
@@ -660,49 +245,14 @@ __global__ void plain_gather_kernel(const Plain32 a)
 
 // ------------------------------------------------ step data builders
 
-__global__ void slice_len_kernel(int n, const int *__restrict__ up, int *len)
+__global__ void permute_rows_kernel(int n, int width, const float *__restrict__ src, const int *__restrict__ perm,
+                                    float *__restrict__ dst)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    int nsl = (n + 31) / 32;
-    if (s >= nsl) return;
-    int m = 0;
-    for (int l = 0; l < 32; l++) {
-        int r = s * 32 + l;
-        if (r < n) m = max(m, up[r + 1] - up[r]);
-    }
-    len[s] = m;
-}
-
-__global__ void sell_fill_kernel(int n, const int *__restrict__ up, const int *__restrict__ uj,
-                                 const double *__restrict__ ux, long long nnz, const int *__restrict__ sp,
-                                 float *__restrict__ sell)
-{
-    int s = blockIdx.x;
-    int lane = threadIdx.x;
-    int r = s * 32 + lane;
-    int s0 = sp[s], s1 = sp[s + 1];
-    int a0 = r < n ? up[r] : 0, len = r < n ? up[r + 1] - a0 : 0;
-    for (int k = 0; k < s1 - s0; k++) {
-        float *slot = sell + (size_t)(s0 + k) * 256;
-        if (k < len) {
-            long long e = a0 + k;
-            slot[lane] = __int_as_float(uj[e]);
-            for (int m = 0; m < 7; m++) slot[32 * (m + 1) + lane] = (float)ux[m * nnz + e];
-        } else {
-            // padding: the row itself with zero weights (a valid, cached address)
-            slot[lane] = __int_as_float(r < n ? r : 0);
-            for (int m = 0; m < 7; m++) slot[32 * (m + 1) + lane] = 0.f;
-        }
-    }
-}
-
-__global__ void rec_fill_kernel(long long nnz, const int *__restrict__ uj, const double *__restrict__ ux,
-                                float *__restrict__ rec)
-{
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nnz) return;
-    rec[e * 8] = __int_as_float(uj[e]);
-    for (int m = 0; m < 7; m++) rec[e * 8 + 1 + m] = (float)ux[m * nnz + e];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * width) return;
+    long long r = t / width;
+    int k = (int)(t - r * width);
+    dst[t] = src[(long long)perm[r] * width + k];
 }
 
 __global__ void coef_kernel(int n, const double *__restrict__ c, const double *__restrict__ mp,
@@ -729,14 +279,6 @@ __global__ void coef_kernel(int n, const double *__restrict__ c, const double *_
 
 // ---------------------------------------------------------- launchers
 
-cudaError_t launch_step32(const Step32 &a, bool kahan, int threads, cudaStream_t st)
-{
-    int blocks = (a.c.n + threads - 1) / threads;
-    if (kahan) step32_kernel<true><<<blocks, threads, 0, st>>>(a);
-    else step32_kernel<false><<<blocks, threads, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_step64(const Step64 &a, int threads, cudaStream_t st)
 {
     int blocks = (a.c.n + threads - 1) / threads;
@@ -744,52 +286,10 @@ cudaError_t launch_step64(const Step64 &a, int threads, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_step32_batched(const Step32 &a, bool kahan, int spl, int warps, cudaStream_t st)
-{
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int threads = 32 * warps;
-    int per_sm = 0;
-    if (kahan) {
-        if (spl == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<true, 1>, threads, 0);
-        else if (spl == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<true, 2>, threads, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<true, 4>, threads, 0);
-    } else {
-        if (spl == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<false, 1>, threads, 0);
-        else if (spl == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<false, 2>, threads, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step32_batched_kernel<false, 4>, threads, 0);
-    }
-    if (per_sm < 1) per_sm = 1;
-    long long need = ((long long)a.c.n + warps - 1) / warps;
-    long long blocks = std::min<long long>((long long)sms * per_sm, need);
-    if (blocks < 1) blocks = 1;
-#define SFG_BATCH(K, P) step32_batched_kernel<K, P><<<(unsigned)blocks, threads, 0, st>>>(a)
-    if (kahan) { if (spl == 1) SFG_BATCH(true, 1); else if (spl == 2) SFG_BATCH(true, 2); else SFG_BATCH(true, 4); }
-    else { if (spl == 1) SFG_BATCH(false, 1); else if (spl == 2) SFG_BATCH(false, 2); else SFG_BATCH(false, 4); }
-#undef SFG_BATCH
-    return cudaGetLastError();
-}
-
-cudaError_t launch_gather32(const StepCommon &c, const float *G, const float *P, int S, cudaStream_t st)
-{
-    int tot = c.nrec * S;
-    if (tot > 0 && c.seis_row >= 0) gather32_kernel<<<(tot + 127) / 128, 128, 0, st>>>(c, G, P, S);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_gather64(const StepCommon &c, const double *G, int S, cudaStream_t st)
 {
     (void)S;
     if (c.nrec > 0 && c.seis_row >= 0) gather64_kernel<<<(c.nrec + 127) / 128, 128, 0, st>>>(c, G);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_snapshot32(const float *G, const float *P, int n, int S, double *su, double *sw,
-                              long long shot_stride, cudaStream_t st)
-{
-    long long tot = (long long)n * S;
-    snapshot32_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(G, P, n, S, su, sw, shot_stride);
     return cudaGetLastError();
 }
 
@@ -859,35 +359,12 @@ cudaError_t launch_plain_gather(const Plain32 &a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t build_sell32(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
-                         float **d_sell, int **d_slice_ptr, long long *slots, cudaStream_t st)
+cudaError_t permute_rows(int n, int width, const float *d_src, const int *d_perm, float **d_dst, cudaStream_t st)
 {
-    int nsl = (n + 31) / 32;
-    int *len = nullptr;
-    cudaError_t e;
-    if ((e = cudaMalloc(&len, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_slice_ptr, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
-    slice_len_kernel<<<(nsl + 127) / 128, 128, 0, st>>>(n, d_up, len);
-    if ((e = exclusive_scan_int(len, *d_slice_ptr, nsl, st)) != cudaSuccess) return e;
-    int tot = 0;
-    cudaMemcpyAsync(&tot, *d_slice_ptr + nsl, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    *slots = tot;
-    if ((e = cudaMalloc(d_sell, sizeof(float) * 256 * std::max<size_t>(tot, 1))) != cudaSuccess) return e;
-    if (nsl) sell_fill_kernel<<<nsl, 32, 0, st>>>(n, d_up, d_uj, d_ux, nnz, *d_slice_ptr, *d_sell);
-    e = cudaGetLastError();
-    cudaStreamSynchronize(st);
-    cudaFree(len);
-    return e;
-}
-
-cudaError_t build_rec32(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
-                        float **d_rec, cudaStream_t st)
-{
-    (void)n; (void)d_up;
-    cudaError_t e = cudaMalloc(d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1));
+    cudaError_t e = cudaMalloc(d_dst, sizeof(float) * width * std::max(n, 1));
     if (e != cudaSuccess) return e;
-    if (nnz) rec_fill_kernel<<<(unsigned)((nnz + 255) / 256), 256, 0, st>>>(nnz, d_uj, d_ux, *d_rec);
+    long long tot = (long long)n * width;
+    if (tot) permute_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, width, d_src, d_perm, *d_dst);
     return cudaGetLastError();
 }
 

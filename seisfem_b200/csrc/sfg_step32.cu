@@ -1,0 +1,836 @@
+// sfg_step32.cu -- fused FP32 time step (time_evolution/elastic_wave.c:519-809)
+// in the two-class layout described in sfg_step32.cuh.
+//
+// One launch per class and step: the class-A kernel (interior rows: totals
+// only, 16 products per row: K1..K4 times U and W, M times Lx1..4, Ly1..4)
+// and the class-Z kernel (split zone: all 32 products on M-PML rows) read the
+// step's input records and write the output records of their own rows, so
+// the two run concurrently.  Each streams its rows' SELL-32 slices once,
+// gathers each neighbour record once, keeps every product in registers and
+// finishes the node (right-hand sides elastic_wave.c:585-591 / 651-657,
+// lumped solve :709-722, Newmark :757-776) in the same thread.  The SpMV
+// products accumulate in FP32; the per-node epilogue runs in FP64 for the
+// compensated precision, with displacements kept as FP32 hi + lo pairs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "sfg_dev.cuh"
+#include "sfg_internal.h"
+#include "sfg_step32.cuh"
+
+namespace sfg {
+
+namespace {
+
+__device__ __forceinline__ float ldgf(const float *p) { return __ldg(p); }
+
+template <int SPL>
+struct VecF;
+template <> struct VecF<1> {
+    float v[1];
+    __device__ __forceinline__ void load(const float *p) { v[0] = __ldg(p); }
+    __device__ __forceinline__ void store(float *p) const { p[0] = v[0]; }
+};
+template <> struct VecF<2> {
+    float v[2];
+    __device__ __forceinline__ void load(const float *p) { float2 t = __ldg(reinterpret_cast<const float2 *>(p)); v[0] = t.x; v[1] = t.y; }
+    __device__ __forceinline__ void store(float *p) const { *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]); }
+};
+template <> struct VecF<4> {
+    float v[4];
+    __device__ __forceinline__ void load(const float *p) { float4 t = __ldg(reinterpret_cast<const float4 *>(p)); v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w; }
+    __device__ __forceinline__ void store(float *p) const { *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]); }
+};
+
+// --------------------------------------------------------------- epilogues
+
+// Newmark, alpha = 1, delta = 1.5 (elastic_wave.c:97, 757-768) for one
+// displacement carried as hi + lo, updated in FP64.
+__device__ __forceinline__ double newmark_comp(float &hi, float &lo, float &V, float &A, double an, double dt)
+{
+    const double Ad = A, Vd = V;
+    const double U = ((double)hi + (double)lo) + Vd * dt + (an - 0.5 * Ad) * (dt * dt);
+    hi = (float)U;
+    lo = (float)(U - (double)hi);
+    V = (float)(Vd + (1.5 * an - 0.5 * Ad) * dt);
+    A = (float)an;
+    return U;
+}
+
+__device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, float an, float dt)
+{
+    U = U + V * dt + (an - 0.5f * A) * (dt * dt);
+    V = V + (1.5f * an - 0.5f * A) * dt;
+    A = an;
+    return U;
+}
+
+// Class A: the summed right-hand sides of the three split fields with
+// dx = dy = dxx = dyy = 0:  a_u = (rhs_u1 + rhs_u2 + rhs_u3) / m,
+// a_w = (rhs_w1 + rhs_w2 + rhs_w3) / m, and L_k = (M L_k) / m.
+// kU, kW: K1..K4 times U, W; mL: M times Lx1..4, Ly1..4.
+// g[12]: own Gc record, p[4]: own Pa record, replaced by the new records.
+template <bool COMP>
+__device__ __forceinline__ void finish_A(const float *kU, const float *kW, const float *mL, float4 c, float im,
+                                         double dt, double src_u, double src_w, float *g, float *p, double &uu,
+                                         double &ww)
+{
+    float Uh = g[0], Wh = g[1], Vu = g[10], Vw = g[11];
+    float Au = p[0], Aw = p[1], lou = p[2], low = p[3];
+    if (COMP) {
+        const double c11 = c.x, c13 = c.y, c33 = c.z, c44 = c.w, m = im;
+        const double au = m * (-c11 * (double)kU[0] - c44 * (double)kU[1] - c13 * (double)kW[2] - c44 * (double)kW[3] +
+                               (((double)mL[0] + (double)mL[1]) + ((double)mL[2] + (double)mL[3])) + src_u);
+        const double aw = m * (-c44 * (double)kW[0] - c33 * (double)kW[1] - c44 * (double)kU[2] - c13 * (double)kU[3] +
+                               (((double)mL[4] + (double)mL[5]) + ((double)mL[6] + (double)mL[7])) + src_w);
+        uu = newmark_comp(Uh, lou, Vu, Au, au, dt);
+        ww = newmark_comp(Wh, low, Vw, Aw, aw, dt);
+    } else {
+        const float au = im * (-c.x * kU[0] - c.w * kU[1] - c.y * kW[2] - c.w * kW[3] +
+                               ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
+        const float aw = im * (-c.w * kW[0] - c.z * kW[1] - c.w * kU[2] - c.y * kU[3] +
+                               ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
+        uu = newmark_plain(Uh, Vu, Au, au, (float)dt);
+        ww = newmark_plain(Wh, Vw, Aw, aw, (float)dt);
+        lou = 0.f;
+        low = 0.f;
+    }
+    g[0] = Uh;
+    g[1] = Wh;
+#pragma unroll
+    for (int k = 0; k < 8; k++) g[2 + k] = im * mL[k];
+    g[10] = Vu;
+    g[11] = Vw;
+    p[0] = Au; p[1] = Aw; p[2] = lou; p[3] = low;
+}
+
+template <typename T>
+struct RhsT {
+    T a[6];          // accelerations of U1 U2 U3 W1 W2 W3
+    T lx[4], ly[4];  // new memory variables
+};
+
+// Split right-hand sides (elastic_wave.c:585-591, 651-657) times 1/m_lump,
+// from the FP32 products: kU[k], kW[k] = K_{k+1} times U, W; m[0..19] = M
+// times U1..W3, V1..V6, Lx1..4, Ly1..4.
+template <typename T>
+__device__ __forceinline__ void rhs_eval(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
+                                         float4 c2, T dt, T src_u, T src_w, RhsT<T> &o)
+{
+    const T c11 = c0.x, c13 = c0.y, c33 = c0.z, c44 = c0.w;
+    const T dx = c1.x, dy = c1.y, dxx = c1.z, dyy = c1.w;
+    const T im = c2.x, dxxp = c2.y, dyyp = c2.z;
+    const T kx = T(1) - dt * dx, ky = T(1) - dt * dy;
+    auto K = [&](const float *v, int k) { return T(v[k]); };
+    auto Mv = [&](int k) { return T(m[k]); };
+    o.a[0] = im * (-c11 * K(kU, 0) - T(2) * dx * Mv(6) - dx * dx * Mv(0) + Mv(12) + Mv(13) + src_u);
+    o.a[1] = im * (-c13 * K(kW, 2) - c44 * K(kW, 3) - (dx + dy) * Mv(7) - dx * dy * Mv(1));
+    o.a[2] = im * (-c44 * K(kU, 1) - T(2) * dy * Mv(8) - dy * dy * Mv(2) + Mv(14) + Mv(15));
+    o.lx[0] = im * (-dt * c11 * dxx * K(kU, 4) + kx * Mv(12));
+    o.lx[1] = im * (-dt * c44 * dyyp * K(kW, 4) + ky * Mv(13));
+    o.lx[2] = im * (-dt * c13 * dxxp * K(kW, 5) + kx * Mv(14));
+    o.lx[3] = im * (-dt * c44 * dyy * K(kU, 5) + ky * Mv(15));
+    o.a[3] = im * (-c44 * K(kW, 0) - T(2) * dx * Mv(9) - dx * dx * Mv(3) + Mv(16) + Mv(17) + src_w);
+    o.a[4] = im * (-c44 * K(kU, 2) - c13 * K(kU, 3) - (dx + dy) * Mv(10) - dx * dy * Mv(4));
+    o.a[5] = im * (-c33 * K(kW, 1) - T(2) * dy * Mv(11) - dy * dy * Mv(5) + Mv(18) + Mv(19));
+    o.ly[0] = im * (-dt * c44 * dxx * K(kW, 4) + kx * Mv(16));
+    o.ly[1] = im * (-dt * c13 * dyyp * K(kU, 4) + ky * Mv(17));
+    o.ly[2] = im * (-dt * c44 * dxxp * K(kU, 5) + kx * Mv(18));
+    o.ly[3] = im * (-dt * c33 * dyy * K(kW, 5) + ky * Mv(19));
+}
+
+// Class Z: split fields.  gs[12] / ps[12]: own Gs / Ps records (replaced);
+// gc[12] receives the new Gc record (totals, memory variables).
+template <bool COMP>
+__device__ __forceinline__ void finish_Z(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
+                                         float4 c2, double dt, double src_u, double src_w, float *gs, float *ps,
+                                         float *gc, double &uu, double &ww)
+{
+    double Ut[6];
+    float L[8];
+    if (COMP) {
+        RhsT<double> r;
+        rhs_eval<double>(kU, kW, m, c0, c1, c2, dt, src_u, src_w, r);
+#pragma unroll
+        for (int k = 0; k < 6; k++) Ut[k] = newmark_comp(gs[k], ps[6 + k], gs[6 + k], ps[k], r.a[k], dt);
+#pragma unroll
+        for (int k = 0; k < 4; k++) { L[k] = (float)r.lx[k]; L[4 + k] = (float)r.ly[k]; }
+    } else {
+        RhsT<float> r;
+        rhs_eval<float>(kU, kW, m, c0, c1, c2, (float)dt, (float)src_u, (float)src_w, r);
+#pragma unroll
+        for (int k = 0; k < 6; k++) { Ut[k] = newmark_plain(gs[k], gs[6 + k], ps[k], r.a[k], (float)dt); ps[6 + k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 4; k++) { L[k] = r.lx[k]; L[4 + k] = r.ly[k]; }
+    }
+    uu = (Ut[0] + Ut[1]) + Ut[2];
+    ww = (Ut[3] + Ut[4]) + Ut[5];
+    gc[0] = (float)uu;
+    gc[1] = (float)ww;
+#pragma unroll
+    for (int k = 0; k < 8; k++) gc[2 + k] = L[k];
+    gc[10] = 0.f;
+    gc[11] = 0.f;
+}
+
+__device__ __forceinline__ bool is_pml_row(float4 c1)
+{
+    return c1.x != 0.f || c1.y != 0.f || c1.z != 0.f || c1.w != 0.f;
+}
+
+// Displacement of permuted row `node` of shot `s` in a finished state:
+// class A: hi + lo of the totals; class Z: sum of the split pairs (FP64).
+__device__ __forceinline__ void total_uw(const State32 &st, int na, int S, long long node, int s, double &u, double &w)
+{
+    if (node < na) {
+        u = (double)st.Gc[(node * GC + 0) * S + s] + (double)st.Pa[(node * PA + 2) * S + s];
+        w = (double)st.Gc[(node * GC + 1) * S + s] + (double)st.Pa[(node * PA + 3) * S + s];
+    } else {
+        const long long z = node - na;
+        u = 0.0;
+        w = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            u += (double)st.Gs[(z * GS + k) * S + s] + (double)st.Ps[(z * PS + 6 + k) * S + s];
+            w += (double)st.Gs[(z * GS + 3 + k) * S + s] + (double)st.Ps[(z * PS + 9 + k) * S + s];
+        }
+    }
+}
+
+// Receiver gather (elastic_wave.c:787-795) of the step's input state.
+__device__ __forceinline__ void gather2_one(const StepCommon &c, int na, const State32 &st, int S, int t)
+{
+    if (c.seis_row < 0 || t >= c.nrec * S) return;
+    const int s = t / c.nrec, r = t - s * c.nrec;
+    double u, w;
+    total_uw(st, na, S, c.rec[r], s, u, w);
+    const size_t o = ((size_t)s * c.seis_rows + c.seis_row) * c.nrec + r;
+    c.seis_u[o] = u;
+    c.seis_w[o] = w;
+}
+
+// ------------------------------------------------- single-shot kernels
+
+template <bool COMP, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
+{
+    const StepCommon &c = a.c;
+    const int i = blockIdx.x * THREADS + threadIdx.x;
+    gather2_one(c, a.na, a.in, 1, i);
+    double eu = 0.0, ew = 0.0;
+    if (i < a.na) {
+        const int lane = i & 31, slice = i >> 5;
+        float kU[4], kW[4], mL[8];
+#pragma unroll
+        for (int k = 0; k < 4; k++) { kU[k] = 0.f; kW[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 8; k++) mL[k] = 0.f;
+        const int s0 = __ldg(a.sliceA + slice), s1 = __ldg(a.sliceA + slice + 1);
+        const float *sd = a.sellA + (size_t)s0 * 192 + lane;
+#pragma unroll 2
+        for (int g = s0; g < s1; ++g, sd += 192) {
+            const int j = __float_as_int(ldgf(sd));
+            const float vm = ldgf(sd + 32);
+            float kv[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+            const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
+            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
+            const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+#pragma unroll
+            for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+            mL[0] += vm * q0.z; mL[1] += vm * q0.w; mL[2] += vm * q1.x; mL[3] += vm * q1.y;
+            mL[4] += vm * q1.z; mL[5] += vm * q1.w; mL[6] += vm * q2.x; mL[7] += vm * q2.y;
+        }
+        const float4 cf = __ldg(a.coefA + i);
+        const float im = __ldg(a.imA + i);
+        double src_u = 0.0, src_w = 0.0;
+        if (i == c.src[0]) {
+            const double ps = c.amp[c.it];
+            src_u = ps * c.sin_af;
+            src_w = ps * c.cos_af;
+        }
+        float g[GC], p[PA];
+        const float4 *gi = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float4 v = __ldg(gi + k);
+            g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
+        }
+        const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.in.Pa) + i);
+        p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
+        finish_A<COMP>(kU, kW, mL, cf, im, c.dt, src_u, src_w, g, p, eu, ew);
+        float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+#pragma unroll
+        for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+        reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
+        eu = eu * eu;
+        ew = ew * ew;
+    }
+    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+}
+
+template <bool COMP, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
+{
+    const StepCommon &c = a.c;
+    const int nz = c.n - a.na;
+    const int local = blockIdx.x * THREADS + threadIdx.x;
+    const int i = a.na + local;
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
+    if (local < nz) {
+        const float4 *cf = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
+        c0 = __ldg(cf); c1 = __ldg(cf + 1); c2 = __ldg(cf + 2);
+    }
+    const bool full = __any_sync(0xffffffffu, local < nz && is_pml_row(c1));
+    double eu = 0.0, ew = 0.0;
+    if (local < nz) {
+        const int lane = local & 31, slice = local >> 5;
+        float kU[6], kW[6], m[20];
+#pragma unroll
+        for (int k = 0; k < 6; k++) { kU[k] = 0.f; kW[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 20; k++) m[k] = 0.f;
+        const int s0 = __ldg(a.sliceZ + slice), s1 = __ldg(a.sliceZ + slice + 1);
+        const float *sd = a.sellZ + (size_t)s0 * 256 + lane;
+        if (full) {
+#pragma unroll 2
+            for (int g = s0; g < s1; ++g, sd += 256) {
+                const int j = __float_as_int(ldgf(sd));
+                const float vm = ldgf(sd + 32);
+                float kv[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
+                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+                // split fields exist for class-Z columns; rows outside the
+                // M-PML that share the warp see zeros for class-A columns (their
+                // damping coefficients are zero, so those products are unused)
+                float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0, z2 = z0;
+                if (j >= a.na) {
+                    const float4 *sj = reinterpret_cast<const float4 *>(a.in.Gs + (size_t)(j - a.na) * GS);
+                    z0 = __ldg(sj); z1 = __ldg(sj + 1); z2 = __ldg(sj + 2);
+                }
+#pragma unroll
+                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                m[0] += vm * z0.x;  m[1] += vm * z0.y;  m[2] += vm * z0.z;  m[3] += vm * z0.w;
+                m[4] += vm * z1.x;  m[5] += vm * z1.y;  m[6] += vm * z1.z;  m[7] += vm * z1.w;
+                m[8] += vm * z2.x;  m[9] += vm * z2.y;  m[10] += vm * z2.z; m[11] += vm * z2.w;
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
+        } else {
+#pragma unroll 2
+            for (int g = s0; g < s1; ++g, sd += 256) {
+                const int j = __float_as_int(ldgf(sd));
+                const float vm = ldgf(sd + 32);
+                float kv[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
+                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+#pragma unroll
+                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
+        }
+        double src_u = 0.0, src_w = 0.0;
+        if (i == c.src[0]) {
+            const double ps = c.amp[c.it];
+            src_u = ps * c.sin_af;
+            src_w = ps * c.cos_af;
+        }
+        float gs[GS], ps_[PS], gc[GC];
+        const float4 *si = reinterpret_cast<const float4 *>(a.in.Gs + (size_t)local * GS);
+        const float4 *pi = reinterpret_cast<const float4 *>(a.in.Ps + (size_t)local * PS);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float4 v = __ldg(si + k), w = __ldg(pi + k);
+            gs[4 * k] = v.x; gs[4 * k + 1] = v.y; gs[4 * k + 2] = v.z; gs[4 * k + 3] = v.w;
+            ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
+        }
+        finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, eu, ew);
+        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+        float4 *so = reinterpret_cast<float4 *>(a.out.Gs + (size_t)local * GS);
+        float4 *po = reinterpret_cast<float4 *>(a.out.Ps + (size_t)local * PS);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            gco[k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
+            so[k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
+            po[k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
+        }
+        eu = eu * eu;
+        ew = ew * ew;
+    }
+    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+}
+
+// --------------------------------------------------------- batched kernels
+
+// Per-shot energies of a block, one atomic pair per shot.
+template <int SPL>
+__device__ __forceinline__ void block_energy_shots(const StepCommon &c, const float *eu, const float *ew)
+{
+    constexpr int S = 32 * SPL;
+    __shared__ float se[8][2][S];
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5, s_base = (threadIdx.x & 31) * SPL;
+#pragma unroll
+    for (int q = 0; q < SPL; q++) { se[w][0][s_base + q] = eu[q]; se[w][1][s_base + q] = ew[q]; }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * S; t += blockDim.x) {
+        const int comp = t / S, s = t - comp * S;
+        double acc = 0.0;
+        for (int k = 0; k < nw; k++) acc += se[k][comp][s];
+        if (s < c.nshot && acc != 0.0) atomicAdd(c.energy + ((size_t)s * c.nsteps + c.it) * 2 + comp, acc);
+    }
+}
+
+// One warp per row, S = 32*SPL shots with the shot index innermost.  The
+// row's records (column + matrix values, 32 B each) are loaded once by the
+// warp, one per lane, and broadcast with shuffles; every matrix entry is
+// applied to all S shots.
+template <bool COMP, int SPL>
+__global__ void __launch_bounds__(256) stepA_batched(const Step2 a)
+{
+    constexpr int S = 32 * SPL;
+    const StepCommon &c = a.c;
+    const int lane = threadIdx.x & 31;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int s_base = lane * SPL;
+    int src[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
+    const double ps = c.amp[c.it];
+    const double src_u = ps * c.sin_af, src_w = ps * c.cos_af;
+    float eu[SPL], ew[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
+    const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
+    for (int i = gtid >> 5; i < a.na; i += warps_total) {
+        float kU[4][SPL], kW[4][SPL], mL[8][SPL];
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
+#pragma unroll
+            for (int k = 0; k < 8; k++) mL[k][q] = 0.f;
+        }
+        const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
+        for (int base = e0; base < e1; base += 32) {
+            const int cnt = min(32, e1 - base);
+            float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+            if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
+            for (int k = 0; k < cnt; k++) {
+                const int j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), k);
+                const float vm = __shfl_sync(0xffffffffu, r0.y, k);
+                const float k1 = __shfl_sync(0xffffffffu, r0.z, k), k2 = __shfl_sync(0xffffffffu, r0.w, k);
+                const float k3 = __shfl_sync(0xffffffffu, r1.x, k), k4 = __shfl_sync(0xffffffffu, r1.y, k);
+                const float kv[4] = {k1, k2, k3, k4};
+                const float *gj = a.in.Gc + (size_t)j * GC * S + s_base;
+                VecF<SPL> x[10];
+#pragma unroll
+                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
+#pragma unroll
+                for (int q = 0; q < SPL; q++) {
+#pragma unroll
+                    for (int t = 0; t < 4; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
+#pragma unroll
+                    for (int t = 0; t < 8; t++) mL[t][q] += vm * x[2 + t].v[q];
+                }
+            }
+        }
+        const float4 cf = __ldg(a.coefA + i);
+        const float im = __ldg(a.imA + i);
+        const float *gi = a.in.Gc + (size_t)i * GC * S + s_base;
+        const float *pi = a.in.Pa + (size_t)i * PA * S + s_base;
+        float *go = a.out.Gc + (size_t)i * GC * S + s_base;
+        float *po = a.out.Pa + (size_t)i * PA * S + s_base;
+        VecF<SPL> gv[GC], pv[PA];
+        gv[0].load(gi);
+        gv[1].load(gi + S);
+        gv[10].load(gi + 10 * S);
+        gv[11].load(gi + 11 * S);
+#pragma unroll
+        for (int v = 0; v < PA; v++) pv[v].load(pi + v * S);
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+            float kUq[4], kWq[4], mq[8], g[GC], p[PA];
+#pragma unroll
+            for (int t = 0; t < 4; t++) { kUq[t] = kU[t][q]; kWq[t] = kW[t][q]; }
+#pragma unroll
+            for (int t = 0; t < 8; t++) mq[t] = mL[t][q];
+            g[0] = gv[0].v[q]; g[1] = gv[1].v[q]; g[10] = gv[10].v[q]; g[11] = gv[11].v[q];
+#pragma unroll
+            for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
+            const bool is_src = (i == src[q]);
+            double uu, ww;
+            finish_A<COMP>(kUq, kWq, mq, cf, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
+#pragma unroll
+            for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
+#pragma unroll
+            for (int v = 0; v < PA; v++) pv[v].v[q] = p[v];
+            eu[q] += (float)(uu * uu);
+            ew[q] += (float)(ww * ww);
+        }
+#pragma unroll
+        for (int v = 0; v < GC; v++) gv[v].store(go + v * S);
+#pragma unroll
+        for (int v = 0; v < PA; v++) pv[v].store(po + v * S);
+    }
+    if (c.energy) block_energy_shots<SPL>(c, eu, ew);
+}
+
+template <bool COMP, int SPL>
+__global__ void __launch_bounds__(256) stepZ_batched(const Step2 a)
+{
+    constexpr int S = 32 * SPL;
+    const StepCommon &c = a.c;
+    const int lane = threadIdx.x & 31;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int s_base = lane * SPL;
+    int src[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
+    const double ps = c.amp[c.it];
+    const double src_u = ps * c.sin_af, src_w = ps * c.cos_af;
+    float eu[SPL], ew[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
+    const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
+    const int nz = c.n - a.na;
+    for (int local = gtid >> 5; local < nz; local += warps_total) {
+        const int i = a.na + local;
+        const float4 *cfp = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
+        const float4 c0 = __ldg(cfp), c1 = __ldg(cfp + 1), c2 = __ldg(cfp + 2);
+        const bool full = is_pml_row(c1);
+        float kU[6][SPL], kW[6][SPL], m[20][SPL];
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+#pragma unroll
+            for (int k = 0; k < 6; k++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
+#pragma unroll
+            for (int k = 0; k < 20; k++) m[k][q] = 0.f;
+        }
+        const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
+        for (int base = e0; base < e1; base += 32) {
+            const int cnt = min(32, e1 - base);
+            float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+            if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
+            for (int k = 0; k < cnt; k++) {
+                const int j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), k);
+                const float vm = __shfl_sync(0xffffffffu, r0.y, k);
+                float kv[6];
+                kv[0] = __shfl_sync(0xffffffffu, r0.z, k); kv[1] = __shfl_sync(0xffffffffu, r0.w, k);
+                kv[2] = __shfl_sync(0xffffffffu, r1.x, k); kv[3] = __shfl_sync(0xffffffffu, r1.y, k);
+                kv[4] = __shfl_sync(0xffffffffu, r1.z, k); kv[5] = __shfl_sync(0xffffffffu, r1.w, k);
+                const float *gj = a.in.Gc + (size_t)j * GC * S + s_base;
+                VecF<SPL> x[10];
+#pragma unroll
+                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
+#pragma unroll
+                for (int q = 0; q < SPL; q++) {
+#pragma unroll
+                    for (int t = 0; t < 4; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
+#pragma unroll
+                    for (int t = 0; t < 8; t++) m[12 + t][q] += vm * x[2 + t].v[q];
+                }
+                if (full) {
+#pragma unroll
+                    for (int q = 0; q < SPL; q++)
+#pragma unroll
+                        for (int t = 4; t < 6; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
+                    // M-PML rows reference class-Z columns only (set-up guarantees it)
+                    if (j >= a.na) {
+                        const float *sj = a.in.Gs + (size_t)(j - a.na) * GS * S + s_base;
+                        VecF<SPL> y[12];
+#pragma unroll
+                        for (int v = 0; v < 12; v++) y[v].load(sj + v * S);
+#pragma unroll
+                        for (int q = 0; q < SPL; q++)
+#pragma unroll
+                            for (int t = 0; t < 12; t++) m[t][q] += vm * y[t].v[q];
+                    }
+                }
+            }
+        }
+        const float *si = a.in.Gs + (size_t)local * GS * S + s_base;
+        const float *pi = a.in.Ps + (size_t)local * PS * S + s_base;
+        float *gco = a.out.Gc + (size_t)i * GC * S + s_base;
+        float *so = a.out.Gs + (size_t)local * GS * S + s_base;
+        float *po = a.out.Ps + (size_t)local * PS * S + s_base;
+        VecF<SPL> sv[GS], pv[PS], cv[GC];
+#pragma unroll
+        for (int v = 0; v < GS; v++) sv[v].load(si + v * S);
+#pragma unroll
+        for (int v = 0; v < PS; v++) pv[v].load(pi + v * S);
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+            float kUq[6], kWq[6], mq[20], gs[GS], ps_[PS], gc[GC];
+#pragma unroll
+            for (int t = 0; t < 6; t++) { kUq[t] = kU[t][q]; kWq[t] = kW[t][q]; }
+#pragma unroll
+            for (int t = 0; t < 20; t++) mq[t] = m[t][q];
+#pragma unroll
+            for (int v = 0; v < GS; v++) { gs[v] = sv[v].v[q]; ps_[v] = pv[v].v[q]; }
+            const bool is_src = (i == src[q]);
+            double uu, ww;
+            finish_Z<COMP>(kUq, kWq, mq, c0, c1, c2, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, gs, ps_, gc,
+                           uu, ww);
+#pragma unroll
+            for (int v = 0; v < GS; v++) { sv[v].v[q] = gs[v]; pv[v].v[q] = ps_[v]; cv[v].v[q] = gc[v]; }
+            eu[q] += (float)(uu * uu);
+            ew[q] += (float)(ww * ww);
+        }
+#pragma unroll
+        for (int v = 0; v < GC; v++) cv[v].store(gco + v * S);
+#pragma unroll
+        for (int v = 0; v < GS; v++) sv[v].store(so + v * S);
+#pragma unroll
+        for (int v = 0; v < PS; v++) pv[v].store(po + v * S);
+    }
+    if (c.energy) block_energy_shots<SPL>(c, eu, ew);
+}
+
+// --------------------------------------------------- gathers, snapshots
+
+__global__ void gather2_kernel(const StepCommon c, int na, const State32 st, int S)
+{
+    gather2_one(c, na, st, S, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void snapshot2_kernel(const State32 st, int n, int na, int S, const int *perm, double *su, double *sw,
+                                 long long shot_stride)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * S) return;
+    const int s = (int)(t % S);
+    const long long node = t / S;
+    double u, w;
+    total_uw(st, na, S, node, s, u, w);
+    const long long o = perm[node];
+    su[s * shot_stride + o] = u;
+    sw[s * shot_stride + o] = w;
+}
+
+// ------------------------------------------------------------ builders
+
+__global__ void range_slice_len(int r0, int r1, const int *__restrict__ up, const int *__restrict__ perm, int *len)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = r1 - r0, nsl = (n + 31) / 32;
+    if (s >= nsl) return;
+    int m = 0;
+    for (int l = 0; l < 32; l++) {
+        const int r = s * 32 + l;
+        if (r < n) {
+            const int o = perm[r0 + r];
+            m = max(m, up[o + 1] - up[o]);
+        }
+    }
+    len[s] = m;
+}
+
+__global__ void range_sell_fill(int r0, int r1, const int *__restrict__ up, const int *__restrict__ uj,
+                                const double *__restrict__ ux, long long nnz, const int *__restrict__ sp,
+                                const int *__restrict__ perm, const int *__restrict__ inv, int planes,
+                                float *__restrict__ sell)
+{
+    const int s = blockIdx.x, lane = threadIdx.x;
+    const int n = r1 - r0, r = s * 32 + lane;
+    const int s0 = sp[s], s1 = sp[s + 1];
+    const int o = r < n ? perm[r0 + r] : 0;
+    const int a0 = r < n ? up[o] : 0, len = r < n ? up[o + 1] - a0 : 0;
+    for (int k = 0; k < s1 - s0; k++) {
+        float *slot = sell + (size_t)(s0 + k) * planes * 32;
+        if (k < len) {
+            const long long e = a0 + k;
+            slot[lane] = __int_as_float(inv[uj[e]]);
+            for (int m = 0; m < planes - 1; m++) slot[32 * (m + 1) + lane] = (float)ux[m * nnz + e];
+        } else {
+            slot[lane] = __int_as_float(r < n ? r0 + r : r0);   // the row itself, zero weights
+            for (int m = 0; m < planes - 1; m++) slot[32 * (m + 1) + lane] = 0.f;
+        }
+    }
+}
+
+__global__ void rec_perm_fill(int n, const int *__restrict__ up, const int *__restrict__ uj,
+                              const double *__restrict__ ux, long long nnz, const int *__restrict__ perm,
+                              const int *__restrict__ inv, const int *__restrict__ upp, float *__restrict__ rec)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int o = perm[r];
+    const int a0 = up[o], len = up[o + 1] - a0;
+    const long long d0 = upp[r];
+    for (int k = 0; k < len; k++) {
+        const long long e = a0 + k, d = d0 + k;
+        rec[d * 8] = __int_as_float(inv[uj[e]]);
+        for (int m = 0; m < 7; m++) rec[d * 8 + 1 + m] = (float)ux[m * nnz + e];
+    }
+}
+
+__global__ void coef2_kernel(int n, int na, const float *__restrict__ coef, const int *__restrict__ perm,
+                             float4 *__restrict__ coefA, float *__restrict__ imA, float *__restrict__ coefZ)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const float *src = coef + (size_t)perm[r] * CREC;
+    if (r < na) {
+        coefA[r] = make_float4(src[0], src[1], src[2], src[3]);
+        imA[r] = src[8];
+    } else {
+        float *d = coefZ + (size_t)(r - na) * CREC;
+        for (int k = 0; k < CREC; k++) d[k] = src[k];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------- launchers
+
+// Launch shapes of the single-shot kernels (threads per block, minimum
+// resident blocks for the register allocation):
+//   0: 128 x 4   1: 128 x 6   2: 256 x 3   3: 256 x 4
+int step2_variants() { return 4; }
+
+#define SFG_SHAPES(KERNEL, COUNT)                                                              \
+    do {                                                                                       \
+        if ((COUNT) <= 0) return cudaSuccess;                                                  \
+        switch (variant) {                                                                     \
+        case 0: SFG_ONE(KERNEL, 128, 4, COUNT); break;                                         \
+        case 1: SFG_ONE(KERNEL, 128, 6, COUNT); break;                                         \
+        case 2: SFG_ONE(KERNEL, 256, 3, COUNT); break;                                         \
+        default: SFG_ONE(KERNEL, 256, 4, COUNT); break;                                        \
+        }                                                                                      \
+    } while (0)
+#define SFG_ONE(KERNEL, T, M, COUNT)                                                           \
+    do {                                                                                       \
+        const int blocks = ((COUNT) + (T) - 1) / (T);                                          \
+        if (comp) KERNEL<true, T, M><<<blocks, T, 0, st>>>(a);                                 \
+        else KERNEL<false, T, M><<<blocks, T, 0, st>>>(a);                                     \
+    } while (0)
+
+cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st)
+{
+    // the fused receiver gather runs on the first nrec threads
+    SFG_SHAPES(stepA_kernel, std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st)
+{
+    SFG_SHAPES(stepZ_kernel, a.c.n - a.na);
+    return cudaGetLastError();
+}
+#undef SFG_ONE
+#undef SFG_SHAPES
+
+template <typename K>
+static long long batched_grid(K kernel, int threads, long long rows, int warps)
+{
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (per_sm < 1) per_sm = 1;
+    const long long need = (rows + warps - 1) / warps;
+    return std::max<long long>(1, std::min<long long>((long long)sms * per_sm, need));
+}
+
+#define SFG_BATCH(KERNEL, ROWS)                                                                          \
+    do {                                                                                                 \
+        const int threads = 32 * warps;                                                                  \
+        if (warps < 1 || warps > 8) return cudaErrorInvalidValue;                                        \
+        if ((ROWS) <= 0) return cudaSuccess;                                                             \
+        if (comp) {                                                                                      \
+            if (spl == 1) { auto k = KERNEL<true, 1>; KERNEL<true, 1><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            else if (spl == 2) { auto k = KERNEL<true, 2>; KERNEL<true, 2><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            else { auto k = KERNEL<true, 4>; KERNEL<true, 4><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+        } else {                                                                                         \
+            if (spl == 1) { auto k = KERNEL<false, 1>; KERNEL<false, 1><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            else if (spl == 2) { auto k = KERNEL<false, 2>; KERNEL<false, 2><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            else { auto k = KERNEL<false, 4>; KERNEL<false, 4><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+        }                                                                                                \
+    } while (0)
+
+cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st)
+{
+    // at least one warp for the receiver gather even without class-A rows
+    SFG_BATCH(stepA_batched, std::max(a.na, 1));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st)
+{
+    SFG_BATCH(stepZ_batched, a.c.n - a.na);
+    return cudaGetLastError();
+}
+#undef SFG_BATCH
+
+cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st)
+{
+    const int tot = c.nrec * S;
+    if (tot > 0 && c.seis_row >= 0) gather2_kernel<<<(tot + 127) / 128, 128, 0, st>>>(c, na, s, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot2(const State32 &s, int n, int na, int S, const int *perm, double *su, double *sw,
+                             long long shot_stride, cudaStream_t st)
+{
+    const long long tot = (long long)n * S;
+    if (tot > 0)
+        snapshot2_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, n, na, S, perm, su, sw, shot_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t build_sell_range(int r0, int r1, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                             const int *d_perm, const int *d_inv, int planes, float **d_sell, int **d_slice,
+                             long long *slots, cudaStream_t st)
+{
+    const int n = r1 - r0, nsl = (n + 31) / 32;
+    int *len = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&len, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(d_slice, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
+    if (nsl) range_slice_len<<<(nsl + 127) / 128, 128, 0, st>>>(r0, r1, d_up, d_perm, len);
+    if ((e = exclusive_scan_int(len, *d_slice, nsl, st)) != cudaSuccess) return e;
+    int tot = 0;
+    cudaMemcpyAsync(&tot, *d_slice + nsl, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    *slots = tot;
+    if ((e = cudaMalloc(d_sell, sizeof(float) * planes * 32 * std::max<size_t>(tot, 1))) != cudaSuccess) return e;
+    if (nsl) range_sell_fill<<<nsl, 32, 0, st>>>(r0, r1, d_up, d_uj, d_ux, nnz, *d_slice, d_perm, d_inv, planes, *d_sell);
+    e = cudaGetLastError();
+    cudaStreamSynchronize(st);
+    cudaFree(len);
+    return e;
+}
+
+cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                           const int *d_perm, const int *d_inv, const int *d_upp, float **d_rec, cudaStream_t st)
+{
+    cudaError_t e = cudaMalloc(d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1));
+    if (e != cudaSuccess) return e;
+    if (n) rec_perm_fill<<<(n + 127) / 128, 128, 0, st>>>(n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, *d_rec);
+    return cudaGetLastError();
+}
+
+cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,
+                        float **d_coefZ, cudaStream_t st)
+{
+    cudaError_t e;
+    if ((e = cudaMalloc(d_coefA, sizeof(float4) * std::max(na, 1))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(d_imA, sizeof(float) * std::max(na, 1))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(d_coefZ, sizeof(float) * CREC * std::max(n - na, 1))) != cudaSuccess) return e;
+    if (n) coef2_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, na, d_coef32, d_perm, *d_coefA, *d_imA, *d_coefZ);
+    return cudaGetLastError();
+}
+
+}  // namespace sfg

@@ -1,0 +1,84 @@
+// sfg_step32.cuh -- the fused FP32 step in the two-class node numbering.
+//
+// Node classes (decided at set-up from the M-PML profiles and the union
+// sparsity pattern):
+//   Z  the split zone: rows inside the M-PML (any of dx, dy, dxx, dyy non-zero)
+//      and every column those rows reference -- the nodes whose split fields
+//      U1 U2 U3 / W1 W2 W3 somebody reads;
+//   A  all other nodes.  Their rows multiply every split-field, K5 and K6
+//      product by a zero damping coefficient, and nobody reads their split
+//      fields, so they carry only the totals U = U1+U2+U3, W = W1+W2+W3 (the
+//      Newmark update, elastic_wave.c:757-768, is linear: the totals follow
+//      the same recursion with the summed accelerations).
+// Numbering: rows [0, na) are class A, rows [na, n) class Z; inside each
+// class, windows of 2048 rows are sorted by (M-PML flag, row length) so that
+// 32-row SELL slices need no padding.  perm[r'] is the mesh node of row r'.
+//
+// State records (node-major, shot index innermost for batches of S shots):
+//   Gc[n][12]   gathered by every row: U W Lx1 Lx2 | Lx3 Lx4 Ly1 Ly2 | Ly3 Ly4
+//               Vu Vw   (U, W: FP32 value of the total; Vu, Vw: total
+//               velocities of class-A rows, 0 in class Z)
+//   Pa[na][4]   class A, private: Au Aw lo_u lo_w
+//   Gs[nz][12]  class Z, gathered by M-PML rows: U1 U2 U3 W1 W2 W3 (high FP32
+//               part) | V1..V6
+//   Ps[nz][12]  class Z, private: A1..A6 | lo1..lo6
+// Compensated precision keeps every displacement as an FP32 pair hi + lo
+// updated in FP64; the plain FP32 variant leaves lo at 0.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sfg_step.cuh"
+
+namespace sfg {
+
+constexpr int GC = 12, PA = 4, GS = 12, PS = 12;
+
+struct State32 {
+    const float *Gc, *Pa, *Gs, *Ps;
+};
+struct State32W {
+    float *Gc, *Pa, *Gs, *Ps;
+};
+
+struct Step2 {
+    StepCommon c;              // c.n = all rows; src / rec in the permuted numbering
+    int na;                    // class-A rows [0, na); class Z [na, n)
+    const float *sellA;        // SELL-32 over rows [0, na): planes col, M, K1..K4
+    const int *sliceA;
+    const float *sellZ;        // SELL-32 over rows [na, n): planes col, M, K1..K6
+    const int *sliceZ;
+    const int *up;             // row-major union records in the permuted numbering
+    const float *rec;          //   [nnz][8]: col, M, K1..K6
+    const float4 *coefA;       // [na] c11 c13 c33 c44
+    const float *imA;          // [na] 1/m_lump (0 on Dirichlet rows)
+    const float *coefZ;        // [n-na][12] (sfg_step.cuh coefficient order)
+    State32 in;
+    State32W out;
+};
+
+// single shot (thread per row); variant = launch shape 0..step2_variants()-1
+int step2_variants();
+cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st);
+cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st);
+// S = 32 * spl shots (warp per row)
+cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
+cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
+// receiver gather of a finished state; snapshots scattered back to mesh order
+cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st);
+cudaError_t launch_snapshot2(const State32 &s, int n, int na, int S, const int *perm, double *snap_u,
+                             double *snap_w, long long shot_stride, cudaStream_t st);
+
+// set-up builders
+// SELL-32 over permuted rows [r0, r1) with `planes` planes (6: col M K1..K4; 8: + K5 K6)
+cudaError_t build_sell_range(int r0, int r1, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                             const int *d_perm, const int *d_inv, int planes, float **d_sell, int **d_slice,
+                             long long *slots, cudaStream_t st);
+// row-major records in the permuted numbering (d_upp: permuted row pointers)
+cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                           const int *d_perm, const int *d_inv, const int *d_upp, float **d_rec, cudaStream_t st);
+// class-A / class-Z coefficient arrays from the [n][12] FP32 record
+cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,
+                        float **d_coefZ, cudaStream_t st);
+
+}  // namespace sfg
