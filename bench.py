@@ -262,7 +262,7 @@ def main():
             traffic = tj.get("bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "step32_kernel (fused SpMV + RHS + solve + Newmark)",
+                "kernel": "stepA/stepZ fused step (SpMV + RHS + lumped solve + Newmark), both classes",
                 "algorithmic_bytes_per_launch": b_step, "avg_launch_us": round(kms * 1e3, 3),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback"}
 
@@ -341,20 +341,26 @@ def main():
 
 
 def step_bytes(ctx, prob, S) -> int:
-    """Algorithmic bytes of one fused FP32 time step (all S shots):
-    matrix stream -- per union entry 4 B column + 4 B each of M, K1..K4, plus
-    K5, K6 on rows inside the M-PML (rows outside it multiply every K5/K6,
-    M*V and M*U_k product by a zero damping coefficient) -- plus the
-    state record read and written once per node and shot (24 + 10 floats)
-    and the per-node coefficient record (12 floats)."""
-    p, _ = ctx.union_pattern()
+    """Algorithmic bytes of one fused FP32 time step (all S shots), for the
+    two-class layout: rows outside the M-PML zone stream column + M + K1..K4
+    (24 B per union entry) and move their totals record (Gc 12 + Pa 4 floats,
+    read and written once); split-zone rows stream 32 B per entry inside the
+    M-PML (K5, K6 too) and move Gc + Gs + Ps (36 floats); per-node
+    coefficients 5 floats (interior) or 12 (split zone).  Gathers of
+    neighbour records are counted once (their owner's read)."""
+    p, j = ctx.union_pattern()
     L = np.diff(p).astype(np.int64)
     mp = ctx.mpml()
     pml = np.any(mp[:4].astype(np.float32) != 0, axis=0)
+    zone = pml.copy()
+    rows = np.repeat(np.arange(len(L)), L)
+    zone[j[pml[rows]]] = True
     N = prob.mesh.node_num
-    mat = int(L[pml].sum()) * 32 + int(L[~pml].sum()) * 24 + 4 * (N // 32 + 1)
-    state = N * S * (24 + 10) * 4 * 2
-    coef = N * 12 * 4
+    na = int((~zone).sum())
+    assert na == ctx.stats()["interior_rows"], (na, ctx.stats()["interior_rows"])
+    mat = int(L[pml].sum()) * 32 + int(L[~pml].sum()) * 24 + 4 * (N // 32 + 2)
+    state = (na * (12 + 4) + (N - na) * (12 + 12 + 12)) * 4 * 2 * S
+    coef = na * 5 * 4 + (N - na) * 12 * 4
     return int(mat + state + coef)
 
 

@@ -95,6 +95,8 @@ typedef struct {
     int kernel_launches;       /* kernels launched by the last run's time loop */
     int rows_per_block;        /* launch shape the autotuner picked */
     int blowup_step;           /* first step whose energy bound failed, -1 if none */
+    int interior_rows;         /* nodes advanced as totals only (outside the M-PML zone) */
+    int pml_rows;              /* rows with a non-zero M-PML profile */
 } sfg_stats;
 
 /* ---------------------------------------------------------- context API */

@@ -46,6 +46,19 @@ static FILE *g_open[64];
 static int g_nopen;
 static jmp_buf g_jmp;
 static int g_in_run;
+/* exit() requested from inside an OpenMP parallel region (the energy bound,
+ * elastic_wave.c:754-785): a worker thread cannot jump out, so the request
+ * is recorded and served by the next shimmed call on the master thread */
+static volatile int g_exit_code;
+
+static void serve_exit(void)
+{
+    if (g_exit_code && g_in_run && !omp_in_parallel()) {
+        int c = g_exit_code;
+        g_exit_code = 0;
+        longjmp(g_jmp, c);
+    }
+}
 /* per-step timestamps: the reference ends every time step by writing "\n"
  * to seismogram_u_shot_k (elastic_wave.c:794) */
 static double *g_step_t;
@@ -60,6 +73,7 @@ static double now_s(void)
 
 static FILE *sfr_fopen(const char *path, const char *mode)
 {
+    serve_exit();
     FILE *f = fopen(path, mode);
     if (!f) return f;
     if (g_nopen < 64) g_open[g_nopen++] = f;
@@ -89,6 +103,7 @@ static int sfr_fclose(FILE *f)
 
 static int sfr_fprintf(FILE *f, const char *fmt, ...)
 {
+    serve_exit();
     va_list ap, ap2;
     va_start(ap, fmt);
     va_copy(ap2, ap);
@@ -111,6 +126,7 @@ static int sfr_fprintf(FILE *f, const char *fmt, ...)
 
 static int sfr_printf(const char *fmt, ...)
 {
+    serve_exit();
     if (!getenv("SFR_VERBOSE")) return 0;
     va_list ap;
     va_start(ap, fmt);
@@ -123,6 +139,10 @@ static void *sfr_malloc(size_t n) { return calloc(1, n ? n : 1); }
 
 static void sfr_exit(int code)
 {
+    if (g_in_run && omp_in_parallel()) {
+        g_exit_code = code ? code : 1;
+        return;
+    }
     if (g_in_run) longjmp(g_jmp, code ? code : 1);
     exit(code);
 }
@@ -275,6 +295,7 @@ int sfr_elastic_wave(const char *workdir, int nthreads, char *type, int node_num
     struct timespec a, b;
     clock_gettime(CLOCK_MONOTONIC, &a);
     g_in_run = 1;
+    g_exit_code = 0;
     int rc = setjmp(g_jmp);
     if (rc == 0)
         elastic_wave(type, node_num, element_num, order, element_node, xy,

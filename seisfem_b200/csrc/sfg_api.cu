@@ -4,7 +4,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +25,20 @@ struct RunCache {
     int threads_fp32 = 0, threads_fp32k = 0;
     int warps_b[3][2] = {{0, 0}, {0, 0}, {0, 0}};   // [spl index][kahan]
 };
+
+// Launch shapes already tuned in this process, keyed by the mesh signature
+// (rows, union nonzeros, interior rows, element type) and device, so that a
+// new context on the same mesh does not tune again.
+struct TuneKey {
+    int device, N, na, type;
+    long long nnz;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(device, N, na, type, nnz) < std::tie(o.device, o.N, o.na, o.type, o.nnz);
+    }
+};
+static std::map<TuneKey, RunCache> g_tuned;
+static std::mutex g_tuned_mu;
 
 struct sfg_ctx {
     int device = 0;
@@ -305,6 +322,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         P.h_inv = std::move(inv);
         P.h_perm = std::move(perm);
         P.na = na;
+        ctx->stats.interior_rows = na;
+        ctx->stats.pml_rows = (int)std::count(pml.begin(), pml.end(), 1);
     }
     CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA, &P.slotsA, st));
     CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ, &P.slotsZ, st));
@@ -315,7 +334,11 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
     cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx); cudaFree(d_scr);
     for (auto &px : ctx->plain_x) { cudaFree(px); px = nullptr; }
-    ctx->tune = RunCache();
+    {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        auto it = g_tuned.find({ctx->device, N, P.na, tc, P.union_nnz});
+        ctx->tune = it != g_tuned.end() ? it->second : RunCache();
+    }
     ctx->ready = true;
     ctx->stats.union_nnz = P.union_nnz;
     for (int k = 0; k < 7; k++) ctx->stats.csr_nnz[k] = P.csr[k].nnz;
@@ -649,6 +672,10 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     cudaEventDestroy(e1);
     *slot = pick + 1;
     if (pl.S == 1) pl.threads = pick; else pl.warps = pick;
+    {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        g_tuned[{ctx->device, ctx->N, ctx->P.na, ctx->P.type_code, ctx->P.union_nnz}] = ctx->tune;
+    }
     return SFG_OK;
 }
 

@@ -112,13 +112,33 @@ cudaError_t exclusive_scan_int(const int *d_in, int *d_out, int n, cudaStream_t 
 
 struct MatList { int m[8]; };   // -1: consistent mass (rho), 0..6: stiffness type
 
+// Shape functions and their r/s derivatives at every quadrature point of the
+// element type: tab[(3*q + c)*16 + k], c = 0 value, 1 d/dr, 2 d/ds.  They do
+// not depend on the element, so they are evaluated once per set-up (same
+// arithmetic as a per-element evaluation, hence the same bits).
+__global__ void shape_table_kernel(int tc, double *tab)
+{
+    const int q = threadIdx.x;
+    if (q >= quad_count(tc)) return;
+    double r, s, w;
+    quad_point(tc, q, r, s, w);
+    double sv[16], sdr[16], sds[16];
+    shape_eval(tc, r, s, sv, sdr, sds);
+    const int p = elem_order(tc);
+    for (int k = 0; k < p; k++) {
+        tab[(3 * q + 0) * 16 + k] = sv[k];
+        tab[(3 * q + 1) * 16 + k] = sdr[k];
+        tab[(3 * q + 2) * 16 + k] = sds[k];
+    }
+}
+
 // One thread per COO entry (e, iq, jq): integrates the requested matrices in
 // the reference's quadrature order (mass_sparse_q4.c:199-256,
 // stiffness_sparse_q4.c:202-271) and writes entry e*p*p + iq*p + jq.
 __global__ void element_coo_kernel(int tc, int p, long long nnz, const int *__restrict__ en,
                                    const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ rho, int nmat, MatList ml,
-                                   int *__restrict__ ci, int *__restrict__ cj,
+                                   const double *__restrict__ tab, int *__restrict__ ci, int *__restrict__ cj,
                                    double *__restrict__ cx, int *flags)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -142,13 +162,12 @@ __global__ void element_coo_kernel(int tc, int p, long long nnz, const int *__re
         quad_point(tc, q, r, s, w);
         double drdx, drdy, dsdx, dsdy;
         map_point(tc, g, r, s, drdx, drdy, dsdx, dsdy);
-        double sv[16], sdr[16], sds[16];
-        shape_eval(tc, r, s, sv, sdr, sds);
-        double phi_i = sv[iq], phi_j = sv[jq];
-        double dxi = sdr[iq] * drdx + sds[iq] * dsdx;
-        double dyi = sdr[iq] * drdy + sds[iq] * dsdy;
-        double dxj = sdr[jq] * drdx + sds[jq] * dsdx;
-        double dyj = sdr[jq] * drdy + sds[jq] * dsdy;
+        const double *t0 = tab + 3 * q * 16, *t1 = t0 + 16, *t2 = t0 + 32;
+        double phi_i = t0[iq], phi_j = t0[jq];
+        double dxi = t1[iq] * drdx + t2[iq] * dsdx;
+        double dyi = t1[iq] * drdy + t2[iq] * dsdy;
+        double dxj = t1[jq] * drdx + t2[jq] * dsdx;
+        double dyj = t1[jq] * drdy + t2[jq] * dsdy;
         double aw = g.area * w;
         for (int m = 0; m < nmat; m++) {
             double term;
@@ -178,12 +197,18 @@ cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x
     long long nnz = (long long)E * p * p;
     MatList ml;
     for (int m = 0; m < 8; m++) ml.m[m] = m < nmat ? mats[m] : 0;
+    double *tab = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&tab, sizeof(double) * 36 * 3 * 16, st);
+    if (e != cudaSuccess) return e;
+    shape_table_kernel<<<1, 64, 0, st>>>(tc, tab);
     int threads = 128;
     long long blocks = (nnz + threads - 1) / threads;
     if (blocks > 0)
         element_coo_kernel<<<(unsigned)blocks, threads, 0, st>>>(tc, p, nnz, d_en, d_x, d_y, d_rho, nmat,
-                                                                  ml, d_ci, d_cj, d_cx, d_flags);
-    return cudaGetLastError();
+                                                                  ml, tab, d_ci, d_cj, d_cx, d_flags);
+    e = cudaGetLastError();
+    cudaFreeAsync(tab, st);
+    return e;
 }
 
 // ------------------------------------------------------------ lumped mass
@@ -192,7 +217,8 @@ cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x
 // the element's own (quad, iq, jq) order (mass_sparse_q4.c:238-246).
 __global__ void element_mass_sums(int tc, int p, int E, const int *__restrict__ en,
                                   const double *__restrict__ x, const double *__restrict__ y,
-                                  const double *__restrict__ rho, double *__restrict__ part)
+                                  const double *__restrict__ rho, const double *__restrict__ tab,
+                                  double *__restrict__ part)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
@@ -204,8 +230,7 @@ __global__ void element_mass_sums(int tc, int p, int E, const int *__restrict__ 
     for (int q = 0; q < nq; q++) {
         double r, s, w;
         quad_point(tc, q, r, s, w);
-        double sv[16], sdr[16], sds[16];
-        shape_eval(tc, r, s, sv, sdr, sds);
+        const double *sv = tab + 3 * q * 16;
         double aw = g.area * w;
         for (int iq = 0; iq < p; iq++) {
             int ip = enE[iq] - 1;
@@ -247,7 +272,8 @@ __global__ void node_lumped_mass(int tc, int p, int N, const int *__restrict__ e
                                  const double *__restrict__ x, const double *__restrict__ y,
                                  const double *__restrict__ rho, const int *__restrict__ row_start,
                                  const int *__restrict__ bucket, const int *__restrict__ cj,
-                                 const double *__restrict__ sums, double *__restrict__ mass)
+                                 const double *__restrict__ sums, const double *__restrict__ tab,
+                                 double *__restrict__ mass)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= N) return;
@@ -264,8 +290,7 @@ __global__ void node_lumped_mass(int tc, int p, int N, const int *__restrict__ e
         for (int q = 0; q < nq; q++) {
             double rr, ss, w;
             quad_point(tc, q, rr, ss, w);
-            double sv[16], sdr[16], sds[16];
-            shape_eval(tc, rr, ss, sv, sdr, sds);
+            const double *sv = tab + 3 * q * 16;
             m = m + g.area * w * rho[r] * sv[iq] * sv[jq];
         }
     }
@@ -280,12 +305,18 @@ cudaError_t launch_lumped_mass(int tc, int N, int E, const int *d_en, const doub
 {
     (void)d_flags;
     int p = elem_order(tc);
-    element_mass_sums<<<(E + 127) / 128, 128, 0, st>>>(tc, p, E, d_en, d_x, d_y, d_rho, d_scratch);
+    double *tab = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&tab, sizeof(double) * 36 * 3 * 16, st);
+    if (e != cudaSuccess) return e;
+    shape_table_kernel<<<1, 64, 0, st>>>(tc, tab);
+    element_mass_sums<<<(E + 127) / 128, 128, 0, st>>>(tc, p, E, d_en, d_x, d_y, d_rho, tab, d_scratch);
     double *sums = d_scratch + 2 * (size_t)E;
     reduce_pairs<<<1, 1024, 0, st>>>(d_scratch, E, sums);
     node_lumped_mass<<<(N + 127) / 128, 128, 0, st>>>(tc, p, N, d_en, d_x, d_y, d_rho, d_row_start,
-                                                       d_bucket, d_cj, sums, d_mass);
-    return cudaGetLastError();
+                                                       d_bucket, d_cj, sums, tab, d_mass);
+    e = cudaGetLastError();
+    cudaFreeAsync(tab, st);
+    return e;
 }
 
 // ------------------------------------------------------------------ M-PML
@@ -592,7 +623,6 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     if (hflags & FLAG_SORT_STACK) { err = "row too long for the device sorter"; return SFG_ERR_ROWLEN; }
 
     // row pointers: union + each stream
-    int *h_ptrs[8] = {nullptr};
     int *up = nullptr;
     if (want_union) {
         SFG_TRY(cudaMalloc(&up, sizeof(int) * ((size_t)N + 1)));
@@ -621,7 +651,6 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
             dvp[s] = c.p; dvj[s] = c.j; dvx[s] = c.x;
         }
     }
-    (void)h_ptrs;
     int **d_tab = nullptr;
     SFG_TRY(cudaMalloc(&d_tab, sizeof(void *) * 24));
     void *htab[24];

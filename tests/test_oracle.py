@@ -1,0 +1,183 @@
+"""The CPU oracle pinned to the reference (no GPU).
+
+* known answer: the 18-entry COO of sparse_matrix/test_coo2csr_lib.c:10-12;
+* bit-exact against the reference compiled from its own sources
+  (oracle/_ref, when built here) and against fixtures it generated
+  (tests/golden/, which travel);
+* the reference's committed EXAMPLE outputs (text, 6 decimals, produced on
+  another machine) reproduced within their printing precision;
+* properties of the assembled matrices.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from seisfem_b200.problem import Mesh, Model, Problem, isotropic_model, small_problem, structured_mesh, locate, line_points
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+KAT = ([0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 2, 2, 2, 1, 1, 1],
+       [0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 2, 1, 3, 2, 1, 3, 2, 1],
+       [1.0, -0.5, -0.5, -0.5, 0.5, 0.0, -0.5, 0.0, 0.5, 1.0, -0.5, -0.5, -0.5, 0.5, 0.0, -0.5, 0.0, 0.5])
+
+
+def test_coo2csr_known_answer(oracle):
+    Bp, Bj, Bx = oracle.coo2csr(4, *KAT)
+    assert Bp.tolist() == [0, 3, 6, 9, 12]
+    assert Bj.tolist() == [0, 1, 2, 0, 1, 3, 0, 2, 3, 1, 2, 3]
+    assert Bx.tolist() == [1, -.5, -.5, -.5, 1, -.5, -.5, 1, -.5, -.5, -.5, 1]
+
+
+def test_coo2csr_fortran_abi_side_effects(reference):
+    # Ai/Aj left incremented by one (coo2csr_lib.f90:27-28), 0-based output
+    import ctypes as C
+    ai = np.array(KAT[0], np.int32)
+    aj = np.array(KAT[1], np.int32)
+    ax = np.array(KAT[2])
+    n, ps, z = C.c_int(18), C.c_int(5), C.c_int()
+    Bp, Bj, Bx = np.zeros(5, np.int32), np.zeros(18, np.int32), np.zeros(18)
+    reference._coo2csr(C.byref(n), C.byref(ps), C.byref(z), ai, aj, ax, Bp, Bj, Bx)
+    assert z.value == 12 and ai.tolist() == [v + 1 for v in KAT[0]] and aj.tolist() == [v + 1 for v in KAT[1]]
+
+
+def test_iargsort_sorts_and_is_a_permutation(oracle):
+    rng = np.random.default_rng(0)
+    for n in (0, 1, 5, 19, 20, 21, 36, 100, 257):
+        v = rng.integers(1, 40, n).astype(np.int32)
+        m = oracle.iargsort(v)
+        assert sorted(m.tolist()) == list(range(n))
+        assert np.all(np.diff(v[m]) >= 0)
+
+
+@pytest.mark.parametrize("etype", ["T3", "T6", "Q4", "Q9"])
+def test_assembly_matches_golden_fixture(oracle, etype):
+    g = np.load(os.path.join(GOLD, "csr_small.npz"))
+    m = Mesh(etype, g[f"{etype}_element_node"], g[f"{etype}_x"], g[f"{etype}_y"], 0.0, 50.0, 0.0, 40.0)
+    rho = g[f"{etype}_rho"]
+    mats = [oracle.mass_coo(m, rho)] + [oracle.stif_coo(m, k) for k in range(1, 7)]
+    for k, coo in enumerate(mats):
+        Bp, Bj, Bx = oracle.coo2csr(m.node_num, *coo)
+        assert np.array_equal(Bp, g[f"{etype}_m{k}_p"]) and np.array_equal(Bj, g[f"{etype}_m{k}_j"])
+        assert np.array_equal(Bx, g[f"{etype}_m{k}_x"])
+    assert np.array_equal(oracle.mass_lumped(m, rho), g[f"{etype}_lump"])
+    assert np.array_equal(oracle.abc_mpml(m, 1, 1, 10.0, (0.0, 50.0, 0.0, 40.0), 3100.0), g[f"{etype}_mpml"])
+
+
+def test_runs_match_golden_fixture(oracle):
+    g = np.load(os.path.join(GOLD, "runs_small.npz"))
+    for t, n, step, dt, pml, seed in [("Q4", 16, 262, 1e-3, 4, 7), ("T3", 16, 262, 1e-3, 4, 8), ("Q9", 8, 262, 5e-4, 2, 9)]:
+        p = small_problem(t, n=n, step=step, pml=pml, seed=seed, dt=dt)
+        r = oracle.run(p)
+        for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+            assert np.array_equal(r[k], g[f"{t}_{n}_{k}"]), (t, k)
+
+
+@pytest.mark.parametrize("etype", ["T3", "T6", "Q4", "Q9"])
+def test_oracle_bit_exact_against_reference_build(oracle, reference, etype):
+    m = structured_mesh(etype, 6, 5, 0.0, 60.0, 0.0, 50.0)
+    rho = 2000.0 + 50.0 * np.cos(np.arange(m.node_num))
+    for a, b in zip(oracle.mass_coo(m, rho), reference.mass(m, rho, 0)):
+        assert np.array_equal(a, b)
+    assert np.array_equal(oracle.mass_lumped(m, rho), reference.mass(m, rho, 1))
+    for k in range(7):
+        a, b = oracle.stif_coo(m, k), reference.stif(m, k)
+        for u, v in zip(a, b):
+            assert np.array_equal(u, v)
+    for use in [(1, 1, 1, 1), (1, 0, 1, 1)]:
+        bounds = (m.xmin, m.xmax, m.ymin, m.ymax)
+        assert np.array_equal(oracle.abc_mpml(m, 2, 2, 10.0, bounds, 2500.0, use),
+                              reference.abc_mpml(m, 2, 2, 10.0, bounds, 2500.0, use))
+    en, x, y = reference.mesh(etype, 6, 5, 0.0, 60.0, 0.0, 50.0)
+    assert np.array_equal(en, m.element_node) and np.array_equal(x, m.x) and np.array_equal(y, m.y)
+
+
+def test_full_run_bit_exact_against_reference_build(oracle, reference):
+    p = small_problem("Q4", n=14, step=150, pml=3, seed=21, shots=2)
+    a, b = oracle.run(p), reference.run(p)
+    assert a["status"] == b["status"] == 0
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_blowup_status_matches_reference(oracle, reference):
+    p = small_problem("T6", n=8, step=200, pml=2, seed=7)
+    assert oracle.run(p)["status"] == reference.run(p)["status"] == 1
+
+
+def test_ricker_and_node_location(oracle):
+    assert oracle.ricker(25.0, 0.0, 1e10, 0.0) == 1e10
+    a = (np.pi * 25.0 * 0.01) ** 2
+    assert abs(oracle.ricker(25.0, 0.0, 1e10, 0.01) - 1e10 * (1 - 2 * a) * np.exp(-a)) < 1e-3
+    m = structured_mesh("Q4", 4, 4, 0.0, 40.0, 0.0, 40.0)
+    # exactly half-way between two nodes: both within edge/2, the last wins
+    assert oracle.node_location(m, 10.0, 15.0, 20.0) == 12
+    assert oracle.node_location(m, 10.0, 500.0, 20.0) == -1
+
+
+@pytest.mark.parametrize("etype", ["T3", "T6", "Q4", "Q9"])
+def test_matrix_properties(oracle, etype):
+    m = structured_mesh(etype, 5, 3, 0.0, 50.0, 0.0, 30.0)
+    N = m.node_num
+    import scipy.sparse as sp
+    def csr(coo):
+        Bp, Bj, Bx = oracle.coo2csr(N, *coo)
+        return sp.csr_matrix((Bx, Bj, Bp), shape=(N, N))
+    M = csr(oracle.mass_coo(m, np.ones(N)))
+    assert abs(M.sum() - 50.0 * 30.0) < 1e-9          # sum of M_geo = area
+    assert abs(M - M.T).max() < 1e-12                  # symmetric
+    K = {k: csr(oracle.stif_coo(m, k)) for k in range(1, 7)}
+    one = np.ones(N)
+    for k in (1, 2, 3, 4):
+        assert np.abs(K[k] @ one).max() < 1e-9         # derivative of a constant
+    assert abs(K[1] - K[1].T).max() < 1e-12 and abs(K[2] - K[2].T).max() < 1e-12
+    assert abs(K[3] - K[4].T).max() < 1e-12
+
+
+def test_example2_snapshots(oracle):
+    """EXAMPLE/example2 (Q4 200x200, h=5, built-in homogeneous model, 1200
+    steps): a smoke check.  The committed snapshots come from an earlier,
+    unknown revision of the reference (the current sources, compiled here,
+    agree with this oracle bit for bit; the committed file differs from both
+    most near the source), so only the wavefield's structure is compared:
+    first snapshot correlation > 0.99, peak amplitude within 5%."""
+    g = np.load(os.path.join(GOLD, "examples.npz"))
+    mesh = structured_mesh("Q4", 200, 200, 0.0, 1000.0, 0.0, 1000.0)
+    N = mesh.node_num
+    # model_elastic_parameter.c:34-45
+    model = isotropic_model(np.full(N, 2000.0), np.full(N, 1154.7), np.full(N, 2200.0))
+    src = locate(mesh, 5.0, [(500.0, 500.0)])
+    rec = locate(mesh, 5.0, line_points(201, (0.0, 0.0), (1000.0, 0.0)))
+    p = Problem(mesh, model, 1200, 0.0005, 15.0, 0.0, 5.0, 20, 20, src, rec, 0)
+    r = oracle.run(p)
+    idx = g["ex2_nodes"]
+    assert r["snap_u"].shape[1] == g["ex2_snap_u"].shape[0] == 7
+    for comp in ("snap_u", "snap_w"):
+        a, b = r[comp][0][1, idx], g["ex2_" + comp][1]
+        assert np.corrcoef(a, b)[0, 1] > 0.99
+        assert abs(np.abs(a).max() / np.abs(b).max() - 1) < 0.05
+    assert np.all(r["seis_u"] == 0)     # receivers on the Dirichlet edge y = 0
+
+
+def test_example6_free_surface_seismograms(oracle):
+    """EXAMPLE/example6 (unstructured T3 mesh, free surface at x = xmax,
+    velocity file model): the reference's committed seismograms, reproduced
+    to their printing precision (%f: 5e-7)."""
+    g = np.load(os.path.join(GOLD, "examples.npz"))
+    mesh = Mesh("T3", g["ex6_element_node"], g["ex6_x"], g["ex6_y"])
+    from seisfem_b200.problem import mesh_bounds_from_nodes
+    mesh_bounds_from_nodes(mesh)
+    N = mesh.node_num
+    # EXAMPLE/example6_surface_wave/mesh/get_velocity_file.c values
+    c = np.stack([np.full(N, 8800000000.0), np.full(N, 2933338804.0), np.full(N, 8800000000.0),
+                  np.full(N, 2933330598.0)])
+    model = Model(np.full(N, 2200.0), np.full(N, 2000.0), np.full(N, 1154.7), c)
+    src = locate(mesh, 5.0, [(500.0, 500.0)])
+    rec = locate(mesh, 5.0, line_points(81, (500.0, 100.0), (500.0, 900.0)))
+    p = Problem(mesh, model, 1200, 0.0005, 10.0, 0.0, 5.0, 20, 20, src, rec, 1)
+    r = oracle.run(p)
+    su = r["seis_u"][0][::10]
+    gu = g["ex6_seis_u"]
+    assert su.shape == gu.shape
+    assert np.abs(su - gu).max() <= 6e-7
+    assert np.abs(r["seis_w"][0][::10] - g["ex6_seis_w"]).max() <= 6e-7
