@@ -34,7 +34,7 @@ from seisfem_b200 import problem as P  # noqa: E402
 
 METRIC = "DOF-steps/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.txt")
 
 
 def workload(name: str, rank: int = 0):
@@ -257,9 +257,7 @@ def main():
     achieved = b_step / (kms * 1e-3) / 1e9
     traffic = None
     if os.path.exists(TRAFFIC_FILE):
-        tj = json.load(open(TRAFFIC_FILE)).get(f"{args.workload}:{args.precision}")
-        if tj:
-            traffic = tj.get("bytes_per_launch")
+        traffic = read_traffic(TRAFFIC_FILE, f"{args.workload}:{args.precision}")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": "stepA/stepZ fused step (SpMV + RHS + lumped solve + Newmark), both classes",
@@ -338,6 +336,16 @@ def main():
         dist.destroy_process_group()
     ctx.close()
     return 0
+
+
+def read_traffic(path, key):
+    """DRAM bytes per time step (dram__bytes_read.sum + dram__bytes_write.sum of
+    the step's kernels) from the ncu summary table: lines `key bytes ...`."""
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 2 and f[0] == key:
+            return int(f[1])
+    return None
 
 
 def step_bytes(ctx, prob, S) -> int:
