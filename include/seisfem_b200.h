@@ -39,6 +39,7 @@ extern "C" {
 #define SFG_ERR_STATE 8       /* call out of order (run before setup, ...) */
 #define SFG_ERR_TIMEOUT 9     /* a bounded device-side wait gave up */
 #define SFG_ERR_NODEVICE 10   /* no CUDA device / wrong architecture */
+#define SFG_ERR_LIMIT 11      /* size above the fixed limit of a no-allocation entry point */
 
 /* ------------------------------------------------------------- precision */
 #define SFG_FP32_KAHAN 0      /* FP32 step, Kahan-compensated displacement (default) */
@@ -188,6 +189,34 @@ int sfg_abc_mpml(int node_num, int element_num, int element_order, int *element_
                  double *mpml_dxx, double *mpml_dyy, double *mpml_dxx_pyx, double *mpml_dyy_pxy);
 /* sparse_matrix/csr_matvec.c:1 (FP64, same per-row summation order) */
 int sfg_csr_matvec(int Bp_size, int *Bp, int *Bj, double *Bx, double *x, double *y);
+
+/* ------------------------------------------------ no-allocation entry point */
+/* No counterpart in the reference.  The M-PML profiles of sfg_abc_mpml
+ * (pml/abc_mpml.c:1-201, bit-identical results) for node arrays that are
+ * already on the device, computed without allocating device memory: for
+ * callers that must not call cudaMalloc/cudaFree while other work runs (both
+ * synchronise the whole device), e.g. an inversion loop that recomputes the
+ * profiles for each new velocity model next to streams that are stepping.
+ *
+ * d_element_node (1-based), d_x, d_y: device arrays; d_out6: device
+ * [6][node_num] = dx, dy, dxx, dyy, dxx*pyx, dyy*pxy; nodes of no element keep
+ * their values.  The work runs on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) and the call returns after it has finished.
+ *
+ * Scratch: a fixed device array of SFG_NOALLOC_MAX_NODES + 256 bytes inside
+ * the library; the call clears what it uses itself, so nothing has to start
+ * at zero.  node_num above SFG_NOALLOC_MAX_NODES returns SFG_ERR_LIMIT.
+ * The first call on each device looks up the scratch address; make it
+ * before any stream capture.  Calls that overlap in time on one device (two
+ * host threads, or two streams) share the scratch and race: serialise them.
+ * Returns SFG_ERR_BADINDEX when an element_node entry is outside
+ * 1..node_num (those entries are skipped). */
+#define SFG_NOALLOC_MAX_NODES (1 << 22)
+int sfg_abc_mpml_device_noalloc(int node_num, int element_num, int element_order, const int *d_element_node,
+                                const double *d_x, const double *d_y, int mpml_nx, int mpml_ny, double h,
+                                double xmin, double xmax, double ymin, double ymax, double vp_max,
+                                int use_mpml_xmin, int use_mpml_xmax, int use_mpml_ymin, int use_mpml_ymax,
+                                double *d_out6, void *stream);
 
 #ifdef __cplusplus
 }

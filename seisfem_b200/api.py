@@ -62,7 +62,8 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_csr_copy", "sfg_lumped_mass_copy", "sfg_lumped_mass_set", "sfg_union_copy", "sfg_mpml_copy", "sfg_run", "sfg_snapshot_rows",
            "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
-           "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec"]
+           "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec",
+           "sfg_abc_mpml_device_noalloc"]
 
 
 def lib(path: str = LIBPATH):

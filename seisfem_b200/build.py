@@ -26,6 +26,7 @@ UNITS = {
     "sfg_step32.cu": [],
     "sfg_api.cu": [],
     "sfg_seams.cu": ["-fmad=false"],
+    "sfg_noalloc.cu": ["-fmad=false"],
 }
 
 

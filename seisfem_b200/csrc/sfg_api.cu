@@ -63,7 +63,8 @@ namespace {
 
 const char *kStatus[] = {"ok", "bad argument", "CUDA error", "device out of memory", "zero-area element",
                          "index out of range", "energy bound exceeded", "row too long",
-                         "call out of order", "device wait timed out", "no usable CUDA device"};
+                         "call out of order", "device wait timed out", "no usable CUDA device",
+                         "size above the fixed limit of a no-allocation entry point"};
 
 int fail(sfg_ctx *c, int code, const std::string &msg)
 {
@@ -122,7 +123,7 @@ extern "C" {
 
 const char *sfg_error_string(int s)
 {
-    return (s >= 0 && s <= 10) ? kStatus[s] : "unknown status";
+    return (s >= 0 && s <= 11) ? kStatus[s] : "unknown status";
 }
 
 const char *sfg_last_error(const sfg_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }

@@ -11,6 +11,7 @@
 
 #include "sfg_elem.cuh"
 #include "sfg_internal.h"
+#include "sfg_mpml.cuh"
 
 namespace sfg {
 
@@ -333,62 +334,9 @@ __global__ void mpml_kernel(int N, const double *__restrict__ xa, const double *
     if (p >= N) return;
     const double pxy = 0.15, pyx = 0.15;
     double vdx = 0.0, vdy = 0.0, vdxx = 0.0, vdyy = 0.0;
-    if (row_start == nullptr || row_start[p + 1] > row_start[p]) {
-        double X = xa[p], Y = ya[p];
-        if (X <= x0 && Y >= y0 && Y <= y1 && uxmin == 1) {
-            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
-            vdy = pyx * vdx;
-            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
-            vdyy = 0.0;
-        } else if (X >= x1 && Y >= y0 && Y <= y1 && uxmax == 1) {
-            vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx);
-            vdy = pyx * vdx;
-            vdxx = d0x * 2 * (X - x1) / (tx * tx);
-            vdyy = 0.0;
-        } else if (Y <= y0 && X >= x0 && X <= x1 && uymin == 1) {
-            vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
-            vdx = pxy * vdy;
-            vdxx = 0.0;
-            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
-        } else if (Y >= y1 && X >= x0 && X <= x1 && uymax == 1) {
-            vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
-            vdx = pxy * vdy;
-            vdxx = 0.0;
-            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
-        } else if (X <= x0 && Y <= y0 && (uxmin == 1 || uymin == 1)) {
-            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx) + pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
-            vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty) + pyx * d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
-            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
-            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
-        } else if (X <= x0 && Y >= y1 && (uxmin == 1 || uymax == 1)) {
-            vdx = d0x * ((x0 - X) / tx) * ((x0 - X) / tx) + pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
-            vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty) + pyx * d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
-            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
-            vdxx = -d0x * 2 * (x0 - X) / (tx * tx);
-        } else if (X >= x1 && Y <= y0 && (uxmax == 1 || uymin == 1)) {
-            if (uymax == 1) {   // the reference tests ymax here (abc_mpml.c:147)
-                vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx) + pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
-                vdxx = d0x * 2 * (X - x1) / (tx * tx);
-                vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty) + pyx * d0x * ((X - x1) / tx) * ((X - x1) / tx);
-            } else {
-                vdx = pxy * d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
-                vdxx = 0.0;
-                vdy = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
-            }
-            vdyy = -d0y * 2 * (y0 - Y) / (ty * ty);
-        } else if (X >= x1 && Y >= y1 && (uxmax == 1 || uymax == 1)) {
-            if (uymax == 1) {
-                vdx = d0x * ((X - x1) / tx) * ((X - x1) / tx) + pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
-                vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty) + pyx * d0x * ((X - x1) / tx) * ((X - x1) / tx);
-                vdxx = d0x * 2 * (X - x1) / (tx * tx);
-            } else {
-                vdx = pxy * d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
-                vdy = d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
-                vdxx = 0.0;
-            }
-            vdyy = d0y * 2 * (Y - y1) / (ty * ty);
-        }
-    }
+    if (row_start == nullptr || row_start[p + 1] > row_start[p])
+        mpml_profile(xa[p], ya[p], d0x, d0y, tx, ty, x0, x1, y0, y1, uxmin, uxmax, uymin, uymax, vdx, vdy, vdxx,
+                     vdyy);
     out[p] = vdx;
     out[(size_t)N + p] = vdy;
     out[2 * (size_t)N + p] = vdxx;
