@@ -44,6 +44,9 @@ def workload(name: str, rank: int = 0):
         p = P.config_1()
     elif name == "q4_400_grf_64shots":
         p = P.config_3a()
+    elif name == "q4_200_grf_64shots":
+        # the batched kernels on a smaller mesh (profiling case; state > L2)
+        p = P.config_3a(n=200, step=500)
     else:
         raise SystemExit(f"unknown workload {name}")
     if rank and len(p.src_node) == 1:

@@ -512,7 +512,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             launches++;
         } else {
             Step2 a;
-            a.c = c; a.na = P.na;
+            a.c = c; a.na = P.na; a.S = S;
             a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
             a.up = P.upp; a.rec = P.recp; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
             a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
@@ -640,12 +640,20 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
         slot = kahan ? &ctx->tune.threads_fp32k : &ctx->tune.threads_fp32;
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
     } else {
-        int si = pl.spl == 1 ? 0 : (pl.spl == 2 ? 1 : 2);
+        // (shots per lane, warps per block), encoded spl * 16 + warps
+        int si = pl.S == 32 ? 0 : (pl.S == 64 ? 1 : 2);
         slot = &ctx->tune.warps_b[si][kahan ? 1 : 0];
-        cand = {2, 4, 8};
+        for (int spl : {1, 2, 4})
+            if (pl.S % (32 * spl) == 0)
+                for (int w : {4, 8})
+                    if (w % (pl.S / (32 * spl)) == 0) cand.push_back(spl * 16 + w);
     }
+    auto apply = [&](LoopPlan &q, int cnd) {
+        if (pl.S == 1) q.threads = cnd;
+        else { q.spl = cnd >> 4; q.warps = cnd & 15; }
+    };
     if (*slot > 0) {   // cached choice, stored + 1
-        if (pl.S == 1) pl.threads = *slot - 1; else pl.warps = *slot - 1;
+        apply(pl, *slot - 1);
         return SFG_OK;
     }
     cudaStream_t st = ctx->stream;
@@ -659,7 +667,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     int pick = cand[0];
     for (int cnd : cand) {
         LoopPlan q = pl;
-        if (pl.S == 1) q.threads = cnd; else q.warps = cnd;
+        apply(q, cnd);
         if (queue_loop(ctx, q, &r2, b, 0, 0, 2, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune warm-up");
         CK(cudaEventRecord(e0, st));
         if (queue_loop(ctx, q, &r2, b, 0, 0, probe, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune launch");
@@ -672,7 +680,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *slot = pick + 1;
-    if (pl.S == 1) pl.threads = pick; else pl.warps = pick;
+    apply(pl, pick);
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
         g_tuned[{ctx->device, ctx->N, ctx->P.na, ctx->P.type_code, ctx->P.union_nnz}] = ctx->tune;
@@ -776,7 +784,7 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     if (e == cudaSuccess) e = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     if ((rc = autotune(ctx, pl, &p->run, p->b)) != SFG_OK) { plan_free(p); return rc; }
-    ctx->stats.rows_per_block = pl.S == 1 ? pl.threads : pl.warps;
+    ctx->stats.rows_per_block = pl.S == 1 ? pl.threads : pl.warps * 16 + pl.spl;
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     cudaError_t er = queue_reset(pl, N, run->step, p->nsnap, p->b, st);

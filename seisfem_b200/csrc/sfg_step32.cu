@@ -371,38 +371,87 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
 
 // --------------------------------------------------------- batched kernels
 
-// Per-shot energies of a block, one atomic pair per shot.
-template <int SPL>
-__device__ __forceinline__ void block_energy_shots(const StepCommon &c, const float *eu, const float *ew)
+// Per-shot energies: each block sums its rows in shared memory, then adds
+// one pair per shot to the step's global sums.
+__device__ __forceinline__ void energy_zero(float *se, int S)
 {
-    constexpr int S = 32 * SPL;
-    __shared__ float se[8][2][S];
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5, s_base = (threadIdx.x & 31) * SPL;
+    for (int t = threadIdx.x; t < 2 * S; t += blockDim.x) se[t] = 0.f;
+    __syncthreads();
+}
+
+template <int SPL>
+__device__ __forceinline__ void energy_flush(const StepCommon &c, float *se, int S, int s_base, const float *eu,
+                                             const float *ew)
+{
 #pragma unroll
-    for (int q = 0; q < SPL; q++) { se[w][0][s_base + q] = eu[q]; se[w][1][s_base + q] = ew[q]; }
+    for (int q = 0; q < SPL; q++) {
+        if (eu[q] != 0.f) atomicAdd(se + s_base + q, eu[q]);
+        if (ew[q] != 0.f) atomicAdd(se + S + s_base + q, ew[q]);
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < 2 * S; t += blockDim.x) {
         const int comp = t / S, s = t - comp * S;
-        double acc = 0.0;
-        for (int k = 0; k < nw; k++) acc += se[k][comp][s];
-        if (s < c.nshot && acc != 0.0) atomicAdd(c.energy + ((size_t)s * c.nsteps + c.it) * 2 + comp, acc);
+        const float v = se[t];
+        if (s < c.nshot && v != 0.f) atomicAdd(c.energy + ((size_t)s * c.nsteps + c.it) * 2 + comp, (double)v);
     }
 }
 
-// One warp per row, S = 32*SPL shots with the shot index innermost.  The
-// row's records (column + matrix values, 32 B each) are loaded once by the
-// warp, one per lane, and broadcast with shuffles; every matrix entry is
-// applied to all S shots.
-template <bool COMP, int SPL>
-__global__ void __launch_bounds__(256) stepA_batched(const Step2 a)
+// Batched kernels: S shots with the shot index innermost ([node][value][S]).
+// A warp advances one row for a chunk of 32*SPL shots (SPL per lane); the
+// S/(32*SPL) chunks of a row go to neighbouring warps of the same block, so
+// the row's matrix records and its neighbours' state are shared through L1.
+// The grid is persistent and its warp count a multiple of the chunk count,
+// so every warp keeps one chunk.  The row's records (column + matrix values,
+// 32 B) are loaded once per warp, one per lane, and broadcast with shuffles;
+// neighbour records of two entries are loaded before either is applied.
+struct Entry {
+    int j;
+    float vm, k[6];
+};
+
+template <int NK>
+__device__ __forceinline__ Entry entry_at(const float4 &r0, const float4 &r1, int k)
 {
-    constexpr int S = 32 * SPL;
+    Entry e;
+    e.j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), k);
+    e.vm = __shfl_sync(0xffffffffu, r0.y, k);
+    e.k[0] = __shfl_sync(0xffffffffu, r0.z, k);
+    e.k[1] = __shfl_sync(0xffffffffu, r0.w, k);
+    e.k[2] = __shfl_sync(0xffffffffu, r1.x, k);
+    e.k[3] = __shfl_sync(0xffffffffu, r1.y, k);
+    if (NK == 6) {
+        e.k[4] = __shfl_sync(0xffffffffu, r1.z, k);
+        e.k[5] = __shfl_sync(0xffffffffu, r1.w, k);
+    }
+    return e;
+}
+
+// K1..K4 times U, W and M times Lx1..4, Ly1..4 of one neighbour record x[10].
+template <int SPL>
+__device__ __forceinline__ void acc_totals(const Entry &e, const VecF<SPL> *x, float (*kU)[SPL], float (*kW)[SPL],
+                                           float (*mL)[SPL])
+{
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
+#pragma unroll
+        for (int t = 0; t < 8; t++) mL[t][q] += e.vm * x[2 + t].v[q];
+    }
+}
+
+template <bool COMP, int SPL>
+__global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_batched(const Step2 a)
+{
+    extern __shared__ float se[];   // [2][S]
     const StepCommon &c = a.c;
+    const int S = a.S, nch = S / (32 * SPL);
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
-    const int warps_total = (gridDim.x * blockDim.x) >> 5;
-    const int s_base = lane * SPL;
+    if (c.energy) energy_zero(se, S);
+    const int warp = gtid >> 5, warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int s_base = (warp % nch) * 32 * SPL + lane * SPL;
     int src[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
@@ -412,7 +461,9 @@ __global__ void __launch_bounds__(256) stepA_batched(const Step2 a)
 #pragma unroll
     for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
     const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
-    for (int i = gtid >> 5; i < a.na; i += warps_total) {
+    const long long tasks = (long long)a.na * nch;
+    for (long long task = warp; task < tasks; task += warps_total) {
+        const int i = (int)(task / nch);
         float kU[4][SPL], kW[4][SPL], mL[8][SPL];
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
@@ -426,23 +477,24 @@ __global__ void __launch_bounds__(256) stepA_batched(const Step2 a)
             const int cnt = min(32, e1 - base);
             float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
             if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
-            for (int k = 0; k < cnt; k++) {
-                const int j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), k);
-                const float vm = __shfl_sync(0xffffffffu, r0.y, k);
-                const float k1 = __shfl_sync(0xffffffffu, r0.z, k), k2 = __shfl_sync(0xffffffffu, r0.w, k);
-                const float k3 = __shfl_sync(0xffffffffu, r1.x, k), k4 = __shfl_sync(0xffffffffu, r1.y, k);
-                const float kv[4] = {k1, k2, k3, k4};
-                const float *gj = a.in.Gc + (size_t)j * GC * S + s_base;
-                VecF<SPL> x[10];
+            int k = 0;
+            for (; k + 1 < cnt; k += 2) {
+                const Entry ea = entry_at<4>(r0, r1, k), eb = entry_at<4>(r0, r1, k + 1);
+                const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
+                const float *gb = a.in.Gc + (size_t)eb.j * GC * S + s_base;
+                VecF<SPL> xa[10], xb[10];
 #pragma unroll
-                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
+                for (int v = 0; v < 10; v++) { xa[v].load(ga + v * S); xb[v].load(gb + v * S); }
+                acc_totals<SPL>(ea, xa, kU, kW, mL);
+                acc_totals<SPL>(eb, xb, kU, kW, mL);
+            }
+            if (k < cnt) {
+                const Entry ea = entry_at<4>(r0, r1, k);
+                const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
+                VecF<SPL> xa[10];
 #pragma unroll
-                for (int q = 0; q < SPL; q++) {
-#pragma unroll
-                    for (int t = 0; t < 4; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
-#pragma unroll
-                    for (int t = 0; t < 8; t++) mL[t][q] += vm * x[2 + t].v[q];
-                }
+                for (int v = 0; v < 10; v++) xa[v].load(ga + v * S);
+                acc_totals<SPL>(ea, xa, kU, kW, mL);
             }
         }
         const float4 cf = __ldg(a.coefA + i);
@@ -483,18 +535,90 @@ __global__ void __launch_bounds__(256) stepA_batched(const Step2 a)
 #pragma unroll
         for (int v = 0; v < PA; v++) pv[v].store(po + v * S);
     }
-    if (c.energy) block_energy_shots<SPL>(c, eu, ew);
+    if (c.energy) energy_flush<SPL>(c, se, S, s_base, eu, ew);
+}
+
+// Split-zone products of one entry: K1..K6 times U, W (K5, K6 only on M-PML
+// rows), M times the split fields y[12] (M-PML rows) and M times Lx, Ly.
+template <int SPL, bool FULL>
+__device__ __forceinline__ void acc_split(const Entry &e, const VecF<SPL> *x, const VecF<SPL> *y, bool has_y,
+                                          float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
+{
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+#pragma unroll
+        for (int t = 0; t < (FULL ? 6 : 4); t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
+#pragma unroll
+        for (int t = 0; t < 8; t++) m[12 + t][q] += e.vm * x[2 + t].v[q];
+        if (FULL && has_y) {
+#pragma unroll
+            for (int t = 0; t < 12; t++) m[t][q] += e.vm * y[t].v[q];
+        }
+    }
+}
+
+template <int SPL, bool FULL>
+__device__ __forceinline__ void row_split(const Step2 &a, const float4 *rec, int e0, int e1, int lane, int s_base,
+                                          float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
+{
+    const int S = a.S;
+    for (int base = e0; base < e1; base += 32) {
+        const int cnt = min(32, e1 - base);
+        float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+        if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
+        int k = 0;
+        for (; k + 1 < cnt; k += 2) {
+            const Entry ea = entry_at<FULL ? 6 : 4>(r0, r1, k), eb = entry_at<FULL ? 6 : 4>(r0, r1, k + 1);
+            const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
+            const float *gb = a.in.Gc + (size_t)eb.j * GC * S + s_base;
+            VecF<SPL> xa[10], xb[10], ya[FULL ? 12 : 1], yb[FULL ? 12 : 1];
+#pragma unroll
+            for (int v = 0; v < 10; v++) { xa[v].load(ga + v * S); xb[v].load(gb + v * S); }
+            // M-PML rows reference class-Z columns only (set-up guarantees it)
+            const bool hya = FULL && ea.j >= a.na, hyb = FULL && eb.j >= a.na;
+            if (FULL) {
+                if (hya) {
+                    const float *sa = a.in.Gs + (size_t)(ea.j - a.na) * GS * S + s_base;
+#pragma unroll
+                    for (int v = 0; v < (FULL ? 12 : 1); v++) ya[v].load(sa + v * S);
+                }
+                if (hyb) {
+                    const float *sb = a.in.Gs + (size_t)(eb.j - a.na) * GS * S + s_base;
+#pragma unroll
+                    for (int v = 0; v < (FULL ? 12 : 1); v++) yb[v].load(sb + v * S);
+                }
+            }
+            acc_split<SPL, FULL>(ea, xa, ya, hya, kU, kW, m);
+            acc_split<SPL, FULL>(eb, xb, yb, hyb, kU, kW, m);
+        }
+        if (k < cnt) {
+            const Entry ea = entry_at<FULL ? 6 : 4>(r0, r1, k);
+            const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
+            VecF<SPL> xa[10], ya[FULL ? 12 : 1];
+#pragma unroll
+            for (int v = 0; v < 10; v++) xa[v].load(ga + v * S);
+            const bool hya = FULL && ea.j >= a.na;
+            if (FULL && hya) {
+                const float *sa = a.in.Gs + (size_t)(ea.j - a.na) * GS * S + s_base;
+#pragma unroll
+                for (int v = 0; v < (FULL ? 12 : 1); v++) ya[v].load(sa + v * S);
+            }
+            acc_split<SPL, FULL>(ea, xa, ya, hya, kU, kW, m);
+        }
+    }
 }
 
 template <bool COMP, int SPL>
-__global__ void __launch_bounds__(256) stepZ_batched(const Step2 a)
+__global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Step2 a)
 {
-    constexpr int S = 32 * SPL;
+    extern __shared__ float se[];   // [2][S]
     const StepCommon &c = a.c;
+    const int S = a.S, nch = S / (32 * SPL);
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int warps_total = (gridDim.x * blockDim.x) >> 5;
-    const int s_base = lane * SPL;
+    if (c.energy) energy_zero(se, S);
+    const int warp = gtid >> 5, warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int s_base = (warp % nch) * 32 * SPL + lane * SPL;
     int src[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
@@ -505,11 +629,12 @@ __global__ void __launch_bounds__(256) stepZ_batched(const Step2 a)
     for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
     const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
     const int nz = c.n - a.na;
-    for (int local = gtid >> 5; local < nz; local += warps_total) {
+    const long long tasks = (long long)nz * nch;
+    for (long long task = warp; task < tasks; task += warps_total) {
+        const int local = (int)(task / nch);
         const int i = a.na + local;
         const float4 *cfp = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
         const float4 c0 = __ldg(cfp), c1 = __ldg(cfp + 1), c2 = __ldg(cfp + 2);
-        const bool full = is_pml_row(c1);
         float kU[6][SPL], kW[6][SPL], m[20][SPL];
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
@@ -519,47 +644,8 @@ __global__ void __launch_bounds__(256) stepZ_batched(const Step2 a)
             for (int k = 0; k < 20; k++) m[k][q] = 0.f;
         }
         const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
-        for (int base = e0; base < e1; base += 32) {
-            const int cnt = min(32, e1 - base);
-            float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
-            if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
-            for (int k = 0; k < cnt; k++) {
-                const int j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), k);
-                const float vm = __shfl_sync(0xffffffffu, r0.y, k);
-                float kv[6];
-                kv[0] = __shfl_sync(0xffffffffu, r0.z, k); kv[1] = __shfl_sync(0xffffffffu, r0.w, k);
-                kv[2] = __shfl_sync(0xffffffffu, r1.x, k); kv[3] = __shfl_sync(0xffffffffu, r1.y, k);
-                kv[4] = __shfl_sync(0xffffffffu, r1.z, k); kv[5] = __shfl_sync(0xffffffffu, r1.w, k);
-                const float *gj = a.in.Gc + (size_t)j * GC * S + s_base;
-                VecF<SPL> x[10];
-#pragma unroll
-                for (int v = 0; v < 10; v++) x[v].load(gj + v * S);
-#pragma unroll
-                for (int q = 0; q < SPL; q++) {
-#pragma unroll
-                    for (int t = 0; t < 4; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
-#pragma unroll
-                    for (int t = 0; t < 8; t++) m[12 + t][q] += vm * x[2 + t].v[q];
-                }
-                if (full) {
-#pragma unroll
-                    for (int q = 0; q < SPL; q++)
-#pragma unroll
-                        for (int t = 4; t < 6; t++) { kU[t][q] += kv[t] * x[0].v[q]; kW[t][q] += kv[t] * x[1].v[q]; }
-                    // M-PML rows reference class-Z columns only (set-up guarantees it)
-                    if (j >= a.na) {
-                        const float *sj = a.in.Gs + (size_t)(j - a.na) * GS * S + s_base;
-                        VecF<SPL> y[12];
-#pragma unroll
-                        for (int v = 0; v < 12; v++) y[v].load(sj + v * S);
-#pragma unroll
-                        for (int q = 0; q < SPL; q++)
-#pragma unroll
-                            for (int t = 0; t < 12; t++) m[t][q] += vm * y[t].v[q];
-                    }
-                }
-            }
-        }
+        if (is_pml_row(c1)) row_split<SPL, true>(a, rec, e0, e1, lane, s_base, kU, kW, m);
+        else row_split<SPL, false>(a, rec, e0, e1, lane, s_base, kU, kW, m);
         const float *si = a.in.Gs + (size_t)local * GS * S + s_base;
         const float *pi = a.in.Ps + (size_t)local * PS * S + s_base;
         float *gco = a.out.Gc + (size_t)i * GC * S + s_base;
@@ -595,7 +681,7 @@ __global__ void __launch_bounds__(256) stepZ_batched(const Step2 a)
 #pragma unroll
         for (int v = 0; v < PS; v++) pv[v].store(po + v * S);
     }
-    if (c.energy) block_energy_shots<SPL>(c, eu, ew);
+    if (c.energy) energy_flush<SPL>(c, se, S, s_base, eu, ew);
 }
 
 // --------------------------------------------------- gathers, snapshots
@@ -733,30 +819,39 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
 #undef SFG_SHAPES
 
 template <typename K>
-static long long batched_grid(K kernel, int threads, long long rows, int warps)
+static long long batched_grid(K kernel, int threads, long long tasks, int warps, size_t smem)
 {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (per_sm < 1) per_sm = 1;
-    const long long need = (rows + warps - 1) / warps;
+    const long long need = (tasks + warps - 1) / warps;
     return std::max<long long>(1, std::min<long long>((long long)sms * per_sm, need));
 }
 
+#define SFG_BATCH_ONE(KERNEL, C, P, ROWS)                                                                \
+    do {                                                                                                 \
+        auto k = KERNEL<C, P>;                                                                           \
+        const long long tasks = (long long)(ROWS) * (a.S / (32 * (P)));                                  \
+        KERNEL<C, P><<<(unsigned)batched_grid(k, threads, tasks, warps, smem), threads, smem, st>>>(a);  \
+    } while (0)
 #define SFG_BATCH(KERNEL, ROWS)                                                                          \
     do {                                                                                                 \
         const int threads = 32 * warps;                                                                  \
-        if (warps < 1 || warps > 8) return cudaErrorInvalidValue;                                        \
+        const size_t smem = sizeof(float) * 2 * (size_t)a.S;                                             \
+        if (warps < 1 || warps > 8 || (spl != 1 && spl != 2 && spl != 4)) return cudaErrorInvalidValue;  \
+        if (a.S < 32 * spl || a.S % (32 * spl) != 0 || warps % (a.S / (32 * spl)) != 0)                  \
+            return cudaErrorInvalidValue;                                                                \
         if ((ROWS) <= 0) return cudaSuccess;                                                             \
         if (comp) {                                                                                      \
-            if (spl == 1) { auto k = KERNEL<true, 1>; KERNEL<true, 1><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
-            else if (spl == 2) { auto k = KERNEL<true, 2>; KERNEL<true, 2><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
-            else { auto k = KERNEL<true, 4>; KERNEL<true, 4><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            if (spl == 1) SFG_BATCH_ONE(KERNEL, true, 1, ROWS);                                          \
+            else if (spl == 2) SFG_BATCH_ONE(KERNEL, true, 2, ROWS);                                     \
+            else SFG_BATCH_ONE(KERNEL, true, 4, ROWS);                                                   \
         } else {                                                                                         \
-            if (spl == 1) { auto k = KERNEL<false, 1>; KERNEL<false, 1><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
-            else if (spl == 2) { auto k = KERNEL<false, 2>; KERNEL<false, 2><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
-            else { auto k = KERNEL<false, 4>; KERNEL<false, 4><<<(unsigned)batched_grid(k, threads, ROWS, warps), threads, 0, st>>>(a); } \
+            if (spl == 1) SFG_BATCH_ONE(KERNEL, false, 1, ROWS);                                         \
+            else if (spl == 2) SFG_BATCH_ONE(KERNEL, false, 2, ROWS);                                    \
+            else SFG_BATCH_ONE(KERNEL, false, 4, ROWS);                                                  \
         }                                                                                                \
     } while (0)
 
@@ -773,6 +868,7 @@ cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, 
     return cudaGetLastError();
 }
 #undef SFG_BATCH
+#undef SFG_BATCH_ONE
 
 cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st)
 {

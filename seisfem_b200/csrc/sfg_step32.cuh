@@ -44,6 +44,7 @@ struct State32W {
 struct Step2 {
     StepCommon c;              // c.n = all rows; src / rec in the permuted numbering
     int na;                    // class-A rows [0, na); class Z [na, n)
+    int S;                     // shots of the batch: the state's innermost stride
     const float *sellA;        // SELL-32 over rows [0, na): planes col, M, K1..K4
     const int *sliceA;
     const float *sellZ;        // SELL-32 over rows [na, n): planes col, M, K1..K6
@@ -61,7 +62,8 @@ struct Step2 {
 int step2_variants();
 cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st);
 cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st);
-// S = 32 * spl shots (warp per row)
+// S = a.S shots, a multiple of 32 * spl; a warp advances 32 * spl shots of
+// one row (spl per lane); warps per block a multiple of S / (32 * spl)
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
 cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
 // receiver gather of a finished state; snapshots scattered back to mesh order
