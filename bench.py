@@ -331,7 +331,7 @@ def main():
                            "parallelism": f"shots over {world} GPU(s)"},
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches,
-                "launch_shape": st["rows_per_block"],
+                "launch_shape": launch_shape(st["rows_per_block"], S),
                 "vs_plain_path": plain,
                 "energy_status": int(res["status"])}
         print(json.dumps(line), flush=True)
@@ -339,6 +339,15 @@ def main():
         dist.destroy_process_group()
     ctx.close()
     return 0
+
+
+def launch_shape(code, S):
+    """The autotuner's pick for the class-A / class-Z kernels."""
+    if S == 1:
+        return {"variant_A": code // 16, "variant_Z": code % 16}
+    a, z = code // 256, code % 256
+    return {"A": {"shots_per_lane": a >> 4, "warps_per_block": a & 15},
+            "Z": {"shots_per_lane": z >> 4, "warps_per_block": z & 15}}
 
 
 def read_traffic(path, key):

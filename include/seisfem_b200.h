@@ -94,8 +94,9 @@ typedef struct {
     long long union_nnz;       /* nonzeros of the union pattern the step kernel streams */
     long long csr_nnz[7];      /* nonzeros of M, K1..K6 after zero elimination */
     int kernel_launches;       /* kernels launched by the last run's time loop */
-    int rows_per_block;        /* launch shape the autotuner picked: threads per block (one
-                                  shot) or warps * 16 + shots per lane (batches) */
+    int rows_per_block;        /* launch shapes the autotuner picked for the class-A and
+                                  class-Z kernels: one shot: a * 16 + z (shape variants);
+                                  batches: a * 256 + z, each spl * 16 + warps per block */
     int blowup_step;           /* first step whose energy bound failed, -1 if none */
     int interior_rows;         /* nodes advanced as totals only (outside the M-PML zone) */
     int pml_rows;              /* rows with a non-zero M-PML profile */

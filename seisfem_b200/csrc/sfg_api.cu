@@ -21,9 +21,9 @@
 using namespace sfg;
 
 struct RunCache {
-    // launch shapes picked by the autotuner, keyed by kernel kind and shot count
-    int threads_fp32 = 0, threads_fp32k = 0;
-    int warps_b[3][2] = {{0, 0}, {0, 0}, {0, 0}};   // [spl index][kahan]
+    // launch shapes picked by the autotuner (stored + 1; 0 = not tuned):
+    // [shots: 1, 32, 64, 128][plain FP32, compensated][class A, class Z]
+    int shape[4][2][2] = {};
 };
 
 // Launch shapes already tuned in this process, keyed by the mesh signature
@@ -427,8 +427,10 @@ struct LoopPlan {
     int kind;            // SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH
     int S;               // shots advanced together (1, 32, 64, 128)
     int spl;             // shots per lane (batched)
-    int threads;         // single-shot launch shape (variant of launch_step32; FP64: threads)
-    int warps;           // batched launch shape
+    int threads;         // FP64 path: threads per block
+    int warps;           // (unused by the FP32 paths since shapes are per class)
+    int shapeA, shapeZ;  // FP32 launch shapes of the class-A / class-Z kernels: one shot:
+                         // variant of launch_stepA/Z; batches: spl * 16 + warps per block
 };
 
 // The fused FP32 kernels run in the two-class node numbering.
@@ -521,11 +523,11 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             // fork: the class-Z kernel on the second stream, class A here; join
             if (cudaEventRecord(ctx->ev_fork, st) != cudaSuccess) return -1;
             if (cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0) != cudaSuccess) return -1;
-            e = S == 1 ? launch_stepZ(a, comp, pl.threads, ctx->stream2)
-                       : launch_stepZ_batched(a, comp, pl.spl, pl.warps, ctx->stream2);
+            e = S == 1 ? launch_stepZ(a, comp, pl.shapeZ, ctx->stream2)
+                       : launch_stepZ_batched(a, comp, pl.shapeZ >> 4, pl.shapeZ & 15, ctx->stream2);
             if (e != cudaSuccess) return -1;
-            e = S == 1 ? launch_stepA(a, comp, pl.threads, st)
-                       : launch_stepA_batched(a, comp, pl.spl, pl.warps, st);
+            e = S == 1 ? launch_stepA(a, comp, pl.shapeA, st)
+                       : launch_stepA_batched(a, comp, pl.shapeA >> 4, pl.shapeA & 15, st);
             if (e != cudaSuccess) return -1;
             if (cudaEventRecord(ctx->ev_join, ctx->stream2) != cudaSuccess) return -1;
             if (cudaStreamWaitEvent(st, ctx->ev_join, 0) != cudaSuccess) return -1;
@@ -628,32 +630,28 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
     return e;
 }
 
-// Time a few steps of each candidate launch shape and keep the fastest
-// (state is reset afterwards by the caller).
+// Time a few steps of each candidate launch shape and keep the fastest:
+// first one shape for both class kernels, then the class-Z kernel's shape with
+// the class-A shape fixed (the two run concurrently, so the step time is the
+// objective).  The caller resets the state afterwards.
 int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
 {
     if (pl.kind == SFG_FP64 || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
-    const bool kahan = pl.kind == SFG_FP32_KAHAN;
-    int *slot;
+    const int kahan = pl.kind == SFG_FP32_KAHAN ? 1 : 0;
+    const int si = pl.S == 1 ? 0 : (pl.S == 32 ? 1 : (pl.S == 64 ? 2 : 3));
+    int *slot = ctx->tune.shape[si][kahan];
     std::vector<int> cand;
     if (pl.S == 1) {
-        slot = kahan ? &ctx->tune.threads_fp32k : &ctx->tune.threads_fp32;
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
     } else {
-        // (shots per lane, warps per block), encoded spl * 16 + warps
-        int si = pl.S == 32 ? 0 : (pl.S == 64 ? 1 : 2);
-        slot = &ctx->tune.warps_b[si][kahan ? 1 : 0];
         for (int spl : {1, 2, 4})
             if (pl.S % (32 * spl) == 0)
                 for (int w : {4, 8})
                     if (w % (pl.S / (32 * spl)) == 0) cand.push_back(spl * 16 + w);
     }
-    auto apply = [&](LoopPlan &q, int cnd) {
-        if (pl.S == 1) q.threads = cnd;
-        else { q.spl = cnd >> 4; q.warps = cnd & 15; }
-    };
-    if (*slot > 0) {   // cached choice, stored + 1
-        apply(pl, *slot - 1);
+    if (slot[0] > 0 && slot[1] > 0) {   // cached choice
+        pl.shapeA = slot[0] - 1;
+        pl.shapeZ = slot[1] - 1;
         return SFG_OK;
     }
     cudaStream_t st = ctx->stream;
@@ -663,24 +661,39 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int pick = cand[0];
-    for (int cnd : cand) {
+    auto time_shape = [&](int sa, int sz, float &ms) -> int {
         LoopPlan q = pl;
-        apply(q, cnd);
+        q.shapeA = sa;
+        q.shapeZ = sz;
         if (queue_loop(ctx, q, &r2, b, 0, 0, 2, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune warm-up");
         CK(cudaEventRecord(e0, st));
         if (queue_loop(ctx, q, &r2, b, 0, 0, probe, st) < 0) return fail(ctx, SFG_ERR_CUDA, "autotune launch");
         CK(cudaEventRecord(e1, st));
         CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) { best = ms; pick = cnd; }
+        return SFG_OK;
+    };
+    float best = 1e30f;
+    int pick_a = cand[0], pick_z = cand[0];
+    for (int cnd : cand) {
+        float ms = 0.f;
+        int rc = time_shape(cnd, cnd, ms);
+        if (rc) return rc;
+        if (ms < best) { best = ms; pick_a = cnd; pick_z = cnd; }
+    }
+    for (int cnd : cand) {
+        if (cnd == pick_a) continue;
+        float ms = 0.f;
+        int rc = time_shape(pick_a, cnd, ms);
+        if (rc) return rc;
+        if (ms < best) { best = ms; pick_z = cnd; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    *slot = pick + 1;
-    apply(pl, pick);
+    slot[0] = pick_a + 1;
+    slot[1] = pick_z + 1;
+    pl.shapeA = pick_a;
+    pl.shapeZ = pick_z;
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
         g_tuned[{ctx->device, ctx->N, ctx->P.na, ctx->P.type_code, ctx->P.union_nnz}] = ctx->tune;
@@ -758,7 +771,7 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     p->run.rec_node = p->rec.data();
     LoopPlan &pl = p->pl;
     pl.kind = run->precision;
-    pl.S = 1; pl.spl = 1; pl.threads = 128; pl.warps = 4;
+    pl.S = 1; pl.spl = 1; pl.threads = 128; pl.warps = 4; pl.shapeA = 0; pl.shapeZ = 0;
     const bool fp32 = pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN;
     int spb = run->shots_per_batch;
     if (fp32) {
@@ -784,7 +797,7 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     if (e == cudaSuccess) e = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     if ((rc = autotune(ctx, pl, &p->run, p->b)) != SFG_OK) { plan_free(p); return rc; }
-    ctx->stats.rows_per_block = pl.S == 1 ? pl.threads : pl.warps * 16 + pl.spl;
+    ctx->stats.rows_per_block = pl.S == 1 ? pl.shapeA * 16 + pl.shapeZ : pl.shapeA * 256 + pl.shapeZ;
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     cudaError_t er = queue_reset(pl, N, run->step, p->nsnap, p->b, st);

@@ -440,12 +440,12 @@ __device__ __forceinline__ void acc_totals(const Entry &e, const VecF<SPL> *x, f
     }
 }
 
-template <bool COMP, int SPL>
+template <bool COMP, int SPL, int S>
 __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_batched(const Step2 a)
 {
-    extern __shared__ float se[];   // [2][S]
+    __shared__ float se[2 * S];
     const StepCommon &c = a.c;
-    const int S = a.S, nch = S / (32 * SPL);
+    constexpr int nch = S / (32 * SPL);
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
@@ -540,80 +540,84 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
 
 // Split-zone products of one entry: K1..K6 times U, W (K5, K6 only on M-PML
 // rows), M times the split fields y[12] (M-PML rows) and M times Lx, Ly.
-template <int SPL, bool FULL>
-__device__ __forceinline__ void acc_split(const Entry &e, const VecF<SPL> *x, const VecF<SPL> *y, bool has_y,
-                                          float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
+template <int SPL>
+__device__ __forceinline__ void acc_split(const Entry &e, const VecF<SPL> *x, const VecF<SPL> *y, bool full,
+                                          bool has_y, float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
 {
 #pragma unroll
     for (int q = 0; q < SPL; q++) {
 #pragma unroll
-        for (int t = 0; t < (FULL ? 6 : 4); t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
+        for (int t = 0; t < 4; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
 #pragma unroll
         for (int t = 0; t < 8; t++) m[12 + t][q] += e.vm * x[2 + t].v[q];
-        if (FULL && has_y) {
+        if (full) {
 #pragma unroll
-            for (int t = 0; t < 12; t++) m[t][q] += e.vm * y[t].v[q];
+            for (int t = 4; t < 6; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
+            if (has_y) {
+#pragma unroll
+                for (int t = 0; t < 12; t++) m[t][q] += e.vm * y[t].v[q];
+            }
         }
     }
 }
 
-template <int SPL, bool FULL>
+// All entries of row-chunk: full = M-PML row (K5, K6 and the split fields of
+// its class-Z columns; M-PML rows reference class-Z columns only).
+template <int SPL, int S>
 __device__ __forceinline__ void row_split(const Step2 &a, const float4 *rec, int e0, int e1, int lane, int s_base,
-                                          float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
+                                          bool full, float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
 {
-    const int S = a.S;
     for (int base = e0; base < e1; base += 32) {
         const int cnt = min(32, e1 - base);
         float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
         if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
         int k = 0;
-        for (; k + 1 < cnt; k += 2) {
-            const Entry ea = entry_at<FULL ? 6 : 4>(r0, r1, k), eb = entry_at<FULL ? 6 : 4>(r0, r1, k + 1);
+        // two entries in flight with 64 shots per warp, one with 32
+        for (; SPL > 1 && k + 1 < cnt; k += 2) {
+            const Entry ea = entry_at<6>(r0, r1, k), eb = entry_at<6>(r0, r1, k + 1);
             const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
             const float *gb = a.in.Gc + (size_t)eb.j * GC * S + s_base;
-            VecF<SPL> xa[10], xb[10], ya[FULL ? 12 : 1], yb[FULL ? 12 : 1];
+            VecF<SPL> xa[10], xb[10], ya[12], yb[12];
 #pragma unroll
             for (int v = 0; v < 10; v++) { xa[v].load(ga + v * S); xb[v].load(gb + v * S); }
-            // M-PML rows reference class-Z columns only (set-up guarantees it)
-            const bool hya = FULL && ea.j >= a.na, hyb = FULL && eb.j >= a.na;
-            if (FULL) {
-                if (hya) {
-                    const float *sa = a.in.Gs + (size_t)(ea.j - a.na) * GS * S + s_base;
-#pragma unroll
-                    for (int v = 0; v < (FULL ? 12 : 1); v++) ya[v].load(sa + v * S);
-                }
-                if (hyb) {
-                    const float *sb = a.in.Gs + (size_t)(eb.j - a.na) * GS * S + s_base;
-#pragma unroll
-                    for (int v = 0; v < (FULL ? 12 : 1); v++) yb[v].load(sb + v * S);
-                }
-            }
-            acc_split<SPL, FULL>(ea, xa, ya, hya, kU, kW, m);
-            acc_split<SPL, FULL>(eb, xb, yb, hyb, kU, kW, m);
-        }
-        if (k < cnt) {
-            const Entry ea = entry_at<FULL ? 6 : 4>(r0, r1, k);
-            const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
-            VecF<SPL> xa[10], ya[FULL ? 12 : 1];
-#pragma unroll
-            for (int v = 0; v < 10; v++) xa[v].load(ga + v * S);
-            const bool hya = FULL && ea.j >= a.na;
-            if (FULL && hya) {
+            const bool hya = full && ea.j >= a.na, hyb = full && eb.j >= a.na;
+            if (hya) {
                 const float *sa = a.in.Gs + (size_t)(ea.j - a.na) * GS * S + s_base;
 #pragma unroll
-                for (int v = 0; v < (FULL ? 12 : 1); v++) ya[v].load(sa + v * S);
+                for (int v = 0; v < 12; v++) ya[v].load(sa + v * S);
             }
-            acc_split<SPL, FULL>(ea, xa, ya, hya, kU, kW, m);
+            if (hyb) {
+                const float *sb = a.in.Gs + (size_t)(eb.j - a.na) * GS * S + s_base;
+#pragma unroll
+                for (int v = 0; v < 12; v++) yb[v].load(sb + v * S);
+            }
+            acc_split<SPL>(ea, xa, ya, full, hya, kU, kW, m);
+            acc_split<SPL>(eb, xb, yb, full, hyb, kU, kW, m);
+        }
+#pragma unroll 1
+        for (; k < cnt; k++) {
+            const Entry ea = entry_at<6>(r0, r1, k);
+            const float *ga = a.in.Gc + (size_t)ea.j * GC * S + s_base;
+            VecF<SPL> xa[10], ya[12];
+#pragma unroll
+            for (int v = 0; v < 10; v++) xa[v].load(ga + v * S);
+            const bool hya = full && ea.j >= a.na;
+            if (hya) {
+                const float *sa = a.in.Gs + (size_t)(ea.j - a.na) * GS * S + s_base;
+#pragma unroll
+                for (int v = 0; v < 12; v++) ya[v].load(sa + v * S);
+            }
+            acc_split<SPL>(ea, xa, ya, full, hya, kU, kW, m);
         }
     }
 }
 
-template <bool COMP, int SPL>
+template <bool COMP, int SPL, int S>
 __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Step2 a)
 {
-    extern __shared__ float se[];   // [2][S]
+    __shared__ float se[2 * S];
     const StepCommon &c = a.c;
-    const int S = a.S, nch = S / (32 * SPL);
+    constexpr int nch = S / (32 * SPL);
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     if (c.energy) energy_zero(se, S);
@@ -644,8 +648,7 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
             for (int k = 0; k < 20; k++) m[k][q] = 0.f;
         }
         const int e0 = __ldg(a.up + i), e1 = __ldg(a.up + i + 1);
-        if (is_pml_row(c1)) row_split<SPL, true>(a, rec, e0, e1, lane, s_base, kU, kW, m);
-        else row_split<SPL, false>(a, rec, e0, e1, lane, s_base, kU, kW, m);
+        row_split<SPL, S>(a, rec, e0, e1, lane, s_base, is_pml_row(c1), kU, kW, m);
         const float *si = a.in.Gs + (size_t)local * GS * S + s_base;
         const float *pi = a.in.Ps + (size_t)local * PS * S + s_base;
         float *gco = a.out.Gc + (size_t)i * GC * S + s_base;
@@ -830,29 +833,31 @@ static long long batched_grid(K kernel, int threads, long long tasks, int warps,
     return std::max<long long>(1, std::min<long long>((long long)sms * per_sm, need));
 }
 
-#define SFG_BATCH_ONE(KERNEL, C, P, ROWS)                                                                \
+#define SFG_BATCH_ONE(KERNEL, C, P, SS, ROWS)                                                            \
     do {                                                                                                 \
-        auto k = KERNEL<C, P>;                                                                           \
-        const long long tasks = (long long)(ROWS) * (a.S / (32 * (P)));                                  \
-        KERNEL<C, P><<<(unsigned)batched_grid(k, threads, tasks, warps, smem), threads, smem, st>>>(a);  \
+        auto k = KERNEL<C, P, SS>;                                                                       \
+        const long long tasks = (long long)(ROWS) * ((SS) / (32 * (P)));                                 \
+        KERNEL<C, P, SS><<<(unsigned)batched_grid(k, threads, tasks, warps, 0), threads, 0, st>>>(a);    \
+    } while (0)
+#define SFG_BATCH_S(KERNEL, C, ROWS)                                                                     \
+    do {                                                                                                 \
+        if (a.S == 32) SFG_BATCH_ONE(KERNEL, C, 1, 32, ROWS);                                            \
+        else if (a.S == 64 && spl == 1) SFG_BATCH_ONE(KERNEL, C, 1, 64, ROWS);                           \
+        else if (a.S == 64) SFG_BATCH_ONE(KERNEL, C, 2, 64, ROWS);                                       \
+        else if (spl == 1) SFG_BATCH_ONE(KERNEL, C, 1, 128, ROWS);                                       \
+        else if (spl == 2) SFG_BATCH_ONE(KERNEL, C, 2, 128, ROWS);                                       \
+        else SFG_BATCH_ONE(KERNEL, C, 4, 128, ROWS);                                                     \
     } while (0)
 #define SFG_BATCH(KERNEL, ROWS)                                                                          \
     do {                                                                                                 \
         const int threads = 32 * warps;                                                                  \
-        const size_t smem = sizeof(float) * 2 * (size_t)a.S;                                             \
         if (warps < 1 || warps > 8 || (spl != 1 && spl != 2 && spl != 4)) return cudaErrorInvalidValue;  \
-        if (a.S < 32 * spl || a.S % (32 * spl) != 0 || warps % (a.S / (32 * spl)) != 0)                  \
+        if ((a.S != 32 && a.S != 64 && a.S != 128) || a.S % (32 * spl) != 0 ||                           \
+            warps % (a.S / (32 * spl)) != 0)                                                             \
             return cudaErrorInvalidValue;                                                                \
         if ((ROWS) <= 0) return cudaSuccess;                                                             \
-        if (comp) {                                                                                      \
-            if (spl == 1) SFG_BATCH_ONE(KERNEL, true, 1, ROWS);                                          \
-            else if (spl == 2) SFG_BATCH_ONE(KERNEL, true, 2, ROWS);                                     \
-            else SFG_BATCH_ONE(KERNEL, true, 4, ROWS);                                                   \
-        } else {                                                                                         \
-            if (spl == 1) SFG_BATCH_ONE(KERNEL, false, 1, ROWS);                                         \
-            else if (spl == 2) SFG_BATCH_ONE(KERNEL, false, 2, ROWS);                                    \
-            else SFG_BATCH_ONE(KERNEL, false, 4, ROWS);                                                  \
-        }                                                                                                \
+        if (comp) SFG_BATCH_S(KERNEL, true, ROWS);                                                       \
+        else SFG_BATCH_S(KERNEL, false, ROWS);                                                           \
     } while (0)
 
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st)
@@ -868,6 +873,7 @@ cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, 
     return cudaGetLastError();
 }
 #undef SFG_BATCH
+#undef SFG_BATCH_S
 #undef SFG_BATCH_ONE
 
 cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st)
