@@ -63,7 +63,11 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec",
-           "sfg_abc_mpml_device_noalloc"]
+           "sfg_abc_mpml_device_noalloc",
+           # learned surrogate (include/seisfem_fno.h)
+           "sfg_fno_gemm", "sfg_fno_dft_combine", "sfg_fno_dft_combine_bwd", "sfg_fno_expand_weights",
+           "sfg_fno_fold_weights", "sfg_fno_gelu_bwd", "sfg_fno_cast_bf16", "sfg_fno_bias_grad", "sfg_fno_swap01",
+           "sfg_fno_zero", "sfg_fno_rel_loss", "sfg_fno_adam"]
 
 
 def lib(path: str = LIBPATH):

@@ -27,6 +27,7 @@ UNITS = {
     "sfg_api.cu": [],
     "sfg_seams.cu": ["-fmad=false"],
     "sfg_noalloc.cu": ["-fmad=false"],
+    "sfg_fno.cu": [],
 }
 
 
@@ -64,7 +65,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers.append(os.path.join(HERE, "..", "include", "seisfem_b200.h"))
+    headers += [os.path.join(HERE, "..", "include", f) for f in ("seisfem_b200.h", "seisfem_fno.h")]
     objs = []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)

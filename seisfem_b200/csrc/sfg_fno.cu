@@ -1,0 +1,558 @@
+// sfg_fno.cu -- kernels of the learned surrogate (no counterpart in the
+// reference): a Fourier neural operator that maps a velocity model and a
+// source position to the receiver gather the FEM would record.
+//
+// Everything the network computes runs here: a strided, batched BF16 GEMM on
+// the tensor cores with FP32 accumulation (lifting, 1x1 convolutions,
+// truncated DFTs, per-mode channel mixing, depth-to-time map, projection and
+// all their gradients), and the pointwise kernels around it (complex
+// recombination of the DFT stages, GELU and its derivative, casts, bias
+// gradients, the relative-L2 loss, Adam).  The host (seisfem_b200/surrogate.py)
+// only sequences these calls on device buffers.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+
+#include "../../include/seisfem_fno.h"
+
+namespace {
+
+// ------------------------------------------------------------------ GEMM
+//
+// sfg_gemm_desc (seisfem_fno.h): C[z][m][n] = alpha * sum_k A[z][m][k] B[z][k][n]
+// with an epilogue (Cin, bias, pre-activation, GELU) or atomic accumulation.
+// A, B: BF16 with arbitrary element strides; C: FP32 or BF16.  The CTA tile
+// is BM x BN x 32 with eight warps; both operands are staged K-contiguous in
+// shared memory (row pitch 40 elements: the fragment loads are free of bank
+// conflicts) and fed to mma.sync m16n8k16 (BF16 in, FP32 accumulate).
+// Split-K (gridDim.z = batches x splits) accumulates FP32 partial sums.
+
+constexpr int BK = 32;
+constexpr int PITCH = BK + 8;
+
+struct GemmArgs {
+    sfg_gemm_desc d;
+    int amode, bmode;          // 0: k contiguous (16-B vectors), 1: m/n contiguous (vectors), 2: scalar
+};
+
+__device__ __forceinline__ float gelu_f(float x)
+{
+    return 0.5f * x * (1.f + erff(x * 0.70710678118654752f));
+}
+
+// Loads rows [r0, r0 + R) x k [k0, k0 + 32) of an operand whose element (r, k)
+// sits at p + r * sr + k * sk into registers: each thread holds R*32/256
+// elements as 16-byte groups.  `mode` picks the vector direction.
+template <int R>
+struct TileLoad {
+    static constexpr int PER = R * BK / 256;   // elements per thread (16 or 8)
+    static constexpr int VEC = 8;
+    static constexpr int NV = PER / VEC;       // vectors per thread
+    uint4 v[NV];
+
+    __device__ __forceinline__ void load(const __nv_bfloat16 *p, long long sr, long long sk, int rows, int kk,
+                                         int r0, int k0, int mode)
+    {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            const int idx = t + q * 256;   // vector index in the tile
+            __align__(16) __nv_bfloat16 e[8];
+            if (mode == 0) {               // 8 consecutive k of one row
+                const int r = idx / (BK / 8), kc = (idx % (BK / 8)) * 8;
+                const int gr = r0 + r, gk = k0 + kc;
+                if (gr < rows && gk + 8 <= kk) {
+                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr * sr + gk));
+                    continue;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    e[u] = (gr < rows && gk + u < kk) ? p[gr * sr + (gk + u) * sk] : __float2bfloat16(0.f);
+            } else if (mode == 1) {        // 8 consecutive rows of one k
+                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
+                const int gr = r0 + r, gk = k0 + kc;
+                if (gk < kk && gr + 8 <= rows) {
+                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr + gk * sk));
+                    continue;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    e[u] = (gr + u < rows && gk < kk) ? p[(gr + u) * sr + gk * sk] : __float2bfloat16(0.f);
+            } else {                       // scalar, same order as mode 0
+                const int r = idx / (BK / 8), kc = (idx % (BK / 8)) * 8;
+                const int gr = r0 + r, gk = k0 + kc;
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    e[u] = (gr < rows && gk + u < kk) ? p[gr * sr + (gk + u) * sk] : __float2bfloat16(0.f);
+            }
+            v[q] = *reinterpret_cast<const uint4 *>(e);
+        }
+    }
+
+    // into s[r][k] (pitch PITCH)
+    __device__ __forceinline__ void store(__nv_bfloat16 *s, int mode) const
+    {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            const int idx = t + q * 256;
+            if (mode == 1) {
+                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
+                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[q]);
+#pragma unroll
+                for (int u = 0; u < 8; u++) s[(r + u) * PITCH + kc] = e[u];
+            } else {
+                const int r = idx / (BK / 8), kc = (idx % (BK / 8)) * 8;
+                *reinterpret_cast<uint4 *>(s + r * PITCH + kc) = v[q];
+            }
+        }
+    }
+};
+
+__device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, const uint32_t *b)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// BM x BN CTA tile, warps arranged WM x WN (WM * WN = 8); each warp owns a
+// (BM/WM) x (BN/WN) sub-tile of m16 x n8 MMA tiles.
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
+{
+    constexpr int TM = BM / WM / 16, TN = BN / WN / 8;
+    __shared__ __align__(16) __nv_bfloat16 As[2][BM * PITCH];
+    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN * PITCH];
+    const sfg_gemm_desc &d = g.d;
+    const int nb = d.batch1 * d.batch2;
+    const int bz = blockIdx.z;
+    const int z = bz % nb, split = bz / nb;
+    const int z1 = z / d.batch2, z2 = z % d.batch2;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ktiles = (d.K + BK - 1) / BK;
+    const int per = (ktiles + d.splits - 1) / d.splits;
+    const int kt0 = split * per, kt1 = min(ktiles, kt0 + per);
+    const __nv_bfloat16 *A = static_cast<const __nv_bfloat16 *>(d.A) + z1 * d.sa1 + z2 * d.sa2;
+    const __nv_bfloat16 *B = static_cast<const __nv_bfloat16 *>(d.B) + z1 * d.sb1 + z2 * d.sb2;
+    const long long cz = z1 * d.sc1 + z2 * d.sc2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp / WN, wn = warp % WN;
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[TM][TN][4];
+#pragma unroll
+    for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
+    TileLoad<BM> la;
+    TileLoad<BN> lb;
+    if (kt0 < kt1) {
+        la.load(A, d.sam, d.sak, d.M, d.K, m0, kt0 * BK, g.amode);
+        lb.load(B, d.sbn, d.sbk, d.N, d.K, n0, kt0 * BK, g.bmode);
+        la.store(As[0], g.amode);
+        lb.store(Bs[0], g.bmode);
+    }
+    __syncthreads();
+    for (int kt = kt0; kt < kt1; kt++) {
+        const int cur = (kt - kt0) & 1;
+        if (kt + 1 < kt1) {
+            la.load(A, d.sam, d.sak, d.M, d.K, m0, (kt + 1) * BK, g.amode);
+            lb.load(B, d.sbn, d.sbk, d.N, d.K, n0, (kt + 1) * BK, g.bmode);
+        }
+        const __nv_bfloat16 *as = As[cur], *bs = Bs[cur];
+#pragma unroll
+        for (int ks = 0; ks < BK; ks += 16) {
+            uint32_t af[TM][4], bf[TN][2];
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                const int r = wm * (BM / WM) + i * 16 + gq;
+                af[i][0] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 2 * tq);
+                af[i][1] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 2 * tq);
+                af[i][2] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 8 + 2 * tq);
+                af[i][3] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 8 + 2 * tq);
+            }
+#pragma unroll
+            for (int j = 0; j < TN; j++) {
+                const int n = wn * (BN / WN) + j * 8 + gq;
+                bf[j][0] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 2 * tq);
+                bf[j][1] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 8 + 2 * tq);
+            }
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int j = 0; j < TN; j++) mma_bf16(acc[i][j], af[i], bf[j]);
+        }
+        if (kt + 1 < kt1) {
+            la.store(As[cur ^ 1], g.amode);
+            lb.store(Bs[cur ^ 1], g.bmode);
+        }
+        __syncthreads();
+    }
+    // epilogue
+#pragma unroll
+    for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int m = m0 + wm * (BM / WM) + i * 16 + gq + (r >= 2 ? 8 : 0);
+                const int n = n0 + wn * (BN / WN) + j * 8 + 2 * tq + (r & 1);
+                if (m >= d.M || n >= d.N) continue;
+                const long long o = cz + m * d.scm + n * d.scn;
+                float v = d.alpha * acc[i][j][r];
+                if (d.atomic) {
+                    atomicAdd(static_cast<float *>(d.C) + o, v);
+                    continue;
+                }
+                if (d.Cin) v += d.beta * d.Cin[o];
+                if (d.bias) v += d.bias[d.bias_on_m ? m : n];
+                if (d.pre) static_cast<__nv_bfloat16 *>(d.pre)[o] = __float2bfloat16(v);
+                if (d.gelu) v = gelu_f(v);
+                if (d.c_bf16) static_cast<__nv_bfloat16 *>(d.C)[o] = __float2bfloat16(v);
+                else static_cast<float *>(d.C)[o] = v;
+            }
+}
+
+// Vector loads need 16-byte aligned groups of 8 elements: the base pointer
+// and every stride other than the contiguous one must keep that alignment.
+int pick_mode(long long s_row, long long s_k, long long s1, long long s2, const void *p)
+{
+    const bool al = (reinterpret_cast<uintptr_t>(p) & 15) == 0 && s1 % 8 == 0 && s2 % 8 == 0;
+    if (s_k == 1 && s_row % 8 == 0 && al) return 0;
+    if (s_row == 1 && s_k % 8 == 0 && al) return 1;
+    return 2;
+}
+
+// ------------------------------------------------------- pointwise kernels
+
+constexpr int KC = 16, KD = 32;    // kept W modes, kept D modes (16 + 16)
+
+// P[z][64][32]: rows 0-31 = cos-rows times [Yre | Yim], rows 32-63 sin-rows.
+// Z = sum_d e^{-i theta} Y:  Zre = C.Yre + S.Yim,  Zim = C.Yim - S.Yre.
+__global__ void dft_combine_kernel(const float *__restrict__ P, __nv_bfloat16 *__restrict__ Z, int B, int C)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)B * C * KD * KC;
+    if (t >= total) return;
+    const int k2 = (int)(t % KC);
+    const int k1 = (int)((t / KC) % KD);
+    const long long zz = t / (KC * KD);            // b * C + c
+    const int c = (int)(zz % C), b = (int)(zz / C);
+    const float *p = P + zz * 64 * 32;
+    const float re = p[k1 * 32 + k2] + p[(32 + k1) * 32 + 16 + k2];
+    const float im = p[k1 * 32 + 16 + k2] - p[(32 + k1) * 32 + k2];
+    const long long mode = k1 * KC + k2;
+    __nv_bfloat16 *o = Z + (mode * B + b) * 2 * C;
+    o[c] = __float2bfloat16(re);
+    o[C + c] = __float2bfloat16(im);
+}
+
+__global__ void dft_combine_bwd_kernel(const __nv_bfloat16 *__restrict__ dZ, __nv_bfloat16 *__restrict__ dP, int B,
+                                       int C)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)B * C * KD * KC;
+    if (t >= total) return;
+    const int k2 = (int)(t % KC);
+    const int k1 = (int)((t / KC) % KD);
+    const long long zz = t / (KC * KD);
+    const int c = (int)(zz % C), b = (int)(zz / C);
+    const long long mode = k1 * KC + k2;
+    const __nv_bfloat16 *g = dZ + (mode * B + b) * 2 * C;
+    const __nv_bfloat16 re = g[c], im = g[C + c];
+    __nv_bfloat16 *p = dP + zz * 64 * 32;
+    p[k1 * 32 + k2] = re;
+    p[(32 + k1) * 32 + 16 + k2] = re;
+    p[k1 * 32 + 16 + k2] = im;
+    p[(32 + k1) * 32 + k2] = __float2bfloat16(-__bfloat162float(im));
+}
+
+__global__ void expand_weights_kernel(const float *__restrict__ Wr, const float *__restrict__ Wi,
+                                      __nv_bfloat16 *__restrict__ Wb, int modes, int C)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)modes * C * C) return;
+    const int o = (int)(t % C), i = (int)((t / C) % C);
+    const long long mode = t / ((long long)C * C);
+    const float r = Wr[t], im = Wi[t];
+    __nv_bfloat16 *w = Wb + mode * 4 * C * C;
+    const int C2 = 2 * C;
+    w[i * C2 + o] = __float2bfloat16(r);
+    w[i * C2 + C + o] = __float2bfloat16(im);
+    w[(C + i) * C2 + o] = __float2bfloat16(-im);
+    w[(C + i) * C2 + C + o] = __float2bfloat16(r);
+}
+
+__global__ void fold_weights_kernel(const float *__restrict__ dWb, float *__restrict__ dWr, float *__restrict__ dWi,
+                                    int modes, int C)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)modes * C * C) return;
+    const int o = (int)(t % C), i = (int)((t / C) % C);
+    const long long mode = t / ((long long)C * C);
+    const float *w = dWb + mode * 4 * C * C;
+    const int C2 = 2 * C;
+    dWr[t] += w[i * C2 + o] + w[(C + i) * C2 + C + o];
+    dWi[t] += w[i * C2 + C + o] - w[(C + i) * C2 + o];
+}
+
+__global__ void gelu_bwd_kernel(const void *__restrict__ dy, int dy_bf16, const __nv_bfloat16 *__restrict__ pre,
+                                __nv_bfloat16 *__restrict__ dx, long long n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float x = __bfloat162float(pre[t]);
+    const float g = dy_bf16 ? __bfloat162float(static_cast<const __nv_bfloat16 *>(dy)[t])
+                            : static_cast<const float *>(dy)[t];
+    // d/dx [x Phi(x)] = Phi(x) + x phi(x)
+    const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+    dx[t] = __float2bfloat16(g * (cdf + x * pdf));
+}
+
+__global__ void cast_bf16_kernel(const float *__restrict__ x, __nv_bfloat16 *__restrict__ y, long long n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) y[t] = __float2bfloat16(x[t]);
+}
+
+// Block (c, slice): the sum over one slice of the outer index and all of the
+// inner index of channel c, added to db[c].
+__global__ void bias_grad_kernel(const __nv_bfloat16 *__restrict__ dy, float *__restrict__ db, int outer, int C,
+                                 long long inner)
+{
+    const int c = blockIdx.x;
+    const long long per = (outer + gridDim.y - 1) / gridDim.y;
+    const long long o0 = blockIdx.y * per, o1 = min((long long)outer, o0 + per);
+    const long long cnt = (o1 > o0 ? o1 - o0 : 0) * inner;
+    float s = 0.f;
+    for (long long q = threadIdx.x; q < cnt; q += blockDim.x) {
+        const long long o = o0 + q / inner, i = q % inner;
+        s += __bfloat162float(dy[(o * C + c) * inner + i]);
+    }
+    __shared__ float red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && red[0] != 0.f) atomicAdd(db + c, red[0]);
+}
+
+// y[j][i][k] = x[i][j][k] (BF16)
+__global__ void swap01_kernel(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__restrict__ y, int n0, int n1,
+                              long long n2)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)n0 * n1 * n2;
+    if (t >= total) return;
+    const long long k = t % n2;
+    const long long i = (t / n2) % n0;
+    const long long j = t / (n2 * n0);
+    y[t] = x[(i * n1 + j) * n2 + k];
+}
+
+__global__ void zero_kernel(float *__restrict__ p, long long n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) p[t] = 0.f;
+}
+
+// per shot: scratch[2b] = |pred-target|^2, scratch[2b+1] = |target|^2
+__global__ void rel_loss_sums(const float *__restrict__ pred, const __nv_bfloat16 *__restrict__ tgt, float *scratch,
+                              long long n)
+{
+    const int b = blockIdx.y;
+    const float *p = pred + b * n;
+    const __nv_bfloat16 *q = tgt + b * n;
+    float e = 0.f, r = 0.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float tv = __bfloat162float(q[i]), d = p[i] - tv;
+        e += d * d;
+        r += tv * tv;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(scratch + 2 * b, e);
+        atomicAdd(scratch + 2 * b + 1, r);
+    }
+}
+
+__global__ void rel_loss_grad(const float *__restrict__ pred, const __nv_bfloat16 *__restrict__ tgt,
+                              const float *__restrict__ scratch, float *loss, __nv_bfloat16 *__restrict__ dpred, int B,
+                              long long n)
+{
+    const int b = blockIdx.y;
+    const float den = fmaxf(scratch[2 * b + 1], 1e-30f);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && loss) loss[b] = scratch[2 * b] / den;
+    if (!dpred) return;
+    const float s = 2.f / ((float)B * den);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dpred[b * n + i] = __float2bfloat16(s * (pred[b * n + i] - __bfloat162float(tgt[b * n + i])));
+}
+
+__global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float gt = g[t];
+    const float mt = b1 * m[t] + (1.f - b1) * gt;
+    const float vt = b2 * v[t] + (1.f - b2) * gt * gt;
+    m[t] = mt;
+    v[t] = vt;
+    p[t] -= lr * (mt / c1) / (sqrtf(vt / c2) + eps);
+}
+
+unsigned grid_of(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+int launched() { return cudaGetLastError() == cudaSuccess ? 0 : 2; }
+
+}  // namespace
+
+extern "C" {
+
+int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
+{
+    if (!dp) return 1;
+    const sfg_gemm_desc &d = *dp;
+    if (!d.A || !d.B || !d.C || d.M <= 0 || d.N <= 0 || d.K <= 0 || d.batch1 <= 0 || d.batch2 <= 0 ||
+        d.splits <= 0)
+        return 1;
+    if ((d.splits > 1 || d.atomic) && (d.c_bf16 || d.Cin || d.bias || d.gelu || d.pre)) return 1;
+    if (d.splits > 1 && !d.atomic) return 1;
+    const long long nb = (long long)d.batch1 * d.batch2 * d.splits;
+    if (nb > 65535) return 1;
+    GemmArgs g;
+    g.d = d;
+    g.amode = pick_mode(d.sam, d.sak, d.sa1, d.sa2, d.A);
+    g.bmode = pick_mode(d.sbn, d.sbk, d.sb1, d.sb2, d.B);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (d.M >= 128 && d.N >= 128) {
+        dim3 grid((d.N + 127) / 128, (d.M + 127) / 128, (unsigned)nb);
+        if (grid.y > 65535) return 1;
+        gemm_bf16_kernel<128, 128, 2, 4><<<grid, 256, 0, st>>>(g);
+    } else if (d.M >= d.N) {
+        dim3 grid((d.N + 63) / 64, (d.M + 127) / 128, (unsigned)nb);
+        if (grid.y > 65535) return 1;
+        gemm_bf16_kernel<128, 64, 4, 2><<<grid, 256, 0, st>>>(g);
+    } else {
+        dim3 grid((d.N + 127) / 128, (d.M + 63) / 64, (unsigned)nb);
+        if (grid.y > 65535) return 1;
+        gemm_bf16_kernel<64, 128, 2, 4><<<grid, 256, 0, st>>>(g);
+    }
+    return launched();
+}
+
+int sfg_fno_dft_combine(const float *P, void *Zmix, int B, int C, void *stream)
+{
+    if (!P || !Zmix || B <= 0 || C <= 0) return 1;
+    const long long n = (long long)B * C * KD * KC;
+    dft_combine_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        P, static_cast<__nv_bfloat16 *>(Zmix), B, C);
+    return launched();
+}
+
+int sfg_fno_dft_combine_bwd(const void *dZmix, void *dP, int B, int C, void *stream)
+{
+    if (!dZmix || !dP || B <= 0 || C <= 0) return 1;
+    const long long n = (long long)B * C * KD * KC;
+    dft_combine_bwd_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16 *>(dZmix), static_cast<__nv_bfloat16 *>(dP), B, C);
+    return launched();
+}
+
+int sfg_fno_expand_weights(const float *Wr, const float *Wi, void *Wblk, int modes, int C, void *stream)
+{
+    if (!Wr || !Wi || !Wblk || modes <= 0 || C <= 0) return 1;
+    const long long n = (long long)modes * C * C;
+    expand_weights_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        Wr, Wi, static_cast<__nv_bfloat16 *>(Wblk), modes, C);
+    return launched();
+}
+
+int sfg_fno_fold_weights(const float *dWblk, float *dWr, float *dWi, int modes, int C, void *stream)
+{
+    if (!dWblk || !dWr || !dWi || modes <= 0 || C <= 0) return 1;
+    const long long n = (long long)modes * C * C;
+    fold_weights_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(dWblk, dWr, dWi, modes, C);
+    return launched();
+}
+
+int sfg_fno_gelu_bwd(const void *dy, int dy_bf16, const void *pre, void *dx, long long n, void *stream)
+{
+    if (!dy || !pre || !dx || n < 0) return 1;
+    if (n) gelu_bwd_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        dy, dy_bf16, static_cast<const __nv_bfloat16 *>(pre), static_cast<__nv_bfloat16 *>(dx), n);
+    return launched();
+}
+
+int sfg_fno_cast_bf16(const float *x, void *y, long long n, void *stream)
+{
+    if (!x || !y || n < 0) return 1;
+    if (n) cast_bf16_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        x, static_cast<__nv_bfloat16 *>(y), n);
+    return launched();
+}
+
+int sfg_fno_bias_grad(const void *dy, float *db, int outer, int C, long long inner, void *stream)
+{
+    if (!dy || !db || outer <= 0 || C <= 0 || C > 65535 || inner <= 0) return 1;
+    const dim3 grid((unsigned)C, (unsigned)std::min(outer, 64));
+    bias_grad_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const __nv_bfloat16 *>(dy), db,
+                                                                           outer, C, inner);
+    return launched();
+}
+
+int sfg_fno_swap01(const void *x, void *y, int n0, int n1, long long n2, void *stream)
+{
+    if (!x || !y || n0 <= 0 || n1 <= 0 || n2 <= 0) return 1;
+    const long long n = (long long)n0 * n1 * n2;
+    swap01_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16 *>(x), static_cast<__nv_bfloat16 *>(y), n0, n1, n2);
+    return launched();
+}
+
+int sfg_fno_zero(float *p, long long n, void *stream)
+{
+    if (!p || n < 0) return 1;
+    if (n) zero_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, n);
+    return launched();
+}
+
+int sfg_fno_rel_loss(const float *pred, const void *target, float *loss, void *dpred, float *scratch, int B,
+                     long long n, void *stream)
+{
+    if (!pred || !target || !scratch || B <= 0 || B > 65535 || n <= 0) return 1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(scratch, 0, sizeof(float) * 2 * B, st) != cudaSuccess) return 2;
+    const unsigned gx = (unsigned)std::min<long long>(grid_of(n, 256), 256);
+    rel_loss_sums<<<dim3(gx, B), 256, 0, st>>>(pred, static_cast<const __nv_bfloat16 *>(target), scratch, n);
+    rel_loss_grad<<<dim3(gx, B), 256, 0, st>>>(pred, static_cast<const __nv_bfloat16 *>(target), scratch, loss,
+                                              static_cast<__nv_bfloat16 *>(dpred), B, n);
+    return launched();
+}
+
+int sfg_fno_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float beta1, float beta2,
+                 float eps, int step, void *stream)
+{
+    if (!p || !g || !m || !v || n < 0 || step < 1) return 1;
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    if (n) adam_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, g, m, v, n, lr, beta1,
+                                                                                       beta2, eps, c1, c2);
+    return launched();
+}
+
+}  // extern "C"

@@ -298,3 +298,23 @@ def small_problem(type_name: str = "Q4", n: int = 40, h: float = 10.0, step: int
     rec = locate(mesh, h, line_points(nrec, (xr, pml * h), (xr, L - pml * h)))
     return Problem(mesh, model, step, dt, f0, 0.0, h, pml, pml, src, rec, free_surface,
                    f"small_{type_name}_{n}")
+
+
+def config_5(seed: int, n: int = 128, h: float = 10.0, samples: int = 1000, nrec: int = 64, pml: int = 16,
+             f0: float = 15.0, corr_len: float = 150.0) -> Problem:
+    """One surrogate training shot: Q4 n x n (1280 m for n = 128), GRF vp
+    (mean 3000, std 400, correlation length 150 m, clipped 1800-4500, seeded),
+    vs = vp/sqrt(3), Gardner density; free surface at x = xmax with the M-PML
+    (16 elements) on the other three sides; the source one element below the
+    surface at a horizontal position drawn uniformly over the receiver span;
+    nrec receivers evenly along the surface row; dt = 1 ms, samples + 2 steps
+    (the loop records step - 2 samples)."""
+    L = n * h
+    mesh = structured_mesh("Q4", n, n, 0.0, L, 0.0, L)
+    model = grf_model(mesh, n, h, corr_len, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 1_000_003))
+    y0, y1 = pml * h, L - pml * h
+    ys = round(rng.uniform(y0, y1) / h) * h
+    src = locate(mesh, h, [(L - h, ys)])
+    rec = locate(mesh, h, line_points(nrec, (L, y0), (L, y1)))
+    return Problem(mesh, model, samples + 2, 1e-3, f0, 0.0, h, pml, pml, src, rec, 1, f"config5_q4_{n}_seed{seed}")
