@@ -35,6 +35,7 @@ from seisfem_b200 import problem as P  # noqa: E402
 METRIC = "DOF-steps/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.txt")
+T6_STABLE_STEPS = 202
 
 
 def workload(name: str, rank: int = 0):
@@ -44,6 +45,9 @@ def workload(name: str, rank: int = 0):
         p = P.config_1()
     elif name == "q4_400_grf_64shots":
         p = P.config_3a()
+    elif name == "t6_300x150_topo_vti":
+        # inside the window before the reference's T6 energy bound trips
+        p = P.config_4(step=T6_STABLE_STEPS)
     elif name == "q4_200_grf_64shots":
         # the batched kernels on a smaller mesh (profiling case; state > L2)
         p = P.config_3a(n=200, step=500)
@@ -163,6 +167,146 @@ def run_reference_arm(args):
     return 0
 
 
+def run_surrogate(args):
+    """Config 5: FEM-generated training shots (Q4 128x128, GRF models, a
+    source drawn along the surface, 64 receivers x 1000 samples), FNO training
+    on the GPU, then held-out shots judged by the FEM: surrogate shots/s at
+    its measured relative L2 error, beside the FEM's shots/s."""
+    import torch
+    from seisfem_b200.surrogate import Surrogate, generate, rel_l2
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ntr, nte = args.train_shots, args.test_shots
+    t0 = time.perf_counter()
+    xtr, ytr, fem_tr = generate(range(5000, 5000 + ntr))
+    t_gen = time.perf_counter() - t0
+    xte, yte, fem_te = generate(range(9000, 9000 + nte))
+    sg = Surrogate(B=16, seed=0)
+    K = sg.net.K
+    # one timed training step for the tensor-core rate (FLOPs counted per GEMM)
+    f0 = K.flops
+    t1 = time.perf_counter()
+    hist = sg.fit(xtr, ytr, epochs=args.epochs, lr=args.lr)
+    torch.cuda.synchronize(dev)
+    t_train = time.perf_counter() - t1
+    train_flops = K.flops - f0
+    steps = args.epochs * (ntr // 16)
+    # inference: warm-up, then K timed passes over the held-out set (CUDA events;
+    # inputs already on the device: value; with host copies: e2e)
+    B = sg.B
+    xb = torch.tensor(xte[:B]).to(dev).to(torch.bfloat16).contiguous()
+    for _ in range(max(3, args.warmup)):
+        sg.net.forward(xb)
+    torch.cuda.synchronize(dev)
+    f1 = K.flops
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(1, args.steps) * (nte // B)
+    e0.record()
+    for _ in range(reps):
+        sg.net.forward(xb)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    fwd_ms = e0.elapsed_time(e1) / reps
+    fwd_flops = (K.flops - f1) / reps
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    pred = sg.predict(xte)
+    torch.cuda.synchronize(dev)
+    t_e2e = time.perf_counter() - t2
+    err = rel_l2(pred, yte)
+    fallback = err > 1e-2
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    fem_rate = 1.0 / float(np.median(np.concatenate([fem_tr, fem_te])))
+    sur_rate = B / (fwd_ms * 1e-3)
+    # hybrid pipeline: every shot runs the surrogate; shots over the bound run the FEM too
+    hybrid = nte / (nte / sur_rate + fallback.sum() / fem_rate)
+    line = {"metric": "surrogate shots/s", "value": sur_rate, "unit": "shots/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": fwd_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "config5_q4_128_fno", "train_shots": ntr, "test_shots": nte,
+                       "grid": [128, 64], "samples": 1000, "width": 64, "modes": 16, "layers": 4,
+                       "batch": B, "epochs": args.epochs},
+            "rel_l2": {"mean": float(err.mean()), "median": float(np.median(err)),
+                       "p10": float(np.percentile(err, 10)), "p90": float(np.percentile(err, 90))},
+            "fallback_fraction": float(fallback.mean()), "fallback_bound": 1e-2,
+            "fem_shots_per_s": fem_rate, "hybrid_shots_per_s": hybrid,
+            "e2e": {"value": nte / t_e2e, "unit": "shots/s",
+                    "h2d_bytes_per_step": int(xte[:B].size * 2), "d2h_bytes_per_step": int(B * 2 * 64 * 1000 * 4)},
+            "roofline": {"bound": "tensor", "achieved": fwd_flops / (fwd_ms * 1e-3) / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": fwd_flops / (fwd_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                         "flops_per_forward": fwd_flops},
+            "train": {"seconds": t_train, "steps": steps, "ms_per_step": t_train / steps * 1e3,
+                      "tflops": train_flops / t_train / 1e12, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]},
+            "fem_generation_seconds": t_gen, "gpu_launches": K.launches}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_group(args):
+    """Config 3b: independent Q4 meshes of uneven sizes, each with its own
+    autotuned launch shapes, advanced by one CUDA-graph launch (sfg_group);
+    the same plans launched one after another give the sequential time."""
+    import torch
+    from seisfem_b200.api import Context, Group, Plan
+    dev = 0
+    torch.cuda.set_device(dev)
+    probs = P.config_3b()
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    ctxs, plans = [], []
+    for p in probs:
+        c = Context(dev)
+        c.setup(p)
+        ctxs.append(c)
+        plans.append(Plan(c, p, precision=args.precision, snap_every=0))
+    grp = Group(plans)
+    for _ in range(args.warmup):
+        grp.launch(sh)
+    torch.cuda.synchronize(dev)
+    for pl in plans:
+        pl.finish(0, stream=sh)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        grp.launch(sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    e0.record(stream)
+    for pl in plans:
+        pl.launch(0, sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_seq = e0.elapsed_time(e1)
+    dof_steps = sum(2 * p.mesh.node_num * (p.step - 2) for p in probs)
+    b_step = sum(step_bytes(c, p, 1) for c, p in zip(ctxs, probs))
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    steps = probs[0].step - 2
+    achieved = b_step * steps / (ms * 1e-3) / 1e9
+    shapes = [launch_shape(c.stats()["rows_per_block"], 1) for c in ctxs]
+    line = {"metric": METRIC, "value": dof_steps / (ms * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config3b_16_q4_meshes", "sizes": [int(round(p.mesh.node_num ** 0.5)) - 1
+                                                                      for p in probs],
+                       "nodes_total": sum(p.mesh.node_num for p in probs), "time_steps": steps,
+                       "precision": args.precision, "shots_per_mesh": 1,
+                       "l2": "per-step working set of all meshes > 126 MB L2"},
+            "sequential_ms": ms_seq, "group_over_sequential": ms_seq / ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "algorithmic_bytes_per_step": b_step},
+            "launch_shapes": shapes, "gpu_launches": grp.launches * args.steps, "e2e": None, "cpu_baseline": None}
+    print(json.dumps(line), flush=True)
+    grp.close()
+    for pl in plans:
+        pl.close()
+    for c in ctxs:
+        c.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -175,10 +319,18 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--compare-plain", action="store_true",
                     help="also time the unfused path (one SpMV launch per product) on one shot")
+    ap.add_argument("--train-shots", type=int, default=4096)
+    ap.add_argument("--test-shots", type=int, default=256)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--lr", type=float, default=2e-3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "surrogate_q4_128":
+        return run_surrogate(args)
+    if args.workload == "q4_16meshes":
+        return run_group(args)
 
     import torch
     import torch.distributed as dist

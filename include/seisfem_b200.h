@@ -160,6 +160,20 @@ int sfg_plan_launch(sfg_plan *plan, int batch, void *stream);
 int sfg_plan_finish(sfg_plan *plan, int batch, double *seis_u, double *seis_w, double *snap_u,
                     double *snap_w, void *stream);
 void sfg_plan_destroy(sfg_plan *plan);
+
+/* Plan groups (no counterpart in the reference): the captured time loops of
+ * several single-batch plans -- independent meshes of any sizes, each with
+ * the launch shapes its own autotuning picked -- as one CUDA graph with no
+ * dependencies between them, so one launch advances all of them side by
+ * side.  Results are read per plan with sfg_plan_finish(plan, 0, ...) after
+ * the group's stream has finished.  A group uses its plans' buffers: do not
+ * launch a member plan while the group runs; destroy the group before its
+ * plans.  All plans must live on one device. */
+typedef struct sfg_group sfg_group;
+int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **group);
+int sfg_group_launch(sfg_group *group, void *stream);
+int sfg_group_launches(const sfg_group *group);   /* kernels one launch runs */
+void sfg_group_destroy(sfg_group *group);
 int sfg_sync(sfg_ctx *ctx);
 
 /* ----------------------------------------------------------- the seams */

@@ -63,7 +63,8 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec",
-           "sfg_abc_mpml_device_noalloc",
+           "sfg_abc_mpml_device_noalloc", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
+           "sfg_group_destroy",
            # learned surrogate (include/seisfem_fno.h)
            "sfg_fno_gemm", "sfg_fno_dft_combine", "sfg_fno_dft_combine_bwd", "sfg_fno_expand_weights",
            "sfg_fno_fold_weights", "sfg_fno_gelu_bwd", "sfg_fno_cast_bf16", "sfg_fno_bias_grad", "sfg_fno_swap01",
@@ -97,6 +98,10 @@ def lib(path: str = LIBPATH):
     L.sfg_sync.argtypes = [C.c_void_p]
     L.sfg_plan_create.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.POINTER(C.c_void_p)]
     L.sfg_plan_batches.argtypes = [C.c_void_p]
+    L.sfg_group_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+    L.sfg_group_launch.argtypes = [C.c_void_p, C.c_void_p]
+    L.sfg_group_launches.argtypes = [C.c_void_p]
+    L.sfg_group_destroy.argtypes = [C.c_void_p]
     L.sfg_plan_launches.argtypes = [C.c_void_p]
     L.sfg_plan_launch.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     L.sfg_plan_finish.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 5
@@ -269,6 +274,38 @@ class Plan:
     def close(self):
         if self.ptr:
             self.L.sfg_plan_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Group:
+    """Several single-batch plans (independent meshes) as one CUDA-graph
+    launch (sfg_group_*); results are read per plan with Plan.finish()."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        self.L = self.plans[0].L
+        arr = (C.c_void_p * len(self.plans))(*[p.ptr.value for p in self.plans])
+        h = C.c_void_p()
+        rc = self.L.sfg_group_create(arr, len(self.plans), C.byref(h))
+        if rc:
+            raise SfgError(rc, "sfg_group_create")
+        self.ptr = h
+        self.launches = self.L.sfg_group_launches(h)
+
+    def launch(self, stream: int = 0):
+        rc = self.L.sfg_group_launch(self.ptr, stream or None)
+        if rc:
+            raise SfgError(rc, "sfg_group_launch")
+
+    def close(self):
+        if self.ptr:
+            self.L.sfg_group_destroy(self.ptr)
             self.ptr = None
 
     def __del__(self):

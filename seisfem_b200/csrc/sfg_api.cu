@@ -936,6 +936,63 @@ void sfg_plan_destroy(sfg_plan *plan)
     plan_free(plan);
 }
 
+// ------------------------------------------------------------ plan groups
+
+struct sfg_group {
+    int device = 0;
+    int launches = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **out)
+{
+    if (!plans || nplans <= 0 || !out) return SFG_ERR_ARG;
+    *out = nullptr;
+    const int dev = plans[0] ? plans[0]->ctx->device : -1;
+    for (int i = 0; i < nplans; i++)
+        if (!plans[i] || plans[i]->ctx->device != dev || plans[i]->nbatch != 1 || !plans[i]->graph) return SFG_ERR_ARG;
+    if (cudaSetDevice(dev) != cudaSuccess) return SFG_ERR_CUDA;
+    sfg_group *g = new sfg_group();
+    g->device = dev;
+    auto bail = [&](int code) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        return code;
+    };
+    if (cudaGraphCreate(&g->graph, 0) != cudaSuccess) return bail(SFG_ERR_CUDA);
+    for (int i = 0; i < nplans; i++) {
+        // no dependencies: the meshes' time loops run side by side
+        cudaGraphNode_t node;
+        if (cudaGraphAddChildGraphNode(&node, g->graph, nullptr, 0, plans[i]->graph) != cudaSuccess)
+            return bail(SFG_ERR_CUDA);
+        g->launches += plans[i]->launches;
+    }
+    if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) return bail(SFG_ERR_CUDA);
+    *out = g;
+    return SFG_OK;
+}
+
+int sfg_group_launch(sfg_group *g, void *stream)
+{
+    if (!g) return SFG_ERR_ARG;
+    if (cudaSetDevice(g->device) != cudaSuccess) return SFG_ERR_CUDA;
+    return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? SFG_OK : SFG_ERR_CUDA;
+}
+
+int sfg_group_launches(const sfg_group *g) { return g ? g->launches : 0; }
+
+void sfg_group_destroy(sfg_group *g)
+{
+    if (!g) return;
+    cudaSetDevice(g->device);
+    cudaDeviceSynchronize();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
 int sfg_sync(sfg_ctx *ctx)
 {
     if (!ctx) return SFG_ERR_ARG;

@@ -784,10 +784,10 @@ __global__ void coef2_kernel(int n, int na, const float *__restrict__ coef, cons
 
 // ---------------------------------------------------------- launchers
 
-// Launch shapes of the single-shot kernels (threads per block, minimum
-// resident blocks for the register allocation):
-//   0: 128 x 4   1: 128 x 6   2: 256 x 3   3: 256 x 4
-int step2_variants() { return 4; }
+// Launch shapes of the single-shot kernels (rows = threads per block,
+// minimum resident blocks for the register allocation):
+//   0: 128 x 4   1: 128 x 6   2: 256 x 3   3: 256 x 4   4: 64 x 16   5: 512 x 2
+int step2_variants() { return 6; }
 
 #define SFG_SHAPES(KERNEL, COUNT)                                                              \
     do {                                                                                       \
@@ -796,6 +796,8 @@ int step2_variants() { return 4; }
         case 0: SFG_ONE(KERNEL, 128, 4, COUNT); break;                                         \
         case 1: SFG_ONE(KERNEL, 128, 6, COUNT); break;                                         \
         case 2: SFG_ONE(KERNEL, 256, 3, COUNT); break;                                         \
+        case 4: SFG_ONE(KERNEL, 64, 16, COUNT); break;                                         \
+        case 5: SFG_ONE(KERNEL, 512, 2, COUNT); break;                                         \
         default: SFG_ONE(KERNEL, 256, 4, COUNT); break;                                        \
         }                                                                                      \
     } while (0)

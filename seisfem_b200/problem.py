@@ -318,3 +318,51 @@ def config_5(seed: int, n: int = 128, h: float = 10.0, samples: int = 1000, nrec
     src = locate(mesh, h, [(L - h, ys)])
     rec = locate(mesh, h, line_points(nrec, (L, y0), (L, y1)))
     return Problem(mesh, model, samples + 2, 1e-3, f0, 0.0, h, pml, pml, src, rec, 1, f"config5_q4_{n}_seed{seed}")
+
+
+def config_4(nx: int = 150, ny: int = 300, h: float = 10.0, step: int = 4000, dt: float = 4e-4, pml: int = 20,
+             amp: float = 40.0, wavelength: float = 600.0, f0: float = 20.0, rec_every: int = 1) -> Problem:
+    """T6 mesh of a 3000 m x 1500 m domain (for nx = 150, ny = 300) with a
+    sinusoidal free-surface topography: the structured T6 grid (x vertical,
+    nx elements; y horizontal, ny elements) is mapped by
+    x' = x + (x / xmax) * amp * sin(2 pi y / wavelength), so the top follows
+    the sinusoid and the bottom stays flat.  VTI medium from Thomsen
+    parameters (vp0 3000, vs0 1500, rho 2200, epsilon 0.2, delta 0.1, axis
+    vertical).  Free surface at the top (x = xmax), M-PML on the bottom and
+    both sides; a vertical force one element below the surface at the centre;
+    receivers on the surface nodes every `rec_every` element edges inside the
+    M-PML span."""
+    xmax, ymax = nx * h, ny * h
+    mesh = structured_mesh("T6", nx, ny, 0.0, xmax, 0.0, ymax)
+    topo = amp * np.sin(2.0 * np.pi * mesh.y / wavelength)
+    mesh.x = mesh.x + (mesh.x / xmax) * topo
+    mesh.xmin, mesh.xmax, mesh.ymin, mesh.ymax = 0.0, xmax, 0.0, ymax
+    model = vti_model(mesh.node_num, 3000.0, 1500.0, 2200.0, 0.2, 0.1)
+    yc = ymax / 2.0
+    xs = xmax + amp * math.sin(2.0 * np.pi * yc / wavelength) - h
+    src = locate(mesh, h / 2.0, [(xs, yc)])
+    ys = np.arange(pml * h, ymax - pml * h + 1e-9, rec_every * h)
+    rec = locate(mesh, h / 2.0, [(xmax + amp * math.sin(2.0 * np.pi * y / wavelength), y) for y in ys])
+    return Problem(mesh, model, step, dt, f0, 0.0, h, pml, pml, src, rec, 1, f"config4_t6_{nx}x{ny}_topo")
+
+
+def config_3b(count: int = 16, lo: int = 100, hi: int = 600, seed: int = 4, h: float = 10.0, step: int = 2000,
+              pml: int = 20, f0: float = 20.0):
+    """Independent Q4 problems with edge lengths drawn from [lo, hi]
+    elements (seeded): each a square of n h with a GRF model (the config-3a
+    recipe, its own seed), one 20 Hz source at the centre, receivers on the
+    top interior row, dt = 1 ms."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = rng.integers(lo, hi + 1, count)
+    probs = []
+    for k, n in enumerate(sizes):
+        n = int(n)
+        L = n * h
+        mesh = structured_mesh("Q4", n, n, 0.0, L, 0.0, L)
+        model = grf_model(mesh, n, h, 200.0, seed=seed * 1000 + k)
+        src = locate(mesh, h, [(round(n / 2) * h, round(n / 2) * h)])
+        xr = L - pml * h
+        nrec = n - 2 * pml + 1
+        rec = locate(mesh, h, line_points(nrec, (xr, pml * h), (xr, L - pml * h)))
+        probs.append(Problem(mesh, model, step, 1e-3, f0, 0.0, h, pml, pml, src, rec, 0, f"config3b_q4_{n}"))
+    return probs

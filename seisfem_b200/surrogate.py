@@ -57,6 +57,7 @@ class Kernels:
         self.L = api.lib()
         self.stream = stream
         self.launches = 0
+        self.flops = 0          # 2 M N K per problem of every GEMM issued
         f = self.L.sfg_fno_gemm
         f.argtypes = [C.POINTER(GemmDesc), C.c_void_p]
         for n, a in [("sfg_fno_dft_combine", [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
@@ -99,6 +100,7 @@ class Kernels:
         import torch
         d.c_bf16 = int(Cout.dtype == torch.bfloat16)
         d.gelu, d.bias_on_m, d.atomic = int(gelu), int(bias_on_m), int(atomic)
+        self.flops += 2 * M * N * K * batch[0] * batch[1]
         self._check(self.L.sfg_fno_gemm(C.byref(d), self.stream), "sfg_fno_gemm")
 
     def call(self, name, *args):

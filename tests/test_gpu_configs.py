@@ -1,0 +1,77 @@
+"""Config 4 (T6 mesh, sinusoidal free-surface topography, VTI) and config 3b
+(uneven meshes in one CUDA-graph launch) at sizes the oracle finishes in
+seconds."""
+import copy
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from seisfem_b200.problem import config_3b, config_4
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-4
+
+
+def test_config4_small_fp32_matches_oracle(ctx, oracle):
+    # 30 x 60 T6 elements with the same topography, medium and time step; 200
+    # steps lie inside the window before the reference's T6 energy bound trips
+    p = config_4(nx=30, ny=60, pml=5, step=202)
+    ref = oracle.run(p)
+    assert ref["status"] == 0
+    ctx.setup(p)
+    out = ctx.run(p, precision="fp32k")
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(out[k], ref[k]) < FP32_TOL, (k, rel_l2(out[k], ref[k]))
+    # the free surface is not Dirichlet: surface receivers move
+    assert np.abs(out["seis_u"]).max() > 0
+
+
+def test_config4_t6_energy_bound_trips_like_the_reference(ctx, oracle):
+    """The reference's lumped T6 scheme with its M-PML grows without bound
+    (flat or sinusoidal top, isotropic or VTI, dt 0.1-0.4 ms); the oracle
+    and both GPU precisions stop at the energy bound, the FP32 path within a
+    few steps of the FP64 one."""
+    p = config_4(nx=30, ny=60, pml=5, step=400)
+    ref = oracle.run(p)
+    assert ref["status"] == 1
+    ctx.setup(p)
+    o64 = ctx.run(p, precision="fp64", raise_on_blowup=False)
+    o32 = ctx.run(p, precision="fp32k", raise_on_blowup=False)
+    assert o64["status"] == 6 and o32["status"] == 6
+    b64, b32 = o64["stats"]["blowup_step"], o32["stats"]["blowup_step"]
+    assert 200 < b64 < 400 and abs(b32 - b64) <= 3, (b64, b32)
+
+
+def test_group_launch_matches_separate_plans(oracle):
+    from seisfem_b200.api import Context, Group, Plan
+    probs = config_3b(count=3, lo=20, hi=50, step=202, pml=4)
+    assert len({p.mesh.node_num for p in probs}) == 3
+    ctxs = [Context(0) for _ in probs]
+    for c, p in zip(ctxs, probs):
+        c.setup(p)
+    plans = [Plan(c, p, precision="fp32k", snap_every=200) for c, p in zip(ctxs, probs)]
+    alone = []
+    for pl in plans:
+        pl.launch(0)
+        alone.append(pl.finish(0))
+    grp = Group(plans)
+    assert grp.launches == sum(pl.launches for pl in plans)
+    for _ in range(2):       # twice: every launch starts from the zero state
+        grp.launch()
+        for c in ctxs:
+            c.L.sfg_sync(c.ptr)
+        for pl, a, p in zip(plans, alone, probs):
+            out = pl.finish(0)
+            for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+                assert np.array_equal(out[k], a[k]), k
+    ref = oracle.run(probs[1])
+    got = plans[1].finish(0)
+    for k in ("seis_u", "seis_w"):
+        assert rel_l2(got[k], ref[k]) < FP32_TOL, k
+    grp.close()
+    for pl in plans:
+        pl.close()
+    for c in ctxs:
+        c.close()
