@@ -35,7 +35,7 @@ from seisfem_b200 import problem as P  # noqa: E402
 METRIC = "DOF-steps/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.txt")
-T6_STABLE_STEPS = 202
+T6_STABLE_STEPS = 602
 
 
 def workload(name: str, rank: int = 0):
