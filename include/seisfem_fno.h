@@ -37,9 +37,13 @@ typedef struct {
     int M, N, K, batch1, batch2, splits;
     float alpha, beta;
     int c_bf16, gelu, bias_on_m, atomic;
+    int engine;                    /* 0: automatic, 1: mma.sync tiles, 2: tcgen05 with TMEM accumulators */
 } sfg_gemm_desc;
 
 int sfg_fno_gemm(const sfg_gemm_desc *d, void *stream);
+/* waits of the tcgen05 GEMM that gave up (bounded mbarrier waits) since the
+ * last reset; a non-zero count means some outputs were not written */
+int sfg_fno_tc_timeouts(int *count, int reset);
 
 /* forward DFT recombination: P[z][64][32] (FP32; rows 0-31 cos, 32-63 sin
  * times [Yre | Yim]) -> Zmix[mode = k1*16+k2][b][ri][c] (BF16), z = b*C + c */

@@ -220,6 +220,226 @@ __global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
             }
 }
 
+// ------------------------------------------------------ tcgen05 GEMM
+//
+// The same descriptor semantics on the 5th-generation tensor cores: a CTA of
+// 128 threads owns a 128 x BN tile of C held in tensor memory (BN FP32
+// columns, one TMEM lane per row).  Each 64-deep K tile of A (128 x 64) and B
+// (BN x 64) is loaded by all threads (the generic strided loads above) into
+// shared memory in the canonical K-major no-swizzle layout: 8-row x 16-byte
+// core matrices, the eight K chunks of a row group adjacent (LBO = 128 B) and
+// row groups 1024 B apart (SBO).  One elected thread issues four
+// tcgen05.mma.kind::f16 (BF16 x BF16 -> FP32, M = 128, N = BN, K = 16) per
+// tile and commits them to the stage's mbarrier; two stages alternate, so the
+// next tile's global loads overlap the MMAs.  Every wait is bounded: on a
+// timeout the kernel records it in g_tc_timeouts and finishes without it.
+
+constexpr int TBK = 64;
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ int g_tc_timeouts;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kWaitLimit; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    // start address >> 4 | LBO (128 B) >> 4 << 16 | SBO (1024 B) >> 4 << 32 | version 1 << 46 | no swizzle
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+// K-major canonical layout of a rows x 64 tile: element (r, k) at byte
+// ((r / 8) * 8 + k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2.
+template <int R>
+struct TcLoad {
+    static constexpr int NV = R * TBK / 8 / 128;   // 16-byte vectors per thread
+    uint4 v[NV];
+
+    __device__ __forceinline__ void load(const __nv_bfloat16 *p, long long sr, long long sk, int rows, int kk,
+                                         int r0, int k0, int mode)
+    {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            const int idx = t + q * 128;
+            __align__(16) __nv_bfloat16 e[8];
+            if (mode == 1) {            // 8 consecutive rows of one k
+                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
+                const int gr = r0 + r, gk = k0 + kc;
+                if (gk < kk && gr + 8 <= rows) {
+                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr + gk * sk));
+                    continue;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    e[u] = (gr + u < rows && gk < kk) ? p[(gr + u) * sr + gk * sk] : __float2bfloat16(0.f);
+            } else {                    // 8 consecutive k of one row
+                const int r = idx / (TBK / 8), kc = (idx % (TBK / 8)) * 8;
+                const int gr = r0 + r, gk = k0 + kc;
+                if (mode == 0 && gr < rows && gk + 8 <= kk) {
+                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr * sr + gk));
+                    continue;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    e[u] = (gr < rows && gk + u < kk) ? p[gr * sr + (gk + u) * sk] : __float2bfloat16(0.f);
+            }
+            v[q] = *reinterpret_cast<const uint4 *>(e);
+        }
+    }
+
+    __device__ __forceinline__ void store(unsigned char *s, int mode) const
+    {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            const int idx = t + q * 128;
+            if (mode == 1) {
+                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
+                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[q]);
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int rr = r + u;
+                    *reinterpret_cast<__nv_bfloat16 *>(s + ((rr / 8) * 8 + kc / 8) * 128 + (rr % 8) * 16 +
+                                                       (kc % 8) * 2) = e[u];
+                }
+            } else {
+                const int r = idx / (TBK / 8), kc = (idx % (TBK / 8)) * 8;
+                *reinterpret_cast<uint4 *>(s + ((r / 8) * 8 + kc / 8) * 128 + (r % 8) * 16) = v[q];
+            }
+        }
+    }
+};
+
+template <int BN>
+__global__ void __launch_bounds__(128) gemm_tc_kernel(const GemmArgs g)
+{
+    constexpr int BM = 128;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *As = smem;                                  // [2][128 * 64 * 2 B]
+    unsigned char *Bs = smem + 2 * BM * TBK * 2;               // [2][BN * 64 * 2 B]
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_base;
+    const sfg_gemm_desc &d = g.d;
+    const int nb = d.batch1 * d.batch2;
+    const int z = blockIdx.z % nb, split = blockIdx.z / nb;
+    const int z1 = z / d.batch2, z2 = z % d.batch2;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ktiles = (d.K + TBK - 1) / TBK;
+    const int per = (ktiles + d.splits - 1) / d.splits;
+    const int kt0 = split * per, kt1 = min(ktiles, kt0 + per);
+    const __nv_bfloat16 *A = static_cast<const __nv_bfloat16 *>(d.A) + z1 * d.sa1 + z2 * d.sa2;
+    const __nv_bfloat16 *B = static_cast<const __nv_bfloat16 *>(d.B) + z1 * d.sb1 + z2 * d.sb2;
+    const long long cz = z1 * d.sc1 + z2 * d.sc2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    TcLoad<BM> la;
+    TcLoad<BN> lb;
+    for (int kt = kt0; kt < kt1; kt++) {
+        const int it = kt - kt0, st = it & 1;
+        la.load(A, d.sam, d.sak, d.M, d.K, m0, kt * TBK, g.amode);
+        lb.load(B, d.sbn, d.sbk, d.N, d.K, n0, kt * TBK, g.bmode);
+        if (it >= 2) ok = mbar_wait(st ? bar1 : bar0, ((it - 2) >> 1) & 1) && ok;   // stage free again
+        la.store(As + st * BM * TBK * 2, g.amode);
+        lb.store(Bs + st * BN * TBK * 2, g.bmode);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(As + st * BM * TBK * 2), b0 = smem_u32(Bs + st * BN * TBK * 2);
+#pragma unroll
+            for (int ks = 0; ks < TBK / 16; ks++) {
+                const uint64_t da = umma_desc(a0 + ks * 256), db = umma_desc(b0 + ks * 256);
+                const uint32_t acc = (it > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                st ? bar1 : bar0));
+        }
+    }
+    const int nt = kt1 - kt0;
+    if (nt > 0) {
+        const int last = nt - 1;
+        ok = mbar_wait((last & 1) ? bar1 : bar0, (last >> 1) & 1) && ok;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok && lane == 0) atomicAdd(&g_tc_timeouts, 1);
+    // epilogue: warp w holds rows 32w .. 32w+31, thread = row
+    const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (nt == 0 || !ok || m >= d.M) continue;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int n = n0 + c0 + j;
+            if (n >= d.N) continue;
+            const long long o = cz + m * d.scm + n * d.scn;
+            float v = d.alpha * __uint_as_float(r[j]);
+            if (d.atomic) {
+                atomicAdd(static_cast<float *>(d.C) + o, v);
+                continue;
+            }
+            if (d.Cin) v += d.beta * d.Cin[o];
+            if (d.bias) v += d.bias[d.bias_on_m ? m : n];
+            if (d.pre) static_cast<__nv_bfloat16 *>(d.pre)[o] = __float2bfloat16(v);
+            if (d.gelu) v = gelu_f(v);
+            if (d.c_bf16) static_cast<__nv_bfloat16 *>(d.C)[o] = __float2bfloat16(v);
+            else static_cast<float *>(d.C)[o] = v;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
 // Vector loads need 16-byte aligned groups of 8 elements: the base pointer
 // and every stride other than the contiguous one must keep that alignment.
 int pick_mode(long long s_row, long long s_k, long long s1, long long s2, const void *p)
@@ -422,7 +642,35 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : 2; }
 
 }  // namespace
 
+// The automatic engine choice: tcgen05 tiles for GEMMs with at least one
+// full 128-row tile, 32 columns and 64-deep K; mma.sync tiles otherwise.
+bool tc_auto(const sfg_gemm_desc &d) { return d.M >= 128 && d.N >= 32 && d.K >= 64; }
+
+template <int BN>
+int launch_tc(const GemmArgs &g, long long nb, cudaStream_t st)
+{
+    const sfg_gemm_desc &d = g.d;
+    const int smem = 2 * 128 * TBK * 2 + 2 * BN * TBK * 2;
+    if (cudaFuncSetAttribute(gemm_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return 2;
+    dim3 grid((d.N + BN - 1) / BN, (d.M + 127) / 128, (unsigned)nb);
+    if (grid.y > 65535) return 1;
+    gemm_tc_kernel<BN><<<grid, 128, smem, st>>>(g);
+    return launched();
+}
+
 extern "C" {
+
+int sfg_fno_tc_timeouts(int *count, int reset)
+{
+    if (!count) return 1;
+    if (cudaMemcpyFromSymbol(count, g_tc_timeouts, sizeof(int)) != cudaSuccess) return 2;
+    if (reset) {
+        const int zero = 0;
+        if (cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)) != cudaSuccess) return 2;
+    }
+    return 0;
+}
 
 int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
 {
@@ -440,6 +688,12 @@ int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
     g.amode = pick_mode(d.sam, d.sak, d.sa1, d.sa2, d.A);
     g.bmode = pick_mode(d.sbn, d.sbk, d.sb1, d.sb2, d.B);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool tc = d.engine == 2 || (d.engine == 0 && tc_auto(d));
+    if (tc && d.N >= 32) {
+        if (d.N >= 128) return launch_tc<128>(g, nb, st);
+        if (d.N >= 64) return launch_tc<64>(g, nb, st);
+        return launch_tc<32>(g, nb, st);
+    }
     if (d.M >= 128 && d.N >= 128) {
         dim3 grid((d.N + 127) / 128, (d.M + 127) / 128, (unsigned)nb);
         if (grid.y > 65535) return 1;

@@ -43,7 +43,8 @@ class GemmDesc(C.Structure):
                 ("sc1", C.c_longlong), ("sc2", C.c_longlong), ("scm", C.c_longlong), ("scn", C.c_longlong),
                 ("M", C.c_int), ("N", C.c_int), ("K", C.c_int), ("batch1", C.c_int), ("batch2", C.c_int),
                 ("splits", C.c_int), ("alpha", C.c_float), ("beta", C.c_float),
-                ("c_bf16", C.c_int), ("gelu", C.c_int), ("bias_on_m", C.c_int), ("atomic", C.c_int)]
+                ("c_bf16", C.c_int), ("gelu", C.c_int), ("bias_on_m", C.c_int), ("atomic", C.c_int),
+                ("engine", C.c_int)]
 
 
 def _ptr(t, off=0):
@@ -58,6 +59,7 @@ class Kernels:
         self.stream = stream
         self.launches = 0
         self.flops = 0          # 2 M N K per problem of every GEMM issued
+        self.engine = 1         # GEMM engine: 0 automatic, 1 mma.sync (measured faster here), 2 tcgen05
         f = self.L.sfg_fno_gemm
         f.argtypes = [C.POINTER(GemmDesc), C.c_void_p]
         for n, a in [("sfg_fno_dft_combine", [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
@@ -84,8 +86,9 @@ class Kernels:
 
     def gemm(self, A, B, Cout, M, N, K, a=(0, 0, 0, 0), b=(0, 0, 0, 0), c=(0, 0, 0, 0), batch=(1, 1),
              aoff=0, boff=0, coff=0, Cin=None, pre=None, bias=None, bias_on_m=False, gelu=False,
-             alpha=1.0, beta=1.0, atomic=False, splits=1):
-        """Strides are (level-1 batch, level-2 batch, row, col) in elements."""
+             alpha=1.0, beta=1.0, atomic=False, splits=1, engine=None):
+        """Strides are (level-1 batch, level-2 batch, row, col) in elements;
+        engine 0 automatic, 1 mma.sync, 2 tcgen05 (default: self.engine)."""
         d = GemmDesc()
         d.A, d.B, d.C = _ptr(A, aoff), _ptr(B, boff), _ptr(Cout, coff)
         d.Cin = _ptr(Cin, coff) if Cin is not None else None
@@ -100,6 +103,7 @@ class Kernels:
         import torch
         d.c_bf16 = int(Cout.dtype == torch.bfloat16)
         d.gelu, d.bias_on_m, d.atomic = int(gelu), int(bias_on_m), int(atomic)
+        d.engine = self.engine if engine is None else engine
         self.flops += 2 * M * N * K * batch[0] * batch[1]
         self._check(self.L.sfg_fno_gemm(C.byref(d), self.stream), "sfg_fno_gemm")
 

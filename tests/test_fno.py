@@ -119,6 +119,50 @@ def test_gemm_matches_fp32(layout):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("N,Kd,layout", [(32, 64, "nn"), (64, 100, "tn"), (128, 300, "nt"), (200, 128, "nn"),
+                                         (96, 64, "strided")])
+def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
+    """The tcgen05/TMEM engine against the mma.sync engine on the same
+    descriptor (both accumulate in FP32), incl. ragged M, N, K and every
+    load path; no bounded wait may give up."""
+    import ctypes
+    import torch
+    from seisfem_b200.surrogate import Kernels
+    K = Kernels()
+    dev = torch.device("cuda:0")
+    cnt = ctypes.c_int()
+    assert K.L.sfg_fno_tc_timeouts(ctypes.byref(cnt), 1) == 0
+    rng = np.random.default_rng(N + Kd)
+    b1, M = 2, 300
+    A = torch.tensor(rng.standard_normal((b1, M, Kd)).astype(np.float32)).to(torch.bfloat16)
+    B = torch.tensor(rng.standard_normal((b1, Kd, N)).astype(np.float32)).to(torch.bfloat16)
+    bias = torch.tensor(rng.standard_normal(N).astype(np.float32), device=dev)
+    if layout in ("tn", "strided"):
+        Ad, sa = A.transpose(1, 2).contiguous().to(dev), (Kd * M, 0, 1, M)
+    else:
+        Ad, sa = A.contiguous().to(dev), (M * Kd, 0, Kd, 1)
+    if layout == "nt":
+        Bd, sb = B.transpose(1, 2).contiguous().to(dev), (N * Kd, 0, 1, Kd)
+    else:
+        Bd, sb = B.contiguous().to(dev), (Kd * N, 0, N, 1)
+    if layout == "strided":
+        Ad2 = torch.zeros(Ad.numel() * 3, dtype=torch.bfloat16, device=dev)
+        Ad2[::3] = Ad.reshape(-1)
+        Ad, sa = Ad2, tuple(3 * v for v in sa)
+    outs = []
+    for eng in (1, 2):
+        C = torch.empty((b1, M, N), dtype=torch.float32, device=dev)
+        K.gemm(Ad, Bd, C, M, N, Kd, a=sa, b=sb, c=(M * N, 0, N, 1), batch=(b1, 1), bias=bias, gelu=True,
+               engine=eng)
+        outs.append(C.cpu().numpy())
+    torch.cuda.synchronize()
+    assert K.L.sfg_fno_tc_timeouts(ctypes.byref(cnt), 1) == 0 and cnt.value == 0
+    ref = torch.nn.functional.gelu(A.float() @ B.float() + bias.cpu()).numpy()
+    assert _rel(outs[1], outs[0]) < 1e-5
+    assert _rel(outs[1], ref) < 2e-3
+
+
+@pytest.mark.gpu
 def test_gemm_split_k_and_batch_sum():
     import torch
     from seisfem_b200.surrogate import Kernels
