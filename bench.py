@@ -307,6 +307,46 @@ def run_group(args):
     return 0
 
 
+def run_gemm_engines(args):
+    """The surrogate's GEMM descriptors timed on both engines of
+    sfg_fno_gemm (mma.sync tiles, tcgen05 with TMEM accumulators)."""
+    import torch
+    from seisfem_b200.surrogate import Kernels
+    K = Kernels()
+    dev = torch.device("cuda", 0)
+    WT, Hp, Cc = 64000, 128, 64
+    cases = [("head 1: M=64000 N=128 K=64 x16, A m-contiguous", WT, Hp, Cc, (16, 1), (Cc * WT, 0, 1, WT),
+              (0, 0, Hp, 1), (WT * Hp, 0, Hp, 1), 16 * Cc * WT, Cc * Hp, 16 * WT * Hp, torch.bfloat16),
+             ("head 1, A k-contiguous", WT, Hp, Cc, (16, 1), (Cc * WT, 0, Cc, 1), (0, 0, Hp, 1), (WT * Hp, 0, Hp, 1),
+              16 * Cc * WT, Cc * Hp, 16 * WT * Hp, torch.bfloat16),
+             ("8192 x 8192 x 1024, FP32 out", 8192, 8192, 1024, (1, 1), (0, 0, 1024, 1), (0, 0, 1, 1024),
+              (0, 0, 8192, 1), 8192 * 1024, 8192 * 1024, 8192 * 8192, torch.float32),
+             ("W-DFT: M=131072 N=32 K=64", 131072, 32, 64, (1, 1), (0, 0, 64, 1), (0, 0, 32, 1), (0, 0, 32, 1),
+              131072 * 64, 64 * 32, 131072 * 32, torch.bfloat16),
+             ("time map: M=64 N=1000 K=128 x1024", 64, 1000, 128, (1024, 1), (128 * 64, 0, 1, 64), (0, 0, 1000, 1),
+              (64 * 1000, 0, 1000, 1), 1024 * 128 * 64, 128 * 1000, 1024 * 64 * 1000, torch.bfloat16)]
+    out = []
+    for name, M, N, Kd, batch, a, b, c, asz, bsz, csz, cdt in cases:
+        A = torch.randn(asz, device=dev).to(torch.bfloat16)
+        B = torch.randn(bsz, device=dev).to(torch.bfloat16)
+        C = torch.empty(csz, device=dev, dtype=cdt)
+        row = {"gemm": name, "flops": 2 * M * N * Kd * batch[0] * batch[1]}
+        for eng, key in ((1, "mma_sync_us"), (2, "tcgen05_us")):
+            for _ in range(max(3, args.warmup)):
+                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            row[key] = e0.elapsed_time(e1) / 10 * 1e3
+        out.append(row)
+        print(json.dumps(row), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,6 +371,8 @@ def main():
         return run_surrogate(args)
     if args.workload == "q4_16meshes":
         return run_group(args)
+    if args.workload == "fno_gemm_engines":
+        return run_gemm_engines(args)
 
     import torch
     import torch.distributed as dist
