@@ -10,6 +10,7 @@
 #include <tuple>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -44,6 +45,7 @@ struct sfg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;       // second branch of each step (class-Z kernel)
+    cudaStream_t stream3 = nullptr;       // output copies that overlap a running loop
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     bool ready = false;
@@ -57,6 +59,10 @@ struct sfg_ctx {
     RunCache tune;
     // plain-path CSR (FP32) built on first use
     float *plain_x[7] = {nullptr};
+    // run buffers come from a stream-ordered pool (no device-wide
+    // synchronisation per run); one pool per device, shared by the contexts
+    // of the process and kept for its lifetime
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -87,6 +93,55 @@ cudaError_t upload(T **d, const T *h, size_t n, cudaStream_t st)
     if (e != cudaSuccess) return e;
     if (n) e = cudaMemcpyAsync(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st);
     return e;
+}
+
+// Stream-ordered allocation from the context's pool on its stream.
+template <typename T>
+cudaError_t palloc(sfg_ctx *ctx, T **p, size_t bytes)
+{
+    return cudaMallocFromPoolAsync((void **)p, std::max<size_t>(bytes, 1), ctx->pool, ctx->stream);
+}
+
+template <typename T>
+void pfree(sfg_ctx *ctx, T *&p)
+{
+    if (p) cudaFreeAsync(p, ctx->stream);
+    p = nullptr;
+}
+
+// Copy `bytes` of device memory to `dst` (host or device) on stream `st` and
+// wait for it.  (A pinned double-buffered staging path measured slower than
+// the driver's own transfer of pageable memory here.)
+cudaError_t copy_out(sfg_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st)
+{
+    (void)ctx;
+    if (!bytes) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+// The stream-ordered pool of a device: created on first use, retains up to
+// 8 GiB of freed run buffers for the next run.
+cudaMemPool_t device_pool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    uint64_t keep = 8ull << 30;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        return nullptr;
+    }
+    pools[device] = pool;
+    return pool;
 }
 
 int type_code_of(const char *t)
@@ -139,9 +194,14 @@ sfg_ctx *sfg_create(int device)
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream3, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         delete c;
+        return nullptr;
+    }
+    if ((c->pool = device_pool(device)) == nullptr) {
+        sfg_destroy(c);
         return nullptr;
     }
     std::memset(&c->stats, 0, sizeof c->stats);
@@ -156,10 +216,11 @@ void sfg_destroy(sfg_ctx *c)
     cudaStreamSynchronize(c->stream);
     free_problem(c->P);
     for (auto &p : c->plain_x) cudaFree(p);
-    cudaStreamDestroy(c->stream);
-    cudaStreamDestroy(c->stream2);
-    cudaEventDestroy(c->ev_fork);
-    cudaEventDestroy(c->ev_join);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->stream3) cudaStreamDestroy(c->stream3);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
 }
 
@@ -178,6 +239,25 @@ int sfg_get_stats(const sfg_ctx *c, sfg_stats *s)
     *s = c->stats;
     return SFG_OK;
 }
+
+// Phase trace for set-up and runs: with SFG_TRACE=1 in the environment each
+// phase waits for its stream and prints its wall time to stderr.
+struct PhaseTrace {
+    bool on;
+    cudaStream_t st;
+    std::chrono::steady_clock::time_point t;
+    explicit PhaseTrace(cudaStream_t s) : on(std::getenv("SFG_TRACE") != nullptr), st(s),
+                                         t(std::chrono::steady_clock::now()) {}
+    void mark(const char *name)
+    {
+        if (!on) return;
+        cudaStreamSynchronize(st);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[sfg] %-28s %8.2f ms\n", name,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
 
 // ------------------------------------------------------------------ set-up
 
@@ -223,6 +303,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
 
     // element matrices: consistent mass (with rho) and stiffness types 1..6
     const int mats[7] = {-1, 1, 2, 3, 4, 5, 6};
+    PhaseTrace tr(st);
+    tr.mark("setup: uploads");
     CK(launch_element_coo(tc, E, d_en, d_x, d_y, d_rho, 7, mats, d_ci, d_cj, d_cx, d_flags, st));
     int hflags = 0;
     CK(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -233,7 +315,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         return fail(ctx, SFG_ERR_ZERO_AREA, "an element has zero area");
     }
     CanonOut co;
+    tr.mark("setup: element matrices");
     int rc = canonicalize(N, nnz, d_ci, d_cj, d_cx, 7, true, true, co, d_flags, st, ctx->err);
+    tr.mark("setup: canonical CSR");
     if (rc != SFG_OK) {
         canon_free(co, false);
         cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
@@ -257,6 +341,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     const double tx = m->edge_size * m->pml_nx, ty = m->edge_size * m->pml_ny;
     const double d0x = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * tx);
     const double d0y = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * ty);
+    tr.mark("setup: lumped mass");
     CK(cudaMalloc(&P.mpml, sizeof(double) * 6 * (size_t)N));
     CK(launch_mpml(N, d_x, d_y, co.row_start, d0x, d0y, tx, ty, m->xmin + tx, m->xmax - tx, m->ymin + ty,
                    m->ymax - ty, 1, 1 - m->free_surface, 1, 1, P.mpml, st));
@@ -279,58 +364,25 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     // rest.  Inside each class, windows of 2048 rows are ordered by (M-PML
     // flag, decreasing length) so that 32-row SELL slices need no padding.
     {
-        // the context stream is non-blocking: finish its work (M-PML profiles,
-        // union pattern) before the host reads the results
+        int na = 0, npml = 0;
+        CK(build_classes(N, P.up, P.uj, P.mpml, P.max_row_len, &P.perm, &P.inv, &P.upp, &na, &npml, st));
+        std::vector<int> perm(N), inv(N);
+        CK(cudaMemcpyAsync(perm.data(), P.perm, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(inv.data(), P.inv, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        const long long nz_all = P.union_nnz;
-        std::vector<int> hup((size_t)N + 1), huj((size_t)std::max<long long>(nz_all, 1));
-        std::vector<double> hmp(4 * (size_t)N);
-        CK(cudaMemcpy(hup.data(), P.up, sizeof(int) * ((size_t)N + 1), cudaMemcpyDeviceToHost));
-        if (nz_all) CK(cudaMemcpy(huj.data(), P.uj, sizeof(int) * nz_all, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(hmp.data(), P.mpml, sizeof(double) * 4 * (size_t)N, cudaMemcpyDeviceToHost));
-        std::vector<char> pml(N, 0), zone(N, 0);
-        for (int r = 0; r < N; r++)
-            for (int k = 0; k < 4; k++)
-                if ((float)hmp[(size_t)k * N + r] != 0.f) pml[r] = 1;
-        for (int r = 0; r < N; r++)
-            if (pml[r]) {
-                zone[r] = 1;
-                for (int e = hup[r]; e < hup[r + 1]; e++) zone[huj[e]] = 1;
-            }
-        std::vector<int> perm;
-        perm.reserve(N);
-        for (int r = 0; r < N; r++) if (!zone[r]) perm.push_back(r);
-        const int na = (int)perm.size();
-        for (int r = 0; r < N; r++) if (zone[r]) perm.push_back(r);
-        const int sigma = 2048;
-        auto len = [&](int r) { return hup[r + 1] - hup[r]; };
-        for (int c = 0; c < 2; c++) {
-            const int r0 = c == 0 ? 0 : na, r1 = c == 0 ? na : N;
-            for (int w0 = r0; w0 < r1; w0 += sigma) {
-                const int w1 = std::min(r1, w0 + sigma);
-                std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int a, int b) {
-                    if (pml[a] != pml[b]) return pml[a] < pml[b];
-                    return len(a) > len(b);
-                });
-            }
-        }
-        std::vector<int> inv(N), upp((size_t)N + 1, 0);
-        for (int r = 0; r < N; r++) inv[perm[r]] = r;
-        for (int r = 0; r < N; r++) upp[r + 1] = upp[r] + len(perm[r]);
-        CK(upload(&P.perm, perm.data(), (size_t)N, st));
-        CK(upload(&P.inv, inv.data(), (size_t)N, st));
-        CK(upload(&P.upp, upp.data(), (size_t)N + 1, st));
         P.h_inv = std::move(inv);
         P.h_perm = std::move(perm);
         P.na = na;
         ctx->stats.interior_rows = na;
-        ctx->stats.pml_rows = (int)std::count(pml.begin(), pml.end(), 1);
+        ctx->stats.pml_rows = npml;
     }
+    tr.mark("setup: M-PML, coef, classes");
     CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA, &P.slotsA, st));
     CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ, &P.slotsZ, st));
     CK(build_rec_perm(N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, P.upp, &P.recp, st));
     CK(build_coef2(N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, st));
     CK(cudaStreamSynchronize(st));
+    tr.mark("setup: SELL, records");
     canon_free(co, true);
     cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
     cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx); cudaFree(d_scr);
@@ -453,22 +505,24 @@ struct BatchBufs {
     float *pst = nullptr, *peq = nullptr, *prhs = nullptr, *panew = nullptr;
 };
 
-void free_bufs(BatchBufs &b)
+// Buffers return to the context's pool; the caller has waited for every
+// stream that used them.
+void free_bufs(sfg_ctx *ctx, BatchBufs &b)
 {
     for (int k = 0; k < 2; k++) {
-        cudaFree(b.G[k]); cudaFree(b.Pv[k]);
-        cudaFree(b.Gc[k]); cudaFree(b.Pa[k]); cudaFree(b.Gs[k]); cudaFree(b.Ps[k]);
+        pfree(ctx, b.G[k]); pfree(ctx, b.Pv[k]);
+        pfree(ctx, b.Gc[k]); pfree(ctx, b.Pa[k]); pfree(ctx, b.Gs[k]); pfree(ctx, b.Ps[k]);
     }
-    cudaFree(b.src); cudaFree(b.rec); cudaFree(b.amp); cudaFree(b.seis_u); cudaFree(b.seis_w);
-    cudaFree(b.snap_u); cudaFree(b.snap_w); cudaFree(b.energy);
-    cudaFree(b.pst); cudaFree(b.peq); cudaFree(b.prhs); cudaFree(b.panew);
+    pfree(ctx, b.src); pfree(ctx, b.rec); pfree(ctx, b.amp); pfree(ctx, b.seis_u); pfree(ctx, b.seis_w);
+    pfree(ctx, b.snap_u); pfree(ctx, b.snap_w); pfree(ctx, b.energy);
+    pfree(ctx, b.pst); pfree(ctx, b.peq); pfree(ctx, b.prhs); pfree(ctx, b.panew);
     b = BatchBufs();
 }
 
 // Queue the whole time loop of one batch on `st` (captured into a graph by
 // the caller).  Returns the number of kernels queued, or -1 on a launch error.
 int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b, int snap_every,
-               int nsnap, int steps_to_run, cudaStream_t st)
+               int nsnap, int steps_to_run, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr)
 {
     const DevProblem &P = ctx->P;
     const int N = P.node_num, S = pl.S, R = run->rec_num, rows = run->step - 2;
@@ -542,6 +596,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
                 e = launch_snapshot2({b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, N, P.na, S, P.perm, b.snap_u + off,
                                      b.snap_w + off, (long long)nsnap * N, st);
             if (e != cudaSuccess) return -1;
+            if (snap_done && cudaEventRecord((*snap_done)[srow], st) != cudaSuccess) return -1;
             launches++;
             srow++;
         }
@@ -569,39 +624,40 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
     b.gs_bytes = (size_t)std::max(nz, 1) * GS * S * sizeof(float);
     cudaStream_t st = ctx->stream;
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
-        CK(cudaMalloc(&b.pst, sizeof(float) * 36 * (size_t)N));
-        CK(cudaMalloc(&b.peq, sizeof(float) * 22 * (size_t)N));
-        CK(cudaMalloc(&b.prhs, sizeof(float) * 14 * (size_t)N));
-        CK(cudaMalloc(&b.panew, sizeof(float) * 6 * (size_t)N));
+        CK(palloc(ctx, &b.pst, sizeof(float) * 36 * (size_t)N));
+        CK(palloc(ctx, &b.peq, sizeof(float) * 22 * (size_t)N));
+        CK(palloc(ctx, &b.prhs, sizeof(float) * 14 * (size_t)N));
+        CK(palloc(ctx, &b.panew, sizeof(float) * 6 * (size_t)N));
     } else if (pl.kind == SFG_FP64) {
         for (int k = 0; k < 2; k++) {
-            CK(cudaMalloc(&b.G[k], b.gbytes));
-            CK(cudaMalloc(&b.Pv[k], b.pbytes));
+            CK(palloc(ctx, &b.G[k], b.gbytes));
+            CK(palloc(ctx, &b.Pv[k], b.pbytes));
         }
     } else {
         for (int k = 0; k < 2; k++) {
-            CK(cudaMalloc(&b.Gc[k], b.gc_bytes));
-            CK(cudaMalloc(&b.Pa[k], b.pa_bytes));
-            CK(cudaMalloc(&b.Gs[k], b.gs_bytes));
-            CK(cudaMalloc(&b.Ps[k], b.gs_bytes));
+            CK(palloc(ctx, &b.Gc[k], b.gc_bytes));
+            CK(palloc(ctx, &b.Pa[k], b.pa_bytes));
+            CK(palloc(ctx, &b.Gs[k], b.gs_bytes));
+            CK(palloc(ctx, &b.Ps[k], b.gs_bytes));
         }
     }
-    CK(cudaMalloc(&b.src, sizeof(int) * S));
-    CK(cudaMalloc(&b.rec, sizeof(int) * std::max(R, 1)));
+    CK(palloc(ctx, &b.src, sizeof(int) * S));
+    CK(palloc(ctx, &b.rec, sizeof(int) * std::max(R, 1)));
     std::vector<int> rec(run->rec_node, run->rec_node + R);
     if (permuted(pl))
         for (int &r : rec) r = ctx->P.h_inv[r];
-    if (R) CK(cudaMemcpy(b.rec, rec.data(), sizeof(int) * R, cudaMemcpyHostToDevice));
+    if (R) CK(cudaMemcpyAsync(b.rec, rec.data(), sizeof(int) * R, cudaMemcpyHostToDevice, st));
     std::vector<double> amp(run->step, 0.0);
     for (int it = 0; it < run->step; it++) amp[it] = ricker(run->f0, run->t0, 1.0e10, (it + 1) * run->dt);
-    CK(upload(&b.amp, amp.data(), amp.size(), st));
-    CK(cudaMalloc(&b.seis_u, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
-    CK(cudaMalloc(&b.seis_w, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
+    CK(palloc(ctx, &b.amp, sizeof(double) * amp.size()));
+    CK(cudaMemcpyAsync(b.amp, amp.data(), sizeof(double) * amp.size(), cudaMemcpyHostToDevice, st));
+    CK(palloc(ctx, &b.seis_u, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
+    CK(palloc(ctx, &b.seis_w, sizeof(double) * std::max<size_t>((size_t)S * rows * R, 1)));
     if (nsnap > 0) {
-        CK(cudaMalloc(&b.snap_u, sizeof(double) * (size_t)S * nsnap * N));
-        CK(cudaMalloc(&b.snap_w, sizeof(double) * (size_t)S * nsnap * N));
+        CK(palloc(ctx, &b.snap_u, sizeof(double) * (size_t)S * nsnap * N));
+        CK(palloc(ctx, &b.snap_w, sizeof(double) * (size_t)S * nsnap * N));
     }
-    CK(cudaMalloc(&b.energy, sizeof(double) * (size_t)S * run->step * 2));
+    CK(palloc(ctx, &b.energy, sizeof(double) * (size_t)S * run->step * 2));
     CK(cudaStreamSynchronize(st));
     return SFG_OK;
 }
@@ -740,12 +796,15 @@ void plan_free(sfg_plan *p)
     if (!p) return;
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
-    free_bufs(p->b);
+    free_bufs(p->ctx, p->b);
     cudaFree(p->d_src_all);
     delete p;
 }
 
-int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
+// capture = false prepares a plan that queues its kernels directly at each
+// launch instead of replaying a captured graph (one-shot runs whose steps are
+// long enough to hide the launch cost).
+int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capture = true)
 {
     if (!ctx || !run || !out) return SFG_ERR_ARG;
     *out = nullptr;
@@ -787,7 +846,9 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     if (pl.kind == SFG_FP32_PLAIN_PATH && (rc = ensure_plain_matrices(ctx)) != SFG_OK) { plan_free(p); return rc; }
     p->nsnap = sfg_snapshot_rows(run->step, run->snap_every);
     p->nbatch = (run->src_num + pl.S - 1) / pl.S;
+    PhaseTrace tr(ctx->stream);
     if ((rc = alloc_bufs(ctx, pl, &p->run, p->nsnap, p->b)) != SFG_OK) { plan_free(p); return rc; }
+    tr.mark("plan: buffers");
     std::vector<int> staged((size_t)p->nbatch * pl.S, -1);
     for (int s = 0; s < run->src_num; s++)
         staged[s] = permuted(pl) ? ctx->P.h_inv[run->src_node[s]] : run->src_node[s];
@@ -797,28 +858,46 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out)
     if (e == cudaSuccess) e = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     if ((rc = autotune(ctx, pl, &p->run, p->b)) != SFG_OK) { plan_free(p); return rc; }
+    tr.mark("plan: staging, autotune");
     ctx->stats.rows_per_block = pl.S == 1 ? pl.shapeA * 16 + pl.shapeZ : pl.shapeA * 256 + pl.shapeZ;
+    if (!capture) {
+        p->launches = 0;   // counted when the loop is queued
+        CK(cudaStreamSynchronize(st));
+        *out = p;
+        return SFG_OK;
+    }
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(e)); }
     cudaError_t er = queue_reset(pl, N, run->step, p->nsnap, p->b, st);
     p->launches = er == cudaSuccess ? queue_loop(ctx, pl, &p->run, p->b, run->snap_every, p->nsnap, run->step - 2, st) : -1;
     e = cudaStreamEndCapture(st, &p->graph);
     if (p->launches < 0 || e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, "graph capture failed"); }
+    tr.mark("plan: capture");
     e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    tr.mark("plan: instantiate");
     if (e != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
     CK(cudaStreamSynchronize(st));
     *out = p;
     return SFG_OK;
 }
 
-int plan_launch(sfg_plan *p, int batch, cudaStream_t st)
+int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr)
 {
     sfg_ctx *ctx = p->ctx;
     if (batch < 0 || batch >= p->nbatch) return fail(ctx, SFG_ERR_ARG, "batch out of range");
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpyAsync(p->b.src, p->d_src_all + (size_t)batch * p->pl.S, sizeof(int) * p->pl.S,
                        cudaMemcpyDeviceToDevice, st));
-    CK(cudaGraphLaunch(p->exec, st));
+    if (p->exec) {
+        CK(cudaGraphLaunch(p->exec, st));
+        return SFG_OK;
+    }
+    const int N = ctx->N;
+    if (queue_reset(p->pl, N, p->run.step, p->nsnap, p->b, st) != cudaSuccess)
+        return fail(ctx, SFG_ERR_CUDA, "state reset failed");
+    const int n = queue_loop(ctx, p->pl, &p->run, p->b, p->run.snap_every, p->nsnap, p->run.step - 2, st, snap_done);
+    if (n < 0) return fail(ctx, SFG_ERR_CUDA, "launch of the time loop failed");
+    p->launches = n;
     return SFG_OK;
 }
 
@@ -832,10 +911,13 @@ int plan_finish(sfg_plan *p, int batch, double *seis_u, double *seis_w, double *
     const int s0 = batch * S, ns = std::min(S, p->run.src_num - s0);
     CK(cudaStreamSynchronize(st));
     const size_t seis_n = (size_t)ns * rows * R, snap_n = (size_t)ns * p->nsnap * N;
-    if (seis_u && R) CK(cudaMemcpy(seis_u + (size_t)s0 * rows * R, p->b.seis_u, sizeof(double) * seis_n, kind));
-    if (seis_w && R) CK(cudaMemcpy(seis_w + (size_t)s0 * rows * R, p->b.seis_w, sizeof(double) * seis_n, kind));
-    if (p->nsnap > 0 && snap_u) CK(cudaMemcpy(snap_u + (size_t)s0 * p->nsnap * N, p->b.snap_u, sizeof(double) * snap_n, kind));
-    if (p->nsnap > 0 && snap_w) CK(cudaMemcpy(snap_w + (size_t)s0 * p->nsnap * N, p->b.snap_w, sizeof(double) * snap_n, kind));
+    (void)kind;
+    if (seis_u && R) CK(copy_out(ctx, seis_u + (size_t)s0 * rows * R, p->b.seis_u, sizeof(double) * seis_n, st));
+    if (seis_w && R) CK(copy_out(ctx, seis_w + (size_t)s0 * rows * R, p->b.seis_w, sizeof(double) * seis_n, st));
+    if (p->nsnap > 0 && snap_u)
+        CK(copy_out(ctx, snap_u + (size_t)s0 * p->nsnap * N, p->b.snap_u, sizeof(double) * snap_n, st));
+    if (p->nsnap > 0 && snap_w)
+        CK(copy_out(ctx, snap_w + (size_t)s0 * p->nsnap * N, p->b.snap_w, sizeof(double) * snap_n, st));
     std::vector<double> en((size_t)S * step * 2);
     CK(cudaMemcpy(en.data(), p->b.energy, sizeof(double) * en.size(), cudaMemcpyDeviceToHost));
     int status = SFG_OK;
@@ -859,21 +941,53 @@ int run_all(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_
 {
     auto t_all = std::chrono::steady_clock::now();
     sfg_plan *p = nullptr;
-    int rc = plan_create(ctx, run, &p);
+    // steps of large problems take far longer on the GPU than their launches
+    // take on the host: queue them directly instead of capturing a graph
+    const bool big = (long long)ctx->N * std::max(1, std::min(run->src_num, 64)) >= (1LL << 18);
+    int rc = plan_create(ctx, run, &p, !big);
     if (rc) return rc;
     cudaStream_t st = user ? user : ctx->stream;
+    PhaseTrace tr(st);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double loop_ms = 0.0;
     int status = SFG_OK;
     ctx->stats.blowup_step = -1;
+    // direct plans: every snapshot row goes to the caller on the copy stream
+    // as soon as it is written, overlapping the rest of the loop
+    std::vector<cudaEvent_t> snap_done;
+    const bool overlap = !p->exec && p->nsnap > 0 && snap_u && snap_w;
+    for (int k = 0; overlap && k < p->nsnap; k++) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) break;
+        snap_done.push_back(ev);
+    }
+    const bool streamed = overlap && (int)snap_done.size() == p->nsnap;
     for (int bidx = 0; bidx < p->nbatch; bidx++) {
         cudaEventRecord(e0, st);
-        rc = plan_launch(p, bidx, st);
+        rc = plan_launch(p, bidx, st, streamed ? &snap_done : nullptr);
         cudaEventRecord(e1, st);
         if (rc) { status = rc; break; }
-        rc = plan_finish(p, bidx, seis_u, seis_w, snap_u, snap_w, st, kind);
+        if (streamed) {
+            const int S = p->pl.S, N = ctx->N, s0 = bidx * S, ns = std::min(S, run->src_num - s0);
+            for (int k = 0; k < p->nsnap && rc == SFG_OK; k++) {
+                if (cudaStreamWaitEvent(ctx->stream3, snap_done[k], 0) != cudaSuccess) { rc = SFG_ERR_CUDA; break; }
+                for (int sh = 0; sh < ns && rc == SFG_OK; sh++) {
+                    const size_t src = ((size_t)sh * p->nsnap + k) * N, dst = ((size_t)(s0 + sh) * p->nsnap + k) * N;
+                    if (cudaMemcpyAsync(snap_u + dst, p->b.snap_u + src, sizeof(double) * N, cudaMemcpyDefault,
+                                        ctx->stream3) != cudaSuccess ||
+                        cudaMemcpyAsync(snap_w + dst, p->b.snap_w + src, sizeof(double) * N, cudaMemcpyDefault,
+                                        ctx->stream3) != cudaSuccess)
+                        rc = SFG_ERR_CUDA;
+                }
+            }
+            if (cudaStreamSynchronize(ctx->stream3) != cudaSuccess) rc = SFG_ERR_CUDA;
+            if (rc) { status = fail(ctx, rc, "snapshot copies failed"); break; }
+        }
+        tr.mark("run: launch + loop");
+        rc = plan_finish(p, bidx, seis_u, seis_w, streamed ? nullptr : snap_u, streamed ? nullptr : snap_w, st, kind);
+        tr.mark("run: outputs to caller");
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         loop_ms += ms;
@@ -882,10 +996,12 @@ int run_all(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (cudaEvent_t ev : snap_done) cudaEventDestroy(ev);
     ctx->stats.loop_ms = loop_ms;
     ctx->stats.dof_steps = 2LL * ctx->N * run->src_num * (long long)(run->step - 2);
     ctx->stats.kernel_launches = p->launches;
     plan_free(p);
+    tr.mark("run: free");
     ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_all).count();
     return status;
 }

@@ -780,6 +780,99 @@ __global__ void coef2_kernel(int n, int na, const float *__restrict__ coef, cons
     }
 }
 
+// ------------------------------------------------- two-class numbering
+
+// pml[r]: any of dx, dy, dxx, dyy non-zero in FP32 (the step's test)
+__global__ void class_flags(int n, const double *__restrict__ mpml, unsigned char *__restrict__ pml,
+                            unsigned char *__restrict__ zone, int *npml)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    bool f = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) f = f || ((float)mpml[(size_t)k * n + r] != 0.f);
+    pml[r] = f ? 1 : 0;
+    zone[r] = 0;
+    if (f) atomicAdd(npml, 1);
+}
+
+// zone: M-PML rows and every column they reference (idempotent writes)
+__global__ void class_zone(int n, const int *__restrict__ up, const int *__restrict__ uj,
+                           const unsigned char *__restrict__ pml, unsigned char *__restrict__ zone)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n || !pml[r]) return;
+    zone[r] = 1;
+    for (int e = up[r]; e < up[r + 1]; e++) zone[uj[e]] = 1;
+}
+
+__global__ void class_split(int n, const unsigned char *__restrict__ zone, int *__restrict__ isA,
+                            int *__restrict__ isZ)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    isA[r] = zone[r] ? 0 : 1;
+    isZ[r] = zone[r] ? 1 : 0;
+}
+
+// class A rows first, then class Z, each in mesh order
+__global__ void class_scatter(int n, const unsigned char *__restrict__ zone, const int *__restrict__ posA,
+                              const int *__restrict__ posZ, int *__restrict__ perm0)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int na = posA[n];
+    perm0[zone[r] ? na + posZ[r] : posA[r]] = r;
+}
+
+// One block per window of 2048 rows (windows restart at the class boundary):
+// a stable sort by (M-PML flag, decreasing row length) -- a bitonic sort of
+// keys that carry the position in the window as their low 11 bits.
+__global__ void __launch_bounds__(1024) class_windows(int n, int na, int maxlen, const int *__restrict__ up,
+                                                      const unsigned char *__restrict__ pml,
+                                                      const int *__restrict__ perm0, int *__restrict__ perm)
+{
+    constexpr int W = 2048;
+    __shared__ unsigned key[W];
+    const int wa = (na + W - 1) / W;
+    const int w = blockIdx.x;
+    const int w0 = w < wa ? w * W : na + (w - wa) * W;
+    const int w1 = w < wa ? min(na, w0 + W) : min(n, w0 + W);
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        unsigned k = 0xFFFFFFFFu;
+        if (w0 + i < w1) {
+            const int r = perm0[w0 + i];
+            const int len = up[r + 1] - up[r];
+            k = ((unsigned)(pml[r] * (maxlen + 1) + (maxlen - len)) << 11) | (unsigned)i;
+        }
+        key[i] = k;
+    }
+    __syncthreads();
+    for (int k = 2; k <= W; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < W; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const bool asc = (i & k) == 0;
+                    const unsigned a = key[i], b = key[ixj];
+                    if ((a > b) == asc) { key[i] = b; key[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < w1 - w0; i += blockDim.x) perm[w0 + i] = perm0[w0 + (int)(key[i] & 2047u)];
+}
+
+__global__ void class_inverse(int n, const int *__restrict__ perm, const int *__restrict__ up, int *__restrict__ inv,
+                              int *__restrict__ lenp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = perm[i];
+    inv[r] = i;
+    lenp[i] = up[r + 1] - up[r];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------- launchers
@@ -935,6 +1028,56 @@ cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm,
     if ((e = cudaMalloc(d_coefZ, sizeof(float) * CREC * std::max(n - na, 1))) != cudaSuccess) return e;
     if (n) coef2_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, na, d_coef32, d_perm, *d_coefA, *d_imA, *d_coefZ);
     return cudaGetLastError();
+}
+
+
+cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double *d_mpml, int maxlen, int **d_perm,
+                          int **d_inv, int **d_upp, int *na_out, int *npml_out, cudaStream_t st)
+{
+    if (maxlen < 0 || maxlen >= (1 << 19)) return cudaErrorInvalidValue;
+    unsigned char *pml = nullptr, *zone = nullptr;
+    int *isA = nullptr, *isZ = nullptr, *posA = nullptr, *posZ = nullptr, *perm0 = nullptr, *lenp = nullptr,
+        *cnt = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void **p, size_t b) { if (e == cudaSuccess) e = cudaMallocAsync(p, std::max<size_t>(b, 4), st); };
+    A((void **)&pml, n); A((void **)&zone, n);
+    A((void **)&isA, sizeof(int) * n); A((void **)&isZ, sizeof(int) * n);
+    A((void **)&posA, sizeof(int) * (n + 1)); A((void **)&posZ, sizeof(int) * (n + 1));
+    A((void **)&perm0, sizeof(int) * n); A((void **)&lenp, sizeof(int) * n); A((void **)&cnt, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(d_perm, sizeof(int) * std::max(n, 1));
+    if (e == cudaSuccess) e = cudaMalloc(d_inv, sizeof(int) * std::max(n, 1));
+    if (e == cudaSuccess) e = cudaMalloc(d_upp, sizeof(int) * (n + 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(int), st);
+    const int g = (n + 255) / 256;
+    int na = 0, npml = 0;
+    if (e == cudaSuccess && n > 0) {
+        class_flags<<<g, 256, 0, st>>>(n, d_mpml, pml, zone, cnt);
+        class_zone<<<g, 256, 0, st>>>(n, d_up, d_uj, pml, zone);
+        class_split<<<g, 256, 0, st>>>(n, zone, isA, isZ);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = exclusive_scan_int(isA, posA, n, st);
+        if (e == cudaSuccess) e = exclusive_scan_int(isZ, posZ, n, st);
+        if (e == cudaSuccess) {
+            class_scatter<<<g, 256, 0, st>>>(n, zone, posA, posZ, perm0);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&na, posA + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&npml, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) {
+            const int windows = (na + 2047) / 2048 + (n - na + 2047) / 2048;
+            class_windows<<<windows, 1024, 0, st>>>(n, na, maxlen, d_up, pml, perm0, *d_perm);
+            class_inverse<<<g, 256, 0, st>>>(n, *d_perm, d_up, *d_inv, lenp);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = exclusive_scan_int(lenp, *d_upp, n, st);
+    }
+    for (void *p : {(void *)pml, (void *)zone, (void *)isA, (void *)isZ, (void *)posA, (void *)posZ, (void *)perm0,
+                    (void *)lenp, (void *)cnt})
+        if (p) cudaFreeAsync(p, st);
+    *na_out = na;
+    *npml_out = npml;
+    return e;
 }
 
 }  // namespace sfg

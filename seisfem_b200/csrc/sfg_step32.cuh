@@ -79,6 +79,11 @@ cudaError_t build_sell_range(int r0, int r1, const int *d_up, const int *d_uj, c
 // row-major records in the permuted numbering (d_upp: permuted row pointers)
 cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
                            const int *d_perm, const int *d_inv, const int *d_upp, float **d_rec, cudaStream_t st);
+// the two-class numbering on the device: perm (class A, then class Z; windows
+// of 2048 rows stably sorted by M-PML flag and decreasing length), its
+// inverse and the permuted row pointers; na = class-A rows, npml = M-PML rows
+cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double *d_mpml, int maxlen, int **d_perm,
+                          int **d_inv, int **d_upp, int *na, int *npml, cudaStream_t st);
 // class-A / class-Z coefficient arrays from the [n][12] FP32 record
 cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,
                         float **d_coefZ, cudaStream_t st);
