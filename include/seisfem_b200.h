@@ -161,6 +161,18 @@ int sfg_plan_finish(sfg_plan *plan, int batch, double *seis_u, double *seis_w, d
                     double *snap_w, void *stream);
 void sfg_plan_destroy(sfg_plan *plan);
 
+/* One model per shot (no counterpart in the reference, which runs one model
+ * per call): shot s of the run uses models[s] -- the same mesh, its own rho,
+ * vp and c[4] of node_num entries -- while the context's set-up model only
+ * supplies the geometric matrices.  Shots of a batch advance together: the
+ * consistent mass is applied as diag(rho) M_geo, each shot carries its own
+ * constants, lumped mass (the reference's normalisation, per model) and
+ * M-PML scale (d0 is proportional to vp_max).  Compensated FP32 only
+ * (SFG_FP32_KAHAN), batches of 32 or 64 shots (shots_per_batch 0, 32 or 64). */
+int sfg_plan_create_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *models, sfg_plan **plan);
+int sfg_run_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *models, double *seis_u,
+                   double *seis_w, double *snap_u, double *snap_w);
+
 /* Plan groups (no counterpart in the reference): the captured time loops of
  * several single-batch plans -- independent meshes of any sizes, each with
  * the launch shapes its own autotuning picked -- as one CUDA graph with no

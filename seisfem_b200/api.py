@@ -63,7 +63,7 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec",
-           "sfg_abc_mpml_device_noalloc", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
+           "sfg_abc_mpml_device_noalloc", "sfg_plan_create_models", "sfg_run_models", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
            "sfg_group_destroy",
            # learned surrogate (include/seisfem_fno.h)
            "sfg_fno_gemm", "sfg_fno_dft_combine", "sfg_fno_dft_combine_bwd", "sfg_fno_expand_weights",
@@ -98,6 +98,8 @@ def lib(path: str = LIBPATH):
     L.sfg_sync.argtypes = [C.c_void_p]
     L.sfg_plan_create.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.POINTER(C.c_void_p)]
     L.sfg_plan_batches.argtypes = [C.c_void_p]
+    L.sfg_run_models.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.c_void_p] + [C.c_void_p] * 4
+    L.sfg_plan_create_models.argtypes = [C.c_void_p, C.POINTER(RunDesc_), C.c_void_p, C.POINTER(C.c_void_p)]
     L.sfg_group_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     L.sfg_group_launch.argtypes = [C.c_void_p, C.c_void_p]
     L.sfg_group_launches.argtypes = [C.c_void_p]
@@ -217,6 +219,32 @@ class Context:
                         PRECISIONS[precision], snap_every if ns else 0, shots_per_batch)
         rc = self.L.sfg_run(self.ptr, C.byref(desc), out["seis_u"].ctypes.data, out["seis_w"].ctypes.data,
                             out["snap_u"].ctypes.data if ns else None, out["snap_w"].ctypes.data if ns else None)
+        self._check(rc, allow=() if raise_on_blowup else (SFG_ERR_BLOWUP,))
+        out["status"] = rc
+        out["stats"] = self.stats()
+        return out
+
+    def run_models(self, prob: Problem, models, shots_per_batch: int = 0, snap_every: int = 0,
+                   raise_on_blowup: bool = True):
+        """Shot s of prob.src_node runs in models[s] (a Model on this mesh):
+        sfg_run_models, compensated FP32, batches of 32 or 64 shots."""
+        src = np.ascontiguousarray(prob.src_node, np.int32)
+        rec = np.ascontiguousarray(prob.rec_node, np.int32)
+        S, R, step, N = len(src), len(rec), prob.step, prob.mesh.node_num
+        if len(models) != S:
+            raise ValueError("one model per shot")
+        keep = [[np.ascontiguousarray(a, np.float64) for a in (md.rho, md.vp, md.vs, md.c)] for md in models]
+        arr = (Model_ * S)(*[Model_(*(a.ctypes.data for a in k)) for k in keep])
+        ns = self.L.sfg_snapshot_rows(step, snap_every) if snap_every else 0
+        out = {"seis_u": np.zeros((S, step - 2, R)), "seis_w": np.zeros((S, step - 2, R))}
+        if ns:
+            out["snap_u"] = np.zeros((S, ns, N))
+            out["snap_w"] = np.zeros((S, ns, N))
+        desc = RunDesc_(step, prob.dt, prob.f0, prob.t0, S, src.ctypes.data, R, rec.ctypes.data,
+                        PRECISIONS["fp32k"], snap_every if ns else 0, shots_per_batch)
+        rc = self.L.sfg_run_models(self.ptr, C.byref(desc), arr, out["seis_u"].ctypes.data,
+                                   out["seis_w"].ctypes.data, out["snap_u"].ctypes.data if ns else None,
+                                   out["snap_w"].ctypes.data if ns else None)
         self._check(rc, allow=() if raise_on_blowup else (SFG_ERR_BLOWUP,))
         out["status"] = rc
         out["stats"] = self.stats()

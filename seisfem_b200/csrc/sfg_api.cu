@@ -160,7 +160,7 @@ void free_problem(DevProblem &P)
     cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
     cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.perm); cudaFree(P.inv);
     cudaFree(P.sellA); cudaFree(P.sellZ); cudaFree(P.sliceA); cudaFree(P.sliceZ); cudaFree(P.upp);
-    cudaFree(P.recp); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ);
+    cudaFree(P.recp); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ); cudaFree(P.rho0);
     P = DevProblem();
 }
 
@@ -384,8 +384,11 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(cudaStreamSynchronize(st));
     tr.mark("setup: SELL, records");
     canon_free(co, true);
-    cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+    cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_flags);
     cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx); cudaFree(d_scr);
+    P.rho0 = d_rho;
+    P.h_rho0.assign(md->rho, md->rho + N);
+    P.h_dir = std::move(dir);
     for (auto &px : ctx->plain_x) { cudaFree(px); px = nullptr; }
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
@@ -503,6 +506,9 @@ struct BatchBufs {
     double *energy = nullptr;
     // unfused path
     float *pst = nullptr, *peq = nullptr, *prhs = nullptr, *panew = nullptr;
+    // one model per shot: the batch's coefficient streams and the row
+    // records with the geometric mass matrix
+    float *cmm = nullptr, *sig = nullptr, *rec_geo = nullptr;
 };
 
 // Buffers return to the context's pool; the caller has waited for every
@@ -516,6 +522,7 @@ void free_bufs(sfg_ctx *ctx, BatchBufs &b)
     pfree(ctx, b.src); pfree(ctx, b.rec); pfree(ctx, b.amp); pfree(ctx, b.seis_u); pfree(ctx, b.seis_w);
     pfree(ctx, b.snap_u); pfree(ctx, b.snap_w); pfree(ctx, b.energy);
     pfree(ctx, b.pst); pfree(ctx, b.peq); pfree(ctx, b.prhs); pfree(ctx, b.panew);
+    pfree(ctx, b.cmm); pfree(ctx, b.sig); pfree(ctx, b.rec_geo);
     b = BatchBufs();
 }
 
@@ -570,7 +577,8 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             Step2 a;
             a.c = c; a.na = P.na; a.S = S;
             a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
-            a.up = P.upp; a.rec = P.recp; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
+            a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
+            a.cmm = b.cmm; a.sig = b.sig;
             a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
             a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
             const bool comp = pl.kind == SFG_FP32_KAHAN;
@@ -785,6 +793,7 @@ struct sfg_plan {
     int nsnap = 0, nbatch = 0, launches = 0;
     BatchBufs b;
     int *d_src_all = nullptr;
+    float *d_cmm_all = nullptr, *d_sig_all = nullptr;   // one model per shot: [batch][N][6][S], [batch][S]
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -798,13 +807,85 @@ void plan_free(sfg_plan *p)
     if (p->graph) cudaGraphDestroy(p->graph);
     free_bufs(p->ctx, p->b);
     cudaFree(p->d_src_all);
+    cudaFree(p->d_cmm_all);
+    cudaFree(p->d_sig_all);
     delete p;
 }
 
 // capture = false prepares a plan that queues its kernels directly at each
 // launch instead of replaying a captured graph (one-shot runs whose steps are
 // long enough to hide the launch cost).
-int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capture = true)
+// Per-shot coefficient streams of one model per shot (see Step2::cmm): the
+// shot's constants, its lumped mass -- the reference's lumped mass with
+// rho = diag scale: m_i = rho_i d_i * sum(rho R) / sum(rho d), d_i the set-up
+// lumped mass over its density, R the row sums of M_geo -- and its density,
+// in the two-class row order; plus vp_max ratios for the M-PML profiles.
+int build_models(sfg_ctx *ctx, sfg_plan *p, const sfg_model *models)
+{
+    const DevProblem &P = ctx->P;
+    const int N = ctx->N, S = p->pl.S, nb = p->nbatch;
+    cudaStream_t st = ctx->stream;
+    std::vector<double> m0(N), R(N);
+    double *d_R = nullptr;
+    CK(cudaMemcpyAsync(m0.data(), P.mass_lump, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    CK(cudaMallocAsync((void **)&d_R, sizeof(double) * N, st));
+    CK(mass_row_sums_geo(N, P.up, P.ux, P.rho0, d_R, st));
+    CK(cudaMemcpyAsync(R.data(), d_R, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(d_R, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<double> d(N);
+    for (int i = 0; i < N; i++) d[i] = P.h_rho0[i] != 0.0 ? m0[i] / P.h_rho0[i] : 0.0;
+    const int ns = p->run.src_num;
+    std::vector<double> scale(ns);   // sum(rho R) / sum(rho d) per shot
+    std::vector<float> cmm((size_t)nb * N * 6 * S, 0.f), sig((size_t)nb * S, 0.f);
+    for (int g = 0; g < ns; g++) {
+        const sfg_model &md = models[g];
+        if (!md.rho || !md.vp || !md.c) return fail(ctx, SFG_ERR_ARG, "incomplete per-shot model");
+        double sr = 0.0, sd = 0.0, vmax = 0.0;
+        for (int i = 0; i < N; i++) {
+            sr += md.rho[i] * R[i];
+            sd += md.rho[i] * d[i];
+            vmax = std::max(vmax, md.vp[i]);
+        }
+        if (!(sd > 0.0)) return fail(ctx, SFG_ERR_ARG, "per-shot model with zero total mass");
+        scale[g] = sr / sd;
+        sig[(size_t)(g / S) * S + g % S] = (float)(ctx->vp_max > 0.0 ? vmax / ctx->vp_max : 1.0);
+    }
+    // node-major fill: the shot index is innermost in the streams
+    for (int b = 0; b < nb; b++) {
+        const int g0 = b * S, g1 = std::min(ns, g0 + S);
+        float *cb = cmm.data() + (size_t)b * N * 6 * S;
+        for (int i = 0; i < N; i++) {
+            float *row = cb + (size_t)P.h_inv[i] * 6 * S;
+            const bool dir = P.h_dir[i] != 0;
+            for (int g = g0; g < g1; g++) {
+                const sfg_model &md = models[g];
+                const int sh = g - g0;
+                const double m = md.rho[i] * d[i] * scale[g];
+                row[0 * S + sh] = (float)md.c[i];
+                row[1 * S + sh] = (float)md.c[(size_t)N + i];
+                row[2 * S + sh] = (float)md.c[2 * (size_t)N + i];
+                row[3 * S + sh] = (float)md.c[3 * (size_t)N + i];
+                row[4 * S + sh] = (float)((dir || !(m > 0.0)) ? 0.0 : 1.0 / m);
+                row[5 * S + sh] = (float)md.rho[i];
+            }
+        }
+    }
+    CK(upload(&p->d_cmm_all, cmm.data(), cmm.size(), st));
+    CK(upload(&p->d_sig_all, sig.data(), sig.size(), st));
+    CK(palloc(ctx, &p->b.cmm, sizeof(float) * (size_t)N * 6 * S));
+    CK(palloc(ctx, &p->b.sig, sizeof(float) * S));
+    CK(cudaMemcpyAsync(p->b.cmm, p->d_cmm_all, sizeof(float) * (size_t)N * 6 * S, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(p->b.sig, p->d_sig_all, sizeof(float) * S, cudaMemcpyDeviceToDevice, st));
+    float *rg = nullptr;
+    CK(build_rec_geo(N, P.up, P.ux, P.union_nnz, P.perm, P.upp, P.rho0, P.recp, &rg, st));
+    p->b.rec_geo = rg;   // pool-ordered allocation on the context stream
+    CK(cudaStreamSynchronize(st));
+    return SFG_OK;
+}
+
+int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capture = true,
+                const sfg_model *models = nullptr)
 {
     if (!ctx || !run || !out) return SFG_ERR_ARG;
     *out = nullptr;
@@ -833,6 +914,11 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capt
     pl.S = 1; pl.spl = 1; pl.threads = 128; pl.warps = 4; pl.shapeA = 0; pl.shapeZ = 0;
     const bool fp32 = pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN;
     int spb = run->shots_per_batch;
+    if (models && (pl.kind != SFG_FP32_KAHAN || (spb != 0 && spb != 32 && spb != 64))) {
+        plan_free(p);
+        return fail(ctx, SFG_ERR_ARG, "one model per shot: compensated FP32 in batches of 32 or 64 shots");
+    }
+    if (models && spb <= 0) spb = run->src_num > 32 ? 64 : 32;
     if (fp32) {
         if (spb <= 0) spb = run->src_num >= 64 ? 64 : (run->src_num >= 16 ? 32 : 1);
         if (spb != 1 && spb != 32 && spb != 64 && spb != 128) {
@@ -848,6 +934,7 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capt
     p->nbatch = (run->src_num + pl.S - 1) / pl.S;
     PhaseTrace tr(ctx->stream);
     if ((rc = alloc_bufs(ctx, pl, &p->run, p->nsnap, p->b)) != SFG_OK) { plan_free(p); return rc; }
+    if (models && (rc = build_models(ctx, p, models)) != SFG_OK) { plan_free(p); return rc; }
     tr.mark("plan: buffers");
     std::vector<int> staged((size_t)p->nbatch * pl.S, -1);
     for (int s = 0; s < run->src_num; s++)
@@ -888,6 +975,13 @@ int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaE
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpyAsync(p->b.src, p->d_src_all + (size_t)batch * p->pl.S, sizeof(int) * p->pl.S,
                        cudaMemcpyDeviceToDevice, st));
+    if (p->d_cmm_all) {
+        const size_t per = (size_t)ctx->N * 6 * p->pl.S;
+        CK(cudaMemcpyAsync(p->b.cmm, p->d_cmm_all + (size_t)batch * per, sizeof(float) * per,
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(p->b.sig, p->d_sig_all + (size_t)batch * p->pl.S, sizeof(float) * p->pl.S,
+                           cudaMemcpyDeviceToDevice, st));
+    }
     if (p->exec) {
         CK(cudaGraphLaunch(p->exec, st));
         return SFG_OK;
@@ -937,14 +1031,14 @@ int plan_finish(sfg_plan *p, int batch, double *seis_u, double *seis_w, double *
 }
 
 int run_all(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_w, double *snap_u,
-            double *snap_w, cudaStream_t user, cudaMemcpyKind kind)
+            double *snap_w, cudaStream_t user, cudaMemcpyKind kind, const sfg_model *models = nullptr)
 {
     auto t_all = std::chrono::steady_clock::now();
     sfg_plan *p = nullptr;
     // steps of large problems take far longer on the GPU than their launches
     // take on the host: queue them directly instead of capturing a graph
     const bool big = (long long)ctx->N * std::max(1, std::min(run->src_num, 64)) >= (1LL << 18);
-    int rc = plan_create(ctx, run, &p, !big);
+    int rc = plan_create(ctx, run, &p, !big, models);
     if (rc) return rc;
     cudaStream_t st = user ? user : ctx->stream;
     PhaseTrace tr(st);
@@ -1025,6 +1119,19 @@ int sfg_run_device(sfg_ctx *ctx, const sfg_run_desc *run, void *d_seis_u, void *
 }
 
 int sfg_plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **plan) { return plan_create(ctx, run, plan); }
+
+int sfg_plan_create_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *models, sfg_plan **plan)
+{
+    if (!models) return SFG_ERR_ARG;
+    return plan_create(ctx, run, plan, true, models);
+}
+
+int sfg_run_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *models, double *seis_u, double *seis_w,
+                   double *snap_u, double *snap_w)
+{
+    if (!ctx || !models) return SFG_ERR_ARG;
+    return run_all(ctx, run, seis_u, seis_w, snap_u, snap_w, nullptr, cudaMemcpyDefault, models);
+}
 
 int sfg_plan_batches(const sfg_plan *plan) { return plan ? plan->nbatch : 0; }
 

@@ -67,6 +67,11 @@ struct DevProblem {
     float *imA = nullptr;            // [na]
     float *coefZ = nullptr;          // [N - na][12]
     double *coefd = nullptr;         // [N][12] FP64 coefficients for the FP64 step
+    // the set-up model's density and the Dirichlet flags, for runs with one
+    // model per shot (geometric mass matrix, per-shot lumped masses)
+    double *rho0 = nullptr;          // [N] device
+    std::vector<double> h_rho0;
+    std::vector<unsigned char> h_dir;
 };
 
 // ---- assembly (sfg_assemble.cu) ------------------------------------------

@@ -440,7 +440,8 @@ __device__ __forceinline__ void acc_totals(const Entry &e, const VecF<SPL> *x, f
     }
 }
 
-template <bool COMP, int SPL, int S>
+// MM: every shot has its own model (a.cmm, a.sig; see Step2).
+template <bool COMP, int SPL, int S, bool MM>
 __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_batched(const Step2 a)
 {
     __shared__ float se[2 * S];
@@ -497,8 +498,14 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
                 acc_totals<SPL>(ea, xa, kU, kW, mL);
             }
         }
-        const float4 cf = __ldg(a.coefA + i);
-        const float im = __ldg(a.imA + i);
+        const float4 cf = MM ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(a.coefA + i);
+        const float im = MM ? 0.f : __ldg(a.imA + i);
+        VecF<SPL> cm[MM ? 6 : 1];
+        if (MM) {
+            const float *cp = a.cmm + (size_t)i * 6 * S + s_base;
+#pragma unroll
+            for (int v = 0; v < (MM ? 6 : 1); v++) cm[v].load(cp + v * S);
+        }
         const float *gi = a.in.Gc + (size_t)i * GC * S + s_base;
         const float *pi = a.in.Pa + (size_t)i * PA * S + s_base;
         float *go = a.out.Gc + (size_t)i * GC * S + s_base;
@@ -520,9 +527,17 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
             g[0] = gv[0].v[q]; g[1] = gv[1].v[q]; g[10] = gv[10].v[q]; g[11] = gv[11].v[q];
 #pragma unroll
             for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
+            float4 cfq = cf;
+            float imq = im;
+            if (MM) {   // the shot's constants, lumped mass and density (M = diag(rho) M_geo)
+                cfq = make_float4(cm[0].v[q], cm[1].v[q], cm[2].v[q], cm[3].v[q]);
+                imq = cm[4].v[q];
+#pragma unroll
+                for (int t = 0; t < 8; t++) mq[t] *= cm[MM ? 5 : 0].v[q];
+            }
             const bool is_src = (i == src[q]);
             double uu, ww;
-            finish_A<COMP>(kUq, kWq, mq, cf, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
+            finish_A<COMP>(kUq, kWq, mq, cfq, imq, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
 #pragma unroll
             for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
 #pragma unroll
@@ -612,7 +627,7 @@ __device__ __forceinline__ void row_split(const Step2 &a, const float4 *rec, int
     }
 }
 
-template <bool COMP, int SPL, int S>
+template <bool COMP, int SPL, int S, bool MM>
 __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Step2 a)
 {
     __shared__ float se[2 * S];
@@ -654,11 +669,16 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
         float *gco = a.out.Gc + (size_t)i * GC * S + s_base;
         float *so = a.out.Gs + (size_t)local * GS * S + s_base;
         float *po = a.out.Ps + (size_t)local * PS * S + s_base;
-        VecF<SPL> sv[GS], pv[PS], cv[GC];
+        VecF<SPL> sv[GS], pv[PS], cv[GC], cm[MM ? 6 : 1];
 #pragma unroll
         for (int v = 0; v < GS; v++) sv[v].load(si + v * S);
 #pragma unroll
         for (int v = 0; v < PS; v++) pv[v].load(pi + v * S);
+        if (MM) {
+            const float *cp = a.cmm + (size_t)i * 6 * S + s_base;
+#pragma unroll
+            for (int v = 0; v < (MM ? 6 : 1); v++) cm[v].load(cp + v * S);
+        }
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
             float kUq[6], kWq[6], mq[20], gs[GS], ps_[PS], gc[GC];
@@ -668,10 +688,19 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
             for (int t = 0; t < 20; t++) mq[t] = m[t][q];
 #pragma unroll
             for (int v = 0; v < GS; v++) { gs[v] = sv[v].v[q]; ps_[v] = pv[v].v[q]; }
+            float4 c0q = c0, c1q = c1, c2q = c2;
+            if (MM) {   // the shot's constants, lumped mass, density; M-PML profiles scale with its vp_max
+                const float sg = a.sig[s_base + q];
+                c0q = make_float4(cm[0].v[q], cm[1].v[q], cm[2].v[q], cm[3].v[q]);
+                c1q = make_float4(c1.x * sg, c1.y * sg, c1.z * sg, c1.w * sg);
+                c2q = make_float4(cm[4].v[q], c2.y * sg, c2.z * sg, c2.w);
+#pragma unroll
+                for (int t = 0; t < 20; t++) mq[t] *= cm[MM ? 5 : 0].v[q];
+            }
             const bool is_src = (i == src[q]);
             double uu, ww;
-            finish_Z<COMP>(kUq, kWq, mq, c0, c1, c2, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, gs, ps_, gc,
-                           uu, ww);
+            finish_Z<COMP>(kUq, kWq, mq, c0q, c1q, c2q, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, gs, ps_,
+                           gc, uu, ww);
 #pragma unroll
             for (int v = 0; v < GS; v++) { sv[v].v[q] = gs[v]; pv[v].v[q] = ps_[v]; cv[v].v[q] = gc[v]; }
             eu[q] += (float)(uu * uu);
@@ -873,6 +902,30 @@ __global__ void class_inverse(int n, const int *__restrict__ perm, const int *__
     lenp[i] = up[r + 1] - up[r];
 }
 
+// one model per shot: the geometric mass matrix M_geo = M / rho0(row) in
+// plane 1 of the row records, and the row sums of M_geo
+__global__ void rec_geo_fill(int n, const int *__restrict__ up, const double *__restrict__ ux,
+                             const int *__restrict__ perm, const int *__restrict__ upp,
+                             const double *__restrict__ rho0, float *__restrict__ rec)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int o = perm[r];
+    const int a0 = up[o], len = up[o + 1] - a0;
+    const long long d0 = upp[r];
+    for (int k = 0; k < len; k++) rec[(d0 + k) * 8 + 1] = (float)(ux[a0 + k] / rho0[o]);
+}
+
+__global__ void row_sums_geo(int n, const int *__restrict__ up, const double *__restrict__ ux,
+                             const double *__restrict__ rho0, double *__restrict__ out)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    double s = 0.0;
+    for (int e = up[o]; e < up[o + 1]; e++) s += ux[e];
+    out[o] = s / rho0[o];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------- launchers
@@ -930,9 +983,15 @@ static long long batched_grid(K kernel, int threads, long long tasks, int warps,
 
 #define SFG_BATCH_ONE(KERNEL, C, P, SS, ROWS)                                                            \
     do {                                                                                                 \
-        auto k = KERNEL<C, P, SS>;                                                                       \
+        auto k = KERNEL<C, P, SS, false>;                                                                \
         const long long tasks = (long long)(ROWS) * ((SS) / (32 * (P)));                                 \
-        KERNEL<C, P, SS><<<(unsigned)batched_grid(k, threads, tasks, warps, 0), threads, 0, st>>>(a);    \
+        KERNEL<C, P, SS, false><<<(unsigned)batched_grid(k, threads, tasks, warps, 0), threads, 0, st>>>(a); \
+    } while (0)
+#define SFG_BATCH_MM(KERNEL, P, SS, ROWS)                                                                \
+    do {                                                                                                 \
+        auto k = KERNEL<true, P, SS, true>;                                                              \
+        const long long tasks = (long long)(ROWS) * ((SS) / (32 * (P)));                                 \
+        KERNEL<true, P, SS, true><<<(unsigned)batched_grid(k, threads, tasks, warps, 0), threads, 0, st>>>(a); \
     } while (0)
 #define SFG_BATCH_S(KERNEL, C, ROWS)                                                                     \
     do {                                                                                                 \
@@ -951,7 +1010,12 @@ static long long batched_grid(K kernel, int threads, long long tasks, int warps,
             warps % (a.S / (32 * spl)) != 0)                                                             \
             return cudaErrorInvalidValue;                                                                \
         if ((ROWS) <= 0) return cudaSuccess;                                                             \
-        if (comp) SFG_BATCH_S(KERNEL, true, ROWS);                                                       \
+        if (a.cmm) {   /* one model per shot: compensated precision, 32 or 64 shots */                   \
+            if (!comp || a.S > 64 || spl > 2 || !a.sig) return cudaErrorInvalidValue;                     \
+            if (a.S == 32) SFG_BATCH_MM(KERNEL, 1, 32, ROWS);                                            \
+            else if (spl == 1) SFG_BATCH_MM(KERNEL, 1, 64, ROWS);                                        \
+            else SFG_BATCH_MM(KERNEL, 2, 64, ROWS);                                                      \
+        } else if (comp) SFG_BATCH_S(KERNEL, true, ROWS);                                                \
         else SFG_BATCH_S(KERNEL, false, ROWS);                                                           \
     } while (0)
 
@@ -970,6 +1034,7 @@ cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, 
 #undef SFG_BATCH
 #undef SFG_BATCH_S
 #undef SFG_BATCH_ONE
+#undef SFG_BATCH_MM
 
 cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st)
 {
@@ -1078,6 +1143,26 @@ cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double 
     *na_out = na;
     *npml_out = npml;
     return e;
+}
+
+
+cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long nnz, const int *d_perm,
+                          const int *d_upp, const double *d_rho0, const float *d_recp, float **d_rec, cudaStream_t st)
+{
+    cudaError_t e = cudaMallocAsync((void **)d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1), st);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(*d_rec, d_recp, sizeof(float) * 8 * nnz, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && n > 0) {
+        rec_geo_fill<<<(n + 255) / 256, 256, 0, st>>>(n, d_up, d_ux, d_perm, d_upp, d_rho0, *d_rec);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t mass_row_sums_geo(int n, const int *d_up, const double *d_ux, const double *d_rho0, double *d_out,
+                              cudaStream_t st)
+{
+    if (n > 0) row_sums_geo<<<(n + 255) / 256, 256, 0, st>>>(n, d_up, d_ux, d_rho0, d_out);
+    return cudaGetLastError();
 }
 
 }  // namespace sfg

@@ -54,6 +54,13 @@ struct Step2 {
     const float4 *coefA;       // [na] c11 c13 c33 c44
     const float *imA;          // [na] 1/m_lump (0 on Dirichlet rows)
     const float *coefZ;        // [n-na][12] (sfg_step.cuh coefficient order)
+    // one model per shot (batched, compensated): rec then carries the
+    // geometric mass matrix M_geo (M = diag(rho) M_geo), cmm[n][6][S] the
+    // shot's c11 c13 c33 c44, 1/m_lump (0 on Dirichlet rows) and rho, and
+    // sig[S] its vp_max over the set-up model's (the M-PML profiles scale
+    // linearly with vp_max); nullptr otherwise
+    const float *cmm;
+    const float *sig;
     State32 in;
     State32W out;
 };
@@ -84,6 +91,12 @@ cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double
 // inverse and the permuted row pointers; na = class-A rows, npml = M-PML rows
 cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double *d_mpml, int maxlen, int **d_perm,
                           int **d_inv, int **d_upp, int *na, int *npml, cudaStream_t st);
+// one model per shot: row records with M_geo = M / rho0(row) in plane 1
+// (stream-ordered allocation), and the row sums of M_geo in mesh order
+cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long nnz, const int *d_perm,
+                          const int *d_upp, const double *d_rho0, const float *d_recp, float **d_rec, cudaStream_t st);
+cudaError_t mass_row_sums_geo(int n, const int *d_up, const double *d_ux, const double *d_rho0, double *d_out,
+                              cudaStream_t st);
 // class-A / class-Z coefficient arrays from the [n][12] FP32 record
 cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,
                         float **d_coefZ, cudaStream_t st);

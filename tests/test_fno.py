@@ -228,24 +228,17 @@ def test_adam_step_matches_reference_formula():
 def test_trained_surrogate_beats_untrained_on_held_out_fem_shots():
     """64 FEM training shots, 16 held out (config-5 mesh, 200 samples): the
     trained network's mean relative L2 error is well below the untrained
-    network's and below the zero predictor's (1.0); its inference is faster
-    per shot than the FEM that made the data."""
-    import time
-    import torch
+    network's and below the zero predictor's (1.0).  (Its speed against the
+    FEM is measured by bench.py's surrogate workload.)"""
     from seisfem_b200.surrogate import Surrogate, generate, rel_l2
     cfg = dict(samples=200)
-    xtr, ytr, fem_s = generate(range(5000, 5064), **cfg)
+    xtr, ytr, _ = generate(range(5000, 5064), **cfg)
     xte, yte, _ = generate(range(9000, 9016), **cfg)
     sg = Surrogate(B=8, T=200, seed=0)
     sg.scale = float(np.sqrt(np.mean(ytr.astype(np.float64) ** 2)))
     e0 = rel_l2(sg.predict(xte), yte).mean()
     hist = sg.fit(xtr, ytr, epochs=40, lr=2e-3)
     assert hist[-1] < hist[0]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     pred = sg.predict(xte)
-    torch.cuda.synchronize()
-    t_sur = (time.perf_counter() - t0) / len(xte)
     e1 = rel_l2(pred, yte).mean()
     assert e1 < 0.8 * e0 and e1 < 1.0, (e0, e1)
-    assert t_sur < np.median(fem_s), (t_sur, np.median(fem_s))

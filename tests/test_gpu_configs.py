@@ -75,3 +75,48 @@ def test_group_launch_matches_separate_plans(oracle):
         pl.close()
     for c in ctxs:
         c.close()
+
+
+def _models_case(shots, seed0=5000, **kw):
+    from seisfem_b200.problem import config_5
+    probs = [config_5(seed0 + k, **kw) for k in range(shots)]
+    p = copy.copy(probs[0])
+    p.src_node = np.concatenate([q.src_node for q in probs]).astype(np.int32)
+    return p, probs
+
+
+def test_one_model_per_shot_matches_separate_runs(oracle):
+    """Batched shots with their own GRF models (config 5 recipe, smaller
+    mesh) against each shot run alone in a context set up with its model,
+    and two shots against the FP64 oracle."""
+    from seisfem_b200.api import Context
+    shots = 35                       # one full batch of 32 and a ragged one
+    p, probs = _models_case(shots, n=40, samples=200, nrec=16, pml=6)
+    ctx = Context(0)
+    ctx.setup(probs[0])
+    got = ctx.run_models(p, [q.model for q in probs], shots_per_batch=32, snap_every=200)
+    for k in (0, 7, 33):
+        c2 = Context(0)
+        c2.setup(probs[k])
+        one = c2.run(probs[k], precision="fp32k", snap_every=200)
+        c2.close()
+        for key in ("seis_u", "seis_w", "snap_u", "snap_w"):
+            assert rel_l2(got[key][k], one[key][0]) < 1e-5, (k, key, rel_l2(got[key][k], one[key][0]))
+    for k in (3, 34):
+        ref = oracle.run(probs[k])
+        for key in ("seis_u", "seis_w"):
+            assert rel_l2(got[key][k], ref[key][0]) < FP32_TOL, (k, key)
+    ctx.close()
+
+
+def test_one_model_per_shot_same_model_equals_batched_run():
+    from seisfem_b200.api import Context
+    p, probs = _models_case(40, n=40, samples=150, nrec=16, pml=6)
+    same = [probs[0].model] * 40
+    ctx = Context(0)
+    ctx.setup(probs[0])
+    a = ctx.run_models(p, same, shots_per_batch=64)
+    b = ctx.run(p, precision="fp32k", shots_per_batch=64, snap_every=0, want_snapshots=False)
+    for key in ("seis_u", "seis_w"):
+        assert rel_l2(a[key], b[key]) < 1e-6, key
+    ctx.close()
