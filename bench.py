@@ -542,7 +542,7 @@ def launch_shape(code, S):
     if S == 1:
         return {"variant_A": code // 16, "variant_Z": code % 16}
     a, z = code // 256, code % 256
-    return {"A": {"shots_per_lane": a >> 4, "warps_per_block": a & 15},
+    return {"A": {"shots_per_lane": (a >> 4) & 15, "warps_per_block": a & 15, "staged_gathers": bool(a & 0x100)},
             "Z": {"shots_per_lane": z >> 4, "warps_per_block": z & 15}}
 
 

@@ -586,10 +586,11 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             if (cudaEventRecord(ctx->ev_fork, st) != cudaSuccess) return -1;
             if (cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0) != cudaSuccess) return -1;
             e = S == 1 ? launch_stepZ(a, comp, pl.shapeZ, ctx->stream2)
-                       : launch_stepZ_batched(a, comp, pl.shapeZ >> 4, pl.shapeZ & 15, ctx->stream2);
+                       : launch_stepZ_batched(a, comp, (pl.shapeZ >> 4) & 15, pl.shapeZ & 15, ctx->stream2);
             if (e != cudaSuccess) return -1;
             e = S == 1 ? launch_stepA(a, comp, pl.shapeA, st)
-                       : launch_stepA_batched(a, comp, pl.shapeA >> 4, pl.shapeA & 15, st);
+                : (pl.shapeA & 0x100) ? launch_stepA_staged(a, comp, st)
+                                      : launch_stepA_batched(a, comp, (pl.shapeA >> 4) & 15, pl.shapeA & 15, st);
             if (e != cudaSuccess) return -1;
             if (cudaEventRecord(ctx->ev_join, ctx->stream2) != cudaSuccess) return -1;
             if (cudaStreamWaitEvent(st, ctx->ev_join, 0) != cudaSuccess) return -1;
@@ -712,6 +713,17 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
             if (pl.S % (32 * spl) == 0)
                 for (int w : {4, 8})
                     if (w % (pl.S / (32 * spl)) == 0) cand.push_back(spl * 16 + w);
+        // class A with staged gathers (64 shots, one model): flag 0x100; the
+        // class-Z kernel ignores the flag
+        if (pl.S == 64 && !b.cmm) cand.push_back(0x100 | (2 * 16 + 8));
+    }
+    // SFG_SHAPE_A / SFG_SHAPE_Z (the encoded shapes above) pin the launch
+    // shapes instead of tuning: for tests and manual tuning
+    const char *fa = std::getenv("SFG_SHAPE_A"), *fz = std::getenv("SFG_SHAPE_Z");
+    if (fa && fz) {
+        pl.shapeA = std::atoi(fa);
+        pl.shapeZ = std::atoi(fz);
+        return SFG_OK;
     }
     if (slot[0] > 0 && slot[1] > 0) {   // cached choice
         pl.shapeA = slot[0] - 1;
@@ -746,7 +758,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
         if (ms < best) { best = ms; pick_a = cnd; pick_z = cnd; }
     }
     for (int cnd : cand) {
-        if (cnd == pick_a) continue;
+        if (cnd == pick_a || (cnd & 0x100)) continue;   // the staged variant exists for class A only
         float ms = 0.f;
         int rc = time_shape(pick_a, cnd, ms);
         if (rc) return rc;

@@ -426,18 +426,40 @@ __device__ __forceinline__ Entry entry_at(const float4 &r0, const float4 &r1, in
     return e;
 }
 
+// acc[q] += a * x[q] for the lane's shots; pairs of shots use the packed
+// FP32x2 FMA of sm_100 (one instruction per two shots, same rounding as two
+// fused multiply-adds).
+template <int SPL>
+__device__ __forceinline__ void axpy(float *acc, float a, const VecF<SPL> &x)
+{
+    if constexpr (SPL == 1) {
+        acc[0] = fmaf(a, x.v[0], acc[0]);
+    } else {
+        const float2 aa = make_float2(a, a);
+        const unsigned long long av = *reinterpret_cast<const unsigned long long *>(&aa);
+#pragma unroll
+        for (int q = 0; q < SPL; q += 2) {
+            float2 c = make_float2(acc[q], acc[q + 1]);
+            const float2 b = make_float2(x.v[q], x.v[q + 1]);
+            unsigned long long cv = *reinterpret_cast<unsigned long long *>(&c);
+            const unsigned long long bv = *reinterpret_cast<const unsigned long long *>(&b);
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(cv) : "l"(av), "l"(bv));
+            c = *reinterpret_cast<float2 *>(&cv);
+            acc[q] = c.x;
+            acc[q + 1] = c.y;
+        }
+    }
+}
+
 // K1..K4 times U, W and M times Lx1..4, Ly1..4 of one neighbour record x[10].
 template <int SPL>
 __device__ __forceinline__ void acc_totals(const Entry &e, const VecF<SPL> *x, float (*kU)[SPL], float (*kW)[SPL],
                                            float (*mL)[SPL])
 {
 #pragma unroll
-    for (int q = 0; q < SPL; q++) {
+    for (int t = 0; t < 4; t++) { axpy<SPL>(kU[t], e.k[t], x[0]); axpy<SPL>(kW[t], e.k[t], x[1]); }
 #pragma unroll
-        for (int t = 0; t < 4; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
-#pragma unroll
-        for (int t = 0; t < 8; t++) mL[t][q] += e.vm * x[2 + t].v[q];
-    }
+    for (int t = 0; t < 8; t++) axpy<SPL>(mL[t], e.vm, x[2 + t]);
 }
 
 // MM: every shot has its own model (a.cmm, a.sig; see Step2).
@@ -553,6 +575,180 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
     if (c.energy) energy_flush<SPL>(c, se, S, s_base, eu, ew);
 }
 
+// ------------------------------------- class A, staged neighbour gathers
+//
+// 64 shots, one warp per row (two shots per lane).  The neighbour records a
+// row needs (values 0..9 of Gc: 2560 contiguous bytes per neighbour) are
+// copied into the warp's own shared-memory buffer with cp.async, up to
+// SME entries per item, two buffers per warp: while the warp computes one
+// item from shared memory the copies of the next are in flight, so each SM
+// keeps many kilobytes of gathers outstanding without spending registers.
+
+constexpr int SME = 5;                       // entries per staged item
+constexpr int SREC = 10 * 64 * 4;            // bytes of one neighbour's values 0..9 (64 shots)
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+struct StageItem {
+    int row, base, cnt, last;                // row, first entry, entries, last item of the row
+};
+
+template <bool COMP>
+__global__ void __launch_bounds__(256, 1) stepA_staged(const Step2 a)
+{
+    constexpr int S = 64, SPL = 2;
+    extern __shared__ __align__(16) unsigned char stage[];   // [warp][2][SME * SREC]
+    __shared__ float se[2 * S];
+    const StepCommon &c = a.c;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
+    if (c.energy) energy_zero(se, S);
+    const int warp = gtid >> 5, warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int s_base = lane * SPL;
+    int src[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) src[q] = s_base + q < c.nshot ? c.src[s_base + q] : -1;
+    const double ps = c.amp[c.it];
+    const double src_u = ps * c.sin_af, src_w = ps * c.cos_af;
+    float eu[SPL], ew[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
+    const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
+    unsigned char *buf0 = stage + (size_t)wib * 2 * SME * SREC;
+    const uint32_t sbuf0 = (uint32_t)__cvta_generic_to_shared(buf0);
+
+    // the item after `it` in this warp's sequence (rows warp, warp + warps_total, ...)
+    auto first_of = [&](int row) {
+        StageItem s;
+        s.row = row;
+        s.base = row < a.na ? __ldg(a.up + row) : 0;
+        const int e1 = row < a.na ? __ldg(a.up + row + 1) : 0;
+        s.cnt = min(SME, e1 - s.base);
+        s.last = s.base + s.cnt >= e1;
+        return s;
+    };
+    auto next_of = [&](const StageItem &it) {
+        if (!it.last) {
+            StageItem s = it;
+            const int e1 = __ldg(a.up + it.row + 1);
+            s.base = it.base + it.cnt;
+            s.cnt = min(SME, e1 - s.base);
+            s.last = s.base + s.cnt >= e1;
+            return s;
+        }
+        return first_of(it.row + warps_total);
+    };
+    // row records of an item (lanes < cnt) and the copies of its neighbours
+    auto issue = [&](const StageItem &it, int b, float4 &r0, float4 &r1) {
+        r0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        r1 = r0;
+        if (it.row < a.na && lane < it.cnt) {
+            r0 = __ldg(rec + 2 * (size_t)(it.base + lane));
+            r1 = __ldg(rec + 2 * (size_t)(it.base + lane) + 1);
+        }
+        if (it.row < a.na) {
+            const uint32_t dst = sbuf0 + (uint32_t)(b * SME * SREC);
+            for (int t = 0; t < it.cnt; t++) {
+                const int j = __shfl_sync(0xffffffffu, __float_as_int(r0.x), t);
+                const unsigned char *g = reinterpret_cast<const unsigned char *>(a.in.Gc + (size_t)j * GC * S);
+#pragma unroll
+                for (int u = 0; u < SREC / 16 / 32; u++) {
+                    const int ch = lane + 32 * u;
+                    cp_async16(dst + t * SREC + ch * 16, g + ch * 16);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+    StageItem cur = first_of(warp);
+    float4 r0, r1, n0, n1;
+    int b = 0;
+    issue(cur, 0, r0, r1);
+    float kU[4][SPL], kW[4][SPL], mL[8][SPL];
+    while (cur.row < a.na) {
+        const StageItem nxt = next_of(cur);
+        issue(nxt, b ^ 1, n0, n1);
+        if (cur.base == __ldg(a.up + cur.row)) {
+#pragma unroll
+            for (int q = 0; q < SPL; q++) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
+#pragma unroll
+                for (int k = 0; k < 8; k++) mL[k][q] = 0.f;
+            }
+        }
+        cp_async_wait1();
+        __syncwarp();
+        const unsigned char *sb = buf0 + b * SME * SREC + lane * 8;
+        for (int t = 0; t < cur.cnt; t++) {
+            const Entry e = entry_at<4>(r0, r1, t);
+            VecF<SPL> x[10];
+#pragma unroll
+            for (int v = 0; v < 10; v++) {
+                const float2 f = *reinterpret_cast<const float2 *>(sb + t * SREC + v * 256);
+                x[v].v[0] = f.x;
+                x[v].v[1] = f.y;
+            }
+            acc_totals<SPL>(e, x, kU, kW, mL);
+        }
+        __syncwarp();
+        if (cur.last) {
+            const int i = cur.row;
+            const float4 cf = __ldg(a.coefA + i);
+            const float im = __ldg(a.imA + i);
+            const float *gi = a.in.Gc + (size_t)i * GC * S + s_base;
+            const float *pi = a.in.Pa + (size_t)i * PA * S + s_base;
+            float *go = a.out.Gc + (size_t)i * GC * S + s_base;
+            float *po = a.out.Pa + (size_t)i * PA * S + s_base;
+            VecF<SPL> gv[GC], pv[PA];
+            gv[0].load(gi);
+            gv[1].load(gi + S);
+            gv[10].load(gi + 10 * S);
+            gv[11].load(gi + 11 * S);
+#pragma unroll
+            for (int v = 0; v < PA; v++) pv[v].load(pi + v * S);
+#pragma unroll
+            for (int q = 0; q < SPL; q++) {
+                float kUq[4], kWq[4], mq[8], g[GC], p[PA];
+#pragma unroll
+                for (int t = 0; t < 4; t++) { kUq[t] = kU[t][q]; kWq[t] = kW[t][q]; }
+#pragma unroll
+                for (int t = 0; t < 8; t++) mq[t] = mL[t][q];
+                g[0] = gv[0].v[q]; g[1] = gv[1].v[q]; g[10] = gv[10].v[q]; g[11] = gv[11].v[q];
+#pragma unroll
+                for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
+                const bool is_src = (i == src[q]);
+                double uu, ww;
+                finish_A<COMP>(kUq, kWq, mq, cf, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu,
+                               ww);
+#pragma unroll
+                for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
+#pragma unroll
+                for (int v = 0; v < PA; v++) pv[v].v[q] = p[v];
+                eu[q] += (float)(uu * uu);
+                ew[q] += (float)(ww * ww);
+            }
+#pragma unroll
+            for (int v = 0; v < GC; v++) gv[v].store(go + v * S);
+#pragma unroll
+            for (int v = 0; v < PA; v++) pv[v].store(po + v * S);
+        }
+        cur = nxt;
+        r0 = n0;
+        r1 = n1;
+        b ^= 1;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (c.energy) energy_flush<SPL>(c, se, S, s_base, eu, ew);
+}
+
 // Split-zone products of one entry: K1..K6 times U, W (K5, K6 only on M-PML
 // rows), M times the split fields y[12] (M-PML rows) and M times Lx, Ly.
 template <int SPL>
@@ -560,18 +756,15 @@ __device__ __forceinline__ void acc_split(const Entry &e, const VecF<SPL> *x, co
                                           bool has_y, float (*kU)[SPL], float (*kW)[SPL], float (*m)[SPL])
 {
 #pragma unroll
-    for (int q = 0; q < SPL; q++) {
+    for (int t = 0; t < 4; t++) { axpy<SPL>(kU[t], e.k[t], x[0]); axpy<SPL>(kW[t], e.k[t], x[1]); }
 #pragma unroll
-        for (int t = 0; t < 4; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
+    for (int t = 0; t < 8; t++) axpy<SPL>(m[12 + t], e.vm, x[2 + t]);
+    if (full) {
 #pragma unroll
-        for (int t = 0; t < 8; t++) m[12 + t][q] += e.vm * x[2 + t].v[q];
-        if (full) {
+        for (int t = 4; t < 6; t++) { axpy<SPL>(kU[t], e.k[t], x[0]); axpy<SPL>(kW[t], e.k[t], x[1]); }
+        if (has_y) {
 #pragma unroll
-            for (int t = 4; t < 6; t++) { kU[t][q] += e.k[t] * x[0].v[q]; kW[t][q] += e.k[t] * x[1].v[q]; }
-            if (has_y) {
-#pragma unroll
-                for (int t = 0; t < 12; t++) m[t][q] += e.vm * y[t].v[q];
-            }
+            for (int t = 0; t < 12; t++) axpy<SPL>(m[t], e.vm, y[t]);
         }
     }
 }
@@ -1024,6 +1217,27 @@ cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, 
     // at least one warp for the receiver gather even without class-A rows
     SFG_BATCH(stepA_batched, std::max(a.na, 1));
     return cudaGetLastError();
+}
+
+cudaError_t launch_stepA_staged(const Step2 &a, bool comp, cudaStream_t st)
+{
+    if (a.S != 64 || a.cmm) return cudaErrorInvalidValue;
+    const int threads = 256;
+    const size_t smem = (size_t)(threads / 32) * 2 * SME * SREC;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long need = ((long long)std::max(a.na, 1) + threads / 32 - 1) / (threads / 32);
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(sms, need));
+    cudaError_t e;
+    if (comp) {
+        e = cudaFuncSetAttribute(stepA_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) stepA_staged<true><<<grid, threads, smem, st>>>(a);
+    } else {
+        e = cudaFuncSetAttribute(stepA_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) stepA_staged<false><<<grid, threads, smem, st>>>(a);
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st)

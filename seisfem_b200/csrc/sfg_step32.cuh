@@ -73,6 +73,9 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
 // one row (spl per lane); warps per block a multiple of S / (32 * spl)
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
 cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
+// class A with staged neighbour gathers (cp.async into per-warp shared-memory
+// buffers), 64 shots, one persistent block of 8 warps per SM
+cudaError_t launch_stepA_staged(const Step2 &a, bool comp, cudaStream_t st);
 // receiver gather of a finished state; snapshots scattered back to mesh order
 cudaError_t launch_gather2(const StepCommon &c, int na, const State32 &s, int S, cudaStream_t st);
 cudaError_t launch_snapshot2(const State32 &s, int n, int na, int S, const int *perm, double *snap_u,

@@ -97,6 +97,21 @@ def test_batched_shots_match_single(ctx, oracle, spb):
         assert rel_l2(batched[k][[0, shots - 1]], ref[k]) < FP32_TOL, k
 
 
+@pytest.mark.parametrize("shape_a", [0x100 | 0x28, 0x24, 0x18])
+def test_batched_launch_shapes_agree(ctx, oracle, shape_a, monkeypatch):
+    """Every class-A variant of 64-shot batches -- the staged-gather kernel
+    (flag 0x100), two and one shots per lane -- gives the single-shot
+    results."""
+    p = small_problem("Q4", n=40, step=202, pml=5, seed=19, shots=64)
+    ctx.setup(p)
+    single = ctx.run(p, precision="fp32k", shots_per_batch=1, want_snapshots=True)
+    monkeypatch.setenv("SFG_SHAPE_A", str(shape_a))
+    monkeypatch.setenv("SFG_SHAPE_Z", str(0x18))
+    batched = ctx.run(p, precision="fp32k", shots_per_batch=64, want_snapshots=True)
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(batched[k], single[k]) < 1e-5, k
+
+
 def test_blowup_detected_like_reference(ctx, oracle):
     p = small_problem("T6", n=16, step=260, pml=4, seed=7)   # dt too large for T6: the energy bound trips
     ref = oracle.run(p)
