@@ -92,7 +92,8 @@ struct TileLoad {
         }
     }
 
-    // into s[r][k] (pitch PITCH)
+    // modes 0 and 2: s[r][k] (pitch PITCH); mode 1: s[k][r] (pitch R + 8),
+    // read back with ldmatrix.trans
     __device__ __forceinline__ void store(__nv_bfloat16 *s, int mode) const
     {
         const int t = threadIdx.x;
@@ -101,9 +102,7 @@ struct TileLoad {
             const int idx = t + q * 256;
             if (mode == 1) {
                 const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
-                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[q]);
-#pragma unroll
-                for (int u = 0; u < 8; u++) s[(r + u) * PITCH + kc] = e[u];
+                *reinterpret_cast<uint4 *>(s + kc * (R + 8) + r) = v[q];
             } else {
                 const int r = idx / (BK / 8), kc = (idx % (BK / 8)) * 8;
                 *reinterpret_cast<uint4 *>(s + r * PITCH + kc) = v[q];
@@ -127,8 +126,10 @@ template <int BM, int BN, int WM, int WN>
 __global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
 {
     constexpr int TM = BM / WM / 16, TN = BN / WN / 8;
-    __shared__ __align__(16) __nv_bfloat16 As[2][BM * PITCH];
-    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN * PITCH];
+    constexpr int ASZ = BM * PITCH > BK * (BM + 8) ? BM * PITCH : BK * (BM + 8);
+    constexpr int BSZ = BN * PITCH > BK * (BN + 8) ? BN * PITCH : BK * (BN + 8);
+    __shared__ __align__(16) __nv_bfloat16 As[2][ASZ];
+    __shared__ __align__(16) __nv_bfloat16 Bs[2][BSZ];
     const sfg_gemm_desc &d = g.d;
     const int nb = d.batch1 * d.batch2;
     const int bz = blockIdx.z;
@@ -170,19 +171,46 @@ __global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
 #pragma unroll
         for (int ks = 0; ks < BK; ks += 16) {
             uint32_t af[TM][4], bf[TN][2];
+            if (g.amode == 1) {
+                // As[k][m]: four 8x8 blocks (m 0-7 / 8-15, k 0-7 / 8-15) transposed by ldmatrix
+                const int lm = (lane >> 3) & 1, lk = lane >> 4, lr = lane & 7;
 #pragma unroll
-            for (int i = 0; i < TM; i++) {
-                const int r = wm * (BM / WM) + i * 16 + gq;
-                af[i][0] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 2 * tq);
-                af[i][1] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 2 * tq);
-                af[i][2] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 8 + 2 * tq);
-                af[i][3] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 8 + 2 * tq);
+                for (int i = 0; i < TM; i++) {
+                    const int mb = wm * (BM / WM) + i * 16;
+                    const uint32_t addr = (uint32_t)__cvta_generic_to_shared(
+                        as + (ks + lk * 8 + lr) * (BM + 8) + mb + lm * 8);
+                    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                                 : "=r"(af[i][0]), "=r"(af[i][1]), "=r"(af[i][2]), "=r"(af[i][3])
+                                 : "r"(addr));
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+                    const int r = wm * (BM / WM) + i * 16 + gq;
+                    af[i][0] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 2 * tq);
+                    af[i][1] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 2 * tq);
+                    af[i][2] = *reinterpret_cast<const uint32_t *>(as + r * PITCH + ks + 8 + 2 * tq);
+                    af[i][3] = *reinterpret_cast<const uint32_t *>(as + (r + 8) * PITCH + ks + 8 + 2 * tq);
+                }
             }
+            if (g.bmode == 1) {
+                // Bs[k][n]: two 8x8 blocks (k 0-7, 8-15) per n8 tile, transposed by ldmatrix
+                const int lk = (lane >> 3) & 1, lr = lane & 7;
 #pragma unroll
-            for (int j = 0; j < TN; j++) {
-                const int n = wn * (BN / WN) + j * 8 + gq;
-                bf[j][0] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 2 * tq);
-                bf[j][1] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 8 + 2 * tq);
+                for (int j = 0; j < TN; j++) {
+                    const int nb = wn * (BN / WN) + j * 8;
+                    const uint32_t addr = (uint32_t)__cvta_generic_to_shared(bs + (ks + lk * 8 + lr) * (BN + 8) + nb);
+                    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];"
+                                 : "=r"(bf[j][0]), "=r"(bf[j][1])
+                                 : "r"(addr));
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; j++) {
+                    const int n = wn * (BN / WN) + j * 8 + gq;
+                    bf[j][0] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 2 * tq);
+                    bf[j][1] = *reinterpret_cast<const uint32_t *>(bs + n * PITCH + ks + 8 + 2 * tq);
+                }
             }
 #pragma unroll
             for (int i = 0; i < TM; i++)
@@ -195,28 +223,58 @@ __global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
         }
         __syncthreads();
     }
-    // epilogue
+    // epilogue: a thread holds columns n, n + 1 of rows m and m + 8; with
+    // unit column stride the pair is read and written as one vector
+    const bool pairs = d.scn == 1 && !d.atomic;
 #pragma unroll
     for (int i = 0; i < TM; i++)
 #pragma unroll
         for (int j = 0; j < TN; j++)
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int m = m0 + wm * (BM / WM) + i * 16 + gq + (r >= 2 ? 8 : 0);
-                const int n = n0 + wn * (BN / WN) + j * 8 + 2 * tq + (r & 1);
+            for (int h = 0; h < 2; h++) {
+                const int m = m0 + wm * (BM / WM) + i * 16 + gq + h * 8;
+                const int n = n0 + wn * (BN / WN) + j * 8 + 2 * tq;
                 if (m >= d.M || n >= d.N) continue;
                 const long long o = cz + m * d.scm + n * d.scn;
-                float v = d.alpha * acc[i][j][r];
-                if (d.atomic) {
-                    atomicAdd(static_cast<float *>(d.C) + o, v);
+                float v0 = d.alpha * acc[i][j][2 * h], v1 = d.alpha * acc[i][j][2 * h + 1];
+                if (pairs && n + 1 < d.N && (o & 1) == 0) {
+                    if (d.Cin) {
+                        const float2 ci = *reinterpret_cast<const float2 *>(d.Cin + o);
+                        v0 += d.beta * ci.x;
+                        v1 += d.beta * ci.y;
+                    }
+                    if (d.bias) {
+                        v0 += d.bias[d.bias_on_m ? m : n];
+                        v1 += d.bias[d.bias_on_m ? m : n + 1];
+                    }
+                    if (d.pre)
+                        *reinterpret_cast<__nv_bfloat162 *>(static_cast<__nv_bfloat16 *>(d.pre) + o) =
+                            __floats2bfloat162_rn(v0, v1);
+                    if (d.gelu) { v0 = gelu_f(v0); v1 = gelu_f(v1); }
+                    if (d.c_bf16)
+                        *reinterpret_cast<__nv_bfloat162 *>(static_cast<__nv_bfloat16 *>(d.C) + o) =
+                            __floats2bfloat162_rn(v0, v1);
+                    else
+                        *reinterpret_cast<float2 *>(static_cast<float *>(d.C) + o) = make_float2(v0, v1);
                     continue;
                 }
-                if (d.Cin) v += d.beta * d.Cin[o];
-                if (d.bias) v += d.bias[d.bias_on_m ? m : n];
-                if (d.pre) static_cast<__nv_bfloat16 *>(d.pre)[o] = __float2bfloat16(v);
-                if (d.gelu) v = gelu_f(v);
-                if (d.c_bf16) static_cast<__nv_bfloat16 *>(d.C)[o] = __float2bfloat16(v);
-                else static_cast<float *>(d.C)[o] = v;
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int nn = n + u;
+                    if (nn >= d.N) continue;
+                    const long long oo = cz + m * d.scm + nn * d.scn;
+                    float v = u ? v1 : v0;
+                    if (d.atomic) {
+                        atomicAdd(static_cast<float *>(d.C) + oo, v);
+                        continue;
+                    }
+                    if (d.Cin) v += d.beta * d.Cin[oo];
+                    if (d.bias) v += d.bias[d.bias_on_m ? m : nn];
+                    if (d.pre) static_cast<__nv_bfloat16 *>(d.pre)[oo] = __float2bfloat16(v);
+                    if (d.gelu) v = gelu_f(v);
+                    if (d.c_bf16) static_cast<__nv_bfloat16 *>(d.C)[oo] = __float2bfloat16(v);
+                    else static_cast<float *>(d.C)[oo] = v;
+                }
             }
 }
 
