@@ -233,10 +233,13 @@ class Reference:
                               pml_nx, pml_ny, h, *bounds, vp_max, *use, out)
         return out.reshape(6, mesh.node_num)
 
-    def run(self, prob, nthreads: int = 0, workdir: str | None = None, want_snapshots: bool = True):
-        """Run the reference elastic_wave() (solver masslump) through its
-        exterior-model path: the model is written to
-        mesh/velocity_and_density.txt with %.17g so it reads back exactly."""
+    def run(self, prob, nthreads: int = 0, workdir: str | None = None, want_snapshots: bool = True,
+            solver: str = "masslump"):
+        """Run the reference elastic_wave() (solver "masslump", or "mgmres":
+        its consistent-mass branch with the reference's own GMRES,
+        solver/mgmres/mgmres.c) through its exterior-model path: the model is
+        written to mesh/velocity_and_density.txt with %.17g so it reads back
+        exactly."""
         m = prob.mesh
         S, R, N, step = len(prob.src_node), len(prob.rec_node), m.node_num, prob.step
         ns = snapshot_rows(step, 200)
@@ -258,7 +261,7 @@ class Reference:
             tmp.encode(), nthreads, m.type_name.encode(), N, m.element_num, m.order, m.element_node,
             m.x, m.y, step, prob.dt, prob.f0, prob.t0, prob.edge_size, m.xmin, m.xmax, m.ymin, m.ymax,
             prob.pml_nx, prob.pml_ny, S, np.ascontiguousarray(prob.src_node, np.int32), R,
-            np.ascontiguousarray(prob.rec_node, np.int32), b"masslump", 1, prob.free_surface,
+            np.ascontiguousarray(prob.rec_node, np.int32), solver.encode(), 1, prob.free_surface,
             out["seis_u"].ctypes.data, out["seis_w"].ctypes.data,
             out["snap_u"].ctypes.data if want_snapshots else None,
             out["snap_w"].ctypes.data if want_snapshots else None, ns, C.byref(secs), step_t.ctypes.data, step)

@@ -153,14 +153,6 @@ void pardiso_unsym(int a, int b, int *c, int *d, double *e, double *f, double *g
     sfr_exit(3);
 }
 
-void pmgmres_ilu_cr(int n, int nz_num, int ia[], int ja[], double a[], double x[], double rhs[],
-                    int itr_max, int mr, double tol_abs, double tol_rel)
-{
-    (void)n; (void)nz_num; (void)ia; (void)ja; (void)a; (void)x; (void)rhs;
-    (void)itr_max; (void)mr; (void)tol_abs; (void)tol_rel;
-    sfr_exit(3);
-}
-
 /* COO -> canonical CSR: the reference's Fortran module, restated in C
  * (oracle/coo2csr_f90abi.c) because no Fortran compiler is available */
 void __coo2csr_lib_MOD_coo2csr_canonical(int *nnz, int *Bp_size, int *csr_size, int *Ai, int *Aj,
@@ -191,6 +183,7 @@ void __coo2csr_lib_MOD_coo2csr_canonical(int *nnz, int *Bp_size, int *csr_size, 
 #include "source_receiver/seismic_source.c"
 #include "source_receiver/set_rec_and_src.c"
 #include "solver/solver_type.c"
+#include "solver/mgmres/mgmres.c"
 #include "time_evolution/elastic_wave.c"
 
 #undef fopen
