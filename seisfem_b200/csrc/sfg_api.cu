@@ -21,6 +21,34 @@
 
 using namespace sfg;
 
+namespace sfg {
+
+// The stream-ordered pool of a device: created on first use, retains up to
+// 8 GiB of freed run buffers for the next run.
+cudaMemPool_t device_pool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    uint64_t keep = 8ull << 30;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        return nullptr;
+    }
+    pools[device] = pool;
+    return pool;
+}
+
+}  // namespace sfg
+
 struct RunCache {
     // launch shapes picked by the autotuner (stored + 1; 0 = not tuned):
     // [shots: 1, 32, 64, 128][plain FP32, compensated][class A, class Z]
@@ -118,30 +146,6 @@ cudaError_t copy_out(sfg_ctx *ctx, void *dst, const void *src, size_t bytes, cud
     if (!bytes) return cudaSuccess;
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st);
     return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
-}
-
-// The stream-ordered pool of a device: created on first use, retains up to
-// 8 GiB of freed run buffers for the next run.
-cudaMemPool_t device_pool(int device)
-{
-    static std::mutex mu;
-    static std::map<int, cudaMemPool_t> pools;
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = pools.find(device);
-    if (it != pools.end()) return it->second;
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = device;
-    cudaMemPool_t pool = nullptr;
-    uint64_t keep = 8ull << 30;
-    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
-    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
-        cudaMemPoolDestroy(pool);
-        return nullptr;
-    }
-    pools[device] = pool;
-    return pool;
 }
 
 int type_code_of(const char *t)
@@ -297,9 +301,10 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(upload(&P.coef64, md->c, (size_t)4 * N, st));
     CK(cudaMalloc(&d_flags, sizeof(int)));
     CK(cudaMemsetAsync(d_flags, 0, sizeof(int), st));
-    CK(cudaMalloc(&d_ci, sizeof(int) * nnz));
-    CK(cudaMalloc(&d_cj, sizeof(int) * nnz));
-    CK(cudaMalloc(&d_cx, sizeof(double) * 7 * nnz));
+    // the COO streams are set-up temporaries: from the device's pool
+    CK(tmp_alloc((void **)&d_ci, sizeof(int) * nnz, st));
+    CK(tmp_alloc((void **)&d_cj, sizeof(int) * nnz, st));
+    CK(tmp_alloc((void **)&d_cx, sizeof(double) * 7 * nnz, st));
 
     // element matrices: consistent mass (with rho) and stiffness types 1..6
     const int mats[7] = {-1, 1, 2, 3, 4, 5, 6};
@@ -311,7 +316,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(cudaStreamSynchronize(st));
     if (hflags & FLAG_ZERO_AREA) {
         cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
-        cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx);
+        cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
         return fail(ctx, SFG_ERR_ZERO_AREA, "an element has zero area");
     }
     CanonOut co;
@@ -319,9 +324,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     int rc = canonicalize(N, nnz, d_ci, d_cj, d_cx, 7, true, true, co, d_flags, st, ctx->err);
     tr.mark("setup: canonical CSR");
     if (rc != SFG_OK) {
-        canon_free(co, false);
+        canon_free(co, false, st);
         cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
-        cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx);
+        cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
         return rc;
     }
     for (int k = 0; k < 7; k++) P.csr[k] = co.csr[k];
@@ -383,9 +388,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(build_coef2(N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, st));
     CK(cudaStreamSynchronize(st));
     tr.mark("setup: SELL, records");
-    canon_free(co, true);
+    canon_free(co, true, st);
     cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_flags);
-    cudaFree(d_ci); cudaFree(d_cj); cudaFree(d_cx); cudaFree(d_scr);
+    cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st); cudaFree(d_scr);
     P.rho0 = d_rho;
     P.h_rho0.assign(md->rho, md->rho + N);
     P.h_dir = std::move(dir);

@@ -133,61 +133,73 @@ __global__ void shape_table_kernel(int tc, double *tab)
     }
 }
 
-// One thread per COO entry (e, iq, jq): integrates the requested matrices in
-// the reference's quadrature order (mass_sparse_q4.c:199-256,
-// stiffness_sparse_q4.c:202-271) and writes entry e*p*p + iq*p + jq.
-__global__ void element_coo_kernel(int tc, int p, long long nnz, const int *__restrict__ en,
+// Element matrices as COO: entry e*p*p + iq*p + jq integrates the requested
+// matrices in the reference's quadrature order (mass_sparse_q4.c:199-256,
+// stiffness_sparse_q4.c:202-271).  A block holds EB elements; its first pass
+// computes drdx, drdy, dsdx, dsdy and area * w of every (element, quadrature
+// point) once into shared memory, the second pass forms every entry from
+// them, one thread per entry.
+__global__ void element_coo_shared(int tc, int p, int E, int EB, const int *__restrict__ en,
                                    const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ rho, int nmat, MatList ml,
                                    const double *__restrict__ tab, int *__restrict__ ci, int *__restrict__ cj,
                                    double *__restrict__ cx, int *flags)
 {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nnz) return;
-    int pp = p * p;
-    int e = (int)(t / pp);
-    int rem = (int)(t - (long long)e * pp);
-    int iq = rem / p, jq = rem - iq * p;
-    const int *enE = en + (long long)e * p;
-    ElemGeom g;
-    elem_geom(tc, enE, x, y, g);
-    if (g.area == 0.0 && rem == 0) atomicOr(flags, FLAG_ZERO_AREA);
-    int ip = enE[iq] - 1, jp = enE[jq] - 1;
-    double rho_ip = rho ? rho[ip] : 0.0;
-    double acc[8];
-#pragma unroll
-    for (int m = 0; m < 8; m++) acc[m] = 0.0;
-    int nq = quad_count(tc);
-    for (int q = 0; q < nq; q++) {
+    extern __shared__ double geo[];   // [EB][nq][5]: drdx drdy dsdx dsdy area*w
+    const int pp = p * p, nq = quad_count(tc);
+    const int e0 = blockIdx.x * EB;
+    const int ne = min(EB, E - e0);
+    for (int k = threadIdx.x; k < ne * nq; k += blockDim.x) {
+        const int le = k / nq, q = k - le * nq, e = e0 + le;
+        ElemGeom g;
+        elem_geom(tc, en + (long long)e * p, x, y, g);
+        if (g.area == 0.0 && q == 0) atomicOr(flags, FLAG_ZERO_AREA);
         double r, s, w;
         quad_point(tc, q, r, s, w);
-        double drdx, drdy, dsdx, dsdy;
-        map_point(tc, g, r, s, drdx, drdy, dsdx, dsdy);
-        const double *t0 = tab + 3 * q * 16, *t1 = t0 + 16, *t2 = t0 + 32;
-        double phi_i = t0[iq], phi_j = t0[jq];
-        double dxi = t1[iq] * drdx + t2[iq] * dsdx;
-        double dyi = t1[iq] * drdy + t2[iq] * dsdy;
-        double dxj = t1[jq] * drdx + t2[jq] * dsdx;
-        double dyj = t1[jq] * drdy + t2[jq] * dsdy;
-        double aw = g.area * w;
-        for (int m = 0; m < nmat; m++) {
-            double term;
-            switch (ml.m[m]) {
-            case -1: term = aw * rho_ip * phi_i * phi_j; break;
-            case 0: term = aw * (dxi * dxj + dyi * dyj); break;
-            case 1: term = aw * (dxi * dxj); break;
-            case 2: term = aw * (dyi * dyj); break;
-            case 3: term = aw * (dxi * dyj); break;
-            case 4: term = aw * (dyi * dxj); break;
-            case 5: term = aw * (phi_i * dxj); break;
-            default: term = aw * (phi_i * dyj); break;
-            }
-            acc[m] = acc[m] + term;
-        }
+        double *o = geo + (size_t)k * 5;
+        map_point(tc, g, r, s, o[0], o[1], o[2], o[3]);
+        o[4] = g.area * w;
     }
-    if (ci) ci[t] = ip;
-    if (cj) cj[t] = jp;
-    for (int m = 0; m < nmat; m++) cx[(long long)m * nnz + t] = acc[m];
+    __syncthreads();
+    const long long nnz = (long long)E * pp;
+    for (int k = threadIdx.x; k < ne * pp; k += blockDim.x) {
+        const int le = k / pp, rem = k - le * pp, iq = rem / p, jq = rem - iq * p;
+        const int e = e0 + le;
+        const long long t = (long long)e * pp + rem;
+        const int *enE = en + (long long)e * p;
+        const int ip = enE[iq] - 1, jp = enE[jq] - 1;
+        const double rho_ip = rho ? rho[ip] : 0.0;
+        double acc[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) acc[m] = 0.0;
+        for (int q = 0; q < nq; q++) {
+            const double *gq = geo + ((size_t)le * nq + q) * 5;
+            const double drdx = gq[0], drdy = gq[1], dsdx = gq[2], dsdy = gq[3], aw = gq[4];
+            const double *t0 = tab + 3 * q * 16, *t1 = t0 + 16, *t2 = t0 + 32;
+            double phi_i = t0[iq], phi_j = t0[jq];
+            double dxi = t1[iq] * drdx + t2[iq] * dsdx;
+            double dyi = t1[iq] * drdy + t2[iq] * dsdy;
+            double dxj = t1[jq] * drdx + t2[jq] * dsdx;
+            double dyj = t1[jq] * drdy + t2[jq] * dsdy;
+            for (int m = 0; m < nmat; m++) {
+                double term;
+                switch (ml.m[m]) {
+                case -1: term = aw * rho_ip * phi_i * phi_j; break;
+                case 0: term = aw * (dxi * dxj + dyi * dyj); break;
+                case 1: term = aw * (dxi * dxj); break;
+                case 2: term = aw * (dyi * dyj); break;
+                case 3: term = aw * (dxi * dyj); break;
+                case 4: term = aw * (dyi * dxj); break;
+                case 5: term = aw * (phi_i * dxj); break;
+                default: term = aw * (phi_i * dyj); break;
+                }
+                acc[m] = acc[m] + term;
+            }
+        }
+        if (ci) ci[t] = ip;
+        if (cj) cj[t] = jp;
+        for (int m = 0; m < nmat; m++) cx[(long long)m * nnz + t] = acc[m];
+    }
 }
 
 cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x, const double *d_y,
@@ -202,11 +214,13 @@ cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x
     cudaError_t e = cudaMallocAsync((void **)&tab, sizeof(double) * 36 * 3 * 16, st);
     if (e != cudaSuccess) return e;
     shape_table_kernel<<<1, 64, 0, st>>>(tc, tab);
-    int threads = 128;
-    long long blocks = (nnz + threads - 1) / threads;
+    const int threads = 256, pp = p * p, nq = quad_count(tc);
+    const int EB = std::max(1, threads / pp);
+    const long long blocks = ((long long)E + EB - 1) / EB;
+    const size_t smem = sizeof(double) * 5 * (size_t)EB * nq;
     if (blocks > 0)
-        element_coo_kernel<<<(unsigned)blocks, threads, 0, st>>>(tc, p, nnz, d_en, d_x, d_y, d_rho, nmat,
-                                                                  ml, tab, d_ci, d_cj, d_cx, d_flags);
+        element_coo_shared<<<(unsigned)blocks, threads, smem, st>>>(tc, p, E, EB, d_en, d_x, d_y, d_rho, nmat,
+                                                                     ml, tab, d_ci, d_cj, d_cx, d_flags);
     e = cudaGetLastError();
     cudaFreeAsync(tab, st);
     return e;
@@ -523,12 +537,12 @@ __global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict_
         if (e_ != cudaSuccess) { err = cudaGetErrorString(e_); return SFG_ERR_CUDA; } \
     } while (0)
 
-void canon_free(CanonOut &o, bool keep_csr)
+void canon_free(CanonOut &o, bool keep_csr, cudaStream_t st)
 {
     if (!keep_csr)
         for (auto &c : o.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
-    cudaFree(o.row_start);
-    cudaFree(o.bucket);
+    if (o.row_start) cudaFreeAsync(o.row_start, st);
+    if (o.bucket) cudaFreeAsync(o.bucket, st);
     o.row_start = nullptr;
     o.bucket = nullptr;
 }
@@ -541,15 +555,16 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     int *cnt = nullptr, *cursor = nullptr, *vec = nullptr, *map = nullptr, *cu = nullptr,
         *cv = nullptr, *maxlen = nullptr;
     size_t nn = (size_t)std::max<long long>(nnz, 1);
-    SFG_TRY(cudaMalloc(&cnt, sizeof(int) * ((size_t)N + 1)));
-    SFG_TRY(cudaMalloc(&cursor, sizeof(int) * ((size_t)N + 1)));
-    SFG_TRY(cudaMalloc(&out.row_start, sizeof(int) * ((size_t)N + 1)));
-    SFG_TRY(cudaMalloc(&out.bucket, sizeof(int) * nn));
-    SFG_TRY(cudaMalloc(&vec, sizeof(int) * nn));
-    SFG_TRY(cudaMalloc(&map, sizeof(int) * nn));
-    SFG_TRY(cudaMalloc(&cu, sizeof(int) * ((size_t)N + 1)));
-    SFG_TRY(cudaMalloc(&cv, sizeof(int) * (size_t)nv * ((size_t)N + 1)));
-    SFG_TRY(cudaMalloc(&maxlen, sizeof(int)));
+    // temporaries (row buckets included) come from the device's pool
+    SFG_TRY(tmp_alloc((void **)&cnt, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(tmp_alloc((void **)&cursor, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(tmp_alloc((void **)&out.row_start, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(tmp_alloc((void **)&out.bucket, sizeof(int) * nn, st));
+    SFG_TRY(tmp_alloc((void **)&vec, sizeof(int) * nn, st));
+    SFG_TRY(tmp_alloc((void **)&map, sizeof(int) * nn, st));
+    SFG_TRY(tmp_alloc((void **)&cu, sizeof(int) * ((size_t)N + 1), st));
+    SFG_TRY(tmp_alloc((void **)&cv, sizeof(int) * (size_t)nv * ((size_t)N + 1), st));
+    SFG_TRY(tmp_alloc((void **)&maxlen, sizeof(int), st));
     SFG_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(cudaMemsetAsync(cursor, 0, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(cudaMemsetAsync(maxlen, 0, sizeof(int), st));
@@ -600,7 +615,7 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
         }
     }
     int **d_tab = nullptr;
-    SFG_TRY(cudaMalloc(&d_tab, sizeof(void *) * 24));
+    SFG_TRY(tmp_alloc((void **)&d_tab, sizeof(void *) * 24, st));
     void *htab[24];
     for (int s = 0; s < 8; s++) { htab[s] = dvp[s]; htab[8 + s] = dvj[s]; htab[16 + s] = dvx[s]; }
     SFG_TRY(cudaMemcpyAsync(d_tab, htab, sizeof(htab), cudaMemcpyHostToDevice, st));
@@ -610,9 +625,9 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
                                         (double *const *)(d_tab + 16));
     SFG_TRY(cudaGetLastError());
     SFG_TRY(cudaStreamSynchronize(st));
-    cudaFree(d_tab);
-    cudaFree(cnt); cudaFree(cursor); cudaFree(vec); cudaFree(map); cudaFree(cu); cudaFree(cv);
-    cudaFree(maxlen);
+    for (void *t : {(void *)d_tab, (void *)cnt, (void *)cursor, (void *)vec, (void *)map, (void *)cu, (void *)cv,
+                    (void *)maxlen})
+        cudaFreeAsync(t, st);
     return SFG_OK;
 }
 

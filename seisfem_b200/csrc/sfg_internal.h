@@ -103,9 +103,21 @@ struct CanonOut {
 int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const double *d_cx, int nv,
                  bool want_union, bool want_csr, CanonOut &out, int *d_flags, cudaStream_t st,
                  std::string &err);
-void canon_free(CanonOut &o, bool keep_csr);
+void canon_free(CanonOut &o, bool keep_csr, cudaStream_t st = 0);
 
 cudaError_t exclusive_scan_int(const int *d_in, int *d_out, int n, cudaStream_t st);
+// the stream-ordered memory pool of a device, shared by the process (kept up
+// to 8 GiB between uses), and a temporary allocation from it on `st`
+cudaMemPool_t device_pool(int device);
+inline cudaError_t tmp_alloc(void **p, size_t bytes, cudaStream_t st)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = device_pool(dev);
+    if (!pool) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, st);
+}
 
 // ---- step data and kernels (sfg_step.cu) ---------------------------------
 int build_step_data(DevProblem &P, const double *d_c, double dt_unused, std::string &err,
