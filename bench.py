@@ -328,24 +328,56 @@ def run_gemm_engines(args):
              ("time map: M=64 N=1000 K=128 x1024", 64, 1000, 128, (1024, 1), (128 * 64, 0, 1, 64), (0, 0, 1000, 1),
               (64 * 1000, 0, 1000, 1), 1024 * 128 * 64, 128 * 1000, 1024 * 64 * 1000, torch.bfloat16)]
     out = []
+    # the head's first GEMM as the network runs it: bias, stored
+    # pre-activation and GELU in the epilogue
+    hpre = torch.empty(16 * WT * Hp, device=dev, dtype=torch.bfloat16)
+    hbias = torch.randn(Hp, device=dev)
+    cases.insert(1, ("head 1 + bias, pre, GELU epilogue", WT, Hp, Cc, (16, 1), (Cc * WT, 0, 1, WT), (0, 0, Hp, 1),
+                     (WT * Hp, 0, Hp, 1), 16 * Cc * WT, Cc * Hp, 16 * WT * Hp, torch.bfloat16))
     for name, M, N, Kd, batch, a, b, c, asz, bsz, csz, cdt in cases:
+        epi = dict(bias=hbias, pre=hpre, gelu=True) if "epilogue" in name else {}
         A = torch.randn(asz, device=dev).to(torch.bfloat16)
         B = torch.randn(bsz, device=dev).to(torch.bfloat16)
         C = torch.empty(csz, device=dev, dtype=cdt)
         row = {"gemm": name, "flops": 2 * M * N * Kd * batch[0] * batch[1]}
         for eng, key in ((1, "mma_sync_us"), (2, "tcgen05_us")):
             for _ in range(max(3, args.warmup)):
-                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng)
+                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng, **epi)
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(10):
-                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng)
+                K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng, **epi)
             e1.record()
             torch.cuda.synchronize(dev)
             row[key] = e0.elapsed_time(e1) / 10 * 1e3
         out.append(row)
         print(json.dumps(row), flush=True)
+    # the whole network (config-5 sizes, 16 shots): forward, and a training
+    # step (forward, loss, backward, Adam), with mma.sync throughout against
+    # the automatic per-GEMM choice
+    from seisfem_b200.surrogate import FNO, init_params
+    Bn, D, W, T = 16, 128, 64, 1000
+    net = FNO(init_params(64, D, T, Hp, seed=1), Bn, D, W, T, dev)
+    x = torch.randn((Bn, 4, D, W), device=dev).to(torch.bfloat16)
+    tgt = torch.randn((Bn, 2, W, T), device=dev).to(torch.bfloat16)
+    row = {"network": "FNO width 64, 16 shots, 128 x 64 grid, 1000 samples"}
+    for eng, key in ((1, "mma_sync"), (0, "auto")):
+        net.K.engine = eng
+        for nm, fn in (("forward", lambda: net.forward(x)), ("train_step", lambda: net.train_step(x, tgt, 1e-4))):
+            for _ in range(max(3, args.warmup)):
+                fn()
+            torch.cuda.synchronize(dev)
+            f0 = net.K.flops
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            row[f"{nm}_{key}_ms"] = e0.elapsed_time(e1) / 5
+            row[f"{nm}_gemm_flops"] = (net.K.flops - f0) // 5
+    print(json.dumps(row), flush=True)
     return 0
 
 

@@ -280,19 +280,23 @@ __global__ void __launch_bounds__(256) gemm_bf16_kernel(const GemmArgs g)
 
 // ------------------------------------------------------ tcgen05 GEMM
 //
-// The same descriptor semantics on the 5th-generation tensor cores: a CTA of
-// 128 threads owns a 128 x BN tile of C held in tensor memory (BN FP32
+// The same descriptor semantics on the 5th-generation tensor cores.  A CTA of
+// 256 threads owns a 128 x BN tile of C held in tensor memory (BN FP32
 // columns, one TMEM lane per row).  Each 64-deep K tile of A (128 x 64) and B
-// (BN x 64) is loaded by all threads (the generic strided loads above) into
-// shared memory in the canonical K-major no-swizzle layout: 8-row x 16-byte
-// core matrices, the eight K chunks of a row group adjacent (LBO = 128 B) and
-// row groups 1024 B apart (SBO).  One elected thread issues four
-// tcgen05.mma.kind::f16 (BF16 x BF16 -> FP32, M = 128, N = BN, K = 16) per
-// tile and commits them to the stage's mbarrier; two stages alternate, so the
-// next tile's global loads overlap the MMAs.  Every wait is bounded: on a
-// timeout the kernel records it in g_tc_timeouts and finishes without it.
+// (BN x 64) is copied by all threads with 16-byte cp.async straight into
+// shared memory in a canonical no-swizzle layout: K-major when the operand is
+// contiguous along K, MN-major when it is contiguous along M (or N), so
+// neither case is transposed on the way.  TSTG stages rotate: while one
+// elected thread issues the four tcgen05.mma.kind::f16 (BF16 x BF16 -> FP32,
+// M = 128, N = BN, K = 16) of a tile and commits them to the stage's
+// mbarrier, the copies of the next TSTG - 1 tiles are in flight.  The
+// epilogue reads TMEM (warp w: lanes 32 (w % 4).., half the columns each),
+// stages the FP32 tile in shared memory and writes C in 8-column vectors.
+// Every wait is bounded: on a timeout the kernel records it in g_tc_timeouts
+// and finishes without it.
 
 constexpr int TBK = 64;
+constexpr int TSTG = 3;
 constexpr long long kWaitLimit = 1LL << 22;
 
 __device__ int g_tc_timeouts;
@@ -318,86 +322,70 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     return false;
 }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+// shared-memory matrix descriptor: start >> 4 | LBO >> 4 << 16 | SBO >> 4 << 32
+// | version 1 << 46, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
-    // start address >> 4 | LBO (128 B) >> 4 << 16 | SBO (1024 B) >> 4 << 32 | version 1 << 46 | no swizzle
-    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           (1ull << 46);
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// K-major canonical layout of a rows x 64 tile: element (r, k) at byte
-// ((r / 8) * 8 + k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2.
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void *src, int bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+// Copies rows [r0, r0 + R) x k [k0, k0 + 64) of an operand, element (r, k) at
+// p + r * sr + k * sk, into its canonical no-swizzle layout at shared address
+// s; bytes outside the matrix are zero-filled by the copy itself.
+//   mode 0 (k contiguous), K-major: (r, k) at ((r/8)*8 + k/8)*128 + (r%8)*16 +
+//     (k%8)*2 -- LBO 128 B (next 8 k), SBO 1024 B (next 8 rows);
+//   mode 1 (r contiguous), MN-major: (r, k) at (k/8)*R*16 + (r/8)*128 +
+//     (k%8)*16 + (r%8)*2 -- SBO 128 B (next 8 rows), LBO R*16 B (next 8 k).
+// Lane l of a warp takes the 16-byte group (l % 8) of a core matrix, so each
+// 8-lane phase writes eight distinct bank groups, and the warp's 32 groups
+// cover whole 32-byte sectors of global memory.
 template <int R>
-struct TcLoad {
-    static constexpr int NV = R * TBK / 8 / 128;   // 16-byte vectors per thread
-    uint4 v[NV];
-
-    __device__ __forceinline__ void load(const __nv_bfloat16 *p, long long sr, long long sk, int rows, int kk,
-                                         int r0, int k0, int mode)
-    {
-        const int t = threadIdx.x;
+__device__ __forceinline__ void tc_fill(uint32_t s, const __nv_bfloat16 *p, long long sr, long long sk, int rows,
+                                        int kk, int r0, int k0, int mode)
+{
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-        for (int q = 0; q < NV; q++) {
-            const int idx = t + q * 128;
-            __align__(16) __nv_bfloat16 e[8];
-            if (mode == 1) {            // 8 consecutive rows of one k
-                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
-                const int gr = r0 + r, gk = k0 + kc;
-                if (gk < kk && gr + 8 <= rows) {
-                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr + gk * sk));
-                    continue;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; u++)
-                    e[u] = (gr + u < rows && gk < kk) ? p[(gr + u) * sr + gk * sk] : __float2bfloat16(0.f);
-            } else {                    // 8 consecutive k of one row
-                const int r = idx / (TBK / 8), kc = (idx % (TBK / 8)) * 8;
-                const int gr = r0 + r, gk = k0 + kc;
-                if (mode == 0 && gr < rows && gk + 8 <= kk) {
-                    v[q] = __ldg(reinterpret_cast<const uint4 *>(p + gr * sr + gk));
-                    continue;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; u++)
-                    e[u] = (gr < rows && gk + u < kk) ? p[gr * sr + (gk + u) * sk] : __float2bfloat16(0.f);
+    for (int q = 0; q < R / 32; q++) {
+        const int wq = (threadIdx.x >> 5) + q * 8;      // warp-group of 32 vectors, 0 .. R/4 - 1
+        uint32_t dst;
+        const __nv_bfloat16 *src = p;
+        int bytes = 0;
+        if (mode == 0) {
+            const int r = (wq >> 1) * 8 + (lane & 7), kc = (wq & 1) * 4 + (lane >> 3);
+            const int gr = r0 + r, gk = k0 + kc * 8;
+            dst = s + ((r >> 3) * 8 + kc) * 128 + (r & 7) * 16;
+            if (gr < rows && gk < kk) {
+                src = p + gr * sr + gk;
+                bytes = 2 * min(8, kk - gk);
             }
-            v[q] = *reinterpret_cast<const uint4 *>(e);
-        }
-    }
-
-    __device__ __forceinline__ void store(unsigned char *s, int mode) const
-    {
-        const int t = threadIdx.x;
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            const int idx = t + q * 128;
-            if (mode == 1) {
-                const int kc = idx / (R / 8), r = (idx % (R / 8)) * 8;
-                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[q]);
-#pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const int rr = r + u;
-                    *reinterpret_cast<__nv_bfloat16 *>(s + ((rr / 8) * 8 + kc / 8) * 128 + (rr % 8) * 16 +
-                                                       (kc % 8) * 2) = e[u];
-                }
-            } else {
-                const int r = idx / (TBK / 8), kc = (idx % (TBK / 8)) * 8;
-                *reinterpret_cast<uint4 *>(s + ((r / 8) * 8 + kc / 8) * 128 + (r % 8) * 16) = v[q];
+        } else {
+            const int k = (wq & 7) * 8 + (lane & 7), rc = (wq >> 3) * 4 + (lane >> 3);
+            const int gr = r0 + rc * 8, gk = k0 + k;
+            dst = s + (k >> 3) * (R * 16) + rc * 128 + (k & 7) * 16;
+            if (gr < rows && gk < kk) {
+                src = p + gr + gk * sk;
+                bytes = 2 * min(8, rows - gr);
             }
         }
+        cp_async16_zfill(dst, src, bytes);
     }
-};
+}
 
 template <int BN>
-__global__ void __launch_bounds__(128) gemm_tc_kernel(const GemmArgs g)
+__global__ void __launch_bounds__(256) gemm_tc_kernel(const GemmArgs g)
 {
     constexpr int BM = 128;
-    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                               ((uint32_t)(BM >> 4) << 24);
+    constexpr int ASTG = BM * TBK * 2, BSTG = BN * TBK * 2;     // bytes of one stage
+    constexpr int TP = BN + 4;                                   // epilogue tile pitch (floats)
+    static_assert(BM * TP * 4 <= TSTG * (ASTG + BSTG), "epilogue tile must fit the stages");
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *As = smem;                                  // [2][128 * 64 * 2 B]
-    unsigned char *Bs = smem + 2 * BM * TBK * 2;               // [2][BN * 64 * 2 B]
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[TSTG];
     __shared__ uint32_t tmem_base;
     const sfg_gemm_desc &d = g.d;
     const int nb = d.batch1 * d.batch2;
@@ -407,14 +395,23 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(const GemmArgs g)
     const int ktiles = (d.K + TBK - 1) / TBK;
     const int per = (ktiles + d.splits - 1) / d.splits;
     const int kt0 = split * per, kt1 = min(ktiles, kt0 + per);
+    const int nt = max(0, kt1 - kt0);
     const __nv_bfloat16 *A = static_cast<const __nv_bfloat16 *>(d.A) + z1 * d.sa1 + z2 * d.sa2;
     const __nv_bfloat16 *B = static_cast<const __nv_bfloat16 *>(d.B) + z1 * d.sb1 + z2 * d.sb2;
     const long long cz = z1 * d.sc1 + z2 * d.sc2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t sA = smem_u32(smem), sB = sA + TSTG * ASTG;
+    // A: K-major (LBO 128, SBO 1024; K = 16 is 256 B on) or MN-major (SBO 128,
+    // LBO 128 * 16; K = 16 is 2 LBO on); B likewise with BN rows
+    const uint32_t a_lbo = g.amode == 1 ? BM * 16 : 128, a_sbo = g.amode == 1 ? 128 : 1024;
+    const uint32_t b_lbo = g.bmode == 1 ? BN * 16 : 128, b_sbo = g.bmode == 1 ? 128 : 1024;
+    const uint32_t a_step = g.amode == 1 ? 2 * BM * 16 : 256, b_step = g.bmode == 1 ? 2 * BN * 16 : 256;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.amode == 1) << 15) |
+                           ((uint32_t)(g.bmode == 1) << 16) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1));
+#pragma unroll
+        for (int s = 0; s < TSTG; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[s])));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     if (warp == 0) {
@@ -427,75 +424,155 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(const GemmArgs g)
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
     bool ok = true;
-    TcLoad<BM> la;
-    TcLoad<BN> lb;
-    for (int kt = kt0; kt < kt1; kt++) {
-        const int it = kt - kt0, st = it & 1;
-        la.load(A, d.sam, d.sak, d.M, d.K, m0, kt * TBK, g.amode);
-        lb.load(B, d.sbn, d.sbk, d.N, d.K, n0, kt * TBK, g.bmode);
-        if (it >= 2) ok = mbar_wait(st ? bar1 : bar0, ((it - 2) >> 1) & 1) && ok;   // stage free again
-        la.store(As + st * BM * TBK * 2, g.amode);
-        lb.store(Bs + st * BN * TBK * 2, g.bmode);
+    // prologue: the first TSTG - 1 tiles in flight (one commit group each)
+#pragma unroll
+    for (int s = 0; s < TSTG - 1; s++) {
+        if (s < nt) {
+            const int k0 = (kt0 + s) * TBK;
+            tc_fill<BM>(sA + s * ASTG, A, d.sam, d.sak, d.M, d.K, m0, k0, g.amode);
+            tc_fill<BN>(sB + s * BSTG, B, d.sbn, d.sbk, d.N, d.K, n0, k0, g.bmode);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int it = 0; it < nt; it++) {
+        const int st = it % TSTG;
+        asm volatile("cp.async.wait_group %0;" ::"n"(TSTG - 2) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && ok) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a0 = smem_u32(As + st * BM * TBK * 2), b0 = smem_u32(Bs + st * BN * TBK * 2);
+            const uint32_t a0 = sA + st * ASTG, b0 = sB + st * BSTG;
 #pragma unroll
             for (int ks = 0; ks < TBK / 16; ks++) {
-                const uint64_t da = umma_desc(a0 + ks * 256), db = umma_desc(b0 + ks * 256);
+                const uint64_t da = umma_desc(a0 + ks * a_step, a_lbo, a_sbo);
+                const uint64_t db = umma_desc(b0 + ks * b_step, b_lbo, b_sbo);
                 const uint32_t acc = (it > 0 || ks > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                st ? bar1 : bar0));
+                smem_u32(&bars[st])));
         }
+        // refill the stage the previous tile used, once its MMAs have read it
+        const int nxt = it + TSTG - 1;
+        if (nxt < nt) {
+            const int sn = nxt % TSTG;
+            if (it >= 1) ok = mbar_wait(smem_u32(&bars[sn]), ((it - 1) / TSTG) & 1) && ok;
+            const int k0 = (kt0 + nxt) * TBK;
+            tc_fill<BM>(sA + sn * ASTG, A, d.sam, d.sak, d.M, d.K, m0, k0, g.amode);
+            tc_fill<BN>(sB + sn * BSTG, B, d.sbn, d.sbk, d.N, d.K, n0, k0, g.bmode);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
-    const int nt = kt1 - kt0;
-    if (nt > 0) {
-        const int last = nt - 1;
-        ok = mbar_wait((last & 1) ? bar1 : bar0, (last >> 1) & 1) && ok;
-    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (nt > 0) ok = mbar_wait(smem_u32(&bars[(nt - 1) % TSTG]), ((nt - 1) / TSTG) & 1) && ok;
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!ok && lane == 0) atomicAdd(&g_tc_timeouts, 1);
-    // epilogue: warp w holds rows 32w .. 32w+31, thread = row
-    const int m = m0 + warp * 32 + lane;
+    // all threads agree on whether the accumulator is complete
+    const int good = __syncthreads_and(ok ? 1 : 0);
+    float *tile = reinterpret_cast<float *>(smem);
+    if (nt > 0 && good) {
+        const int row = (warp & 3) * 32 + lane;
+        const int cb = (warp >> 2) * (BN / 2);
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t r[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (nt == 0 || !ok || m >= d.M) continue;
+        for (int c0 = cb; c0 < cb + BN / 2; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float4 *t4 = reinterpret_cast<float4 *>(tile + row * TP + c0);
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const int n = n0 + c0 + j;
-            if (n >= d.N) continue;
-            const long long o = cz + m * d.scm + n * d.scn;
-            float v = d.alpha * __uint_as_float(r[j]);
-            if (d.atomic) {
-                atomicAdd(static_cast<float *>(d.C) + o, v);
-                continue;
-            }
-            if (d.Cin) v += d.beta * d.Cin[o];
-            if (d.bias) v += d.bias[d.bias_on_m ? m : n];
-            if (d.pre) static_cast<__nv_bfloat16 *>(d.pre)[o] = __float2bfloat16(v);
-            if (d.gelu) v = gelu_f(v);
-            if (d.c_bf16) static_cast<__nv_bfloat16 *>(d.C)[o] = __float2bfloat16(v);
-            else static_cast<float *>(d.C)[o] = v;
+            for (int j = 0; j < 4; j++)
+                t4[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                    __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    if (nt == 0 || !good) return;
+    // C in vectors of 8 columns: consecutive threads take consecutive vectors
+    // of a row
+    constexpr int VPR = BN / 8;
+    for (int v = threadIdx.x; v < BM * VPR; v += 256) {
+        const int rr = v / VPR, cc = (v % VPR) * 8;
+        const int m = m0 + rr, nbase = n0 + cc;
+        if (m >= d.M || nbase >= d.N) continue;
+        const int cnt = min(8, d.N - nbase);
+        const float4 *t4 = reinterpret_cast<const float4 *>(tile + rr * TP + cc);
+        const float4 q0 = t4[0], q1 = t4[1];
+        float x[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const long long o = cz + m * d.scm + (long long)nbase * d.scn;
+        if (d.atomic) {
+            for (int j = 0; j < cnt; j++) atomicAdd(static_cast<float *>(d.C) + o + j * d.scn, d.alpha * x[j]);
+            continue;
+        }
+        const bool vec = cnt == 8 && d.scn == 1 && (o & 7) == 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) x[j] *= d.alpha;
+        if (d.Cin) {
+            if (vec && (reinterpret_cast<uintptr_t>(d.Cin) & 15) == 0) {
+                const float4 a0 = *reinterpret_cast<const float4 *>(d.Cin + o);
+                const float4 a1 = *reinterpret_cast<const float4 *>(d.Cin + o + 4);
+                const float cin[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[j] += d.beta * cin[j];
+            } else {
+                for (int j = 0; j < cnt; j++) x[j] += d.beta * d.Cin[o + j * d.scn];
+            }
+        }
+        if (d.bias) {
+            if (d.bias_on_m) {
+                const float b = d.bias[m];
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[j] += b;
+            } else {
+                for (int j = 0; j < cnt; j++) x[j] += d.bias[nbase + j];
+            }
+        }
+        if (d.pre) {
+            __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(d.pre) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.pre) & 15) == 0) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
+                *reinterpret_cast<uint4 *>(pp) = *reinterpret_cast<const uint4 *>(h);
+            } else {
+                for (int j = 0; j < cnt; j++) pp[j * d.scn] = __float2bfloat16(x[j]);
+            }
+        }
+        if (d.gelu) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = gelu_f(x[j]);
+        }
+        if (d.c_bf16) {
+            __nv_bfloat16 *cp = static_cast<__nv_bfloat16 *>(d.C) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
+                *reinterpret_cast<uint4 *>(cp) = *reinterpret_cast<const uint4 *>(h);
+            } else {
+                for (int j = 0; j < cnt; j++) cp[j * d.scn] = __float2bfloat16(x[j]);
+            }
+        } else {
+            float *cp = static_cast<float *>(d.C) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+                *reinterpret_cast<float4 *>(cp) = make_float4(x[0], x[1], x[2], x[3]);
+                *reinterpret_cast<float4 *>(cp + 4) = make_float4(x[4], x[5], x[6], x[7]);
+            } else {
+                for (int j = 0; j < cnt; j++) cp[j * d.scn] = x[j];
+            }
+        }
+    }
 }
 
 // Vector loads need 16-byte aligned groups of 8 elements: the base pointer
@@ -708,12 +785,12 @@ template <int BN>
 int launch_tc(const GemmArgs &g, long long nb, cudaStream_t st)
 {
     const sfg_gemm_desc &d = g.d;
-    const int smem = 2 * 128 * TBK * 2 + 2 * BN * TBK * 2;
+    const int smem = TSTG * (128 + BN) * TBK * 2;
     if (cudaFuncSetAttribute(gemm_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return 2;
     dim3 grid((d.N + BN - 1) / BN, (d.M + 127) / 128, (unsigned)nb);
     if (grid.y > 65535) return 1;
-    gemm_tc_kernel<BN><<<grid, 128, smem, st>>>(g);
+    gemm_tc_kernel<BN><<<grid, 256, smem, st>>>(g);
     return launched();
 }
 
@@ -747,7 +824,7 @@ int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
     g.bmode = pick_mode(d.sbn, d.sbk, d.sb1, d.sb2, d.B);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const bool tc = d.engine == 2 || (d.engine == 0 && tc_auto(d));
-    if (tc && d.N >= 32) {
+    if (tc && d.N >= 32 && g.amode != 2 && g.bmode != 2) {   // cp.async needs 16-byte groups
         if (d.N >= 128) return launch_tc<128>(g, nb, st);
         if (d.N >= 64) return launch_tc<64>(g, nb, st);
         return launch_tc<32>(g, nb, st);

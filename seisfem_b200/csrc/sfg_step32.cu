@@ -9,8 +9,9 @@
 // gathers each neighbour record once, keeps every product in registers and
 // finishes the node (right-hand sides elastic_wave.c:585-591 / 651-657,
 // lumped solve :709-722, Newmark :757-776) in the same thread.  The SpMV
-// products accumulate in FP32; the per-node epilogue runs in FP64 for the
-// compensated precision, with displacements kept as FP32 hi + lo pairs.
+// products and the per-node epilogue run in FP32; the compensated precision
+// keeps every displacement as an FP32 hi + lo pair updated with a Kahan sum,
+// and forms the class-Z totals U1+U2+U3, W1+W2+W3 from those pairs in FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,16 +47,19 @@ template <> struct VecF<4> {
 // --------------------------------------------------------------- epilogues
 
 // Newmark, alpha = 1, delta = 1.5 (elastic_wave.c:97, 757-768) for one
-// displacement carried as hi + lo, updated in FP64.
-__device__ __forceinline__ double newmark_comp(float &hi, float &lo, float &V, float &A, double an, double dt)
+// displacement carried as hi + lo: the step's increment is added with a
+// compensated (Kahan) sum in FP32, so the rounding error of the running
+// displacement does not build up over the steps.  Returns hi + lo.
+__device__ __forceinline__ float newmark_kahan(float &hi, float &lo, float &V, float &A, float an, float dt)
 {
-    const double Ad = A, Vd = V;
-    const double U = ((double)hi + (double)lo) + Vd * dt + (an - 0.5 * Ad) * (dt * dt);
-    hi = (float)U;
-    lo = (float)(U - (double)hi);
-    V = (float)(Vd + (1.5 * an - 0.5 * Ad) * dt);
-    A = (float)an;
-    return U;
+    const float d = V * dt + (an - 0.5f * A) * (dt * dt);
+    const float y = d + lo;
+    const float t = hi + y;
+    lo = y - (t - hi);
+    hi = t;
+    V = V + (1.5f * an - 0.5f * A) * dt;
+    A = an;
+    return t + lo;
 }
 
 __device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, float an, float dt)
@@ -73,24 +77,19 @@ __device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, flo
 // g[12]: own Gc record, p[4]: own Pa record, replaced by the new records.
 template <bool COMP>
 __device__ __forceinline__ void finish_A(const float *kU, const float *kW, const float *mL, float4 c, float im,
-                                         double dt, double src_u, double src_w, float *g, float *p, double &uu,
-                                         double &ww)
+                                         double dt, double src_u, double src_w, float *g, float *p, float &uu,
+                                         float &ww)
 {
     float Uh = g[0], Wh = g[1], Vu = g[10], Vw = g[11];
     float Au = p[0], Aw = p[1], lou = p[2], low = p[3];
+    const float au = im * (-c.x * kU[0] - c.w * kU[1] - c.y * kW[2] - c.w * kW[3] +
+                           ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
+    const float aw = im * (-c.w * kW[0] - c.z * kW[1] - c.w * kU[2] - c.y * kU[3] +
+                           ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
     if (COMP) {
-        const double c11 = c.x, c13 = c.y, c33 = c.z, c44 = c.w, m = im;
-        const double au = m * (-c11 * (double)kU[0] - c44 * (double)kU[1] - c13 * (double)kW[2] - c44 * (double)kW[3] +
-                               (((double)mL[0] + (double)mL[1]) + ((double)mL[2] + (double)mL[3])) + src_u);
-        const double aw = m * (-c44 * (double)kW[0] - c33 * (double)kW[1] - c44 * (double)kU[2] - c13 * (double)kU[3] +
-                               (((double)mL[4] + (double)mL[5]) + ((double)mL[6] + (double)mL[7])) + src_w);
-        uu = newmark_comp(Uh, lou, Vu, Au, au, dt);
-        ww = newmark_comp(Wh, low, Vw, Aw, aw, dt);
+        uu = newmark_kahan(Uh, lou, Vu, Au, au, (float)dt);
+        ww = newmark_kahan(Wh, low, Vw, Aw, aw, (float)dt);
     } else {
-        const float au = im * (-c.x * kU[0] - c.w * kU[1] - c.y * kW[2] - c.w * kW[3] +
-                               ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
-        const float aw = im * (-c.w * kW[0] - c.z * kW[1] - c.w * kU[2] - c.y * kU[3] +
-                               ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
         uu = newmark_plain(Uh, Vu, Au, au, (float)dt);
         ww = newmark_plain(Wh, Vw, Aw, aw, (float)dt);
         lou = 0.f;
@@ -145,29 +144,32 @@ __device__ __forceinline__ void rhs_eval(const float *kU, const float *kW, const
 template <bool COMP>
 __device__ __forceinline__ void finish_Z(const float *kU, const float *kW, const float *m, float4 c0, float4 c1,
                                          float4 c2, double dt, double src_u, double src_w, float *gs, float *ps,
-                                         float *gc, double &uu, double &ww)
+                                         float *gc, float &uu, float &ww)
 {
-    double Ut[6];
     float L[8];
+    RhsT<float> r;
+    rhs_eval<float>(kU, kW, m, c0, c1, c2, (float)dt, (float)src_u, (float)src_w, r);
+    float su, sw;
     if (COMP) {
-        RhsT<double> r;
-        rhs_eval<double>(kU, kW, m, c0, c1, c2, dt, src_u, src_w, r);
 #pragma unroll
-        for (int k = 0; k < 6; k++) Ut[k] = newmark_comp(gs[k], ps[6 + k], gs[6 + k], ps[k], r.a[k], dt);
-#pragma unroll
-        for (int k = 0; k < 4; k++) { L[k] = (float)r.lx[k]; L[4 + k] = (float)r.ly[k]; }
+        for (int k = 0; k < 6; k++) newmark_kahan(gs[k], ps[6 + k], gs[6 + k], ps[k], r.a[k], (float)dt);
+        // the totals from the compensated split fields (each hi + lo) in FP64:
+        // inside the M-PML the split fields are far larger than their sum
+        su = (float)((((double)gs[0] + ps[6]) + ((double)gs[1] + ps[7])) + ((double)gs[2] + ps[8]));
+        sw = (float)((((double)gs[3] + ps[9]) + ((double)gs[4] + ps[10])) + ((double)gs[5] + ps[11]));
     } else {
-        RhsT<float> r;
-        rhs_eval<float>(kU, kW, m, c0, c1, c2, (float)dt, (float)src_u, (float)src_w, r);
+        float Ut[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) { Ut[k] = newmark_plain(gs[k], gs[6 + k], ps[k], r.a[k], (float)dt); ps[6 + k] = 0.f; }
-#pragma unroll
-        for (int k = 0; k < 4; k++) { L[k] = r.lx[k]; L[4 + k] = r.ly[k]; }
+        su = (Ut[0] + Ut[1]) + Ut[2];
+        sw = (Ut[3] + Ut[4]) + Ut[5];
     }
-    uu = (Ut[0] + Ut[1]) + Ut[2];
-    ww = (Ut[3] + Ut[4]) + Ut[5];
-    gc[0] = (float)uu;
-    gc[1] = (float)ww;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { L[k] = r.lx[k]; L[4 + k] = r.ly[k]; }
+    uu = su;
+    ww = sw;
+    gc[0] = su;
+    gc[1] = sw;
 #pragma unroll
     for (int k = 0; k < 8; k++) gc[2 + k] = L[k];
     gc[10] = 0.f;
@@ -260,13 +262,14 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
         }
         const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.in.Pa) + i);
         p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
-        finish_A<COMP>(kU, kW, mL, cf, im, c.dt, src_u, src_w, g, p, eu, ew);
+        float uu, ww;
+        finish_A<COMP>(kU, kW, mL, cf, im, c.dt, src_u, src_w, g, p, uu, ww);
         float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
 #pragma unroll
         for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
         reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
-        eu = eu * eu;
-        ew = ew * ew;
+        eu = (double)uu * uu;
+        ew = (double)ww * ww;
     }
     block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
 }
@@ -353,7 +356,8 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
             gs[4 * k] = v.x; gs[4 * k + 1] = v.y; gs[4 * k + 2] = v.z; gs[4 * k + 3] = v.w;
             ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
         }
-        finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, eu, ew);
+        float uu, ww;
+        finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, uu, ww);
         float4 *gco = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
         float4 *so = reinterpret_cast<float4 *>(a.out.Gs + (size_t)local * GS);
         float4 *po = reinterpret_cast<float4 *>(a.out.Ps + (size_t)local * PS);
@@ -363,8 +367,8 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
             so[k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
             po[k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
         }
-        eu = eu * eu;
-        ew = ew * ew;
+        eu = (double)uu * uu;
+        ew = (double)ww * ww;
     }
     block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
 }
@@ -558,14 +562,14 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
                 for (int t = 0; t < 8; t++) mq[t] *= cm[MM ? 5 : 0].v[q];
             }
             const bool is_src = (i == src[q]);
-            double uu, ww;
+            float uu, ww;
             finish_A<COMP>(kUq, kWq, mq, cfq, imq, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
 #pragma unroll
             for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
 #pragma unroll
             for (int v = 0; v < PA; v++) pv[v].v[q] = p[v];
-            eu[q] += (float)(uu * uu);
-            ew[q] += (float)(ww * ww);
+            eu[q] += uu * uu;
+            ew[q] += ww * ww;
         }
 #pragma unroll
         for (int v = 0; v < GC; v++) gv[v].store(go + v * S);
@@ -725,15 +729,15 @@ __global__ void __launch_bounds__(256, 1) stepA_staged(const Step2 a)
 #pragma unroll
                 for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
                 const bool is_src = (i == src[q]);
-                double uu, ww;
+                float uu, ww;
                 finish_A<COMP>(kUq, kWq, mq, cf, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu,
                                ww);
 #pragma unroll
                 for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
 #pragma unroll
                 for (int v = 0; v < PA; v++) pv[v].v[q] = p[v];
-                eu[q] += (float)(uu * uu);
-                ew[q] += (float)(ww * ww);
+                eu[q] += uu * uu;
+                ew[q] += ww * ww;
             }
 #pragma unroll
             for (int v = 0; v < GC; v++) gv[v].store(go + v * S);
@@ -891,13 +895,13 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
                 for (int t = 0; t < 20; t++) mq[t] *= cm[MM ? 5 : 0].v[q];
             }
             const bool is_src = (i == src[q]);
-            double uu, ww;
+            float uu, ww;
             finish_Z<COMP>(kUq, kWq, mq, c0q, c1q, c2q, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, gs, ps_,
                            gc, uu, ww);
 #pragma unroll
             for (int v = 0; v < GS; v++) { sv[v].v[q] = gs[v]; pv[v].v[q] = ps_[v]; cv[v].v[q] = gc[v]; }
-            eu[q] += (float)(uu * uu);
-            ew[q] += (float)(ww * ww);
+            eu[q] += uu * uu;
+            ew[q] += ww * ww;
         }
 #pragma unroll
         for (int v = 0; v < GC; v++) cv[v].store(gco + v * S);

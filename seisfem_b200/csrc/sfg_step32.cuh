@@ -23,7 +23,7 @@
 //               part) | V1..V6
 //   Ps[nz][12]  class Z, private: A1..A6 | lo1..lo6
 // Compensated precision keeps every displacement as an FP32 pair hi + lo
-// updated in FP64; the plain FP32 variant leaves lo at 0.
+// updated with a Kahan sum; the plain FP32 variant leaves lo at 0.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -59,7 +59,7 @@ class Kernels:
         self.stream = stream
         self.launches = 0
         self.flops = 0          # 2 M N K per problem of every GEMM issued
-        self.engine = 1         # GEMM engine: 0 automatic, 1 mma.sync (measured faster here), 2 tcgen05
+        self.engine = 0         # GEMM engine: 0 automatic (tcgen05 for M >= 128, N >= 32, K >= 64), 1 mma.sync, 2 tcgen05
         f = self.L.sfg_fno_gemm
         f.argtypes = [C.POINTER(GemmDesc), C.c_void_p]
         for n, a in [("sfg_fno_dft_combine", [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

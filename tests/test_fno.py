@@ -79,11 +79,15 @@ def test_host_sequencing_matches_oracle_on_cpu():
 # ------------------------------------------------------------------ GPU
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("engine", [1, 2])
 @pytest.mark.parametrize("layout", ["nn", "tn", "nt", "strided"])
-def test_gemm_matches_fp32(layout):
+def test_gemm_matches_fp32(layout, engine):
+    """Every epilogue term (alpha, beta Cin, bias, stored pre-activation,
+    GELU) on both engines; odd strides take the mma.sync engine."""
     import torch
     from seisfem_b200.surrogate import Kernels
     K = Kernels()
+    K.engine = engine
     dev = torch.device("cuda:0")
     rng = np.random.default_rng(3)
     b1, b2, M, N, Kd = 3, 2, 150, 70, 90
@@ -120,7 +124,7 @@ def test_gemm_matches_fp32(layout):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,Kd,layout", [(32, 64, "nn"), (64, 100, "tn"), (128, 300, "nt"), (200, 128, "nn"),
-                                         (96, 64, "strided")])
+                                         (136, 72, "tt"), (40, 200, "tt"), (96, 64, "strided")])
 def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
     """The tcgen05/TMEM engine against the mma.sync engine on the same
     descriptor (both accumulate in FP32), incl. ragged M, N, K and every
@@ -137,11 +141,11 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
     A = torch.tensor(rng.standard_normal((b1, M, Kd)).astype(np.float32)).to(torch.bfloat16)
     B = torch.tensor(rng.standard_normal((b1, Kd, N)).astype(np.float32)).to(torch.bfloat16)
     bias = torch.tensor(rng.standard_normal(N).astype(np.float32), device=dev)
-    if layout in ("tn", "strided"):
+    if layout in ("tn", "tt", "strided"):       # A m-contiguous: the MN-major tile layout
         Ad, sa = A.transpose(1, 2).contiguous().to(dev), (Kd * M, 0, 1, M)
     else:
         Ad, sa = A.contiguous().to(dev), (M * Kd, 0, Kd, 1)
-    if layout == "nt":
+    if layout in ("nt", "tt"):                  # B k-contiguous: the K-major tile layout
         Bd, sb = B.transpose(1, 2).contiguous().to(dev), (N * Kd, 0, 1, Kd)
     else:
         Bd, sb = B.contiguous().to(dev), (Kd * N, 0, N, 1)
@@ -163,10 +167,12 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
 
 
 @pytest.mark.gpu
-def test_gemm_split_k_and_batch_sum():
+@pytest.mark.parametrize("engine", [1, 2])
+def test_gemm_split_k_and_batch_sum(engine):
     import torch
     from seisfem_b200.surrogate import Kernels
     K = Kernels()
+    K.engine = engine
     dev = torch.device("cuda:0")
     rng = np.random.default_rng(4)
     b, M, N, Kd = 4, 64, 48, 5000
@@ -181,7 +187,10 @@ def test_gemm_split_k_and_batch_sum():
 
 
 @pytest.mark.gpu
-def test_gpu_forward_and_gradients_match_oracle():
+@pytest.mark.parametrize("engine", [0, 1, 2])
+def test_gpu_forward_and_gradients_match_oracle(engine):
+    """Engine 0 picks per GEMM, 1 is mma.sync throughout, 2 takes tcgen05
+    for every GEMM it can."""
     import torch
     import fno_oracle
     from fno_emulator import EmuKernels
@@ -190,6 +199,7 @@ def test_gpu_forward_and_gradients_match_oracle():
     y_ref, l_ref, g_ref = fno_oracle.loss_and_grads(prm, x.float().numpy(), t.float().numpy())
     dev = torch.device("cuda:0")
     net = FNO(prm, s["B"], s["D"], s["W"], s["T"], dev)
+    net.K.engine = engine
     y, loss, g = _run(net, x.to(dev), t.to(dev))
     torch.cuda.synchronize()
     emu = FNO(prm, s["B"], s["D"], s["W"], s["T"], "cpu", kernels=EmuKernels())
