@@ -164,7 +164,7 @@ void free_problem(DevProblem &P)
     cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
     cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.perm); cudaFree(P.inv);
     cudaFree(P.sellA); cudaFree(P.sellZ); cudaFree(P.sliceA); cudaFree(P.sliceZ); cudaFree(P.upp);
-    cudaFree(P.recp); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ); cudaFree(P.rho0);
+    cudaFree(P.recp); cudaFree(P.recA); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ); cudaFree(P.rho0);
     P = DevProblem();
 }
 
@@ -582,7 +582,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             Step2 a;
             a.c = c; a.na = P.na; a.S = S;
             a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
-            a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
+            a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.recA = P.recA; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
             a.cmm = b.cmm; a.sig = b.sig;
             a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
             a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
@@ -754,16 +754,23 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
         CK(cudaEventElapsedTime(&ms, e0, e1));
         return SFG_OK;
     };
+    // class-A shapes outside the kernel's launch bounds are skipped; the
+    // class-Z kernel ignores the staged flag
+    auto valid_a = [&](int s) {
+        return pl.S == 1 || (s & 0x100) || (s & 15) <= stepA_batched_max_warps((s >> 4) & 15, b.cmm != nullptr);
+    };
     float best = 1e30f;
-    int pick_a = cand[0], pick_z = cand[0];
+    int pick_a = -1, pick_z = cand[0];
     for (int cnd : cand) {
+        if (!valid_a(cnd)) continue;
         float ms = 0.f;
         int rc = time_shape(cnd, cnd, ms);
         if (rc) return rc;
         if (ms < best) { best = ms; pick_a = cnd; pick_z = cnd; }
     }
+    if (pick_a < 0) return fail(ctx, SFG_ERR_ARG, "no launch shape fits the class-A kernel");
     for (int cnd : cand) {
-        if (cnd == pick_a || (cnd & 0x100)) continue;   // the staged variant exists for class A only
+        if (cnd == pick_z || (cnd & 0x100)) continue;
         float ms = 0.f;
         int rc = time_shape(pick_a, cnd, ms);
         if (rc) return rc;
@@ -952,6 +959,12 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capt
     PhaseTrace tr(ctx->stream);
     if ((rc = alloc_bufs(ctx, pl, &p->run, p->nsnap, p->b)) != SFG_OK) { plan_free(p); return rc; }
     if (models && (rc = build_models(ctx, p, models)) != SFG_OK) { plan_free(p); return rc; }
+    if (fp32 && pl.S > 1 && !models && !ctx->P.recA) {   // batches with one model read folded class-A records
+        DevProblem &P = ctx->P;
+        const cudaError_t ef = build_rec_fold(N, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, P.upp, P.coef64,
+                                              &P.recA, ctx->stream);
+        if (ef != cudaSuccess) { plan_free(p); return fail(ctx, SFG_ERR_CUDA, cudaGetErrorString(ef)); }
+    }
     tr.mark("plan: buffers");
     std::vector<int> staged((size_t)p->nbatch * pl.S, -1);
     for (int s = 0; s < run->src_num; s++)

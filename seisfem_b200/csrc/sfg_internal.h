@@ -63,6 +63,7 @@ struct DevProblem {
     long long slotsA = 0, slotsZ = 0;
     int *upp = nullptr;              // permuted union row pointers
     float *recp = nullptr;           // permuted row-major records [union_nnz][8]
+    float *recA = nullptr;           // folded class-A records (batches with one model), built on first use
     float4 *coefA = nullptr;         // [na]
     float *imA = nullptr;            // [na]
     float *coefZ = nullptr;          // [N - na][12]

@@ -70,22 +70,29 @@ __device__ __forceinline__ float newmark_plain(float &U, float &V, float &A, flo
     return U;
 }
 
+// Stiffness part of the class-A right-hand sides from the products kU, kW
+// (K1..K4 times U, W) and the row's c11 c13 c33 c44 (elastic_wave.c:585-591,
+// 651-657 with the damping terms zero).
+__device__ __forceinline__ void stiff_sums(const float *kU, const float *kW, float4 c, float &su, float &sw)
+{
+    su = -c.x * kU[0] - c.w * kU[1] - c.y * kW[2] - c.w * kW[3];
+    sw = -c.w * kW[0] - c.z * kW[1] - c.w * kU[2] - c.y * kU[3];
+}
+
 // Class A: the summed right-hand sides of the three split fields with
 // dx = dy = dxx = dyy = 0:  a_u = (rhs_u1 + rhs_u2 + rhs_u3) / m,
 // a_w = (rhs_w1 + rhs_w2 + rhs_w3) / m, and L_k = (M L_k) / m.
-// kU, kW: K1..K4 times U, W; mL: M times Lx1..4, Ly1..4.
+// su, sw: the stiffness sums (stiff_sums, or accumulated from folded
+// records); mL: M times Lx1..4, Ly1..4.
 // g[12]: own Gc record, p[4]: own Pa record, replaced by the new records.
 template <bool COMP>
-__device__ __forceinline__ void finish_A(const float *kU, const float *kW, const float *mL, float4 c, float im,
-                                         double dt, double src_u, double src_w, float *g, float *p, float &uu,
-                                         float &ww)
+__device__ __forceinline__ void finish_A(float su, float sw, const float *mL, float im, double dt, double src_u,
+                                         double src_w, float *g, float *p, float &uu, float &ww)
 {
     float Uh = g[0], Wh = g[1], Vu = g[10], Vw = g[11];
     float Au = p[0], Aw = p[1], lou = p[2], low = p[3];
-    const float au = im * (-c.x * kU[0] - c.w * kU[1] - c.y * kW[2] - c.w * kW[3] +
-                           ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
-    const float aw = im * (-c.w * kW[0] - c.z * kW[1] - c.w * kU[2] - c.y * kU[3] +
-                           ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
+    const float au = im * (su + ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
+    const float aw = im * (sw + ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
     if (COMP) {
         uu = newmark_kahan(Uh, lou, Vu, Au, au, (float)dt);
         ww = newmark_kahan(Wh, low, Vw, Aw, aw, (float)dt);
@@ -262,8 +269,9 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
         }
         const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.in.Pa) + i);
         p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
-        float uu, ww;
-        finish_A<COMP>(kU, kW, mL, cf, im, c.dt, src_u, src_w, g, p, uu, ww);
+        float uu, ww, su, sw;
+        stiff_sums(kU, kW, cf, su, sw);
+        finish_A<COMP>(su, sw, mL, im, c.dt, src_u, src_w, g, p, uu, ww);
         float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
 #pragma unroll
         for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
@@ -466,9 +474,38 @@ __device__ __forceinline__ void acc_totals(const Entry &e, const VecF<SPL> *x, f
     for (int t = 0; t < 8; t++) axpy<SPL>(mL[t], e.vm, x[2 + t]);
 }
 
-// MM: every shot has its own model (a.cmm, a.sig; see Step2).
+// Folded records (Step2::recA): the stiffness sums directly, two products
+// into each, plus M times Lx1..4, Ly1..4.
+template <int SPL>
+__device__ __forceinline__ void acc_folded(const Entry &e, const VecF<SPL> *x, float *su, float *sw,
+                                           float (*mL)[SPL])
+{
+    axpy<SPL>(su, e.k[0], x[0]);
+    axpy<SPL>(sw, e.k[2], x[1]);
+    axpy<SPL>(su, e.k[1], x[1]);
+    axpy<SPL>(sw, e.k[3], x[0]);
+#pragma unroll
+    for (int t = 0; t < 8; t++) axpy<SPL>(mL[t], e.vm, x[2 + t]);
+}
+
+// The products of one entry: folded records (one model for every shot) or
+// K1..K4 (each shot with its own constants, MM).
+template <bool MM, int SPL>
+__device__ __forceinline__ void acc_entry(const Entry &e, const VecF<SPL> *x, float (*kU)[SPL], float (*kW)[SPL],
+                                          float (*mL)[SPL])
+{
+    if constexpr (MM) acc_totals<SPL>(e, x, kU, kW, mL);
+    else acc_folded<SPL>(e, x, kU[0], kW[0], mL);
+}
+
+// MM: every shot has its own model (a.cmm, a.sig; see Step2) and the kernel
+// reads the raw records a.rec; otherwise the folded records a.recA.  Two
+// shots per lane with folded records run in blocks of at most 4 warps, 5 per
+// SM (at most 102 registers): 20 resident warps measured 4-5 % faster than
+// 16 at 110 registers, and 24 at 80 registers slower again.
 template <bool COMP, int SPL, int S, bool MM>
-__global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_batched(const Step2 a)
+__global__ void __launch_bounds__(SPL == 2 && !MM ? 128 : 256, SPL == 1 ? 3 : (SPL == 2 ? (MM ? 2 : 5) : 1))
+    stepA_batched(const Step2 a)
 {
     __shared__ float se[2 * S];
     const StepCommon &c = a.c;
@@ -487,15 +524,16 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
     float eu[SPL], ew[SPL];
 #pragma unroll
     for (int q = 0; q < SPL; q++) { eu[q] = 0.f; ew[q] = 0.f; }
-    const float4 *rec = reinterpret_cast<const float4 *>(a.rec);
+    const float4 *rec = reinterpret_cast<const float4 *>(MM ? a.rec : a.recA);
+    constexpr int NK = MM ? 4 : 1;    // accumulators per component: K1..K4 products, or the folded sum
     const long long tasks = (long long)a.na * nch;
     for (long long task = warp; task < tasks; task += warps_total) {
         const int i = (int)(task / nch);
-        float kU[4][SPL], kW[4][SPL], mL[8][SPL];
+        float kU[NK][SPL], kW[NK][SPL], mL[8][SPL];
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
+            for (int k = 0; k < NK; k++) { kU[k][q] = 0.f; kW[k][q] = 0.f; }
 #pragma unroll
             for (int k = 0; k < 8; k++) mL[k][q] = 0.f;
         }
@@ -512,8 +550,8 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
                 VecF<SPL> xa[10], xb[10];
 #pragma unroll
                 for (int v = 0; v < 10; v++) { xa[v].load(ga + v * S); xb[v].load(gb + v * S); }
-                acc_totals<SPL>(ea, xa, kU, kW, mL);
-                acc_totals<SPL>(eb, xb, kU, kW, mL);
+                acc_entry<MM, SPL>(ea, xa, kU, kW, mL);
+                acc_entry<MM, SPL>(eb, xb, kU, kW, mL);
             }
             if (k < cnt) {
                 const Entry ea = entry_at<4>(r0, r1, k);
@@ -521,10 +559,9 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
                 VecF<SPL> xa[10];
 #pragma unroll
                 for (int v = 0; v < 10; v++) xa[v].load(ga + v * S);
-                acc_totals<SPL>(ea, xa, kU, kW, mL);
+                acc_entry<MM, SPL>(ea, xa, kU, kW, mL);
             }
         }
-        const float4 cf = MM ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(a.coefA + i);
         const float im = MM ? 0.f : __ldg(a.imA + i);
         VecF<SPL> cm[MM ? 6 : 1];
         if (MM) {
@@ -545,25 +582,28 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 3 : (SPL == 2 ? 2 : 1)) stepA_
         for (int v = 0; v < PA; v++) pv[v].load(pi + v * S);
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
-            float kUq[4], kWq[4], mq[8], g[GC], p[PA];
-#pragma unroll
-            for (int t = 0; t < 4; t++) { kUq[t] = kU[t][q]; kWq[t] = kW[t][q]; }
+            float mq[8], g[GC], p[PA];
 #pragma unroll
             for (int t = 0; t < 8; t++) mq[t] = mL[t][q];
             g[0] = gv[0].v[q]; g[1] = gv[1].v[q]; g[10] = gv[10].v[q]; g[11] = gv[11].v[q];
 #pragma unroll
             for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
-            float4 cfq = cf;
-            float imq = im;
-            if (MM) {   // the shot's constants, lumped mass and density (M = diag(rho) M_geo)
-                cfq = make_float4(cm[0].v[q], cm[1].v[q], cm[2].v[q], cm[3].v[q]);
+            float imq = im, su, sw;
+            if constexpr (MM) {   // the shot's constants, lumped mass and density (M = diag(rho) M_geo)
+                float kUq[4], kWq[4];
+#pragma unroll
+                for (int t = 0; t < 4; t++) { kUq[t] = kU[t][q]; kWq[t] = kW[t][q]; }
+                stiff_sums(kUq, kWq, make_float4(cm[0].v[q], cm[1].v[q], cm[2].v[q], cm[3].v[q]), su, sw);
                 imq = cm[4].v[q];
 #pragma unroll
-                for (int t = 0; t < 8; t++) mq[t] *= cm[MM ? 5 : 0].v[q];
+                for (int t = 0; t < 8; t++) mq[t] *= cm[5].v[q];
+            } else {
+                su = kU[0][q];
+                sw = kW[0][q];
             }
             const bool is_src = (i == src[q]);
             float uu, ww;
-            finish_A<COMP>(kUq, kWq, mq, cfq, imq, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
+            finish_A<COMP>(su, sw, mq, imq, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
 #pragma unroll
             for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
 #pragma unroll
@@ -729,9 +769,9 @@ __global__ void __launch_bounds__(256, 1) stepA_staged(const Step2 a)
 #pragma unroll
                 for (int v = 0; v < PA; v++) p[v] = pv[v].v[q];
                 const bool is_src = (i == src[q]);
-                float uu, ww;
-                finish_A<COMP>(kUq, kWq, mq, cf, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu,
-                               ww);
+                float uu, ww, su, sw;
+                stiff_sums(kUq, kWq, cf, su, sw);
+                finish_A<COMP>(su, sw, mq, im, c.dt, is_src ? src_u : 0.0, is_src ? src_w : 0.0, g, p, uu, ww);
 #pragma unroll
                 for (int v = 0; v < GC; v++) gv[v].v[q] = g[v];
 #pragma unroll
@@ -991,6 +1031,40 @@ __global__ void rec_perm_fill(int n, const int *__restrict__ up, const int *__re
     }
 }
 
+// Class-A rows with one model for every shot: the row's elastic constants
+// folded into its stiffness entries, formed in FP64 from the union values and
+// rounded once.  Planes: column, M (as rec_perm_fill), then
+//   -(c11 K1 + c44 K2) (times U) and -(c13 K3 + c44 K4) (times W), summed into
+//   the u right-hand side;
+//   -(c44 K1 + c33 K2) (times W) and -(c44 K3 + c13 K4) (times U), into the w
+//   right-hand side;
+// planes 6, 7 zero.  c: [4][n] c11, c13, c33, c44 in mesh order.
+__global__ void rec_fold_fill(int na, int n, const int *__restrict__ up, const int *__restrict__ uj,
+                              const double *__restrict__ ux, long long nnz, const int *__restrict__ perm,
+                              const int *__restrict__ inv, const int *__restrict__ upp, const double *__restrict__ c,
+                              float *__restrict__ rec)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    const int o = perm[r];
+    const double c11 = c[o], c13 = c[(size_t)n + o], c33 = c[2 * (size_t)n + o], c44 = c[3 * (size_t)n + o];
+    const int a0 = up[o], len = up[o + 1] - a0;
+    const long long d0 = upp[r];
+    for (int k = 0; k < len; k++) {
+        const long long e = a0 + k, d = d0 + k;
+        const double K1 = ux[nnz + e], K2 = ux[2 * nnz + e], K3 = ux[3 * nnz + e], K4 = ux[4 * nnz + e];
+        float *q = rec + d * 8;
+        q[0] = __int_as_float(inv[uj[e]]);
+        q[1] = (float)ux[e];
+        q[2] = (float)(-(c11 * K1 + c44 * K2));
+        q[3] = (float)(-(c13 * K3 + c44 * K4));
+        q[4] = (float)(-(c44 * K1 + c33 * K2));
+        q[5] = (float)(-(c44 * K3 + c13 * K4));
+        q[6] = 0.f;
+        q[7] = 0.f;
+    }
+}
+
 __global__ void coef2_kernel(int n, int na, const float *__restrict__ coef, const int *__restrict__ perm,
                              float4 *__restrict__ coefA, float *__restrict__ imA, float *__restrict__ coefZ)
 {
@@ -1216,8 +1290,12 @@ static long long batched_grid(K kernel, int threads, long long tasks, int warps,
         else SFG_BATCH_S(KERNEL, false, ROWS);                                                           \
     } while (0)
 
+// largest block of the batched class-A kernel (its launch bounds)
+int stepA_batched_max_warps(int spl, bool models) { return spl == 2 && !models ? 4 : 8; }
+
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st)
 {
+    if (warps > stepA_batched_max_warps(spl, a.cmm != nullptr)) return cudaErrorInvalidValue;
     // at least one warp for the receiver gather even without class-A rows
     SFG_BATCH(stepA_batched, std::max(a.na, 1));
     return cudaGetLastError();
@@ -1300,6 +1378,21 @@ cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double
     if (e != cudaSuccess) return e;
     if (n) rec_perm_fill<<<(n + 127) / 128, 128, 0, st>>>(n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, *d_rec);
     return cudaGetLastError();
+}
+
+cudaError_t build_rec_fold(int n, int na, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                           const int *d_perm, const int *d_inv, const int *d_upp, const double *d_c, float **d_rec,
+                           cudaStream_t st)
+{
+    int nnz_a = 0;
+    cudaError_t e = cudaMemcpyAsync(&nnz_a, d_upp + na, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMalloc(d_rec, sizeof(float) * 8 * std::max(nnz_a, 1));
+    if (e == cudaSuccess && na > 0) {
+        rec_fold_fill<<<(na + 127) / 128, 128, 0, st>>>(na, n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, d_c, *d_rec);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,

@@ -51,6 +51,8 @@ struct Step2 {
     const int *sliceZ;
     const int *up;             // row-major union records in the permuted numbering
     const float *rec;          //   [nnz][8]: col, M, K1..K6
+    const float *recA;         // class-A rows, one model: [upp[na]][8] col, M and the
+                               //   constants folded into K1..K4 (rec_fold_fill)
     const float4 *coefA;       // [na] c11 c13 c33 c44
     const float *imA;          // [na] 1/m_lump (0 on Dirichlet rows)
     const float *coefZ;        // [n-na][12] (sfg_step.cuh coefficient order)
@@ -72,6 +74,7 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
 // S = a.S shots, a multiple of 32 * spl; a warp advances 32 * spl shots of
 // one row (spl per lane); warps per block a multiple of S / (32 * spl)
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
+int stepA_batched_max_warps(int spl, bool models);
 cudaError_t launch_stepZ_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
 // class A with staged neighbour gathers (cp.async into per-warp shared-memory
 // buffers), 64 shots, one persistent block of 8 warps per SM
@@ -101,6 +104,10 @@ cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long 
 cudaError_t mass_row_sums_geo(int n, const int *d_up, const double *d_ux, const double *d_rho0, double *d_out,
                               cudaStream_t st);
 // class-A / class-Z coefficient arrays from the [n][12] FP32 record
+// the folded class-A records of Step2::recA (c: [4][n] c11 c13 c33 c44, mesh order)
+cudaError_t build_rec_fold(int n, int na, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
+                           const int *d_perm, const int *d_inv, const int *d_upp, const double *d_c, float **d_rec,
+                           cudaStream_t st);
 cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm, float4 **d_coefA, float **d_imA,
                         float **d_coefZ, cudaStream_t st);
 
