@@ -590,12 +590,14 @@ def read_traffic(path, key):
 
 def step_bytes(ctx, prob, S) -> int:
     """Algorithmic bytes of one fused FP32 time step (all S shots), for the
-    two-class layout: rows outside the M-PML zone stream column + M + K1..K4
-    (24 B per union entry) and move their totals record (Gc 12 + Pa 4 floats,
-    read and written once); split-zone rows stream 32 B per entry inside the
-    M-PML (K5, K6 too) and move Gc + Gs + Ps (36 floats); per-node
-    coefficients 5 floats (interior) or 12 (split zone).  Gathers of
-    neighbour records are counted once (their owner's read)."""
+    two-class layout.  Matrix: one shot streams SELL slots of column + M +
+    K1..K4 (24 B per union entry) outside the M-PML and 32 B inside it (K5,
+    K6 too), or, with the value dictionary, 8 B slots (column, tuple id) plus
+    one density per row; batches read 32 B row records per entry.  State:
+    rows outside the M-PML zone move their totals record (Gc 12 + Pa 4
+    floats, read and written once), split-zone rows Gc + Gs + Ps (36 floats),
+    per shot; per-node coefficients 5 floats (interior) or 12 (split zone).
+    Gathers of neighbour records are counted once (their owner's read)."""
     p, j = ctx.union_pattern()
     L = np.diff(p).astype(np.int64)
     mp = ctx.mpml()
@@ -606,7 +608,12 @@ def step_bytes(ctx, prob, S) -> int:
     N = prob.mesh.node_num
     na = int((~zone).sum())
     assert na == ctx.stats()["interior_rows"], (na, ctx.stats()["interior_rows"])
-    mat = int(L[pml].sum()) * 32 + int(L[~pml].sum()) * 24 + 4 * (N // 32 + 2)
+    if S > 1:
+        mat = int(L.sum()) * 32 + 4 * (N + 1)
+    elif ctx.stats()["value_tuples"] > 0:
+        mat = int(L.sum()) * 8 + 4 * (N // 32 + 2) + 4 * N
+    else:
+        mat = int(L[pml].sum()) * 32 + int(L[~pml].sum()) * 24 + 4 * (N // 32 + 2)
     state = (na * (12 + 4) + (N - na) * (12 + 12 + 12)) * 4 * 2 * S
     coef = na * 5 * 4 + (N - na) * 12 * 4
     return int(mat + state + coef)

@@ -100,6 +100,8 @@ typedef struct {
     int blowup_step;           /* first step whose energy bound failed, -1 if none */
     int interior_rows;         /* nodes advanced as totals only (outside the M-PML zone) */
     int pml_rows;              /* rows with a non-zero M-PML profile */
+    int value_tuples;          /* distinct (M / rho, K1..K6) tuples the one-shot step kernels read
+                                  from a dictionary; 0 when they stream full values per entry */
 } sfg_stats;
 
 /* ---------------------------------------------------------- context API */

@@ -52,7 +52,7 @@ class Stats_(C.Structure):
     _fields_ = [("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_ms", C.c_double),
                 ("dof_steps", C.c_longlong), ("union_nnz", C.c_longlong), ("csr_nnz", C.c_longlong * 7),
                 ("kernel_launches", C.c_int), ("rows_per_block", C.c_int), ("blowup_step", C.c_int),
-                ("interior_rows", C.c_int), ("pml_rows", C.c_int)]
+                ("interior_rows", C.c_int), ("pml_rows", C.c_int), ("value_tuples", C.c_int)]
 
 
 _LIB = None

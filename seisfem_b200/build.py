@@ -28,6 +28,7 @@ UNITS = {
     "sfg_seams.cu": ["-fmad=false"],
     "sfg_noalloc.cu": ["-fmad=false"],
     "sfg_fno.cu": [],
+    "sfg_dict.cu": [],
 }
 
 

@@ -164,6 +164,7 @@ void free_problem(DevProblem &P)
     cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
     cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.perm); cudaFree(P.inv);
     cudaFree(P.sellA); cudaFree(P.sellZ); cudaFree(P.sliceA); cudaFree(P.sliceZ); cudaFree(P.upp);
+    cudaFree(P.dict); cudaFree(P.sellAd); cudaFree(P.sellZd); cudaFree(P.rowrho);
     cudaFree(P.recp); cudaFree(P.recA); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ); cudaFree(P.rho0);
     P = DevProblem();
 }
@@ -382,8 +383,34 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         ctx->stats.pml_rows = npml;
     }
     tr.mark("setup: M-PML, coef, classes");
-    CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA, &P.slotsA, st));
-    CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ, &P.slotsZ, st));
+    // The one-shot kernels' matrix slots: (column, tuple id) when the union
+    // entries reduce to a small value dictionary (meshes of congruent
+    // elements), else column + M + K1..K4 (class A) or K1..K6 (class Z).
+    // SFG_NO_VALUE_DICT=1 keeps the full-value slots (to compare the two).
+    {
+        const char *nd = std::getenv("SFG_NO_VALUE_DICT");
+        int *tid = nullptr, zero_id = 0;
+        const int T = (nd && *nd && *nd != '0')
+                          ? 0
+                          : build_value_dict(N, P.up, P.ux, P.union_nnz, d_rho, &tid, &P.dict, &zero_id, st);
+        if (T < 0) return fail(ctx, SFG_ERR_CUDA, "value dictionary");
+        P.dict_n = T;
+        if (T > 0) {
+            CK(build_sell_range_dict(0, P.na, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellAd, &P.sliceA,
+                                     &P.slotsA, st));
+            CK(build_sell_range_dict(P.na, N, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellZd, &P.sliceZ,
+                                     &P.slotsZ, st));
+            CK(build_row_density(N, d_rho, P.perm, &P.rowrho, st));
+            CK(cudaStreamSynchronize(st));
+            cudaFree(tid);
+        } else {
+            CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA,
+                                &P.slotsA, st));
+            CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ,
+                                &P.slotsZ, st));
+        }
+        ctx->stats.value_tuples = T;
+    }
     CK(build_rec_perm(N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, P.upp, &P.recp, st));
     CK(build_coef2(N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, st));
     CK(cudaStreamSynchronize(st));
@@ -582,6 +609,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             Step2 a;
             a.c = c; a.na = P.na; a.S = S;
             a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
+            a.sellAd = P.sellAd; a.sellZd = P.sellZd; a.dict = P.dict; a.dict_n = P.dict_n; a.rowrho = P.rowrho;
             a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.recA = P.recA; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
             a.cmm = b.cmm; a.sig = b.sig;
             a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};

@@ -64,6 +64,11 @@ struct DevProblem {
     int *upp = nullptr;              // permuted union row pointers
     float *recp = nullptr;           // permuted row-major records [union_nnz][8]
     float *recA = nullptr;           // folded class-A records (batches with one model), built on first use
+    // value dictionary of the one-shot kernels (sfg_dict.cu); dict_n = 0 without one
+    int dict_n = 0;
+    float4 *dict = nullptr;          // [2 dict_n]
+    int2 *sellAd = nullptr, *sellZd = nullptr;   // SELL-32 slots (column, tuple id)
+    float *rowrho = nullptr;         // [N] row density, permuted
     float4 *coefA = nullptr;         // [na]
     float *imA = nullptr;            // [na]
     float *coefZ = nullptr;          // [N - na][12]

@@ -221,9 +221,45 @@ __device__ __forceinline__ void gather2_one(const StepCommon &c, int na, const S
 
 // ------------------------------------------------- single-shot kernels
 
-template <bool COMP, int THREADS, int MINB>
+// The (column, tuple id) slots of one row in a SELL-32 slice, read two slots
+// ahead of use: their stream latency then overlaps the gathers of the slots
+// in hand instead of preceding them.
+struct DictSlots {
+    const int2 *p;
+    int left;
+    int2 s0, s1;
+    __device__ __forceinline__ void init(const int2 *base, int n)
+    {
+        p = base;
+        left = n;
+        s0 = n > 0 ? __ldg(p) : make_int2(0, 0);
+        s1 = n > 1 ? __ldg(p + 32) : make_int2(0, 0);
+        p += 64;
+    }
+    __device__ __forceinline__ int2 next()
+    {
+        const int2 r = s0;
+        s0 = s1;
+        s1 = left > 2 ? __ldg(p) : make_int2(0, 0);
+        p += 32;
+        left--;
+        return r;
+    }
+};
+
+// the dictionary's tuples into shared memory (2 float4 each)
+template <int THREADS>
+__device__ __forceinline__ void load_dict(const Step2 &a, float4 *stab)
+{
+    for (int t = threadIdx.x; t < 2 * a.dict_n; t += THREADS) stab[t] = __ldg(a.dict + t);
+    __syncthreads();
+}
+
+template <bool COMP, int THREADS, int MINB, bool DICT>
 __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
 {
+    extern __shared__ float4 stab[];
+    if (DICT) load_dict<THREADS>(a, stab);
     const StepCommon &c = a.c;
     const int i = blockIdx.x * THREADS + threadIdx.x;
     gather2_one(c, a.na, a.in, 1, i);
@@ -236,14 +272,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
 #pragma unroll
         for (int k = 0; k < 8; k++) mL[k] = 0.f;
         const int s0 = __ldg(a.sliceA + slice), s1 = __ldg(a.sliceA + slice + 1);
-        const float *sd = a.sellA + (size_t)s0 * 192 + lane;
-#pragma unroll 2
-        for (int g = s0; g < s1; ++g, sd += 192) {
-            const int j = __float_as_int(ldgf(sd));
-            const float vm = ldgf(sd + 32);
-            float kv[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+        auto acc = [&](int j, float vm, const float *kv) {
             const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
             const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
             const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
@@ -251,6 +280,29 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
             for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
             mL[0] += vm * q0.z; mL[1] += vm * q0.w; mL[2] += vm * q1.x; mL[3] += vm * q1.y;
             mL[4] += vm * q1.z; mL[5] += vm * q1.w; mL[6] += vm * q2.x; mL[7] += vm * q2.y;
+        };
+        if (DICT) {
+            DictSlots ss;
+            ss.init(a.sellAd + (size_t)s0 * 32 + lane, s1 - s0);
+#pragma unroll 2
+            for (int g = s0; g < s1; ++g) {
+                const int2 cv = ss.next();
+                const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
+                const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
+                acc(cv.x, t0.x, kv);
+            }
+            const float rho = __ldg(a.rowrho + i);
+#pragma unroll
+            for (int k = 0; k < 8; k++) mL[k] *= rho;
+        } else {
+            const float *sd = a.sellA + (size_t)s0 * 192 + lane;
+#pragma unroll 2
+            for (int g = s0; g < s1; ++g, sd += 192) {
+                float kv[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                acc(__float_as_int(ldgf(sd)), ldgf(sd + 32), kv);
+            }
         }
         const float4 cf = __ldg(a.coefA + i);
         const float im = __ldg(a.imA + i);
@@ -282,9 +334,11 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
     block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
 }
 
-template <bool COMP, int THREADS, int MINB>
+template <bool COMP, int THREADS, int MINB, bool DICT>
 __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
 {
+    extern __shared__ float4 stab[];
+    if (DICT) load_dict<THREADS>(a, stab);
     const StepCommon &c = a.c;
     const int nz = c.n - a.na;
     const int local = blockIdx.x * THREADS + threadIdx.x;
@@ -304,15 +358,31 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
 #pragma unroll
         for (int k = 0; k < 20; k++) m[k] = 0.f;
         const int s0 = __ldg(a.sliceZ + slice), s1 = __ldg(a.sliceZ + slice + 1);
-        const float *sd = a.sellZ + (size_t)s0 * 256 + lane;
+        const float *sd = DICT ? nullptr : a.sellZ + (size_t)s0 * 256 + lane;
+        DictSlots ss;
+        if (DICT) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
+        // slot g's column, M and K1..K(NK): from the dictionary or the full-value planes
+        auto slot = [&](int &j, float &vm, float *kv, int nk) {
+            if (DICT) {
+                const int2 cv = ss.next();
+                const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
+                j = cv.x;
+                vm = t0.x;
+                kv[0] = t0.y; kv[1] = t0.z; kv[2] = t0.w; kv[3] = t1.x;
+                if (nk == 6) { kv[4] = t1.y; kv[5] = t1.z; }
+            } else {
+                j = __float_as_int(ldgf(sd));
+                vm = ldgf(sd + 32);
+                for (int k = 0; k < nk; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+                sd += 256;
+            }
+        };
         if (full) {
 #pragma unroll 2
-            for (int g = s0; g < s1; ++g, sd += 256) {
-                const int j = __float_as_int(ldgf(sd));
-                const float vm = ldgf(sd + 32);
-                float kv[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+            for (int g = s0; g < s1; ++g) {
+                int j;
+                float vm, kv[6];
+                slot(j, vm, kv, 6);
                 const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
                 const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
                 const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
@@ -334,12 +404,10 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
             }
         } else {
 #pragma unroll 2
-            for (int g = s0; g < s1; ++g, sd += 256) {
-                const int j = __float_as_int(ldgf(sd));
-                const float vm = ldgf(sd + 32);
-                float kv[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
+            for (int g = s0; g < s1; ++g) {
+                int j;
+                float vm, kv[4];
+                slot(j, vm, kv, 4);
                 const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
                 const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
                 const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
@@ -348,6 +416,11 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
                 m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
                 m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
             }
+        }
+        if (DICT) {
+            const float rho = __ldg(a.rowrho + i);
+#pragma unroll
+            for (int k = 0; k < 20; k++) m[k] *= rho;
         }
         double src_u = 0.0, src_w = 0.0;
         if (i == c.src[0]) {
@@ -1206,6 +1279,13 @@ __global__ void row_sums_geo(int n, const int *__restrict__ up, const double *__
 //   0: 128 x 4   1: 128 x 6   2: 256 x 3   3: 256 x 4   4: 64 x 16   5: 512 x 2
 int step2_variants() { return 6; }
 
+cudaError_t launch_range_slice_len(int r0, int r1, const int *d_up, const int *d_perm, int *d_len, cudaStream_t st)
+{
+    const int nsl = (r1 - r0 + 31) / 32;
+    if (nsl) range_slice_len<<<(nsl + 127) / 128, 128, 0, st>>>(r0, r1, d_up, d_perm, d_len);
+    return cudaGetLastError();
+}
+
 #define SFG_SHAPES(KERNEL, COUNT)                                                              \
     do {                                                                                       \
         if ((COUNT) <= 0) return cudaSuccess;                                                  \
@@ -1221,12 +1301,20 @@ int step2_variants() { return 6; }
 #define SFG_ONE(KERNEL, T, M, COUNT)                                                           \
     do {                                                                                       \
         const int blocks = ((COUNT) + (T) - 1) / (T);                                          \
-        if (comp) KERNEL<true, T, M><<<blocks, T, 0, st>>>(a);                                 \
-        else KERNEL<false, T, M><<<blocks, T, 0, st>>>(a);                                     \
+        const size_t smem = sizeof(float4) * 2 * (size_t)a.dict_n;                             \
+        if (a.dict_n > 0) {                                                                    \
+            if (comp) KERNEL<true, T, M, true><<<blocks, T, smem, st>>>(a);                    \
+            else KERNEL<false, T, M, true><<<blocks, T, smem, st>>>(a);                        \
+        } else {                                                                               \
+            if (comp) KERNEL<true, T, M, false><<<blocks, T, 0, st>>>(a);                      \
+            else KERNEL<false, T, M, false><<<blocks, T, 0, st>>>(a);                          \
+        }                                                                                      \
     } while (0)
 
 cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st)
 {
+    if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
+        return cudaErrorInvalidValue;
     // the fused receiver gather runs on the first nrec threads
     SFG_SHAPES(stepA_kernel, std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0));
     return cudaGetLastError();
@@ -1234,6 +1322,8 @@ cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st
 
 cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st)
 {
+    if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
+        return cudaErrorInvalidValue;
     SFG_SHAPES(stepZ_kernel, a.c.n - a.na);
     return cudaGetLastError();
 }

@@ -49,6 +49,15 @@ struct Step2 {
     const int *sliceA;
     const float *sellZ;        // SELL-32 over rows [na, n): planes col, M, K1..K6
     const int *sliceZ;
+    // value dictionary (sfg_dict.cu; dict_n = 0 without one): the one-shot
+    // kernels then read SELL-32 slots (column, tuple id) from sellAd / sellZd
+    // (same slices as sellA / sellZ), the tuple (M / rho_row, K1..K6) from
+    // dict[2 id], dict[2 id + 1], and scale the mass products by rowrho
+    const int2 *sellAd;
+    const int2 *sellZd;
+    const float4 *dict;
+    int dict_n;
+    const float *rowrho;       // [n] row density, permuted numbering
     const int *up;             // row-major union records in the permuted numbering
     const float *rec;          //   [nnz][8]: col, M, K1..K6
     const float *recA;         // class-A rows, one model: [upp[na]][8] col, M and the
@@ -104,6 +113,19 @@ cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long 
 cudaError_t mass_row_sums_geo(int n, const int *d_up, const double *d_ux, const double *d_rho0, double *d_out,
                               cudaStream_t st);
 // class-A / class-Z coefficient arrays from the [n][12] FP32 record
+// value dictionary of the one-shot kernels (sfg_dict.cu): at most kDictMax
+// tuples of (M / rho_row, K1..K6), two float4 each in shared memory
+constexpr int kDictMax = 512;
+// tuples found (0: not applicable, the kernels keep full-value slots; -1 on a
+// CUDA error); d_tid[nnz] the tuple id of every union entry, d_table[2 T]
+int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, const double *d_rho, int **d_tid,
+                     float4 **d_table, int *zero_id, cudaStream_t st);
+cudaError_t build_sell_range_dict(int r0, int r1, const int *d_up, const int *d_uj, const int *d_tid, int zero_id,
+                                  const int *d_perm, const int *d_inv, int2 **d_sell, int **d_slice, long long *slots,
+                                  cudaStream_t st);
+cudaError_t build_row_density(int n, const double *d_rho, const int *d_perm, float **d_out, cudaStream_t st);
+cudaError_t launch_range_slice_len(int r0, int r1, const int *d_up, const int *d_perm, int *d_len, cudaStream_t st);
+
 // the folded class-A records of Step2::recA (c: [4][n] c11 c13 c33 c44, mesh order)
 cudaError_t build_rec_fold(int n, int na, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
                            const int *d_perm, const int *d_inv, const int *d_upp, const double *d_c, float **d_rec,
