@@ -489,11 +489,14 @@ def main():
     traffic = None
     if os.path.exists(TRAFFIC_FILE):
         traffic = read_traffic(TRAFFIC_FILE, f"{args.workload}:{args.precision}")
+    b_ref = reference_layout_bytes(ctx, prob, S)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": "stepA/stepZ fused step (SpMV + RHS + lumped solve + Newmark), both classes",
                 "algorithmic_bytes_per_launch": b_step, "avg_launch_us": round(kms * 1e3, 3),
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback"}
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback",
+                "reference_layout_bytes_per_launch": b_ref,
+                "reference_layout_frac": round(b_ref / (kms * 1e-3) / 1e9 / peak, 4)}
 
     # e2e: public C-ABI call with host buffers (GPU assembly + run + outputs)
     e2e = None
@@ -586,6 +589,17 @@ def read_traffic(path, key):
         if len(f) >= 2 and f[0] == key:
             return int(f[1])
     return None
+
+
+def reference_layout_bytes(ctx, prob, S) -> int:
+    """Bytes per step of the unreduced layout: every union entry with its
+    column and all 7 FP32 values, 64 state floats per node and shot (26
+    fields, 6 compensations, read and written) and 11 coefficient streams
+    per node: Z_u (4 + 7 w) + 4 (N + 1) + N w (64 S + 11), w = 4.  The
+    kernels move fewer bytes (step_bytes); this is the work they replace."""
+    N = prob.mesh.node_num
+    Zu = int(ctx.stats()["union_nnz"])
+    return Zu * (4 + 7 * 4) + 4 * (N + 1) + N * 4 * (64 * S + 11)
 
 
 def step_bytes(ctx, prob, S) -> int:

@@ -44,14 +44,28 @@ __device__ __forceinline__ double entry_value(const double *ux, long long nnz, l
     return k == 0 ? v / rho : v;
 }
 
+// row of union entry e (rows' entries are contiguous and ordered)
+__device__ __forceinline__ int row_of(const int *__restrict__ up, int n, long long e)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (up[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// one thread per union entry (coalesced reads of the value planes)
 __global__ void dict_scale(int n, const int *__restrict__ up, const double *__restrict__ ux, long long nnz,
                            const double *__restrict__ rho, DictScratch *s)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double m[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (r < n)
-        for (long long e = up[r]; e < up[r + 1]; e++)
-            for (int k = 0; k < 7; k++) m[k] = fmax(m[k], fabs(entry_value(ux, nnz, e, k, rho[r])));
+    if (e < nnz) {
+        const double rr = rho[row_of(up, n, e)];
+        for (int k = 0; k < 7; k++) m[k] = fabs(entry_value(ux, nnz, e, k, rr));
+    }
     for (int k = 0; k < 7; k++) {
         double v = m[k];
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -114,17 +128,14 @@ __global__ void dict_insert_zero(DictScratch *s, int *zero_slot)
 __global__ void dict_insert_entries(int n, const int *__restrict__ up, const double *__restrict__ ux, long long nnz,
                                     const double *__restrict__ rho, DictScratch *s, int *__restrict__ slot_of)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    for (long long e = up[r]; e < up[r + 1]; e++) {
-        double v[7];
-        long long q[7];
-        for (int k = 0; k < 7; k++) v[k] = entry_value(ux, nnz, e, k, rho[r]);
-        quantise(s, v, q);
-        const int slot = dict_insert(s, q);
-        if (slot < 0) return;
-        slot_of[e] = slot;
-    }
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const double rr = rho[row_of(up, n, e)];
+    double v[7];
+    long long q[7];
+    for (int k = 0; k < 7; k++) v[k] = entry_value(ux, nnz, e, k, rr);
+    quantise(s, v, q);
+    slot_of[e] = dict_insert(s, q);
 }
 
 // every entry against the tuple its slot recorded (a hash collision between
@@ -132,17 +143,17 @@ __global__ void dict_insert_entries(int n, const int *__restrict__ up, const dou
 __global__ void dict_verify(int n, const int *__restrict__ up, const double *__restrict__ ux, long long nnz,
                             const double *__restrict__ rho, DictScratch *s, const int *__restrict__ slot_of)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    for (long long e = up[r]; e < up[r + 1]; e++) {
-        double v[7];
-        long long q[7];
-        for (int k = 0; k < 7; k++) v[k] = entry_value(ux, nnz, e, k, rho[r]);
-        quantise(s, v, q);
-        const int slot = slot_of[e];
-        for (int k = 0; k < 7; k++)
-            if (s->q[slot][k] != q[k]) s->bad = 1;
-    }
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const double rr = rho[row_of(up, n, e)];
+    double v[7];
+    long long q[7];
+    for (int k = 0; k < 7; k++) v[k] = entry_value(ux, nnz, e, k, rr);
+    quantise(s, v, q);
+    const int slot = slot_of[e];
+    bool ok = slot >= 0;
+    for (int k = 0; k < 7 && ok; k++) ok = s->q[slot][k] == q[k];
+    if (!ok) s->bad = 1;
 }
 
 // one block: compact ids in slot order, and the tuple values
@@ -231,18 +242,18 @@ int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, 
     if (e == cudaSuccess) e = cudaMallocAsync((void **)&slot_of, sizeof(int) * std::max<long long>(nnz, 1), st);
     if (e == cudaSuccess) e = cudaMallocAsync((void **)&zslot, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s, 0, sizeof(DictScratch), st);
-    const int g = (n + 127) / 128;
-    if (e == cudaSuccess && n > 0) {
-        dict_scale<<<g, 128, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s);
+    const unsigned g = (unsigned)((nnz + 255) / 256);
+    if (e == cudaSuccess && n > 0 && nnz > 0) {
+        dict_scale<<<g, 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s);
         dict_insert_zero<<<1, 1, 0, st>>>(s, zslot);
-        dict_insert_entries<<<g, 128, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s, slot_of);
+        dict_insert_entries<<<g, 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s, slot_of);
         e = cudaGetLastError();
     }
     int count = 0, bad = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&count, &s->count, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess && n > 0 && count <= kDictMax) {
-        dict_verify<<<g, 128, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s, slot_of);
+    if (e == cudaSuccess && n > 0 && nnz > 0 && count <= kDictMax) {
+        dict_verify<<<g, 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s, slot_of);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, &s->bad, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
