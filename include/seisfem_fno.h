@@ -65,6 +65,8 @@ int sfg_fno_bias_grad(const void *dy, float *db, int outer, int C, long long inn
 int sfg_fno_swap01(const void *x, void *y, int n0, int n1, long long n2, void *stream);
 /* p[0..n) = 0 (FP32) */
 int sfg_fno_zero(float *p, long long n, void *stream);
+/* p[0..n) *= a (FP32): the 1/ranks of gradients summed over data-parallel ranks */
+int sfg_fno_scale(float *p, long long n, float a, void *stream);
 /* relative-L2 loss of a batch: pred (FP32) vs target (BF16), [B][n] each;
  * loss[b] = |pred-target|^2 / |target|^2 and dpred = 2 (pred-target) /
  * (B |target|^2) (BF16); scratch: 2*B floats */

@@ -721,6 +721,12 @@ __global__ void zero_kernel(float *__restrict__ p, long long n)
     if (t < n) p[t] = 0.f;
 }
 
+__global__ void scale_kernel(float *__restrict__ p, long long n, float a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) p[t] *= a;
+}
+
 // per shot: scratch[2b] = |pred-target|^2, scratch[2b+1] = |target|^2
 __global__ void rel_loss_sums(const float *__restrict__ pred, const __nv_bfloat16 *__restrict__ tgt, float *scratch,
                               long long n)
@@ -918,6 +924,13 @@ int sfg_fno_zero(float *p, long long n, void *stream)
 {
     if (!p || n < 0) return 1;
     if (n) zero_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, n);
+    return launched();
+}
+
+int sfg_fno_scale(float *p, long long n, float a, void *stream)
+{
+    if (!p || n < 0) return 1;
+    if (n) scale_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, n, a);
     return launched();
 }
 

@@ -74,7 +74,8 @@ class Kernels:
                      ("sfg_fno_adam", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float,
                                        C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
                      ("sfg_fno_swap01", [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_void_p]),
-                     ("sfg_fno_zero", [C.c_void_p, C.c_longlong, C.c_void_p])]:
+                     ("sfg_fno_zero", [C.c_void_p, C.c_longlong, C.c_void_p]),
+                     ("sfg_fno_scale", [C.c_void_p, C.c_longlong, C.c_float, C.c_void_p])]:
             getattr(self.L, n).argtypes = a
             getattr(self.L, n).restype = C.c_int
         f.restype = C.c_int
@@ -178,7 +179,12 @@ class FNO:
         f32 = dict(dtype=torch.float32, device=self.dev)
         bf = dict(dtype=torch.bfloat16, device=self.dev)
         self.p = {k: torch.tensor(np.ascontiguousarray(v), **f32) for k, v in params.items()}
-        self.g = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        # all gradients in one flat buffer: one all-reduce per step for data parallelism
+        self.gflat = torch.zeros(sum(v.numel() for v in self.p.values()), **f32)
+        self.g, off = {}, 0
+        for k, v in self.p.items():
+            self.g[k] = self.gflat[off:off + v.numel()].view(v.shape)
+            off += v.numel()
         self.m = {k: torch.zeros_like(v) for k, v in self.p.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.p.items()}
         self.step_count = 0
@@ -311,8 +317,7 @@ class FNO:
         return self.loss
 
     def zero_grad(self):
-        for g in self.g.values():
-            self.K.call("sfg_fno_zero", g, g.numel())
+        self.K.call("sfg_fno_zero", self.gflat, self.gflat.numel())
 
     def backward(self, x):
         """Gradients of all parameters (into self.g, accumulated) from self.dy."""
@@ -360,6 +365,17 @@ class FNO:
                c=(0, 0, self.cin, 1), batch=(B, 1), atomic=True, splits=8)
         K.call("sfg_fno_bias_grad", self.gact, g["lift_b"], B, Cc, P)
 
+    def allreduce_grads(self, group=None):
+        """Data parallelism: average the gradients over the ranks of `group`
+        (torch.distributed: NCCL between GPUs, gloo on CPUs), one all-reduce
+        of the flat gradient buffer.  Every rank's loss is the mean over its
+        own shots, so the average is the gradient of the mean over all."""
+        import torch.distributed as dist
+        world = dist.get_world_size(group)
+        if world > 1:
+            dist.all_reduce(self.gflat, op=dist.ReduceOp.SUM, group=group)
+            self.K.call("sfg_fno_scale", self.gflat, self.gflat.numel(), 1.0 / world)
+
     def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
         self.step_count += 1
         for k, p in self.p.items():
@@ -367,11 +383,15 @@ class FNO:
                         lr, beta1, beta2, eps, self.step_count)
         self.refresh_weights()
 
-    def train_step(self, x, target, lr=1e-3):
+    def train_step(self, x, target, lr=1e-3, group=None):
+        """One Adam step on this batch; with `group` (data parallelism) the
+        gradients are averaged over its ranks first."""
         self.zero_grad()
         self.forward(x)
         self.loss_and_grad(target)
         self.backward(x)
+        if group is not None:
+            self.allreduce_grads(group)
         self.adam(lr)
         return self.loss
 
@@ -438,46 +458,63 @@ def rel_l2(pred: np.ndarray, ref: np.ndarray) -> np.ndarray:
 
 
 class Surrogate:
-    """Training and inference around FNO on one GPU.  Targets are scaled by
-    one global factor (their RMS over the training set)."""
+    """Training and inference around FNO on one GPU (`device`: a CUDA index,
+    or a torch device with `kernels` standing in for the CUDA library).
+    Targets are scaled by one global factor (their RMS over the training
+    set).  With a torch.distributed `group`, fit() trains data-parallel:
+    every rank takes B shots of each global batch of B * ranks and the
+    gradients are averaged before each Adam step."""
 
     def __init__(self, B: int = 16, C_: int = 64, Hp: int = 128, D: int = 128, W: int = 64, T: int = 1000,
-                 device: int = 0, seed: int = 0, stream=None):
+                 device=0, seed: int = 0, stream=None, kernels=None):
         import torch
         self.torch = torch
-        self.dev = torch.device("cuda", device)
+        self.dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
         self.B, self.D, self.W, self.T = B, D, W, T
-        self.net = FNO(init_params(C_, D, T, Hp, seed=seed), B, D, W, T, self.dev, stream=stream)
+        self.net = FNO(init_params(C_, D, T, Hp, seed=seed), B, D, W, T, self.dev, stream=stream, kernels=kernels)
         self.scale = 1.0
 
     def _batch(self, arr, idx, dtype):
         t = self.torch.tensor(arr[idx], dtype=self.torch.float32)
         return t.to(self.dev).to(dtype).contiguous()
 
-    def fit(self, x: np.ndarray, y: np.ndarray, epochs: int, lr: float = 2e-3, seed: int = 0, log=None):
-        """Adam on the relative-L2 loss; returns the mean loss per epoch."""
+    def fit(self, x: np.ndarray, y: np.ndarray, epochs: int, lr: float = 2e-3, seed: int = 0, log=None,
+            group=None):
+        """Adam on the relative-L2 loss; returns the mean loss per epoch (over
+        all ranks' shots).  Every rank passes the same x, y and seed; with
+        `group`, rank r trains on shots [r B, (r + 1) B) of each global batch
+        of the epoch's permutation."""
         torch = self.torch
+        rank, world = 0, 1
+        if group is not None:
+            import torch.distributed as dist
+            rank, world = dist.get_rank(group), dist.get_world_size(group)
         self.scale = float(np.sqrt(np.mean(y.astype(np.float64) ** 2))) or 1.0
-        n = (len(x) // self.B) * self.B
+        G = self.B * world
+        n = (len(x) // G) * G
         xd = torch.tensor(x[:n]).to(self.dev).to(torch.bfloat16)
         yd = (torch.tensor(y[:n]) / self.scale).to(self.dev).to(torch.bfloat16)
         rng = np.random.default_rng(seed)
         hist = []
-        steps = epochs * (n // self.B)
+        steps = epochs * (n // G)
         it = 0
         for ep in range(epochs):
             perm = rng.permutation(n)
-            tot = 0.0
-            for k in range(0, n, self.B):
-                idx = torch.tensor(perm[k:k + self.B], device=self.dev)
+            tot = torch.zeros(1, dtype=torch.float64)
+            for k in range(0, n, G):
+                idx = torch.tensor(perm[k + rank * self.B:k + (rank + 1) * self.B], device=self.dev)
                 xb = xd.index_select(0, idx).contiguous()
                 yb = yd.index_select(0, idx).contiguous()
                 # cosine learning-rate decay
                 lr_t = lr * 0.5 * (1 + math.cos(math.pi * it / max(steps, 1)))
-                loss = self.net.train_step(xb, yb, lr_t)
+                loss = self.net.train_step(xb, yb, lr_t, group=group if world > 1 else None)
                 tot += float(loss.sum().item())
                 it += 1
-            hist.append(tot / n)
+            if world > 1:
+                import torch.distributed as dist
+                tot = tot.to(self.dev) if dist.get_backend(group) == "nccl" else tot
+                dist.all_reduce(tot, group=group)
+            hist.append(float(tot.item()) / n)
             if log:
                 log(f"epoch {ep}: loss {hist[-1]:.4f}")
         return hist

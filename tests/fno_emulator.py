@@ -14,7 +14,9 @@ KC, KD = 16, 32
 
 
 def _view(t, size, stride, off):
-    return torch.as_strided(t.view(-1), size, stride, off)
+    # element offsets count from the tensor's first element (which need not
+    # start its storage: the gradients are views into one flat buffer)
+    return torch.as_strided(t.view(-1), size, stride, t.storage_offset() + off)
 
 
 class EmuKernels:
@@ -99,6 +101,9 @@ class EmuKernels:
 
     def zero(self, p, n):
         p.view(-1)[:n] = 0
+
+    def scale(self, p, n, a):
+        p.view(-1)[:n] *= a
 
     def rel_loss(self, pred, target, loss, dpred, scratch, B, n):
         p = pred.view(B, n)
