@@ -219,6 +219,14 @@ int sfg_abc_mpml(int node_num, int element_num, int element_order, int *element_
                  double *mpml_dxx, double *mpml_dyy, double *mpml_dxx_pyx, double *mpml_dyy_pxy);
 /* sparse_matrix/csr_matvec.c:1 (FP64, same per-row summation order) */
 int sfg_csr_matvec(int Bp_size, int *Bp, int *Bj, double *Bx, double *x, double *y);
+/* source_receiver/node_location.c:1-35 for npts points at once (host code):
+ * out[k] = the LAST node index with |x - px[k]| <= edge_size / 2 and
+ * |y - py[k]| <= edge_size / 2 (the reference's comparison), -1 when none;
+ * a grid of edge_size cells replaces the O(node_num) scan per point.  The
+ * reference's callers (set_source_node.c, set_receiver_node.c) print its
+ * "-1" message themselves when they see -1. */
+int sfg_node_location(int node_num, double edge_size, const double *x, const double *y, int npts,
+                      const double *px, const double *py, int *out);
 
 /* ------------------------------------------------ no-allocation entry point */
 /* No counterpart in the reference.  The M-PML profiles of sfg_abc_mpml

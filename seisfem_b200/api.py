@@ -62,7 +62,7 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_csr_copy", "sfg_lumped_mass_copy", "sfg_lumped_mass_set", "sfg_union_copy", "sfg_mpml_copy", "sfg_run", "sfg_snapshot_rows",
            "sfg_get_stats", "sfg_run_device", "sfg_sync", "sfg_plan_create", "sfg_plan_batches",
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
-           "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec",
+           "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec", "sfg_node_location",
            "sfg_abc_mpml_device_noalloc", "sfg_plan_create_models", "sfg_run_models", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
            "sfg_group_destroy",
            # learned surrogate (include/seisfem_fno.h)
@@ -120,6 +120,24 @@ def lib(path: str = LIBPATH):
     L.sfg_csr_matvec.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
     _LIB = L
     return L
+
+
+def node_location(x, y, edge_size: float, px, py):
+    """Node index per point (sfg_node_location: the last node within
+    edge_size / 2 in both axes, -1 when none)."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    px = np.ascontiguousarray(np.atleast_1d(px), np.float64)
+    py = np.ascontiguousarray(np.atleast_1d(py), np.float64)
+    out = np.empty(len(px), np.int32)
+    f = lib().sfg_node_location
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = f(len(x), float(edge_size), x.ctypes.data, y.ctypes.data, len(px), px.ctypes.data, py.ctypes.data,
+           out.ctypes.data)
+    if rc:
+        raise SfgError(rc, "sfg_node_location")
+    return out
 
 
 def _xy(x, y):

@@ -29,6 +29,7 @@ UNITS = {
     "sfg_noalloc.cu": ["-fmad=false"],
     "sfg_fno.cu": [],
     "sfg_dict.cu": [],
+    "sfg_locate.cu": ["-fmad=false"],
 }
 
 

@@ -210,7 +210,11 @@ def line_points(n, first, last):
 
 
 def locate(mesh, edge_size, pts):
-    out = np.array([node_location(mesh, edge_size, px, py) for px, py in pts], np.int32)
+    """Node indices of points (sfg_node_location: the reference's rule with a
+    grid instead of a scan per point)."""
+    from .api import node_location as locate_all
+    pts = np.asarray(pts, np.float64).reshape(-1, 2)
+    out = locate_all(mesh.x, mesh.y, edge_size, pts[:, 0], pts[:, 1])
     if (out < 0).any():
         raise ValueError("a source or receiver lies outside the mesh")
     return out
