@@ -223,7 +223,9 @@ __device__ __forceinline__ void gather2_one(const StepCommon &c, int na, const S
 
 // The (column, tuple id) slots of one row in a SELL-32 slice, read two slots
 // ahead of use: their stream latency then overlaps the gathers of the slots
-// in hand instead of preceding them.
+// in hand instead of preceding them.  Streams that no other row reads (slots,
+// coefficients, private state) load with the evict-first hint (ld.global.cs),
+// leaving L1 to the neighbour gathers.
 struct DictSlots {
     const int2 *p;
     int left;
@@ -232,15 +234,15 @@ struct DictSlots {
     {
         p = base;
         left = n;
-        s0 = n > 0 ? __ldg(p) : make_int2(0, 0);
-        s1 = n > 1 ? __ldg(p + 32) : make_int2(0, 0);
+        s0 = n > 0 ? __ldcs(p) : make_int2(0, 0);
+        s1 = n > 1 ? __ldcs(p + 32) : make_int2(0, 0);
         p += 64;
     }
     __device__ __forceinline__ int2 next()
     {
         const int2 r = s0;
         s0 = s1;
-        s1 = left > 2 ? __ldg(p) : make_int2(0, 0);
+        s1 = left > 2 ? __ldcs(p) : make_int2(0, 0);
         p += 32;
         left--;
         return r;
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
                 const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
                 acc(cv.x, t0.x, kv);
             }
-            const float rho = __ldg(a.rowrho + i);
+            const float rho = __ldcs(a.rowrho + i);
 #pragma unroll
             for (int k = 0; k < 8; k++) mL[k] *= rho;
         } else {
@@ -304,8 +306,8 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
                 acc(__float_as_int(ldgf(sd)), ldgf(sd + 32), kv);
             }
         }
-        const float4 cf = __ldg(a.coefA + i);
-        const float im = __ldg(a.imA + i);
+        const float4 cf = __ldcs(a.coefA + i);
+        const float im = __ldcs(a.imA + i);
         double src_u = 0.0, src_w = 0.0;
         if (i == c.src[0]) {
             const double ps = c.amp[c.it];
@@ -319,7 +321,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
             const float4 v = __ldg(gi + k);
             g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
         }
-        const float4 pv = __ldg(reinterpret_cast<const float4 *>(a.in.Pa) + i);
+        const float4 pv = __ldcs(reinterpret_cast<const float4 *>(a.in.Pa) + i);
         p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
         float uu, ww, su, sw;
         stiff_sums(kU, kW, cf, su, sw);
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
     if (local < nz) {
         const float4 *cf = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
-        c0 = __ldg(cf); c1 = __ldg(cf + 1); c2 = __ldg(cf + 2);
+        c0 = __ldcs(cf); c1 = __ldcs(cf + 1); c2 = __ldcs(cf + 2);
     }
     const bool full = __any_sync(0xffffffffu, local < nz && is_pml_row(c1));
     double eu = 0.0, ew = 0.0;
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
             }
         }
         if (DICT) {
-            const float rho = __ldg(a.rowrho + i);
+            const float rho = __ldcs(a.rowrho + i);
 #pragma unroll
             for (int k = 0; k < 20; k++) m[k] *= rho;
         }
@@ -433,7 +435,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
         const float4 *pi = reinterpret_cast<const float4 *>(a.in.Ps + (size_t)local * PS);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const float4 v = __ldg(si + k), w = __ldg(pi + k);
+            const float4 v = __ldg(si + k), w = __ldcs(pi + k);
             gs[4 * k] = v.x; gs[4 * k + 1] = v.y; gs[4 * k + 2] = v.z; gs[4 * k + 3] = v.w;
             ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
         }
