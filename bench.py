@@ -196,14 +196,14 @@ def run_surrogate(args):
     B = sg.B
     xb = torch.tensor(xte[:B]).to(dev).to(torch.bfloat16).contiguous()
     for _ in range(max(3, args.warmup)):
-        sg.net.forward(xb)
+        sg.net.forward(xb, keep_pre=False)
     torch.cuda.synchronize(dev)
     f1 = K.flops
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = max(1, args.steps) * (nte // B)
     e0.record()
     for _ in range(reps):
-        sg.net.forward(xb)
+        sg.net.forward(xb, keep_pre=False)
     e1.record()
     torch.cuda.synchronize(dev)
     fwd_ms = e0.elapsed_time(e1) / reps
@@ -340,7 +340,7 @@ def run_gemm_engines(args):
         B = torch.randn(bsz, device=dev).to(torch.bfloat16)
         C = torch.empty(csz, device=dev, dtype=cdt)
         row = {"gemm": name, "flops": 2 * M * N * Kd * batch[0] * batch[1]}
-        for eng, key in ((1, "mma_sync_us"), (2, "tcgen05_us")):
+        for eng, key in ((1, "mma_sync_us"), (3, "tcgen05_cp_async_us"), (2, "tcgen05_tma_us")):
             for _ in range(max(3, args.warmup)):
                 K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng, **epi)
             torch.cuda.synchronize(dev)
@@ -364,7 +364,8 @@ def run_gemm_engines(args):
     row = {"network": "FNO width 64, 16 shots, 128 x 64 grid, 1000 samples"}
     for eng, key in ((1, "mma_sync"), (0, "auto")):
         net.K.engine = eng
-        for nm, fn in (("forward", lambda: net.forward(x)), ("train_step", lambda: net.train_step(x, tgt, 1e-4))):
+        for nm, fn in (("forward", lambda: net.forward(x, keep_pre=False)),
+                       ("train_step", lambda: net.train_step(x, tgt, 1e-4))):
             for _ in range(max(3, args.warmup)):
                 fn()
             torch.cuda.synchronize(dev)

@@ -37,7 +37,9 @@ typedef struct {
     int M, N, K, batch1, batch2, splits;
     float alpha, beta;
     int c_bf16, gelu, bias_on_m, atomic;
-    int engine;                    /* 0: automatic, 1: mma.sync tiles, 2: tcgen05 with TMEM accumulators */
+    int engine;                    /* 0: automatic, 1: mma.sync tiles, 2: tcgen05 with TMEM accumulators
+                                      (operand tiles by TMA where the strides allow, else cp.async),
+                                      3: tcgen05 with cp.async operand tiles */
 } sfg_gemm_desc;
 
 int sfg_fno_gemm(const sfg_gemm_desc *d, void *stream);

@@ -9,6 +9,7 @@
 // recombination of the DFT stages, GELU and its derivative, casts, bias
 // gradients, the relative-L2 loss, Adam).  The host (seisfem_b200/surrogate.py)
 // only sequences these calls on device buffers.
+#include <cuda.h>          // CUtensorMap and its enums (the encoder is looked up at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -36,6 +37,7 @@ constexpr int PITCH = BK + 8;
 struct GemmArgs {
     sfg_gemm_desc d;
     int amode, bmode;          // 0: k contiguous (16-B vectors), 1: m/n contiguous (vectors), 2: scalar
+    int tz1a, tz2a, tz1b, tz2b;   // TMA engine: the operand's tensor map follows batch index 1 / 2
 };
 
 __device__ __forceinline__ float gelu_f(float x)
@@ -377,6 +379,120 @@ __device__ __forceinline__ void tc_fill(uint32_t s, const __nv_bfloat16 *p, long
     }
 }
 
+// The accumulator of a 128 x BN tile (TMEM lanes = rows) through shared
+// memory to C: 8 warps read TMEM (warp w: lanes 32 (w % 4).., half the
+// columns each) into an FP32 tile, free the TMEM columns, then every thread
+// writes 8-column vectors with the descriptor's epilogue (alpha, beta Cin,
+// bias, pre-activation, GELU) or atomic accumulation.  `have` = the
+// accumulator is complete (some K tiles, no wait gave up).
+template <int BN>
+__device__ __forceinline__ void tc_epilogue(const sfg_gemm_desc &d, uint32_t tmem, float *tile, int m0, int n0,
+                                            long long cz, bool have)
+{
+    constexpr int BM = 128;
+    constexpr int TP = BN + 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (have) {
+        const int row = (warp & 3) * 32 + lane;
+        const int cb = (warp >> 2) * (BN / 2);
+#pragma unroll 1
+        for (int c0 = cb; c0 < cb + BN / 2; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float4 *t4 = reinterpret_cast<float4 *>(tile + row * TP + c0);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                t4[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                    __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    if (!have) return;
+    // C in vectors of 8 columns: consecutive threads take consecutive vectors
+    // of a row
+    constexpr int VPR = BN / 8;
+    for (int v = threadIdx.x; v < BM * VPR; v += 256) {
+        const int rr = v / VPR, cc = (v % VPR) * 8;
+        const int m = m0 + rr, nbase = n0 + cc;
+        if (m >= d.M || nbase >= d.N) continue;
+        const int cnt = min(8, d.N - nbase);
+        const float4 *t4 = reinterpret_cast<const float4 *>(tile + rr * TP + cc);
+        const float4 q0 = t4[0], q1 = t4[1];
+        float x[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        const long long o = cz + m * d.scm + (long long)nbase * d.scn;
+        if (d.atomic) {
+            for (int j = 0; j < cnt; j++) atomicAdd(static_cast<float *>(d.C) + o + j * d.scn, d.alpha * x[j]);
+            continue;
+        }
+        const bool vec = cnt == 8 && d.scn == 1 && (o & 7) == 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) x[j] *= d.alpha;
+        if (d.Cin) {
+            if (vec && (reinterpret_cast<uintptr_t>(d.Cin) & 15) == 0) {
+                const float4 a0 = *reinterpret_cast<const float4 *>(d.Cin + o);
+                const float4 a1 = *reinterpret_cast<const float4 *>(d.Cin + o + 4);
+                const float cin[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[j] += d.beta * cin[j];
+            } else {
+                for (int j = 0; j < cnt; j++) x[j] += d.beta * d.Cin[o + j * d.scn];
+            }
+        }
+        if (d.bias) {
+            if (d.bias_on_m) {
+                const float b = d.bias[m];
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[j] += b;
+            } else {
+                for (int j = 0; j < cnt; j++) x[j] += d.bias[nbase + j];
+            }
+        }
+        if (d.pre) {
+            __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(d.pre) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.pre) & 15) == 0) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
+                *reinterpret_cast<uint4 *>(pp) = *reinterpret_cast<const uint4 *>(h);
+            } else {
+                for (int j = 0; j < cnt; j++) pp[j * d.scn] = __float2bfloat16(x[j]);
+            }
+        }
+        if (d.gelu) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = gelu_f(x[j]);
+        }
+        if (d.c_bf16) {
+            __nv_bfloat16 *cp = static_cast<__nv_bfloat16 *>(d.C) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
+                *reinterpret_cast<uint4 *>(cp) = *reinterpret_cast<const uint4 *>(h);
+            } else {
+                for (int j = 0; j < cnt; j++) cp[j * d.scn] = __float2bfloat16(x[j]);
+            }
+        } else {
+            float *cp = static_cast<float *>(d.C) + o;
+            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+                *reinterpret_cast<float4 *>(cp) = make_float4(x[0], x[1], x[2], x[3]);
+                *reinterpret_cast<float4 *>(cp + 4) = make_float4(x[4], x[5], x[6], x[7]);
+            } else {
+                for (int j = 0; j < cnt; j++) cp[j * d.scn] = x[j];
+            }
+        }
+    }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(256) gemm_tc_kernel(const GemmArgs g)
 {
@@ -473,106 +589,154 @@ __global__ void __launch_bounds__(256) gemm_tc_kernel(const GemmArgs g)
     if (!ok && lane == 0) atomicAdd(&g_tc_timeouts, 1);
     // all threads agree on whether the accumulator is complete
     const int good = __syncthreads_and(ok ? 1 : 0);
-    float *tile = reinterpret_cast<float *>(smem);
-    if (nt > 0 && good) {
-        const int row = (warp & 3) * 32 + lane;
-        const int cb = (warp >> 2) * (BN / 2);
-#pragma unroll 1
-        for (int c0 = cb; c0 < cb + BN / 2; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            float4 *t4 = reinterpret_cast<float4 *>(tile + row * TP + c0);
+    tc_epilogue<BN>(d, tmem, reinterpret_cast<float *>(smem), m0, n0, cz, nt > 0 && good);
+}
+
+// ------------------------------------------------ tcgen05 GEMM with TMA
+//
+// The same tile and epilogue, with the operand tiles brought in by the
+// Tensor Memory Accelerator: one thread issues, per stage, the bulk tensor
+// copies of the A and B tiles (cp.async.bulk.tensor, completion counted in
+// bytes on the stage's mbarrier) and then the stage's four
+// tcgen05.mma.kind::f16, committed to a second mbarrier that frees the stage
+// for the copies TSTG tiles later.  The tiles land in shared memory in the
+// canonical 128-byte-swizzled layouts: K-major for a k-contiguous operand
+// (one box of 64 k x R rows, rows 128 B apart, 8-row groups 1024 B apart),
+// MN-major for an m/n-contiguous one (R / 64 boxes of 64 m/n x 64 k, k rows
+// 128 B apart, 8-row groups 1024 B apart, 64-element blocks 8 KB apart).
+// The copies zero-fill outside the matrix, so ragged M, N and K need no
+// special case.  The other 255 threads wait for the last commit and run the
+// epilogue.  Every wait is bounded (g_tc_timeouts).
+
+// shared-memory descriptor with the 128-byte swizzle (layout type 2)
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return umma_desc(saddr, lbo, sbo) | (2ull << 61);
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+// the k-tile at k0 of rows [r0, r0 + R) of one operand (MODE 0: k
+// contiguous, MODE 1: rows contiguous) into the stage at dst
+template <int MODE, int R>
+__device__ __forceinline__ void tma_operand(uint32_t dst, const CUtensorMap *map, int k0, int r0, int z2, int z1,
+                                            uint32_t bar)
+{
+    if (MODE == 0) {
+        tma_load_4d(dst, map, k0, r0, z2, z1, bar);
+    } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++)
-                t4[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
-                                    __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+        for (int j = 0; j < R / 64; j++) tma_load_4d(dst + j * 8192, map, r0 + 64 * j, k0, z2, z1, bar);
+    }
+}
+
+template <int BN, int AMODE, int BMODE>
+__global__ void __launch_bounds__(256) gemm_tma_kernel(const __grid_constant__ GemmArgs g,
+                                                        const __grid_constant__ CUtensorMap ta,
+                                                        const __grid_constant__ CUtensorMap tb)
+{
+    constexpr int BM = 128;
+    constexpr int ASTG = BM * TBK * 2, BSTG = BN * TBK * 2;     // bytes of one stage
+    static_assert(BM * (BN + 4) * 4 <= TSTG * (ASTG + BSTG), "epilogue tile must fit the stages");
+    static_assert(BMODE == 0 || BN % 64 == 0, "MN-major tiles come in 64-element blocks");
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[TSTG], empty[TSTG];
+    __shared__ uint32_t tmem_base;
+    const sfg_gemm_desc &d = g.d;
+    const int nb = d.batch1 * d.batch2;
+    const int z = blockIdx.z % nb, split = blockIdx.z / nb;
+    const int z1 = z / d.batch2, z2 = z % d.batch2;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ktiles = (d.K + TBK - 1) / TBK;
+    const int per = (ktiles + d.splits - 1) / d.splits;
+    const int kt0 = split * per, kt1 = min(ktiles, kt0 + per);
+    const int nt = max(0, kt1 - kt0);
+    const long long cz = z1 * d.sc1 + z2 * d.sc2;
+    const int warp = threadIdx.x >> 5;
+    // stages on a 1024-byte boundary (the swizzle atom); the launch adds the slack
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t sA = (raw + 1023u) & ~1023u, sB = sA + TSTG * ASTG;
+    unsigned char *stages = smem_raw + (sA - raw);
+    const int az1 = g.tz1a ? z1 : 0, az2 = g.tz2a ? z2 : 0, bz1 = g.tz1b ? z1 : 0, bz2 = g.tz2b ? z2 : 0;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)AMODE << 15) |
+                               ((uint32_t)BMODE << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    // K = 16 steps: 32 bytes along a K-major row, two 8-row groups of an MN-major tile
+    constexpr uint32_t A_STEP = AMODE ? 2048 : 32, B_STEP = BMODE ? 2048 : 32;
+    constexpr uint32_t A_LBO = AMODE ? 8192 : 16, B_LBO = BMODE ? 8192 : 16;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < TSTG; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
         }
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
-    if (nt == 0 || !good) return;
-    // C in vectors of 8 columns: consecutive threads take consecutive vectors
-    // of a row
-    constexpr int VPR = BN / 8;
-    for (int v = threadIdx.x; v < BM * VPR; v += 256) {
-        const int rr = v / VPR, cc = (v % VPR) * 8;
-        const int m = m0 + rr, nbase = n0 + cc;
-        if (m >= d.M || nbase >= d.N) continue;
-        const int cnt = min(8, d.N - nbase);
-        const float4 *t4 = reinterpret_cast<const float4 *>(tile + rr * TP + cc);
-        const float4 q0 = t4[0], q1 = t4[1];
-        float x[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-        const long long o = cz + m * d.scm + (long long)nbase * d.scn;
-        if (d.atomic) {
-            for (int j = 0; j < cnt; j++) atomicAdd(static_cast<float *>(d.C) + o + j * d.scn, d.alpha * x[j]);
-            continue;
-        }
-        const bool vec = cnt == 8 && d.scn == 1 && (o & 7) == 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        auto issue = [&](int s, int t) {
+            const uint32_t bar = smem_u32(&full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(ASTG + BSTG)
+                         : "memory");
+            const int k0 = (kt0 + t) * TBK;
+            tma_operand<AMODE, BM>(sA + s * ASTG, &ta, k0, m0, az2, az1, bar);
+            tma_operand<BMODE, BN>(sB + s * BSTG, &tb, k0, n0, bz2, bz1, bar);
+        };
+        int issued = 0, used = 0;
+        for (; issued < min(TSTG, nt); issued++) issue(issued, issued);
+        for (int it = 0; it < nt; it++) {
+            const int st = it % TSTG;
+            if (!mbar_wait(smem_u32(&full[st]), (it / TSTG) & 1)) { ok = false; break; }
+            used = it + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = sA + st * ASTG, b0 = sB + st * BSTG;
 #pragma unroll
-        for (int j = 0; j < 8; j++) x[j] *= d.alpha;
-        if (d.Cin) {
-            if (vec && (reinterpret_cast<uintptr_t>(d.Cin) & 15) == 0) {
-                const float4 a0 = *reinterpret_cast<const float4 *>(d.Cin + o);
-                const float4 a1 = *reinterpret_cast<const float4 *>(d.Cin + o + 4);
-                const float cin[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-#pragma unroll
-                for (int j = 0; j < 8; j++) x[j] += d.beta * cin[j];
-            } else {
-                for (int j = 0; j < cnt; j++) x[j] += d.beta * d.Cin[o + j * d.scn];
+            for (int ks = 0; ks < TBK / 16; ks++) {
+                const uint64_t da = umma_desc_sw128(a0 + ks * A_STEP, A_LBO, 1024);
+                const uint64_t db = umma_desc_sw128(b0 + ks * B_STEP, B_LBO, 1024);
+                const uint32_t acc = (it > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&empty[st])));
+            // refill the stage the previous tile used, once its MMAs have read it
+            const int prev = it - 1;
+            if (prev >= 0 && prev + TSTG < nt) {
+                if (!mbar_wait(smem_u32(&empty[prev % TSTG]), (prev / TSTG) & 1)) { ok = false; break; }
+                issue(prev % TSTG, prev + TSTG);
+                issued++;
             }
         }
-        if (d.bias) {
-            if (d.bias_on_m) {
-                const float b = d.bias[m];
-#pragma unroll
-                for (int j = 0; j < 8; j++) x[j] += b;
-            } else {
-                for (int j = 0; j < cnt; j++) x[j] += d.bias[nbase + j];
-            }
-        }
-        if (d.pre) {
-            __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(d.pre) + o;
-            if (vec && (reinterpret_cast<uintptr_t>(d.pre) & 15) == 0) {
-                __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
-                *reinterpret_cast<uint4 *>(pp) = *reinterpret_cast<const uint4 *>(h);
-            } else {
-                for (int j = 0; j < cnt; j++) pp[j * d.scn] = __float2bfloat16(x[j]);
-            }
-        }
-        if (d.gelu) {
-#pragma unroll
-            for (int j = 0; j < 8; j++) x[j] = gelu_f(x[j]);
-        }
-        if (d.c_bf16) {
-            __nv_bfloat16 *cp = static_cast<__nv_bfloat16 *>(d.C) + o;
-            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
-                __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) h[j] = __float2bfloat16(x[j]);
-                *reinterpret_cast<uint4 *>(cp) = *reinterpret_cast<const uint4 *>(h);
-            } else {
-                for (int j = 0; j < cnt; j++) cp[j * d.scn] = __float2bfloat16(x[j]);
-            }
-        } else {
-            float *cp = static_cast<float *>(d.C) + o;
-            if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
-                *reinterpret_cast<float4 *>(cp) = make_float4(x[0], x[1], x[2], x[3]);
-                *reinterpret_cast<float4 *>(cp + 4) = make_float4(x[4], x[5], x[6], x[7]);
-            } else {
-                for (int j = 0; j < cnt; j++) cp[j * d.scn] = x[j];
-            }
-        }
+        // after a wait gave up: let the copies already issued land before the block exits
+        for (int t = used; !ok && t < issued; t++) mbar_wait(smem_u32(&full[t % TSTG]), (t / TSTG) & 1);
     }
+    if (nt > 0) ok = mbar_wait(smem_u32(&empty[(nt - 1) % TSTG]), ((nt - 1) / TSTG) & 1) && ok;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok && (threadIdx.x & 31) == 0) atomicAdd(&g_tc_timeouts, 1);
+    const int good = __syncthreads_and(ok ? 1 : 0);
+    tc_epilogue<BN>(d, tmem, reinterpret_cast<float *>(stages), m0, n0, cz, nt > 0 && good);
 }
 
 // Vector loads need 16-byte aligned groups of 8 elements: the base pointer
@@ -787,6 +951,96 @@ int launched() { return cudaGetLastError() == cudaSuccess ? 0 : 2; }
 // full 128-row tile, 32 columns and 64-deep K; mma.sync tiles otherwise.
 bool tc_auto(const sfg_gemm_desc &d) { return d.M >= 128 && d.N >= 32 && d.K >= 64; }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver the runtime loaded (no link-time
+// dependency on libcuda); null when unavailable
+EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of one BF16 operand of `rows` x K (element (r, k) at
+// base + r * s_row + k * s_k, batches at s1 / s2), boxes as gemm_tma_kernel
+// loads them with the 128-byte swizzle: mode 0 (s_k = 1) dims {K, rows, b2,
+// b1}, box {64, R}; mode 1 (s_row = 1) dims {rows, K, b2, b1}, box {64, 64}.
+// A batch dimension with stride 0 (an operand shared by every batch) or a
+// single batch is kept at extent 1 and coordinate 0 (t1 / t2 = 0).
+bool operand_map(CUtensorMap *map, const void *base, int mode, int rows, int K, long long s_row, long long s_k,
+                 long long s1, long long s2, int b1, int b2, int R, int &t1, int &t2)
+{
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    cuuint64_t dim[4], str[3];
+    cuuint32_t box[4], es[4] = {1, 1, 1, 1};
+    if (mode == 0) {
+        dim[0] = (cuuint64_t)K; dim[1] = (cuuint64_t)rows; str[0] = (cuuint64_t)s_row * 2;
+        box[0] = 64; box[1] = (cuuint32_t)R;
+    } else {
+        dim[0] = (cuuint64_t)rows; dim[1] = (cuuint64_t)K; str[0] = (cuuint64_t)s_k * 2;
+        box[0] = 64; box[1] = 64;
+    }
+    auto up16 = [](cuuint64_t v) { return (v + 15) / 16 * 16; };
+    t2 = (b2 > 1 && s2 != 0) ? 1 : 0;
+    t1 = (b1 > 1 && s1 != 0) ? 1 : 0;
+    dim[2] = t2 ? (cuuint64_t)b2 : 1;
+    str[1] = t2 ? (cuuint64_t)s2 * 2 : up16(str[0] * dim[1]);
+    dim[3] = t1 ? (cuuint64_t)b1 : 1;
+    str[2] = t1 ? (cuuint64_t)s1 * 2 : up16(str[1] * dim[2]);
+    box[2] = box[3] = 1;
+    for (int i = 0; i < 3; i++)
+        if (str[i] == 0 || str[i] % 16 != 0 || str[i] >= (1ull << 40)) return false;
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dim, str, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int AM, int BMD>
+int launch_tma_shape(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb, long long nb, cudaStream_t st)
+{
+    const sfg_gemm_desc &d = g.d;
+    const int smem = TSTG * (128 + BN) * TBK * 2 + 1024;
+    if (cudaFuncSetAttribute(gemm_tma_kernel<BN, AM, BMD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return 2;
+    dim3 grid((d.N + BN - 1) / BN, (d.M + 127) / 128, (unsigned)nb);
+    if (grid.y > 65535) return 1;
+    gemm_tma_kernel<BN, AM, BMD><<<grid, 256, smem, st>>>(g, ta, tb);
+    return launched();
+}
+
+// tcgen05 with TMA operand tiles; -1 when the operands do not allow it
+// (the caller then takes the cp.async engine)
+template <int BN>
+int launch_tma(GemmArgs g, long long nb, cudaStream_t st)
+{
+    const sfg_gemm_desc &d = g.d;
+    if (g.bmode == 1 && BN % 64 != 0) return -1;
+    CUtensorMap ta, tb;
+    if (!operand_map(&ta, d.A, g.amode, d.M, d.K, d.sam, d.sak, d.sa1, d.sa2, d.batch1, d.batch2, 128, g.tz1a,
+                     g.tz2a) ||
+        !operand_map(&tb, d.B, g.bmode, d.N, d.K, d.sbn, d.sbk, d.sb1, d.sb2, d.batch1, d.batch2, BN, g.tz1b,
+                     g.tz2b))
+        return -1;
+    if (g.amode == 0 && g.bmode == 0) return launch_tma_shape<BN, 0, 0>(g, ta, tb, nb, st);
+    if (g.amode == 1 && g.bmode == 0) return launch_tma_shape<BN, 1, 0>(g, ta, tb, nb, st);
+    if constexpr (BN % 64 == 0) {
+        if (g.amode == 0) return launch_tma_shape<BN, 0, 1>(g, ta, tb, nb, st);
+        return launch_tma_shape<BN, 1, 1>(g, ta, tb, nb, st);
+    }
+    return -1;
+}
+
 template <int BN>
 int launch_tc(const GemmArgs &g, long long nb, cudaStream_t st)
 {
@@ -826,11 +1080,17 @@ int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
     if (nb > 65535) return 1;
     GemmArgs g;
     g.d = d;
+    g.tz1a = g.tz2a = g.tz1b = g.tz2b = 0;
     g.amode = pick_mode(d.sam, d.sak, d.sa1, d.sa2, d.A);
     g.bmode = pick_mode(d.sbn, d.sbk, d.sb1, d.sb2, d.B);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool tc = d.engine == 2 || (d.engine == 0 && tc_auto(d));
-    if (tc && d.N >= 32 && g.amode != 2 && g.bmode != 2) {   // cp.async needs 16-byte groups
+    const bool tc = d.engine == 2 || d.engine == 3 || (d.engine == 0 && tc_auto(d));
+    if (tc && d.N >= 32 && g.amode != 2 && g.bmode != 2) {   // copies move 16-byte groups
+        if (d.engine != 3) {   // TMA operand tiles where the operands allow them
+            const int r = d.N >= 128 ? launch_tma<128>(g, nb, st) : d.N >= 64 ? launch_tma<64>(g, nb, st)
+                                                                              : launch_tma<32>(g, nb, st);
+            if (r >= 0) return r;
+        }
         if (d.N >= 128) return launch_tc<128>(g, nb, st);
         if (d.N >= 64) return launch_tc<64>(g, nb, st);
         return launch_tc<32>(g, nb, st);

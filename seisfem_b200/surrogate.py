@@ -59,7 +59,9 @@ class Kernels:
         self.stream = stream
         self.launches = 0
         self.flops = 0          # 2 M N K per problem of every GEMM issued
-        self.engine = 0         # GEMM engine: 0 automatic (tcgen05 for M >= 128, N >= 32, K >= 64), 1 mma.sync, 2 tcgen05
+        # GEMM engine: 0 automatic (tcgen05 for M >= 128, N >= 32, K >= 64), 1 mma.sync,
+        # 2 tcgen05 (TMA operand tiles where the strides allow), 3 tcgen05 with cp.async tiles
+        self.engine = 0
         f = self.L.sfg_fno_gemm
         f.argtypes = [C.POINTER(GemmDesc), C.c_void_p]
         for n, a in [("sfg_fno_dft_combine", [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
@@ -89,7 +91,8 @@ class Kernels:
              aoff=0, boff=0, coff=0, Cin=None, pre=None, bias=None, bias_on_m=False, gelu=False,
              alpha=1.0, beta=1.0, atomic=False, splits=1, engine=None):
         """Strides are (level-1 batch, level-2 batch, row, col) in elements;
-        engine 0 automatic, 1 mma.sync, 2 tcgen05 (default: self.engine)."""
+        engine 0 automatic, 1 mma.sync, 2 tcgen05 (TMA tiles), 3 tcgen05 (cp.async tiles);
+        default: self.engine."""
         d = GemmDesc()
         d.A, d.B, d.C = _ptr(A, aoff), _ptr(B, boff), _ptr(Cout, coff)
         d.Cin = _ptr(Cin, coff) if Cin is not None else None
@@ -287,8 +290,10 @@ class FNO:
         K.gemm(self.dY1, self.Fw, ds, BCD, W, 32, a=(0, 0, 32, 1), b=(0, 0, 1, 32), c=(0, 0, W, 1))
 
     # ------------------------------------------------------------ network
-    def forward(self, x):
-        """x: BF16 [B][cin][D][W] on the device -> self.y (FP32 [B][2][W][T])."""
+    def forward(self, x, keep_pre: bool = True):
+        """x: BF16 [B][cin][D][W] on the device -> self.y (FP32 [B][2][W][T]).
+        keep_pre=False (inference) skips storing the pre-activations that
+        only backward() reads."""
         K, B, Cc, D, W, T, Hp = self.K, self.B, self.C, self.D, self.W, self.T, self.Hp
         P = D * W
         K.gemm(self.bf["lift_w"], x, self.v_act[0], Cc, P, self.cin, a=(0, 0, self.cin, 1),
@@ -298,12 +303,14 @@ class FNO:
             last = l == self.Lyr - 1
             K.gemm(self.bf[f"cw{l}"], self.v_act[l], self.v_act[l + 1], Cc, P, Cc, a=(0, 0, Cc, 1),
                    b=(Cc * P, 0, P, 1), c=(Cc * P, 0, P, 1), batch=(B, 1), Cin=self.s,
-                   bias=self.p[f"cb{l}"], bias_on_m=True, pre=None if last else self.pre[l], gelu=not last)
+                   bias=self.p[f"cb{l}"], bias_on_m=True, pre=None if (last or not keep_pre) else self.pre[l],
+                   gelu=not last)
         # depth -> time: u[z][w][t] = sum_d v4[z][d][w] Wt[d][t] + bt[t]
         K.gemm(self.v_act[self.Lyr], self.bf["time_w"], self.u, W, T, D, a=(D * W, 0, 1, W), b=(0, 0, T, 1),
                c=(W * T, 0, T, 1), batch=(B * Cc, 1), bias=self.p["time_b"])
         K.gemm(self.u, self.bf["p1_w"], self.h1, W * T, Hp, Cc, a=(Cc * W * T, 0, 1, W * T), b=(0, 0, Hp, 1),
-               c=(W * T * Hp, 0, Hp, 1), batch=(B, 1), bias=self.p["p1_b"], pre=self.hpre, gelu=True)
+               c=(W * T * Hp, 0, Hp, 1), batch=(B, 1), bias=self.p["p1_b"], pre=self.hpre if keep_pre else None,
+               gelu=True)
         K.gemm(self.h1, self.bf["p2_w"], self.y, W * T, 2, Hp, a=(W * T * Hp, 0, Hp, 1), b=(0, 0, 2, 1),
                c=(2 * W * T, 0, 1, W * T), batch=(B, 1), bias=self.p["p2_b"])
         return self.y
@@ -527,6 +534,6 @@ class Surrogate:
             xb = np.zeros((self.B, 4, self.D, self.W), np.float32)
             m = min(self.B, len(x) - k)
             xb[:m] = x[k:k + m]
-            y = self.net.forward(torch.tensor(xb).to(self.dev).to(torch.bfloat16).contiguous())
+            y = self.net.forward(torch.tensor(xb).to(self.dev).to(torch.bfloat16).contiguous(), keep_pre=False)
             out[k:k + m] = y[:m].float().cpu().numpy().reshape(m, 2, self.W, self.T) * self.scale
         return out

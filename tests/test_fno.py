@@ -79,7 +79,7 @@ def test_host_sequencing_matches_oracle_on_cpu():
 # ------------------------------------------------------------------ GPU
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("engine", [1, 2])
+@pytest.mark.parametrize("engine", [1, 2, 3])
 @pytest.mark.parametrize("layout", ["nn", "tn", "nt", "strided"])
 def test_gemm_matches_fp32(layout, engine):
     """Every epilogue term (alpha, beta Cin, bias, stored pre-activation,
@@ -126,8 +126,9 @@ def test_gemm_matches_fp32(layout, engine):
 @pytest.mark.parametrize("N,Kd,layout", [(32, 64, "nn"), (64, 100, "tn"), (128, 300, "nt"), (200, 128, "nn"),
                                          (136, 72, "tt"), (40, 200, "tt"), (96, 64, "strided")])
 def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
-    """The tcgen05/TMEM engine against the mma.sync engine on the same
-    descriptor (both accumulate in FP32), incl. ragged M, N, K and every
+    """The tcgen05/TMEM engine -- operand tiles by TMA (engine 2) and by
+    cp.async (engine 3) -- against the mma.sync engine on the same
+    descriptor (all accumulate in FP32), incl. ragged M, N, K and every
     load path; no bounded wait may give up."""
     import ctypes
     import torch
@@ -154,7 +155,7 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
         Ad2[::3] = Ad.reshape(-1)
         Ad, sa = Ad2, tuple(3 * v for v in sa)
     outs = []
-    for eng in (1, 2):
+    for eng in (1, 2, 3):
         C = torch.empty((b1, M, N), dtype=torch.float32, device=dev)
         K.gemm(Ad, Bd, C, M, N, Kd, a=sa, b=sb, c=(M * N, 0, N, 1), batch=(b1, 1), bias=bias, gelu=True,
                engine=eng)
@@ -162,12 +163,13 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
     torch.cuda.synchronize()
     assert K.L.sfg_fno_tc_timeouts(ctypes.byref(cnt), 1) == 0 and cnt.value == 0
     ref = torch.nn.functional.gelu(A.float() @ B.float() + bias.cpu()).numpy()
-    assert _rel(outs[1], outs[0]) < 1e-5
-    assert _rel(outs[1], ref) < 2e-3
+    for o in outs[1:]:
+        assert _rel(o, outs[0]) < 1e-5
+        assert _rel(o, ref) < 2e-3
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("engine", [1, 2])
+@pytest.mark.parametrize("engine", [1, 2, 3])
 def test_gemm_split_k_and_batch_sum(engine):
     import torch
     from seisfem_b200.surrogate import Kernels
@@ -210,6 +212,20 @@ def test_gpu_forward_and_gradients_match_oracle(engine):
     for k in prm:
         assert _rel(g[k], g_ref[k]) < 3e-2, k
         assert _rel(g[k], ge[k]) < 2e-2, k
+
+
+@pytest.mark.gpu
+def test_inference_forward_equals_training_forward():
+    """keep_pre=False only skips the stores backward() reads."""
+    import torch
+    s = SMALL
+    prm, x, _ = _case(seed=4)
+    net = FNO(prm, s["B"], s["D"], s["W"], s["T"], torch.device("cuda:0"))
+    xd = x.to("cuda:0")
+    a = net.forward(xd).clone()
+    b = net.forward(xd, keep_pre=False).clone()
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
 
 
 @pytest.mark.gpu
