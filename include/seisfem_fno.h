@@ -59,6 +59,15 @@ int sfg_fno_expand_weights(const float *Wr, const float *Wi, void *Wblk, int mod
 int sfg_fno_fold_weights(const float *dWblk, float *dWr, float *dWi, int modes, int C, void *stream);
 /* dx = dy * gelu'(pre) (dy FP32 or BF16, pre BF16, dx BF16) */
 int sfg_fno_gelu_bwd(const void *dy, int dy_bf16, const void *pre, void *dx, long long n, void *stream);
+/* The surrogate's head for inference in one kernel: y[b][j][m] = b2[j] +
+ * sum_n GELU(alpha (A B)[b][m][n] + bias[n]) w2[n][j] for j < n2, with the
+ * first GEMM given by *d (A and B contiguous along M and N, N <= 128, one
+ * batch level, d->C unused) and y at y + b * y_batch + j * y_ch + m; the
+ * hidden activations never reach memory.  Returns 1 for a bad argument, 3
+ * when the operands' layout does not fit (the caller then runs the two
+ * GEMMs). */
+int sfg_fno_head_infer(const sfg_gemm_desc *d, const float *w2, const float *b2, float *y, long long y_batch,
+                       long long y_ch, int n2, void *stream);
 /* FP32 -> BF16 */
 int sfg_fno_cast_bf16(const float *x, void *y, long long n, void *stream);
 /* bias gradient of a [outer][C][inner] tensor (BF16): db[c] += sum over outer, inner */

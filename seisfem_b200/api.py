@@ -68,7 +68,8 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            # learned surrogate (include/seisfem_fno.h)
            "sfg_fno_gemm", "sfg_fno_dft_combine", "sfg_fno_dft_combine_bwd", "sfg_fno_expand_weights",
            "sfg_fno_fold_weights", "sfg_fno_gelu_bwd", "sfg_fno_cast_bf16", "sfg_fno_bias_grad", "sfg_fno_swap01",
-           "sfg_fno_zero", "sfg_fno_scale", "sfg_fno_rel_loss", "sfg_fno_adam", "sfg_fno_tc_timeouts"]
+           "sfg_fno_zero", "sfg_fno_scale", "sfg_fno_rel_loss", "sfg_fno_adam", "sfg_fno_tc_timeouts",
+           "sfg_fno_head_infer"]
 
 
 def lib(path: str = LIBPATH):

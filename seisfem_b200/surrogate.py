@@ -111,6 +111,30 @@ class Kernels:
         self.flops += 2 * M * N * K * batch[0] * batch[1]
         self._check(self.L.sfg_fno_gemm(C.byref(d), self.stream), "sfg_fno_gemm")
 
+    def head_infer(self, A, B, y, M, N, K, a, b, batch, bias, w2, b2, y_batch, y_ch):
+        """sfg_fno_head_infer: GELU(A B + bias) times w2 (+ b2) into y without
+        storing the hidden layer; False when the layout does not fit (the
+        caller then runs the two GEMMs)."""
+        d = GemmDesc()
+        d.A, d.B = _ptr(A), _ptr(B)
+        d.bias = _ptr(bias)
+        d.sa1, d.sa2, d.sam, d.sak = a
+        d.sb1, d.sb2, d.sbk, d.sbn = b
+        d.M, d.N, d.K = M, N, K
+        d.batch1, d.batch2, d.splits = batch, 1, 1
+        d.alpha, d.beta = 1.0, 0.0
+        d.gelu = 1
+        f = self.L.sfg_fno_head_infer
+        f.argtypes = [C.POINTER(GemmDesc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong, C.c_int,
+                      C.c_void_p]
+        f.restype = C.c_int
+        rc = f(C.byref(d), _ptr(w2), _ptr(b2), _ptr(y), y_batch, y_ch, w2.shape[1], self.stream)
+        if rc == 3:
+            return False
+        self._check(rc, "sfg_fno_head_infer")
+        self.flops += 2 * M * N * K * batch + 2 * M * N * w2.shape[1] * batch
+        return True
+
     def call(self, name, *args):
         """Pointwise entry point `name`; tensor arguments pass as device pointers."""
         import torch
@@ -293,7 +317,7 @@ class FNO:
     def forward(self, x, keep_pre: bool = True):
         """x: BF16 [B][cin][D][W] on the device -> self.y (FP32 [B][2][W][T]).
         keep_pre=False (inference) skips storing the pre-activations that
-        only backward() reads."""
+        only backward() reads and fuses the two head projections."""
         K, B, Cc, D, W, T, Hp = self.K, self.B, self.C, self.D, self.W, self.T, self.Hp
         P = D * W
         K.gemm(self.bf["lift_w"], x, self.v_act[0], Cc, P, self.cin, a=(0, 0, self.cin, 1),
@@ -308,11 +332,18 @@ class FNO:
         # depth -> time: u[z][w][t] = sum_d v4[z][d][w] Wt[d][t] + bt[t]
         K.gemm(self.v_act[self.Lyr], self.bf["time_w"], self.u, W, T, D, a=(D * W, 0, 1, W), b=(0, 0, T, 1),
                c=(W * T, 0, T, 1), batch=(B * Cc, 1), bias=self.p["time_b"])
-        K.gemm(self.u, self.bf["p1_w"], self.h1, W * T, Hp, Cc, a=(Cc * W * T, 0, 1, W * T), b=(0, 0, Hp, 1),
-               c=(W * T * Hp, 0, Hp, 1), batch=(B, 1), bias=self.p["p1_b"], pre=self.hpre if keep_pre else None,
-               gelu=True)
-        K.gemm(self.h1, self.bf["p2_w"], self.y, W * T, 2, Hp, a=(W * T * Hp, 0, Hp, 1), b=(0, 0, 2, 1),
-               c=(2 * W * T, 0, 1, W * T), batch=(B, 1), bias=self.p["p2_b"])
+        # head: inference runs both projections in one kernel (the hidden layer
+        # stays on chip, FP32 second projection); training stores h1, hpre
+        fused = (not keep_pre and hasattr(K, "head_infer") and
+                 K.head_infer(self.u, self.bf["p1_w"], self.y, W * T, Hp, Cc, a=(Cc * W * T, 0, 1, W * T),
+                              b=(0, 0, Hp, 1), batch=B, bias=self.p["p1_b"], w2=self.p["p2_w"], b2=self.p["p2_b"],
+                              y_batch=2 * W * T, y_ch=W * T))
+        if not fused:
+            K.gemm(self.u, self.bf["p1_w"], self.h1, W * T, Hp, Cc, a=(Cc * W * T, 0, 1, W * T), b=(0, 0, Hp, 1),
+                   c=(W * T * Hp, 0, Hp, 1), batch=(B, 1), bias=self.p["p1_b"], pre=self.hpre if keep_pre else None,
+                   gelu=True)
+            K.gemm(self.h1, self.bf["p2_w"], self.y, W * T, 2, Hp, a=(W * T * Hp, 0, Hp, 1), b=(0, 0, 2, 1),
+                   c=(2 * W * T, 0, 1, W * T), batch=(B, 1), bias=self.p["p2_b"])
         return self.y
 
     def loss_and_grad(self, target, want_grad=True):
