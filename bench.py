@@ -193,24 +193,26 @@ def run_surrogate(args):
     steps = args.epochs * (ntr // 16)
     # inference: warm-up, then K timed passes over the held-out set (CUDA events;
     # inputs already on the device: value; with host copies: e2e)
-    B = sg.B
+    B = args.infer_batch
+    inet = sg.inference_net(B)
+    K = inet.K
     xb = torch.tensor(xte[:B]).to(dev).to(torch.bfloat16).contiguous()
     for _ in range(max(3, args.warmup)):
-        sg.net.forward(xb, keep_pre=False)
+        inet.forward(xb, keep_pre=False)
     torch.cuda.synchronize(dev)
     f1 = K.flops
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = max(1, args.steps) * (nte // B)
+    reps = max(1, args.steps) * max(1, nte // B)
     e0.record()
     for _ in range(reps):
-        sg.net.forward(xb, keep_pre=False)
+        inet.forward(xb, keep_pre=False)
     e1.record()
     torch.cuda.synchronize(dev)
     fwd_ms = e0.elapsed_time(e1) / reps
     fwd_flops = (K.flops - f1) / reps
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
-    pred = sg.predict(xte)
+    pred = sg.predict(xte, batch=B)
     torch.cuda.synchronize(dev)
     t_e2e = time.perf_counter() - t2
     err = rel_l2(pred, yte)
@@ -228,7 +230,7 @@ def run_surrogate(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
             "config": {"workload": "config5_q4_128_fno", "train_shots": ntr, "test_shots": nte,
                        "grid": [128, 64], "samples": 1000, "width": 64, "modes": 16, "layers": 4,
-                       "batch": B, "epochs": args.epochs},
+                       "train_batch": sg.B, "inference_batch": B, "epochs": args.epochs},
             "rel_l2": {"mean": float(err.mean()), "median": float(np.median(err)),
                        "p10": float(np.percentile(err, 10)), "p90": float(np.percentile(err, 90))},
             "fallback_fraction": float(fallback.mean()), "fallback_bound": 1e-2,
@@ -240,7 +242,8 @@ def run_surrogate(args):
                          "flops_per_forward": fwd_flops},
             "train": {"seconds": t_train, "steps": steps, "ms_per_step": t_train / steps * 1e3,
                       "tflops": train_flops / t_train / 1e12, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]},
-            "fem_generation_seconds": t_gen, "gpu_launches": K.launches}
+            "fem_generation_seconds": t_gen,
+            "gpu_launches": sg.net.K.launches + (inet.K.launches if inet is not sg.net else 0)}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -398,6 +401,7 @@ def main():
     ap.add_argument("--test-shots", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--infer-batch", type=int, default=64, help="surrogate shots per inference pass")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

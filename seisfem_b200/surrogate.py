@@ -557,14 +557,29 @@ class Surrogate:
                 log(f"epoch {ep}: loss {hist[-1]:.4f}")
         return hist
 
-    def predict(self, x: np.ndarray) -> np.ndarray:
-        """Gathers [n][2][W][T] (physical units) for inputs [n][4][D][W]."""
+    def inference_net(self, batch: int):
+        """The network with the current weights for `batch` shots per pass
+        (larger batches make larger GEMMs; the training batch is self.B)."""
+        if batch == self.B:
+            return self.net
+        key = (batch, self.net.step_count)
+        if getattr(self, "_infer", (None, None))[0] != key:
+            self._infer = (key, FNO(self.net.params_numpy(), batch, self.D, self.W, self.T, self.dev,
+                                    stream=self.net.K.stream, kernels=None if isinstance(self.net.K, Kernels)
+                                    else self.net.K))
+        return self._infer[1]
+
+    def predict(self, x: np.ndarray, batch: int | None = None) -> np.ndarray:
+        """Gathers [n][2][W][T] (physical units) for inputs [n][4][D][W],
+        `batch` shots per forward pass (default: the training batch)."""
         torch = self.torch
+        net = self.inference_net(batch or self.B)
+        Bp = net.B
         out = np.empty((len(x), 2, self.W, self.T), np.float32)
-        for k in range(0, len(x), self.B):
-            xb = np.zeros((self.B, 4, self.D, self.W), np.float32)
-            m = min(self.B, len(x) - k)
+        for k in range(0, len(x), Bp):
+            xb = np.zeros((Bp, 4, self.D, self.W), np.float32)
+            m = min(Bp, len(x) - k)
             xb[:m] = x[k:k + m]
-            y = self.net.forward(torch.tensor(xb).to(self.dev).to(torch.bfloat16).contiguous(), keep_pre=False)
+            y = net.forward(torch.tensor(xb).to(self.dev).to(torch.bfloat16).contiguous(), keep_pre=False)
             out[k:k + m] = y[:m].float().cpu().numpy().reshape(m, 2, self.W, self.T) * self.scale
         return out

@@ -277,3 +277,5 @@ def test_trained_surrogate_beats_untrained_on_held_out_fem_shots():
     pred = sg.predict(xte)
     e1 = rel_l2(pred, yte).mean()
     assert e1 < 0.8 * e0 and e1 < 1.0, (e0, e1)
+    # a larger inference batch: the same per-shot arithmetic
+    assert _rel(sg.predict(xte, batch=16), pred) < 1e-5
