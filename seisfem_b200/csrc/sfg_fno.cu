@@ -651,28 +651,63 @@ __device__ __forceinline__ void tma_operand(uint32_t dst, const CUtensorMap *map
     }
 }
 
-// The fused head of the surrogate's inference: the tile's rows through
-// alpha, bias and GELU, then the n2 dot products with w2 (all BN columns are
-// in this tile: the grid has one column of tiles), written to y.
+// The fused head of the surrogate's inference, straight from TMEM: warp w
+// reads rows 32 (w % 4).. and half the columns (tcgen05.ld, 16 at a time),
+// applies alpha, bias and GELU in registers and accumulates the n2 dot
+// products with w2 (bias and w2 staged in shared memory, read as
+// broadcasts); the two column halves of a row meet in shared memory and the
+// lower half writes y.  The hidden layer never leaves the SM.
 template <int BN>
-__device__ __forceinline__ void head_store(const GemmArgs &g, const float *tile, int m0, int z1)
+__device__ __forceinline__ void head_from_tmem(const GemmArgs &g, uint32_t tmem, float *scratch, int m0, int z1,
+                                               bool have)
 {
-    constexpr int TP = BN + 4;
     const sfg_gemm_desc &d = g.d;
-    const int rr = threadIdx.x >> 1, half = threadIdx.x & 1;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    const int c_end = min(d.N, (half + 1) * (BN / 2));
-    for (int c = half * (BN / 2); c < c_end; c++) {
-        const float v = gelu_f(d.alpha * tile[rr * TP + c] + (d.bias ? d.bias[c] : 0.f));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *sb = scratch;                    // [BN] bias
+    float *sw = scratch + BN;               // [BN][4] w2 (zero past N and n2)
+    float *part = scratch + 5 * BN;         // [128][4] sums of the upper column half
+    for (int c = threadIdx.x; c < BN; c += 256) {
+        sb[c] = (c < d.N && d.bias) ? d.bias[c] : 0.f;
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (j < g.n2) acc[j] += v * __ldg(g.w2 + c * g.n2 + j);
+        for (int j = 0; j < 4; j++) sw[4 * c + j] = (c < d.N && j < g.n2) ? g.w2[c * g.n2 + j] : 0.f;
     }
+    __syncthreads();
+    const int row = (warp & 3) * 32 + lane;
+    const int cb = (warp >> 2) * (BN / 2);
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (have) {
+#pragma unroll 1
+        for (int c0 = cb; c0 < cb + BN / 2; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (c0 >= d.N) continue;
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 1);
-    const int m = m0 + rr;
-    if (half == 0 && m < d.M)
-        for (int j = 0; j < g.n2; j++) g.y[z1 * g.ys1 + j * g.ysj + m] = acc[j] + (g.b2 ? g.b2[j] : 0.f);
+            for (int j = 0; j < 16; j++) {
+                const int c = c0 + j;
+                const float v = gelu_f(d.alpha * __uint_as_float(r[j]) + sb[c]);
+                const float4 w = *reinterpret_cast<const float4 *>(sw + 4 * c);
+                acc[0] += v * w.x; acc[1] += v * w.y; acc[2] += v * w.z; acc[3] += v * w.w;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    if (warp >= 4) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) part[4 * row + j] = acc[j];
+    }
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    const int m = m0 + row;
+    if (have && warp < 4 && m < d.M)
+        for (int j = 0; j < g.n2; j++)
+            g.y[z1 * g.ys1 + j * g.ysj + m] = acc[j] + part[4 * row + j] + (g.b2 ? g.b2[j] : 0.f);
 }
 
 template <int BN, int AMODE, int BMODE, bool HEAD = false>
@@ -774,8 +809,7 @@ __global__ void __launch_bounds__(256) gemm_tma_kernel(const __grid_constant__ G
     if (!ok && (threadIdx.x & 31) == 0) atomicAdd(&g_tc_timeouts, 1);
     const int good = __syncthreads_and(ok ? 1 : 0);
     if constexpr (HEAD) {
-        tc_tile_to_smem<BN>(tmem, reinterpret_cast<float *>(stages), nt > 0 && good);
-        if (nt > 0 && good) head_store<BN>(g, reinterpret_cast<const float *>(stages), m0, z1);
+        head_from_tmem<BN>(g, tmem, reinterpret_cast<float *>(stages), m0, z1, nt > 0 && good);
     } else {
         tc_epilogue<BN>(d, tmem, reinterpret_cast<float *>(stages), m0, n0, cz, nt > 0 && good);
     }
