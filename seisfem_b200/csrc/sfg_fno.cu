@@ -869,6 +869,56 @@ __global__ void dft_combine_bwd_kernel(const __nv_bfloat16 *__restrict__ dZ, __n
     p[(32 + k1) * 32 + k2] = __float2bfloat16(-__bfloat162float(im));
 }
 
+// Tiled versions for C a multiple of 16: a block takes 16 channels of one
+// shot and 128 modes and turns the transpose between the per-plane P layout
+// and the per-mode Zmix layout through shared memory, so both sides move
+// whole 32-byte sectors (the one-thread-per-element versions above write or
+// read Zmix two bytes at a time).
+constexpr int CMB_C = 16, CMB_M = 128;
+
+__global__ void __launch_bounds__(256) dft_combine_tiled(const float *__restrict__ P, __nv_bfloat16 *__restrict__ Z,
+                                                         int B, int C)
+{
+    __shared__ __align__(16) __nv_bfloat16 s[CMB_M][2][CMB_C];
+    const int b = blockIdx.z, c0 = blockIdx.y * CMB_C, mode0 = blockIdx.x * CMB_M;
+    for (int idx = threadIdx.x; idx < CMB_C * CMB_M; idx += 256) {
+        const int cl = idx / CMB_M, ml = idx % CMB_M, mode = mode0 + ml;
+        const int k1 = mode / KC, k2 = mode % KC;
+        const float *p = P + ((long long)b * C + c0 + cl) * 64 * 32;
+        s[ml][0][cl] = __float2bfloat16(p[k1 * 32 + k2] + p[(32 + k1) * 32 + 16 + k2]);
+        s[ml][1][cl] = __float2bfloat16(p[k1 * 32 + 16 + k2] - p[(32 + k1) * 32 + k2]);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CMB_M * 2 * 2; idx += 256) {
+        const int ml = idx >> 2, part = (idx >> 1) & 1, h = idx & 1;
+        __nv_bfloat16 *o = Z + ((long long)(mode0 + ml) * B + b) * 2 * C + part * C + c0 + h * 8;
+        *reinterpret_cast<uint4 *>(o) = *reinterpret_cast<const uint4 *>(&s[ml][part][h * 8]);
+    }
+}
+
+__global__ void __launch_bounds__(256) dft_combine_bwd_tiled(const __nv_bfloat16 *__restrict__ dZ,
+                                                             __nv_bfloat16 *__restrict__ dP, int B, int C)
+{
+    __shared__ __align__(16) __nv_bfloat16 s[CMB_M][2][CMB_C];
+    const int b = blockIdx.z, c0 = blockIdx.y * CMB_C, mode0 = blockIdx.x * CMB_M;
+    for (int idx = threadIdx.x; idx < CMB_M * 2 * 2; idx += 256) {
+        const int ml = idx >> 2, part = (idx >> 1) & 1, h = idx & 1;
+        const __nv_bfloat16 *g = dZ + ((long long)(mode0 + ml) * B + b) * 2 * C + part * C + c0 + h * 8;
+        *reinterpret_cast<uint4 *>(&s[ml][part][h * 8]) = *reinterpret_cast<const uint4 *>(g);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CMB_C * CMB_M; idx += 256) {
+        const int cl = idx / CMB_M, ml = idx % CMB_M, mode = mode0 + ml;
+        const int k1 = mode / KC, k2 = mode % KC;
+        const __nv_bfloat16 re = s[ml][0][cl], im = s[ml][1][cl];
+        __nv_bfloat16 *p = dP + ((long long)b * C + c0 + cl) * 64 * 32;
+        p[k1 * 32 + k2] = re;
+        p[(32 + k1) * 32 + 16 + k2] = re;
+        p[k1 * 32 + 16 + k2] = im;
+        p[(32 + k1) * 32 + k2] = __float2bfloat16(-__bfloat162float(im));
+    }
+}
+
 __global__ void expand_weights_kernel(const float *__restrict__ Wr, const float *__restrict__ Wi,
                                       __nv_bfloat16 *__restrict__ Wb, int modes, int C)
 {
@@ -1219,6 +1269,12 @@ int sfg_fno_dft_combine(const float *P, void *Zmix, int B, int C, void *stream)
 {
     if (!P || !Zmix || B <= 0 || C <= 0) return 1;
     const long long n = (long long)B * C * KD * KC;
+    const bool aligned = (reinterpret_cast<uintptr_t>(Zmix) & 15) == 0;
+    if (C % CMB_C == 0 && aligned && B <= 65535) {
+        dft_combine_tiled<<<dim3(KD * KC / CMB_M, C / CMB_C, B), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            P, static_cast<__nv_bfloat16 *>(Zmix), B, C);
+        return launched();
+    }
     dft_combine_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         P, static_cast<__nv_bfloat16 *>(Zmix), B, C);
     return launched();
@@ -1228,6 +1284,12 @@ int sfg_fno_dft_combine_bwd(const void *dZmix, void *dP, int B, int C, void *str
 {
     if (!dZmix || !dP || B <= 0 || C <= 0) return 1;
     const long long n = (long long)B * C * KD * KC;
+    const bool aligned = (reinterpret_cast<uintptr_t>(dZmix) & 15) == 0;
+    if (C % CMB_C == 0 && aligned && B <= 65535) {
+        dft_combine_bwd_tiled<<<dim3(KD * KC / CMB_M, C / CMB_C, B), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            static_cast<const __nv_bfloat16 *>(dZmix), static_cast<__nv_bfloat16 *>(dP), B, C);
+        return launched();
+    }
     dft_combine_bwd_kernel<<<grid_of(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16 *>(dZmix), static_cast<__nv_bfloat16 *>(dP), B, C);
     return launched();

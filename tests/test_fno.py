@@ -215,6 +215,33 @@ def test_gpu_forward_and_gradients_match_oracle(engine):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("C", [8, 32, 64])
+def test_dft_recombination_kernels(C):
+    """Forward and backward recombination of the D-DFT outputs (tiled
+    kernels for C a multiple of 16, the element-wise ones otherwise)
+    against the CPU emulation."""
+    import torch
+    from fno_emulator import EmuKernels
+    from seisfem_b200.surrogate import Kernels
+    K, E = Kernels(), EmuKernels()
+    B = 3
+    rng = np.random.default_rng(C)
+    P = torch.tensor(rng.standard_normal((B * C, 64, 32)).astype(np.float32))
+    Zc = torch.zeros(512 * B * 2 * C, dtype=torch.bfloat16)
+    E.dft_combine(P, Zc, B, C)
+    Zg = torch.zeros_like(Zc, device="cuda:0")
+    K.call("sfg_fno_dft_combine", P.to("cuda:0"), Zg, B, C)
+    dZ = torch.tensor(rng.standard_normal(512 * B * 2 * C).astype(np.float32)).to(torch.bfloat16)
+    dPc = torch.zeros((B * C, 64, 32), dtype=torch.bfloat16)
+    E.dft_combine_bwd(dZ, dPc, B, C)
+    dPg = torch.zeros_like(dPc, device="cuda:0")
+    K.call("sfg_fno_dft_combine_bwd", dZ.to("cuda:0"), dPg, B, C)
+    torch.cuda.synchronize()
+    assert torch.equal(Zg.cpu(), Zc)
+    assert torch.equal(dPg.cpu(), dPc)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("hp", [16, 128])
 def test_inference_forward_matches_training_forward(hp):
     """keep_pre=False skips the stores backward() reads and, where the
