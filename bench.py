@@ -343,7 +343,8 @@ def run_gemm_engines(args):
         B = torch.randn(bsz, device=dev).to(torch.bfloat16)
         C = torch.empty(csz, device=dev, dtype=cdt)
         row = {"gemm": name, "flops": 2 * M * N * Kd * batch[0] * batch[1]}
-        for eng, key in ((1, "mma_sync_us"), (3, "tcgen05_cp_async_us"), (2, "tcgen05_tma_us")):
+        for eng, key in ((1, "mma_sync_us"), (3, "tcgen05_cp_async_us"), (4, "tcgen05_tma_us"),
+                         (2, "tcgen05_tma_persistent_us")):
             for _ in range(max(3, args.warmup)):
                 K.gemm(A, B, C, M, N, Kd, a=a, b=b, c=c, batch=batch, engine=eng, **epi)
             torch.cuda.synchronize(dev)

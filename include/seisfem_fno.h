@@ -37,9 +37,11 @@ typedef struct {
     int M, N, K, batch1, batch2, splits;
     float alpha, beta;
     int c_bf16, gelu, bias_on_m, atomic;
-    int engine;                    /* 0: automatic, 1: mma.sync tiles, 2: tcgen05 with TMEM accumulators
-                                      (operand tiles by TMA where the strides allow, else cp.async),
-                                      3: tcgen05 with cp.async operand tiles */
+    int engine;                    /* 0: automatic, 1: mma.sync tiles, 2: tcgen05 with TMEM accumulators,
+                                      persistent CTAs (TMA operand tiles where the strides allow, else
+                                      cp.async), 3: tcgen05 with cp.async operand tiles, 4: tcgen05 with
+                                      TMA tiles, one output tile per CTA.  Automatic: tcgen05 for
+                                      M >= 64, N >= 32, K >= 64, persistent from 8 k-tiles per tile */
 } sfg_gemm_desc;
 
 int sfg_fno_gemm(const sfg_gemm_desc *d, void *stream);

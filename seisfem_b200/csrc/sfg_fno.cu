@@ -815,6 +815,295 @@ __global__ void __launch_bounds__(256) gemm_tma_kernel(const __grid_constant__ G
     }
 }
 
+// ------------------------------------- persistent tcgen05 GEMM (TMA tiles)
+//
+// One CTA per SM walks a list of output tiles (batch, split, 128-row tile,
+// BN-column tile; consecutive tiles share their A rows).  Three roles run
+// side by side on their own mbarriers:
+//   warp 0 (one thread)  TMA producer: the A and B k-tiles of every tile in
+//                        turn into a ring of PSTG stages;
+//   warp 1 (one thread)  MMA issuer: tcgen05.mma into one of two TMEM
+//                        accumulators, a commit per stage (frees it for the
+//                        producer) and one per tile (hands the accumulator to
+//                        the epilogue);
+//   warps 4-7            epilogue: tcgen05.ld of the accumulator (warp w:
+//                        TMEM lanes 32 (w % 4)..), the descriptor's epilogue
+//                        in registers, 16-column stores per row, then the
+//                        accumulator back to the MMA issuer.
+// So the loads of tile i + 1 and its MMAs overlap the epilogue of tile i,
+// and TMEM allocation, barrier set-up and tensor-map prefetch happen once per
+// CTA instead of once per tile.  Every wait is bounded; the first one that
+// gives up sets a flag that ends every other wait of the CTA at once.
+
+constexpr int PSTG = 4;
+
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, volatile int *abort)
+{
+    for (long long i = 0; i < kWaitLimit; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 63) == 63 && *abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+struct TileCoord {
+    int z1, z2, m0, n0, kt0, nt;
+    long long cz;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const sfg_gemm_desc &d, int item, int tm, int tn, int BN)
+{
+    TileCoord c;
+    const int per_z = tm * tn;
+    const int zs = item / per_z, rem = item % per_z;
+    const int nb = d.batch1 * d.batch2;
+    const int z = zs % nb, split = zs / nb;
+    c.z1 = z / d.batch2;
+    c.z2 = z % d.batch2;
+    c.m0 = (rem / tn) * 128;
+    c.n0 = (rem % tn) * BN;
+    const int ktiles = (d.K + TBK - 1) / TBK;
+    const int per = (ktiles + d.splits - 1) / d.splits;
+    c.kt0 = split * per;
+    c.nt = max(0, min(ktiles, c.kt0 + per) - c.kt0);
+    c.cz = c.z1 * d.sc1 + c.z2 * d.sc2;
+    return c;
+}
+
+// Columns n0 .. n0 + 15 of row m with the descriptor's epilogue.
+__device__ __forceinline__ void store_row16(const sfg_gemm_desc &d, const uint32_t *r, int m, int n0, long long cz)
+{
+    if (m >= d.M || n0 >= d.N) return;
+    const int cnt = min(16, d.N - n0);
+    const long long o = cz + m * d.scm + (long long)n0 * d.scn;
+    float x[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) x[j] = d.alpha * __uint_as_float(r[j]);
+    if (d.atomic) {
+        for (int j = 0; j < cnt; j++) atomicAdd(static_cast<float *>(d.C) + o + j * d.scn, x[j]);
+        return;
+    }
+    const bool vec = cnt == 16 && d.scn == 1 && (o & 7) == 0;
+    if (d.Cin) {
+        if (vec && (reinterpret_cast<uintptr_t>(d.Cin) & 15) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float4 a = *reinterpret_cast<const float4 *>(d.Cin + o + 4 * q);
+                x[4 * q] += d.beta * a.x; x[4 * q + 1] += d.beta * a.y;
+                x[4 * q + 2] += d.beta * a.z; x[4 * q + 3] += d.beta * a.w;
+            }
+        } else {
+            for (int j = 0; j < cnt; j++) x[j] += d.beta * d.Cin[o + j * d.scn];
+        }
+    }
+    if (d.bias) {
+        if (d.bias_on_m) {
+            const float b = d.bias[m];
+#pragma unroll
+            for (int j = 0; j < 16; j++) x[j] += b;
+        } else {
+            for (int j = 0; j < cnt; j++) x[j] += d.bias[n0 + j];
+        }
+    }
+    if (d.pre) {
+        __nv_bfloat16 *pp = static_cast<__nv_bfloat16 *>(d.pre) + o;
+        if (vec && (reinterpret_cast<uintptr_t>(d.pre) & 15) == 0) {
+            __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) h[j] = __float2bfloat16(x[j]);
+            reinterpret_cast<uint4 *>(pp)[0] = reinterpret_cast<const uint4 *>(h)[0];
+            reinterpret_cast<uint4 *>(pp)[1] = reinterpret_cast<const uint4 *>(h)[1];
+        } else {
+            for (int j = 0; j < cnt; j++) pp[j * d.scn] = __float2bfloat16(x[j]);
+        }
+    }
+    if (d.gelu) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] = gelu_f(x[j]);
+    }
+    if (d.c_bf16) {
+        __nv_bfloat16 *cp = static_cast<__nv_bfloat16 *>(d.C) + o;
+        if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+            __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) h[j] = __float2bfloat16(x[j]);
+            reinterpret_cast<uint4 *>(cp)[0] = reinterpret_cast<const uint4 *>(h)[0];
+            reinterpret_cast<uint4 *>(cp)[1] = reinterpret_cast<const uint4 *>(h)[1];
+        } else {
+            for (int j = 0; j < cnt; j++) cp[j * d.scn] = __float2bfloat16(x[j]);
+        }
+    } else {
+        float *cp = static_cast<float *>(d.C) + o;
+        if (vec && (reinterpret_cast<uintptr_t>(d.C) & 15) == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                reinterpret_cast<float4 *>(cp)[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+        } else {
+            for (int j = 0; j < cnt; j++) cp[j * d.scn] = x[j];
+        }
+    }
+}
+
+template <int BN, int AMODE, int BMODE>
+__global__ void __launch_bounds__(256, 1) gemm_persist_kernel(const __grid_constant__ GemmArgs g,
+                                                               const __grid_constant__ CUtensorMap ta,
+                                                               const __grid_constant__ CUtensorMap tb, int items)
+{
+    constexpr int BM = 128;
+    constexpr int ASTG = BM * TBK * 2, BSTG = BN * TBK * 2;
+    static_assert(BMODE == 0 || BN % 64 == 0, "MN-major tiles come in 64-element blocks");
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[PSTG], empty[PSTG], tfull[2], tempty[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    const sfg_gemm_desc &d = g.d;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tm = (d.M + BM - 1) / BM, tn = (d.N + BN - 1) / BN;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t sA = (raw + 1023u) & ~1023u, sB = sA + PSTG * ASTG;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)AMODE << 15) |
+                               ((uint32_t)BMODE << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    constexpr uint32_t A_STEP = AMODE ? 2048 : 32, B_STEP = BMODE ? 2048 : 32;
+    constexpr uint32_t A_LBO = AMODE ? 8192 : 16, B_LBO = BMODE ? 8192 : 16;
+    volatile int *abort = &abort_flag;
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+#pragma unroll
+        for (int s = 0; s < PSTG; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
+        }
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tfull[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&tempty[b])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(2 * BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        long long gk = 0;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const TileCoord tc = tile_coord(d, item, tm, tn, BN);
+            const int az1 = g.tz1a ? tc.z1 : 0, az2 = g.tz2a ? tc.z2 : 0;
+            const int bz1 = g.tz1b ? tc.z1 : 0, bz2 = g.tz2b ? tc.z2 : 0;
+            for (int t = 0; t < tc.nt; t++, gk++) {
+                const int s = (int)(gk % PSTG);
+                if (gk >= PSTG && !mbar_wait_or_abort(smem_u32(&empty[s]), (uint32_t)(((gk / PSTG) - 1) & 1), abort)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t bar = smem_u32(&full[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(ASTG + BSTG)
+                             : "memory");
+                const int k0 = (tc.kt0 + t) * TBK;
+                tma_operand<AMODE, BM>(sA + s * ASTG, &ta, k0, tc.m0, az2, az1, bar);
+                tma_operand<BMODE, BN>(sB + s * BSTG, &tb, k0, tc.n0, bz2, bz1, bar);
+            }
+        }
+        // on an abort, let the copies already issued land before the CTA ends
+        if (!ok)
+            for (long long q = (gk > PSTG ? gk - PSTG : 0); q < gk; q++)
+                mbar_wait(smem_u32(&full[q % PSTG]), (uint32_t)((q / PSTG) & 1));
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        long long gk = 0;
+        int j = 0;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x, j++) {
+            const TileCoord tc = tile_coord(d, item, tm, tn, BN);
+            const int ab = j & 1, use = j >> 1;
+            if (use >= 1 && !mbar_wait_or_abort(smem_u32(&tempty[ab]), (uint32_t)((use - 1) & 1), abort)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t acc_addr = tmem + (uint32_t)(ab * BN);
+            for (int t = 0; t < tc.nt; t++, gk++) {
+                const int s = (int)(gk % PSTG);
+                if (!mbar_wait_or_abort(smem_u32(&full[s]), (uint32_t)((gk / PSTG) & 1), abort)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a0 = sA + s * ASTG, b0 = sB + s * BSTG;
+#pragma unroll
+                for (int ks = 0; ks < TBK / 16; ks++) {
+                    const uint64_t da = umma_desc_sw128(a0 + ks * A_STEP, A_LBO, 1024);
+                    const uint64_t db = umma_desc_sw128(b0 + ks * B_STEP, B_LBO, 1024);
+                    const uint32_t acc = (t > 0 || ks > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(acc_addr),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&empty[s])));
+            }
+            if (!ok) break;
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&tfull[ab])));
+        }
+    } else if (warp >= 4) {
+        // epilogue
+        const int row = (warp & 3) * 32 + lane;
+        int j = 0;
+        for (int item = blockIdx.x; item < items; item += gridDim.x, j++) {
+            const TileCoord tc = tile_coord(d, item, tm, tn, BN);
+            const int ab = j & 1, use = j >> 1;
+            if (!mbar_wait_or_abort(smem_u32(&tfull[ab]), (uint32_t)(use & 1), abort)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r[16];
+                __syncwarp();   // tcgen05.ld is .aligned: the warp converges after the stores' branches
+                const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(ab * BN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (tc.nt > 0) store_row16(d, r, tc.m0 + row, tc.n0 + c0, tc.cz);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[ab])) : "memory");
+        }
+    }
+    if (!ok && (threadIdx.x & 31) == 0) atomicAdd(&g_tc_timeouts, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+}
+
 // Vector loads need 16-byte aligned groups of 8 elements: the base pointer
 // and every stride other than the contiguous one must keep that alignment.
 int pick_mode(long long s_row, long long s_k, long long s1, long long s2, const void *p)
@@ -1147,10 +1436,29 @@ int launch_tma_shape(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMap
     return launched();
 }
 
-// tcgen05 with TMA operand tiles; -1 when the operands do not allow it
-// (the caller then takes the cp.async engine)
+template <int BN, int AM, int BMD>
+int launch_persist_shape(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb, long long nb,
+                         cudaStream_t st)
+{
+    const sfg_gemm_desc &d = g.d;
+    const int smem = PSTG * (128 + BN) * TBK * 2 + 1024;
+    if (cudaFuncSetAttribute(gemm_persist_kernel<BN, AM, BMD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess)
+        return 2;
+    const long long items = nb * (long long)((d.M + 127) / 128) * ((d.N + BN - 1) / BN);
+    if (items > 0x7fffffffLL) return 1;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)std::min<long long>(items, sms);
+    gemm_persist_kernel<BN, AM, BMD><<<grid, 256, smem, st>>>(g, ta, tb, (int)items);
+    return launched();
+}
+
+// tcgen05 with TMA operand tiles (persistent, or one tile per CTA); -1 when
+// the operands do not allow it (the caller then takes the cp.async engine)
 template <int BN>
-int launch_tma(GemmArgs g, long long nb, cudaStream_t st)
+int launch_tma(GemmArgs g, long long nb, cudaStream_t st, bool persistent)
 {
     const sfg_gemm_desc &d = g.d;
     if (g.bmode == 1 && BN % 64 != 0) return -1;
@@ -1160,6 +1468,15 @@ int launch_tma(GemmArgs g, long long nb, cudaStream_t st)
         !operand_map(&tb, d.B, g.bmode, d.N, d.K, d.sbn, d.sbk, d.sb1, d.sb2, d.batch1, d.batch2, BN, g.tz1b,
                      g.tz2b))
         return -1;
+    if (persistent) {
+        if (g.amode == 0 && g.bmode == 0) return launch_persist_shape<BN, 0, 0>(g, ta, tb, nb, st);
+        if (g.amode == 1 && g.bmode == 0) return launch_persist_shape<BN, 1, 0>(g, ta, tb, nb, st);
+        if constexpr (BN % 64 == 0) {
+            if (g.amode == 0) return launch_persist_shape<BN, 0, 1>(g, ta, tb, nb, st);
+            return launch_persist_shape<BN, 1, 1>(g, ta, tb, nb, st);
+        }
+        return -1;
+    }
     if (g.amode == 0 && g.bmode == 0) return launch_tma_shape<BN, 0, 0>(g, ta, tb, nb, st);
     if (g.amode == 1 && g.bmode == 0) return launch_tma_shape<BN, 1, 0>(g, ta, tb, nb, st);
     if constexpr (BN % 64 == 0) {
@@ -1216,11 +1533,18 @@ int sfg_fno_gemm(const sfg_gemm_desc *dp, void *stream)
     g.amode = pick_mode(d.sam, d.sak, d.sa1, d.sa2, d.A);
     g.bmode = pick_mode(d.sbn, d.sbk, d.sb1, d.sb2, d.B);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool tc = d.engine == 2 || d.engine == 3 || (d.engine == 0 && tc_auto(d));
+    const bool tc = d.engine == 2 || d.engine == 3 || d.engine == 4 || (d.engine == 0 && tc_auto(d));
     if (tc && d.N >= 32 && g.amode != 2 && g.bmode != 2) {   // copies move 16-byte groups
         if (d.engine != 3) {   // TMA operand tiles where the operands allow them
-            const int r = d.N >= 128 ? launch_tma<128>(g, nb, st) : d.N >= 64 ? launch_tma<64>(g, nb, st)
-                                                                              : launch_tma<32>(g, nb, st);
+            // persistent CTAs where the main loop dominates (at least 8 k-tiles
+            // per output tile); where a tile has only a few k-tiles, one tile
+            // per CTA with the 256-thread staged epilogue is faster (measured:
+            // head GEMM, K = 64, 161 vs 205 us; 8192^2 x 1024, 202 vs 187 us)
+            const int kt = (d.K + TBK - 1) / TBK, per = (kt + d.splits - 1) / d.splits;
+            const bool pers = d.engine == 2 || (d.engine == 0 && per >= 8);
+            const int r = d.N >= 128 ? launch_tma<128>(g, nb, st, pers)
+                          : d.N >= 64 ? launch_tma<64>(g, nb, st, pers)
+                                      : launch_tma<32>(g, nb, st, pers);
             if (r >= 0) return r;
         }
         if (d.N >= 128) return launch_tc<128>(g, nb, st);

@@ -59,8 +59,9 @@ class Kernels:
         self.stream = stream
         self.launches = 0
         self.flops = 0          # 2 M N K per problem of every GEMM issued
-        # GEMM engine: 0 automatic (tcgen05 for M >= 128, N >= 32, K >= 64), 1 mma.sync,
-        # 2 tcgen05 (TMA operand tiles where the strides allow), 3 tcgen05 with cp.async tiles
+        # GEMM engine: 0 automatic (tcgen05 for M >= 64, N >= 32, K >= 64), 1 mma.sync,
+        # 2 tcgen05 (persistent, TMA operand tiles where the strides allow), 3 tcgen05 with
+        # cp.async tiles, 4 tcgen05 with TMA tiles and one output tile per CTA
         self.engine = 0
         f = self.L.sfg_fno_gemm
         f.argtypes = [C.POINTER(GemmDesc), C.c_void_p]
@@ -91,7 +92,8 @@ class Kernels:
              aoff=0, boff=0, coff=0, Cin=None, pre=None, bias=None, bias_on_m=False, gelu=False,
              alpha=1.0, beta=1.0, atomic=False, splits=1, engine=None):
         """Strides are (level-1 batch, level-2 batch, row, col) in elements;
-        engine 0 automatic, 1 mma.sync, 2 tcgen05 (TMA tiles), 3 tcgen05 (cp.async tiles);
+        engine 0 automatic, 1 mma.sync, 2 tcgen05 (persistent, TMA tiles), 3 tcgen05 (cp.async
+        tiles), 4 tcgen05 (TMA tiles, one output tile per CTA);
         default: self.engine."""
         d = GemmDesc()
         d.A, d.B, d.C = _ptr(A, aoff), _ptr(B, boff), _ptr(Cout, coff)

@@ -79,7 +79,7 @@ def test_host_sequencing_matches_oracle_on_cpu():
 # ------------------------------------------------------------------ GPU
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("engine", [1, 2, 3])
+@pytest.mark.parametrize("engine", [1, 2, 3, 4])
 @pytest.mark.parametrize("layout", ["nn", "tn", "nt", "strided"])
 def test_gemm_matches_fp32(layout, engine):
     """Every epilogue term (alpha, beta Cin, bias, stored pre-activation,
@@ -126,10 +126,10 @@ def test_gemm_matches_fp32(layout, engine):
 @pytest.mark.parametrize("N,Kd,layout", [(32, 64, "nn"), (64, 100, "tn"), (128, 300, "nt"), (200, 128, "nn"),
                                          (136, 72, "tt"), (40, 200, "tt"), (96, 64, "strided")])
 def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
-    """The tcgen05/TMEM engine -- operand tiles by TMA (engine 2) and by
-    cp.async (engine 3) -- against the mma.sync engine on the same
-    descriptor (all accumulate in FP32), incl. ragged M, N, K and every
-    load path; no bounded wait may give up."""
+    """The tcgen05/TMEM engines -- persistent with TMA tiles (2), cp.async
+    tiles (3), TMA tiles one output tile per CTA (4) -- against the mma.sync
+    engine on the same descriptor (all accumulate in FP32), incl. ragged M,
+    N, K and every load path; no bounded wait may give up."""
     import ctypes
     import torch
     from seisfem_b200.surrogate import Kernels
@@ -155,7 +155,7 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
         Ad2[::3] = Ad.reshape(-1)
         Ad, sa = Ad2, tuple(3 * v for v in sa)
     outs = []
-    for eng in (1, 2, 3):
+    for eng in (1, 2, 3, 4):
         C = torch.empty((b1, M, N), dtype=torch.float32, device=dev)
         K.gemm(Ad, Bd, C, M, N, Kd, a=sa, b=sb, c=(M * N, 0, N, 1), batch=(b1, 1), bias=bias, gelu=True,
                engine=eng)
@@ -169,7 +169,7 @@ def test_tcgen05_gemm_matches_mma_sync(N, Kd, layout):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("engine", [1, 2, 3])
+@pytest.mark.parametrize("engine", [1, 2, 3, 4])
 def test_gemm_split_k_and_batch_sum(engine):
     import torch
     from seisfem_b200.surrogate import Kernels
