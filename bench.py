@@ -167,6 +167,101 @@ def run_reference_arm(args):
     return 0
 
 
+ACOUSTIC_WORKLOADS = {"acoustic_pml_q4_800": dict(n=800, pml=True), "acoustic_q4_800": dict(n=800, pml=False)}
+
+
+def acoustic_bytes(N: int, union_nnz: int, pml: bool) -> int:
+    """Algorithmic bytes of one fused acoustic time step (FP64): per union
+    entry its column (4 B) and matrix values (M, K0: 16 B; M, K1, K5, K2, K6:
+    40 B); per node its row length (4 B), coefficients ((vp dt)^2 and the
+    lumped mass, plus four PML profiles), one read of each gathered state
+    vector (u_now, u_old; or u1 now/old, u2 now/old, p1, p2, u) and the
+    written vectors (u; or u1, u2, p1, p2, u)."""
+    if pml:
+        return union_nnz * (4 + 40) + N * (4 + 6 * 8 + 7 * 8 + 5 * 8)
+    return union_nnz * (4 + 16) + N * (4 + 2 * 8 + 2 * 8 + 8)
+
+
+def run_acoustic(args):
+    """The scalar acoustic solvers (sfg_acoustic_run): one bench step = one
+    complete run (assembly on the GPU, time loop, outputs copied back).
+    value: node-steps per second of the time loop (CUDA events around the
+    loop's graph launch inside the library); e2e: the same work over the
+    wall time of the whole C-ABI call with host arrays in and out."""
+    import torch
+    from seisfem_b200.api import Context
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    c = P.acoustic_grf(**ACOUSTIC_WORKLOADS[args.workload])
+    m, N, steps = c.mesh, c.mesh.node_num, c.step - 2
+    n_el = ACOUSTIC_WORKLOADS[args.workload]["n"]
+    ctx = Context(0)
+    run = lambda: ctx.acoustic_run(m, c.vp, c.step, c.dt, c.f0, 0.0, c.src, c.pml, c.edge_size, c.pml_n, c.pml_n)
+    for _ in range(args.warmup):
+        r = run()
+    assert r["status"] == 0, r["status"]
+    cpath = os.path.join(tempfile.gettempdir(), "sfg_clocks_acoustic.csv")
+    cproc, cf = clocks_start(cpath)
+    loop_ms, wall = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = run()
+        wall.append(time.perf_counter() - t0)
+        loop_ms.append(r["stats"]["loop_ms"])
+    clocks = clocks_stop(cproc, cf, cpath, 0)
+    st = r["stats"]
+    ms = float(np.sum(loop_ms)) / args.steps
+    value = N * steps / (ms * 1e-3)
+    b_step = acoustic_bytes(N, st["union_nnz"], c.pml)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = b_step * steps / (ms * 1e-3) / 1e9
+    rows = r["snap"].shape[0]
+    line = {"metric": "node-steps/s", "value": value, "unit": "node-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": c.name, "nodes": N, "elements": f"Q4 {n_el}x{n_el}",
+                       "time_steps": steps, "pml": c.pml, "solver": "acoustic_pml.c" if c.pml else "acoustic.c",
+                       "l2": "per-step working set > 126 MB L2" if b_step > 126e6 else "per-step working set fits L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "algorithmic_bytes_per_step": b_step},
+            "e2e": {"value": N * steps / float(np.mean(wall)), "unit": "node-steps/s",
+                    "h2d_bytes_per_step": int(m.element_node.nbytes + 3 * 8 * N),
+                    "d2h_bytes_per_step": int(rows * N * 8 + c.step * 8)},
+            "setup_ms": st["setup_ms"], "gpu_launches": st["kernel_launches"] * args.steps, "clocks": clocks,
+            "cpu_baseline": None}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = acoustic_reference(c, nsteps=24)
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def acoustic_reference(c, nsteps: int) -> dict:
+    """The reference's acoustic solver (oracle/_ref, else the oracle port) on
+    this host's cores, on a bounded sample of the workload: nsteps time steps
+    after its set-up, each timed from its end-of-step energy.dat write."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    m, N = c.mesh, c.mesh.node_num
+    if os.path.exists(O.LIBACOUSTIC):
+        out = O.ReferenceAcoustic().run(m, c.vp, 2 + nsteps, c.dt, c.f0, 0.0, c.src, c.pml, c.edge_size, c.pml_n,
+                                        c.pml_n, nthreads=cores)
+        per_step = float(np.median(out["step_seconds"]))
+        kind, what = "reference", "reference acoustic_pml()" if c.pml else "reference acoustic()"
+    else:
+        t0 = time.perf_counter()
+        O.Oracle().acoustic_run(m, c.vp, 2 + nsteps, c.dt, c.f0, 0.0, c.src, c.pml, c.edge_size, c.pml_n,
+                                c.pml_n, nthreads=cores)
+        per_step = (time.perf_counter() - t0) / nsteps
+        kind, what = "port", "oracle port (set-up included)"
+    return {"value": N / per_step, "unit": "node-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{c.name}: {what}, {nsteps} time steps on {cores} host threads; median per-step time",
+            "seconds_per_step": per_step}
+
+
 def run_surrogate(args):
     """Config 5: FEM-generated training shots (Q4 128x128, GRF models, a
     source drawn along the surface, 64 receivers x 1000 samples), FNO training
@@ -405,8 +500,26 @@ def main():
     ap.add_argument("--infer-batch", type=int, default=64, help="surrogate shots per inference pass")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == "reference" and args.workload in ACOUSTIC_WORKLOADS:
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        c = P.acoustic_grf(**ACOUSTIC_WORKLOADS[args.workload])
+        cpu = acoustic_reference(c, nsteps=args.warmup + args.steps)
+        v = cpu["value"]
+        print(json.dumps({"impl": "reference", "metric": "node-steps/s", "value": v, "unit": "node-steps/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 / v * c.mesh.node_num, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": c.name, "nodes": c.mesh.node_num,
+                                     "time_steps_per_bench_step": 1},
+                          "cpu_baseline": cpu,
+                          "e2e": {"value": v, "unit": "node-steps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload in ACOUSTIC_WORKLOADS:
+        return run_acoustic(args)
     if args.workload == "surrogate_q4_128":
         return run_surrogate(args)
     if args.workload == "q4_16meshes":

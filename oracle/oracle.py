@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBSFO = os.path.join(HERE, "_build", "libsfo.so")
 LIBREF = os.path.join(HERE, "_ref", "libsfref.so")
+LIBACOUSTIC = os.path.join(HERE, "_ref", "libsfacoustic.so")
 
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -47,6 +48,24 @@ class _Problem(C.Structure):
     ]
 
 
+class _AcousticProblem(C.Structure):
+    _fields_ = [
+        ("type_code", C.c_int), ("node_num", C.c_int), ("element_num", C.c_int), ("order", C.c_int),
+        ("element_node", C.POINTER(C.c_int)),
+        ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)), ("vp", C.POINTER(C.c_double)),
+        ("step", C.c_int), ("dt", C.c_double), ("f0", C.c_double), ("t0", C.c_double),
+        ("source_node", C.c_int), ("pml", C.c_int),
+        ("edge_size", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+        ("ymax", C.c_double), ("pml_nx", C.c_int), ("pml_ny", C.c_int), ("nthreads", C.c_int),
+    ]
+
+
+def acoustic_snapshot_rows(step: int, pml: bool) -> int:
+    """Rows of u the reference's acoustic solvers print: the zero row, then
+    every 10 steps (acoustic.c:197) or 20 (acoustic_pml.c:448)."""
+    return snapshot_rows(step, 20 if pml else 10)
+
+
 def snapshot_rows(step: int, snap_every: int = 200) -> int:
     return 1 + sum(1 for it in range(2, step) if (it + 1) % snap_every == 0)
 
@@ -70,6 +89,9 @@ class Oracle:
         L.sfo_node_location.argtypes = [C.c_int, C.c_double, _f64p, _f64p, C.c_double, C.c_double]
         L.sfo_elastic_run.argtypes = [C.POINTER(_Problem)] + [C.c_void_p] * 6
         L.sfo_csr_matvec.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.sfo_acoustic_run.argtypes = [C.POINTER(_AcousticProblem), C.c_void_p, C.c_void_p]
+        L.sfo_abc_pml.argtypes = ([C.c_int, C.c_int, C.c_int, _i32p, _f64p, _f64p, C.c_int, C.c_int] +
+                                  [C.c_double] * 6 + [C.c_int] * 4 + [_f64p] * 4)
 
     # assembly -----------------------------------------------------------
     def mass_coo(self, mesh, rho):
@@ -162,6 +184,75 @@ class Oracle:
         out["status"] = rc
         out["setup_seconds"], out["loop_seconds"] = float(timing[0]), float(timing[1])
         return out
+
+
+    def abc_pml(self, mesh, pml_nx, pml_ny, h, bounds, vp_max, use=(1, 1, 1, 1)):
+        out = np.zeros((4, mesh.node_num))
+        self.lib.sfo_abc_pml(mesh.node_num, mesh.element_num, mesh.order, mesh.element_node, mesh.x, mesh.y,
+                             pml_nx, pml_ny, h, *bounds, vp_max, *use, out[0], out[1], out[2], out[3])
+        return out
+
+    def acoustic_run(self, mesh, vp, step, dt, f0, t0, source_node, pml=False, edge_size=0.0,
+                     pml_nx=0, pml_ny=0, nthreads: int = 0):
+        """The acoustic solvers (acoustic.c / acoustic_pml.c) restated:
+        {"snap": [rows][N], "energy": [step], "status"}."""
+        N = mesh.node_num
+        vp = np.ascontiguousarray(vp, np.float64)
+        rows = acoustic_snapshot_rows(step, pml)
+        snap, energy = np.zeros((rows, N)), np.zeros(step)
+        pb = _AcousticProblem(TYPE_CODES[mesh.type_name], N, mesh.element_num, mesh.order,
+                              _ptr(mesh.element_node, C.c_int), _ptr(mesh.x, C.c_double),
+                              _ptr(mesh.y, C.c_double), _ptr(vp, C.c_double), step, dt, f0, t0,
+                              source_node, int(bool(pml)), edge_size, mesh.xmin, mesh.xmax, mesh.ymin,
+                              mesh.ymax, pml_nx, pml_ny, nthreads)
+        rc = self.lib.sfo_acoustic_run(C.byref(pb), snap.ctypes.data, energy.ctypes.data)
+        return {"snap": snap, "energy": energy, "status": rc}
+
+
+class ReferenceAcoustic:
+    """The reference's acoustic solvers compiled in place (oracle/_ref)."""
+
+    def __init__(self, path: str = LIBACOUSTIC):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (reference not built here)")
+        L = self.lib = C.CDLL(path)
+        tail = [_f64p, _f64p, C.c_long, _f64p, C.c_long, C.POINTER(C.c_long), C.POINTER(C.c_long),
+                C.POINTER(C.c_double)]
+        head = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, _i32p, _f64p, _f64p, C.c_int,
+                C.c_double, C.c_double, C.c_double]
+        L.sfa_acoustic.argtypes = head + [C.c_int, C.c_char_p] + tail
+        L.sfa_acoustic_pml.argtypes = head + [C.c_double] * 5 + [C.c_int] * 3 + [C.c_char_p] + tail
+        L.sfa_set_step_times.argtypes = [C.c_void_p, C.c_long]
+
+    def run(self, mesh, vp, step, dt, f0, t0, source_node, pml=False, edge_size=0.0, pml_nx=0, pml_ny=0,
+            nthreads: int = 0, solver: str = "masslump", workdir: str | None = None):
+        """{"snap": [rows][N] (rows printed so far), "energy": [step],
+        "energy_values", "status", "seconds"}; status 0, 1 (exit on the energy
+        bound), 3 (unknown solver)."""
+        N = mesh.node_num
+        rows = acoustic_snapshot_rows(step, pml)
+        snap, energy = np.zeros(rows * N), np.zeros(step)
+        ns, ne, secs = C.c_long(), C.c_long(), C.c_double()
+        tmp = workdir or tempfile.mkdtemp(prefix="sfacoustic_")
+        vp = np.ascontiguousarray(vp, np.float64)
+        common = (tmp.encode(), nthreads, mesh.type_name.encode(), N, mesh.element_num, mesh.order,
+                  mesh.element_node, mesh.x, mesh.y, step, dt, f0, t0)
+        outs = (vp, snap, snap.size, energy, energy.size, C.byref(ns), C.byref(ne), C.byref(secs))
+        stamps = np.zeros(step)
+        self.lib.sfa_set_step_times(stamps.ctypes.data, step)
+        try:
+            if pml:
+                rc = self.lib.sfa_acoustic_pml(*common, edge_size, mesh.xmin, mesh.xmax, mesh.ymin, mesh.ymax,
+                                               pml_nx, pml_ny, source_node, solver.encode(), *outs)
+            else:
+                rc = self.lib.sfa_acoustic(*common, source_node, solver.encode(), *outs)
+        finally:
+            self.lib.sfa_set_step_times(None, 0)
+        # seconds of each completed time step (from its energy.dat write)
+        step_seconds = np.diff(stamps[1:ne.value]) if ne.value > 2 else np.zeros(0)
+        return {"snap": snap.reshape(rows, N)[:ns.value // N], "energy": energy[:ne.value],
+                "energy_values": ne.value, "status": rc, "seconds": secs.value, "step_seconds": step_seconds,
+                "workdir": tmp}
 
 
 class Reference:

@@ -919,3 +919,190 @@ int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,
 #endif
     return status;
 }
+
+/* ------------------------------------------------------ scalar acoustics */
+
+void sfo_abc_pml(int node_num, int element_num, int order, const int *element_node,
+                 const double *x, const double *y, int pml_nx, int pml_ny, double h,
+                 double xmin, double xmax, double ymin, double ymax, double vp_max,
+                 int use_xmin, int use_xmax, int use_ymin, int use_ymax,
+                 double *pdx, double *pdy, double *pdxx, double *pdyy)
+{
+    /* pml/abc_pml.c:41-103: classical quadratic profile per axis, written for
+     * every node of every element (nodes of no element are zeroed here) */
+    const double Rcoef = 0.0001;
+    const double tx = h * pml_nx, ty = h * pml_ny;
+    const double x0 = xmin + tx, x1 = xmax - tx, y0 = ymin + ty, y1 = ymax - ty;
+    const double d0x = 3.0 * vp_max * log10(1.0 / Rcoef) / (2.0 * tx);
+    const double d0y = 3.0 * vp_max * log10(1.0 / Rcoef) / (2.0 * ty);
+    for (int i = 0; i < node_num; i++) pdx[i] = pdy[i] = pdxx[i] = pdyy[i] = 0.0;
+    for (long long k = 0; k < (long long)element_num * order; k++) {
+        const int p = element_node[k] - 1;
+        const double X = x[p], Y = y[p];
+        if (X <= x0 && use_xmin == 1) {
+            pdx[p] = d0x * ((x0 - X) / tx) * ((x0 - X) / tx);
+            pdxx[p] = -d0x * 2 * (x0 - X) / (tx * tx);
+        } else if (X >= x1 && use_xmax == 1) {
+            pdx[p] = d0x * ((X - x1) / tx) * ((X - x1) / tx);
+            pdxx[p] = d0x * 2 * (X - x1) / (tx * tx);
+        } else {
+            pdx[p] = 0.0;
+            pdxx[p] = 0.0;
+        }
+        if (Y <= y0 && use_ymin == 1) {
+            pdy[p] = d0y * ((y0 - Y) / ty) * ((y0 - Y) / ty);
+            pdyy[p] = -d0y * 2 * (y0 - Y) / (ty * ty);
+        } else if (Y >= y1 && use_ymax == 1) {
+            pdy[p] = d0y * ((Y - y1) / ty) * ((Y - y1) / ty);
+            pdyy[p] = d0y * 2 * (Y - y1) / (ty * ty);
+        } else {
+            pdy[p] = 0.0;
+            pdyy[p] = 0.0;
+        }
+    }
+}
+
+int sfo_acoustic_snapshot_rows(int step, int pml)
+{
+    /* acoustic.c:147-154,197-205 (every 10 steps) and acoustic_pml.c:260-268,
+     * 448-455 (every 20), after the zero row */
+    return sfo_snapshot_rows(step, pml ? 20 : 10);
+}
+
+int sfo_acoustic_run(const sfo_acoustic_problem *pb, double *snap, double *energy)
+{
+    /* time_evolution/acoustic.c:1-223 (pml == 0) and
+     * time_evolution/acoustic_pml.c:3-485 (pml == 1), solver "masslump".
+     * The mass matrices carry no density (the files call mass_sparse_all
+     * without rho): M = integral phi_i phi_j, lumped as in mass_sparse_q4.c. */
+    const int N = pb->node_num, E = pb->element_num, P = pb->order, tc = pb->type_code;
+    if (N <= 0 || E <= 0 || sfo_element_order(tc) != P || pb->step < 3) return 2;
+    if (pb->source_node < -1 || pb->source_node >= N) return 2;
+#ifdef _OPENMP
+    int saved_threads = omp_get_max_threads();
+    if (pb->nthreads > 0) omp_set_num_threads(pb->nthreads);
+#endif
+    const long long nnz = (long long)E * P * P;
+    const double dt = pb->dt;
+    const double *vp = pb->vp;
+    double *ones = (double *)malloc(sizeof(double) * N);
+    for (int i = 0; i < N; i++) ones[i] = 1.0;
+    double *mass_lump = (double *)malloc(sizeof(double) * N);
+    int *ci = (int *)malloc(sizeof(int) * nnz), *cj = (int *)malloc(sizeof(int) * nnz);
+    double *cx = (double *)malloc(sizeof(double) * nnz);
+    int bad = sfo_mass_lumped(tc, N, E, pb->element_node, pb->x, pb->y, ones, mass_lump);
+    csr_t M = {0}, K[4] = {{0}};
+    /* acoustic.c:95-98: K0; acoustic_pml.c:183-187: K1, K5, K2, K6 */
+    const int types_pml[4] = {1, 5, 2, 6};
+    const int nk = pb->pml ? 4 : 1;
+    if (!bad) bad = sfo_mass_coo(tc, N, E, pb->element_node, pb->x, pb->y, ones, ci, cj, cx);
+    if (!bad) build_csr((int)nnz, N + 1, ci, cj, cx, &M);
+    for (int k = 0; k < nk && !bad; k++) {
+        bad = sfo_stif_coo(tc, pb->pml ? types_pml[k] : 0, N, E, pb->element_node, pb->x, pb->y, ci, cj, cx);
+        if (!bad) build_csr((int)nnz, N + 1, ci, cj, cx, &K[k]);
+    }
+    free(ci); free(cj); free(cx); free(ones);
+    int status = bad ? 3 : 0;
+    double *pdx = NULL, *pdy = NULL, *pdxx = NULL, *pdyy = NULL;
+    double *buf = NULL;
+    int srow = 0;
+    if (!bad && !pb->pml) {
+        /* acoustic.c:124-207 */
+        buf = (double *)calloc((size_t)6 * N, sizeof(double));
+        double *u_old = buf, *u_now = buf + N, *y1 = buf + 2 * (size_t)N, *y2 = buf + 3 * (size_t)N,
+               *y3 = buf + 4 * (size_t)N, *rhs = buf + 5 * (size_t)N;
+        if (snap) memcpy(snap + (size_t)srow++ * N, u_old, sizeof(double) * N);
+        if (energy) energy[0] = energy[1] = 0.0;
+        for (int it = 2; it < pb->step; it++) {
+            const double time = (it + 1) * dt;
+            const double ps = sfo_ricker(pb->f0, pb->t0, 1.0, time);
+            sfo_csr_matvec(N + 1, K[0].p, K[0].j, K[0].x, u_now, y1);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u_now, y2);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u_old, y3);
+            for (int i = 0; i < N; i++) {
+                rhs[i] = (i == pb->source_node) * ps - vp[i] * vp[i] * dt * dt * y1[i] + 2.0 * y2[i] - y3[i];
+                u_old[i] = u_now[i];
+            }
+            for (int i = 0; i < N; i++)
+                if (mass_lump[i] != 0.0) u_now[i] = rhs[i] / (1.0 * mass_lump[i]);
+            double e = 0.0;
+            for (int i = 0; i < N; i++) e += u_now[i] * u_now[i];
+            if (energy) energy[it] = e;
+            if ((it + 1) % 10 == 0 && snap) memcpy(snap + (size_t)srow++ * N, u_now, sizeof(double) * N);
+        }
+    } else if (!bad) {
+        /* acoustic_pml.c:170-178 (vp_max), 178-179 (profiles), 270-456 */
+        double vp_max = vp[0];
+        for (int i = 0; i < N; i++) if (vp[i] > vp_max) vp_max = vp[i];
+        pdx = (double *)malloc(sizeof(double) * N); pdy = (double *)malloc(sizeof(double) * N);
+        pdxx = (double *)malloc(sizeof(double) * N); pdyy = (double *)malloc(sizeof(double) * N);
+        sfo_abc_pml(N, E, P, pb->element_node, pb->x, pb->y, pb->pml_nx, pb->pml_ny, pb->edge_size,
+                    pb->xmin, pb->xmax, pb->ymin, pb->ymax, vp_max, 1, 1, 1, 1, pdx, pdy, pdxx, pdyy);
+        buf = (double *)calloc((size_t)15 * N, sizeof(double));
+        double *u_now = buf, *u1_old = buf + N, *u1_now = buf + 2 * (size_t)N, *u2_old = buf + 3 * (size_t)N,
+               *u2_now = buf + 4 * (size_t)N, *p1_now = buf + 5 * (size_t)N, *p2_now = buf + 6 * (size_t)N,
+               *y1 = buf + 7 * (size_t)N, *y2 = buf + 8 * (size_t)N, *y3 = buf + 9 * (size_t)N,
+               *y4 = buf + 10 * (size_t)N, *rhs1 = buf + 11 * (size_t)N, *rhs2 = buf + 12 * (size_t)N,
+               *rhs3 = buf + 13 * (size_t)N, *rhs4 = buf + 14 * (size_t)N;
+        const csr_t *K1 = &K[0], *K5 = &K[1], *K2 = &K[2], *K6 = &K[3];
+        if (snap) memcpy(snap + (size_t)srow++ * N, u_now, sizeof(double) * N);
+        if (energy) energy[0] = energy[1] = 0.0;
+        for (int it = 2; it < pb->step; it++) {
+            const double time = (it + 1) * dt;
+            const double ps = sfo_ricker(pb->f0, pb->t0, 1.0, time);
+            /* equation 1 (:289-306) */
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u1_now, y1);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u1_old, y2);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, p1_now, y3);
+            sfo_csr_matvec(N + 1, K1->p, K1->j, K1->x, u_now, y4);
+            for (int i = 0; i < N; i++)
+                rhs1[i] = 2.0 * y1[i] - y2[i] - 2.0 * dt * pdx[i] * y1[i] + 2 * dt * pdx[i] * y2[i]
+                        - dt * dt * pdx[i] * pdx[i] * y1[i] + vp[i] * vp[i] * dt * dt * y4[i]
+                        + vp[i] * vp[i] * dt * dt * y3[i] + (i == pb->source_node) * ps;
+            /* equation 2 (:308-320) */
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, p1_now, y1);
+            sfo_csr_matvec(N + 1, K5->p, K5->j, K5->x, u_now, y2);
+            for (int i = 0; i < N; i++) rhs2[i] = y1[i] - dt * pdx[i] * y1[i] - dt * pdxx[i] * y2[i];
+            /* equation 3 (:322-339) */
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u2_now, y1);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, u2_old, y2);
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, p2_now, y3);
+            sfo_csr_matvec(N + 1, K2->p, K2->j, K2->x, u_now, y4);
+            for (int i = 0; i < N; i++)
+                rhs3[i] = 2.0 * y1[i] - y2[i] - 2.0 * dt * pdy[i] * y1[i] + 2 * dt * pdy[i] * y2[i]
+                        - dt * dt * pdy[i] * pdy[i] * y1[i] + vp[i] * vp[i] * dt * dt * y4[i]
+                        + vp[i] * vp[i] * dt * dt * y3[i];
+            /* equation 4 (:341-353) */
+            sfo_csr_matvec(N + 1, M.p, M.j, M.x, p2_now, y1);
+            sfo_csr_matvec(N + 1, K6->p, K6->j, K6->x, u_now, y2);
+            for (int i = 0; i < N; i++) rhs4[i] = y1[i] - dt * pdy[i] * y1[i] - dt * pdyy[i] * y2[i];
+            /* :355-375 */
+            for (int i = 0; i < N; i++) { u1_old[i] = u1_now[i]; u2_old[i] = u2_now[i]; }
+            for (int i = 0; i < N; i++)
+                if (mass_lump[i] != 0.0) {
+                    u1_now[i] = rhs1[i] / (1.0 * mass_lump[i]);
+                    p1_now[i] = rhs2[i] / (1.0 * mass_lump[i]);
+                    u2_now[i] = rhs3[i] / (1.0 * mass_lump[i]);
+                    p2_now[i] = rhs4[i] / (1.0 * mass_lump[i]);
+                }
+            /* :432-447: the run ends as soon as the running sum passes 1e7 */
+            double e = 0.0;
+            int blow = 0;
+            for (int i = 0; i < N; i++) {
+                u_now[i] = u1_now[i] + u2_now[i];
+                e += u_now[i] * u_now[i];
+                if (e > 10e6) { blow = 1; break; }
+            }
+            if (blow) { status = 1; break; }
+            if (energy) energy[it] = e;
+            if ((it + 1) % 20 == 0 && snap) memcpy(snap + (size_t)srow++ * N, u_now, sizeof(double) * N);
+        }
+    }
+    free(buf); free(pdx); free(pdy); free(pdxx); free(pdyy); free(mass_lump);
+    free(M.p); free(M.j); free(M.x);
+    for (int k = 0; k < 4; k++) { free(K[k].p); free(K[k].j); free(K[k].x); }
+#ifdef _OPENMP
+    omp_set_num_threads(saved_threads);
+#endif
+    return status;
+}

@@ -108,6 +108,35 @@ int sfo_snapshot_rows(int step, int snap_every);
 void sfo_csr_matvec(int p_size, const int *Bp, const int *Bj, const double *Bx,
                     const double *x, double *y);
 
+/* Scalar acoustic solvers (time_evolution/acoustic.c, acoustic_pml.c),
+ * solver "masslump", geometric mass matrix (no density).
+ *   snap:   [sfo_acoustic_snapshot_rows(step, pml)][node_num]: the zero row,
+ *           then u after every step with (it + 1) % 10 == 0 (20 with PML)
+ *   energy: [step] sum of u^2 per step (entries 0 and 1 are 0)
+ * Returns 0; 1 when acoustic_pml's energy bound (1e7) ended the run (the
+ * outputs keep what was written before that step); 2 on bad input; 3 on a
+ * zero-area element. */
+typedef struct {
+    int type_code, node_num, element_num, order;
+    const int *element_node;
+    const double *x, *y;
+    const double *vp;
+    int step; double dt, f0, t0;
+    int source_node;        /* 0-based; -1: no source */
+    int pml;                /* 0: acoustic.c, 1: acoustic_pml.c (PML on four sides) */
+    double edge_size, xmin, xmax, ymin, ymax;
+    int pml_nx, pml_ny;
+    int nthreads;
+} sfo_acoustic_problem;
+
+int sfo_acoustic_run(const sfo_acoustic_problem *pb, double *snap, double *energy);
+int sfo_acoustic_snapshot_rows(int step, int pml);
+void sfo_abc_pml(int node_num, int element_num, int order, const int *element_node,
+                 const double *x, const double *y, int pml_nx, int pml_ny, double h,
+                 double xmin, double xmax, double ymin, double ymax, double vp_max,
+                 int use_xmin, int use_xmax, int use_ymin, int use_ymax,
+                 double *pdx, double *pdy, double *pdxx, double *pdyy);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,16 @@ class Stats_(C.Structure):
                 ("interior_rows", C.c_int), ("pml_rows", C.c_int), ("value_tuples", C.c_int)]
 
 
+class AcousticDesc_(C.Structure):
+    _fields_ = [("pml", C.c_int), ("step", C.c_int), ("dt", C.c_double), ("f0", C.c_double), ("t0", C.c_double),
+                ("source_node", C.c_int), ("mass_lump", C.c_void_p)]
+
+
+class AcousticStats_(C.Structure):
+    _fields_ = [("setup_ms", C.c_double), ("loop_ms", C.c_double), ("union_nnz", C.c_longlong),
+                ("csr_nnz", C.c_longlong * 5), ("kernel_launches", C.c_int), ("blowup_step", C.c_int)]
+
+
 _LIB = None
 
 # every symbol the header declares (checked by the CPU test suite)
@@ -65,6 +75,8 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec", "sfg_node_location",
            "sfg_abc_mpml_device_noalloc", "sfg_plan_create_models", "sfg_run_models", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
            "sfg_group_destroy",
+           # scalar acoustic solvers (include/seisfem_acoustic.h)
+           "sfg_acoustic_snapshot_rows", "sfg_acoustic_run", "acoustic", "acoustic_pml",
            # learned surrogate (include/seisfem_fno.h)
            "sfg_fno_gemm", "sfg_fno_dft_combine", "sfg_fno_dft_combine_bwd", "sfg_fno_expand_weights",
            "sfg_fno_fold_weights", "sfg_fno_gelu_bwd", "sfg_fno_cast_bf16", "sfg_fno_bias_grad", "sfg_fno_swap01",
@@ -119,6 +131,9 @@ def lib(path: str = LIBPATH):
     L.sfg_abc_mpml.argtypes = ([C.c_int, C.c_int, C.c_int, _i32p, C.c_void_p, C.c_int, C.c_int] +
                                [C.c_double] * 6 + [C.c_int] * 4 + [_f64p] * 6)
     L.sfg_csr_matvec.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    L.sfg_acoustic_snapshot_rows.argtypes = [C.c_int, C.c_int]
+    L.sfg_acoustic_run.argtypes = [C.c_void_p, C.POINTER(Mesh_), C.c_void_p, C.POINTER(AcousticDesc_),
+                                   C.c_void_p, C.c_void_p, C.POINTER(AcousticStats_)]
     _LIB = L
     return L
 
@@ -185,6 +200,33 @@ class Context:
         self._check(self.L.sfg_setup(self.ptr, C.byref(mesh), C.byref(model)))
         self.node_num = m.node_num
         return self
+
+    def acoustic_run(self, mesh, vp, step: int, dt: float, f0: float, t0: float, source_node: int,
+                     pml: bool = False, edge_size: float = 0.0, pml_nx: int = 0, pml_ny: int = 0,
+                     mass_lump=None, snapshots: bool = True) -> dict:
+        """The scalar acoustic solvers (time_evolution/acoustic.c, acoustic_pml.c)
+        on the GPU: {"snap": [rows][N] or None, "energy": [step], "status",
+        "stats"}.  ``mesh`` is a problem.Mesh; ``mass_lump`` (optional) replaces
+        the lumped mass assembled on the GPU.  A run that the PML solver's
+        energy bound ends returns status SFG_ERR_BLOWUP with the outputs
+        written before it."""
+        en, x, y = (np.ascontiguousarray(a) for a in (mesh.element_node, mesh.x, mesh.y))
+        vp = np.ascontiguousarray(vp, np.float64)
+        tname = mesh.type_name.encode()
+        md = Mesh_(tname, mesh.node_num, mesh.element_num, mesh.order, en.ctypes.data, x.ctypes.data,
+                   y.ctypes.data, mesh.xmin, mesh.xmax, mesh.ymin, mesh.ymax, edge_size, pml_nx, pml_ny, 0)
+        ml = None if mass_lump is None else np.ascontiguousarray(mass_lump, np.float64)
+        desc = AcousticDesc_(int(bool(pml)), step, dt, f0, t0, source_node, None if ml is None else ml.ctypes.data)
+        rows = self.L.sfg_acoustic_snapshot_rows(step, int(bool(pml)))
+        snap = np.zeros((rows, mesh.node_num)) if snapshots else None
+        energy = np.zeros(step)
+        st = AcousticStats_()
+        rc = self._check(self.L.sfg_acoustic_run(self.ptr, C.byref(md), vp.ctypes.data, C.byref(desc),
+                                                 None if snap is None else snap.ctypes.data, energy.ctypes.data,
+                                                 C.byref(st)), allow=(SFG_ERR_BLOWUP,))
+        stats = {k: getattr(st, k) for k, _ in AcousticStats_._fields_}
+        stats["csr_nnz"] = list(st.csr_nnz)
+        return {"snap": snap, "energy": energy, "status": rc, "stats": stats}
 
     def csr(self, matrix: int):
         n = C.c_int()

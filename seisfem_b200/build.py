@@ -30,7 +30,9 @@ UNITS = {
     "sfg_fno.cu": [],
     "sfg_dict.cu": [],
     "sfg_locate.cu": ["-fmad=false"],
+    "sfg_acoustic.cu": ["-fmad=false"],
 }
+C_UNITS = ["elastic_wave_dropin.c", "acoustic_dropin.c"]
 
 
 def _nvcc() -> str:
@@ -67,7 +69,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers += [os.path.join(HERE, "..", "include", f) for f in ("seisfem_b200.h", "seisfem_fno.h")]
+    headers += [os.path.join(HERE, "..", "include", f) for f in ("seisfem_b200.h", "seisfem_fno.h", "seisfem_acoustic.h")]
     objs = []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
@@ -78,11 +80,12 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             _run(cmd, verbose or ptxas_info)
-    csrc = os.path.join(CSRC, "elastic_wave_dropin.c")
-    cobj = os.path.join(BUILD, "elastic_wave_dropin.o")
-    objs.append(cobj)
-    if force or _stale(cobj, [csrc] + headers):
-        _run([_cc(), "-O2", "-fPIC", "-std=gnu11", "-Wall", "-c", csrc, "-o", cobj], verbose)
+    for unit in C_UNITS:
+        csrc = os.path.join(CSRC, unit)
+        cobj = os.path.join(BUILD, unit.replace(".c", ".o"))
+        objs.append(cobj)
+        if force or _stale(cobj, [csrc] + headers):
+            _run([_cc(), "-O2", "-fPIC", "-std=gnu11", "-Wall", "-c", csrc, "-o", cobj], verbose)
     if force or _stale(OUT, objs):
         _run([nvcc, *ARCH, "-shared", "-o", OUT, *objs, "-cudart", "static"], verbose)
     return OUT

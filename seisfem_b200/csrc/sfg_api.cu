@@ -1284,3 +1284,13 @@ int sfg_sync(sfg_ctx *ctx)
 }
 
 }  // extern "C"
+
+// ------------------------------------------- context access for other units
+namespace sfg {
+
+int ctx_device(const sfg_ctx *c) { return c->device; }
+cudaStream_t ctx_stream(const sfg_ctx *c) { return c->stream; }
+int ctx_fail(sfg_ctx *c, int code, const std::string &msg) { return fail(c, code, msg); }
+double ricker_amplitude(double f0, double t0, double mag, double t) { return ricker(f0, t0, mag, t); }
+
+}  // namespace sfg

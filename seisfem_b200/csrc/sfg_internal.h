@@ -132,6 +132,13 @@ int build_step_data(DevProblem &P, const double *d_c, double dt_unused, std::str
 struct RunBuffers;
 struct StepLaunch;
 
+// ---- context access for units other than sfg_api.cu ----------------------
+int ctx_device(const sfg_ctx *c);
+cudaStream_t ctx_stream(const sfg_ctx *c);
+int ctx_fail(sfg_ctx *c, int code, const std::string &msg);   // records msg, returns code
+// Ricker wavelet, source_receiver/seismic_source.c:16-24
+double ricker_amplitude(double f0, double t0, double mag, double t);
+
 }  // namespace sfg
 
 namespace sfg {

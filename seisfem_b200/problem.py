@@ -370,3 +370,26 @@ def config_3b(count: int = 16, lo: int = 100, hi: int = 600, seed: int = 4, h: f
         rec = locate(mesh, h, line_points(nrec, (xr, pml * h), (xr, L - pml * h)))
         probs.append(Problem(mesh, model, step, 1e-3, f0, 0.0, h, pml, pml, src, rec, 0, f"config3b_q4_{n}"))
     return probs
+
+
+class AcousticCase:
+    """A scalar acoustic run (time_evolution/acoustic.c / acoustic_pml.c):
+    mesh, vp per node, source node and loop parameters."""
+
+    def __init__(self, mesh, vp, src, step, dt, f0, pml, edge_size, pml_n, name):
+        self.mesh, self.vp, self.src, self.step, self.dt, self.f0 = mesh, vp, src, step, dt, f0
+        self.pml, self.edge_size, self.pml_n, self.name = pml, edge_size, pml_n, name
+
+
+def acoustic_grf(n: int = 800, h: float = 10.0, step: int = 1002, dt: float = 5e-4, pml: bool = True,
+                 pml_n: int = 20, seed: int = 6) -> AcousticCase:
+    """Q4 n x n elements, GRF vp (mean 3000 m/s, std 400, correlation length
+    200 m, clipped to 1800-4500, seeded), 20 Hz Ricker source at the centre,
+    classical PML pml_n elements thick on four sides; dt keeps vp dt / h at
+    or below 0.225."""
+    L = n * h
+    mesh = structured_mesh("Q4", n, n, 0.0, L, 0.0, L)
+    vp = gaussian_random_field((n + 1, n + 1), h, 200.0, 3000.0, 400.0, 1800.0, 4500.0, seed).ravel()
+    src = locate(mesh, h, [(L / 2, L / 2)])[0]
+    kind = "pml" if pml else "plain"
+    return AcousticCase(mesh, vp, int(src), step, dt, 20.0, pml, h, pml_n, f"acoustic_{kind}_q4_{n}")

@@ -6,12 +6,17 @@ reference sources are available; the fixtures travel, the reference does not).
                   M-PML profiles (oracle/_ref, compiled from the reference's C)
   runs_small.npz  small complete elastic_wave() runs of the reference (FP64
                   seismograms and snapshots captured from its output calls)
+  acoustic_small.npz  small runs of the reference's scalar acoustic solvers
+                  (time_evolution/acoustic.c and acoustic_pml.c, compiled in
+                  place by oracle/ref_acoustic_harness.c): u snapshots and
+                  energy per step, with the seeded vp, the lumped mass of
+                  density 1 and the canonical CSR of stiffness type 0
   examples.npz    subsets of the reference's committed EXAMPLE outputs
                   (example 2: Q4 internal mesh, snapshots; example 6: T3
                   exterior mesh with a free surface, seismograms) and the mesh
                   of example 6 (its input files)
 
-Usage: make -C oracle && python tests/golden/make_golden.py
+Usage: make -C oracle && python tests/golden/make_golden.py [acoustic]
 """
 from __future__ import annotations
 
@@ -27,7 +32,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 REF = os.environ.get("SEISFEM_REFERENCE", "/root/reference")
 
-from oracle import Reference  # noqa: E402
+from oracle import Reference, ReferenceAcoustic  # noqa: E402
 from seisfem_b200.problem import small_problem, structured_mesh  # noqa: E402
 
 
@@ -62,6 +67,40 @@ def runs_small(R):
     np.savez_compressed(os.path.join(HERE, "runs_small.npz"), **out)
 
 
+# (type, nx, ny, step, dt, pml, seed): Q9 and T6 with PML, and T6 without,
+# exceed the reference's own energy bound / grow without bound -- kept, the
+# outputs before that point are the fixture.  Without PML every mesh has at
+# least `step` nodes: acoustic.c sizes its energy array by the node count.
+ACOUSTIC_RUNS = [("Q4", 16, 12, 202, 1e-3, 0, 21), ("Q4", 16, 12, 202, 1e-3, 1, 22),
+                 ("T3", 16, 14, 202, 1e-3, 0, 23), ("T3", 14, 12, 202, 1e-3, 1, 24),
+                 ("Q9", 8, 6, 202, 5e-4, 0, 25), ("Q9", 8, 6, 202, 5e-4, 1, 26),
+                 ("T6", 8, 6, 62, 5e-4, 0, 27), ("T6", 8, 6, 202, 5e-4, 1, 28)]
+
+
+def acoustic_case(t, nx, ny, seed):
+    """Mesh, vp and source node of one acoustic fixture case (also used by the tests)."""
+    m = structured_mesh(t, nx, ny, 0.0, 10.0 * nx, 0.0, 10.0 * ny)
+    rng = np.random.default_rng(seed)
+    vp = 1800.0 + 400.0 * rng.random(m.node_num)
+    src = int(np.argmin((m.x - 5.0 * nx) ** 2 + (m.y - 5.0 * ny) ** 2))
+    return m, vp, src
+
+
+def acoustic_small(R, RA):
+    out = {}
+    for t, nx, ny, step, dt, pml, seed in ACOUSTIC_RUNS:
+        m, vp, src = acoustic_case(t, nx, ny, seed)
+        r = RA.run(m, vp, step, dt, 25.0, 0.0, src, bool(pml), 10.0, 3, 3, nthreads=4)
+        key = f"{t}_{'pml' if pml else 'plain'}"
+        out[key + "_snap"], out[key + "_energy"] = r["snap"], r["energy"]
+        out[key + "_status"] = np.int32(r["status"])
+        out[key + "_lump"] = R.mass(m, np.ones(m.node_num), 1)
+        if not pml:
+            Bp, Bj, Bx = R.coo2csr(m.node_num, *R.stif(m, 0))
+            out[key + "_k0_p"], out[key + "_k0_j"], out[key + "_k0_x"] = Bp, Bj, Bx
+    np.savez_compressed(os.path.join(HERE, "acoustic_small.npz"), **out)
+
+
 def read_rows(path, stride=1, max_rows=None):
     rows = []
     with open(path) as f:
@@ -93,8 +132,11 @@ def examples():
 
 if __name__ == "__main__":
     R = Reference()
-    csr_small(R)
-    runs_small(R)
-    examples()
-    for f in ("csr_small.npz", "runs_small.npz", "examples.npz"):
+    only_acoustic = sys.argv[1:] == ["acoustic"]
+    if not only_acoustic:
+        csr_small(R)
+        runs_small(R)
+        examples()
+    acoustic_small(R, ReferenceAcoustic())
+    for f in ("csr_small.npz", "runs_small.npz", "examples.npz", "acoustic_small.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
