@@ -181,3 +181,12 @@ def test_example6_free_surface_seismograms(oracle):
     assert su.shape == gu.shape
     assert np.abs(su - gu).max() <= 6e-7
     assert np.abs(r["seis_w"][0][::10] - g["ex6_seis_w"]).max() <= 6e-7
+
+
+@pytest.mark.parametrize("etype", ["T3", "T6", "Q4", "Q9"])
+def test_structured_mesh_matches_reference_mesher(reference, etype):
+    # mesh/mesh_element.c and mesh/mesh_xy.c (seisfem.c:216-232), compiled in place
+    m = structured_mesh(etype, 7, 5, 0.0, 70.0, -10.0, 40.0)
+    en, x, y = reference.mesh(etype, 7, 5, 0.0, 70.0, -10.0, 40.0)
+    assert np.array_equal(m.element_node, en)
+    assert np.array_equal(m.x, x) and np.array_equal(m.y, y)
