@@ -112,6 +112,21 @@ def test_batched_launch_shapes_agree(ctx, oracle, shape_a, monkeypatch):
         assert rel_l2(batched[k], single[k]) < 1e-5, k
 
 
+@pytest.mark.parametrize("variant_a", range(6))
+def test_single_shot_launch_shapes_agree(ctx, oracle, variant_a, monkeypatch):
+    """Every launch shape of the one-shot class-A kernel (threads per block
+    and minimum resident blocks of its launch bounds) against the FP64
+    oracle."""
+    p = small_problem("Q9", n=20, step=302, pml=4, seed=23)
+    ctx.setup(p)
+    monkeypatch.setenv("SFG_SHAPE_A", str(variant_a))
+    monkeypatch.setenv("SFG_SHAPE_Z", "3")
+    out = ctx.run(p, precision="fp32k", want_snapshots=True)
+    ref = oracle.run(p)
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(out[k], ref[k]) < FP32_TOL, k
+
+
 def test_blowup_detected_like_reference(ctx, oracle):
     p = small_problem("T6", n=16, step=260, pml=4, seed=7)   # dt too large for T6: the energy bound trips
     ref = oracle.run(p)
