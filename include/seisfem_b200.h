@@ -40,6 +40,7 @@ extern "C" {
 #define SFG_ERR_TIMEOUT 9     /* a bounded device-side wait gave up */
 #define SFG_ERR_NODEVICE 10   /* no CUDA device / wrong architecture */
 #define SFG_ERR_LIMIT 11      /* size above the fixed limit of a no-allocation entry point */
+#define SFG_ERR_NOCONV 12     /* a consistent-mass solve did not converge in its iterations */
 
 /* ------------------------------------------------------------- precision */
 #define SFG_FP32_KAHAN 0      /* FP32 step, Kahan-compensated displacement (default) */
@@ -48,6 +49,11 @@ extern "C" {
 #define SFG_FP32_PLAIN_PATH 3 /* FP32, one SpMV launch per product + pointwise
                                  kernels, as elastic_wave.c structures the step
                                  (the unfused baseline) */
+#define SFG_FP64_CONSISTENT 4 /* FP64 step with the consistent mass matrix: the 14 right-hand
+                                 sides solved with M (solver "pardiso" / "mgmres",
+                                 elastic_wave.c:664-680, 730-746) by Jacobi-preconditioned
+                                 conjugate gradients to 1e-12 relative residual; one shot at
+                                 a time, no Dirichlet zeroing (as the reference's branch) */
 
 /* matrices: 0 = consistent mass M, 1..6 = stiffness types 1..6
  * (elastic_wave.c:6-17; stif type 0 is not on the path) */
@@ -81,7 +87,8 @@ typedef struct {
     double dt, f0, t0;
     int src_num;  const int *src_node;   /* 0-based node per shot */
     int rec_num;  const int *rec_node;   /* 0-based node per receiver */
-    int precision;             /* SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH */
+    int precision;             /* SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH,
+                                  SFG_FP64_CONSISTENT */
     int snap_every;            /* 0: no snapshots; 200 reproduces the reference */
     int shots_per_batch;       /* shots advanced together; 0 = automatic */
 } sfg_run_desc;

@@ -44,7 +44,7 @@ class _Problem(C.Structure):
         ("src_num", C.c_int), ("src_node", C.POINTER(C.c_int)),
         ("rec_num", C.c_int), ("rec_node", C.POINTER(C.c_int)),
         ("free_surface", C.c_int), ("snap_every", C.c_int), ("nthreads", C.c_int),
-        ("timing", C.POINTER(C.c_double)),
+        ("timing", C.POINTER(C.c_double)), ("consistent", C.c_int),
     ]
 
 
@@ -154,8 +154,11 @@ class Oracle:
         return y
 
     # time loop ------------------------------------------------------------
-    def run(self, prob, snap_every: int = 200, nthreads: int = 0, energy: bool = False):
-        """FP64 elastic_wave() run; returns dict of seismograms/snapshots."""
+    def run(self, prob, snap_every: int = 200, nthreads: int = 0, energy: bool = False,
+            solver: str = "masslump"):
+        """FP64 elastic_wave() run; returns dict of seismograms/snapshots.
+        solver "masslump", or "mgmres" / "pardiso": the consistent-mass branch
+        (the systems solved with M by Jacobi-preconditioned CG)."""
         m = prob.mesh
         S, R, N, step = len(prob.src_node), len(prob.rec_node), m.node_num, prob.step
         ns = snapshot_rows(step, snap_every)
@@ -176,7 +179,7 @@ class Oracle:
             step, prob.dt, prob.f0, prob.t0, prob.edge_size,
             m.xmin, m.xmax, m.ymin, m.ymax, prob.pml_nx, prob.pml_ny,
             S, _ptr(prob.src_node, C.c_int), R, _ptr(prob.rec_node, C.c_int),
-            prob.free_surface, snap_every, nthreads, _ptr(timing, C.c_double))
+            prob.free_surface, snap_every, nthreads, _ptr(timing, C.c_double), int(solver != "masslump"))
         ptrs = [out[k].ctypes.data for k in ("seis_u", "seis_w", "snap_u", "snap_w")]
         ptrs += [out["energy_u"].ctypes.data, out["energy_w"].ctypes.data] if energy else [None, None]
         rc = self.lib.sfo_elastic_run(C.byref(pb), *ptrs)

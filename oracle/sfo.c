@@ -694,6 +694,47 @@ static int build_csr(int nnz, int p_size, const int *ci, const int *cj, const do
     return m->nnz;
 }
 
+/* M x = b by conjugate gradients with the Jacobi preconditioner (M is
+ * symmetric positive definite), x holding the first guess; stops when
+ * |r| <= 1e-12 |b| (or |r|^2 <= 1e-200).  work: 4 * n doubles.  Returns 0,
+ * or 1 after 1000 iterations without convergence.  It stands in for the
+ * reference's PARDISO (direct) and restarted GMRES + ILU (tolerance 1e-8)
+ * solves of the same systems. */
+static int cg_mass(const csr_t *M, const double *dinv, const double *b, double *x, double *work, int n)
+{
+    double *r = work, *z = work + n, *p = work + 2 * (size_t)n, *q = work + 3 * (size_t)n;
+    sfo_csr_matvec(n + 1, M->p, M->j, M->x, x, q);
+    double bb = 0.0, rz = 0.0, rr = 0.0;
+    for (int i = 0; i < n; i++) {
+        r[i] = b[i] - q[i];
+        z[i] = r[i] * dinv[i];
+        p[i] = z[i];
+        bb += b[i] * b[i];
+        rz += r[i] * z[i];
+        rr += r[i] * r[i];
+    }
+    for (int it = 0; it < 1000; it++) {
+        if (rr <= 1e-24 * bb || rr <= 1e-200) return 0;
+        sfo_csr_matvec(n + 1, M->p, M->j, M->x, p, q);
+        double pq = 0.0;
+        for (int i = 0; i < n; i++) pq += p[i] * q[i];
+        const double alpha = rz / pq;
+        double rz1 = 0.0;
+        rr = 0.0;
+        for (int i = 0; i < n; i++) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+            z[i] = r[i] * dinv[i];
+            rz1 += r[i] * z[i];
+            rr += r[i] * r[i];
+        }
+        const double beta = rz1 / rz;
+        rz = rz1;
+        for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    }
+    return 1;
+}
+
 int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,
                     double *snap_u, double *snap_w, double *energy_u, double *energy_w)
 {
@@ -766,6 +807,14 @@ int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,
     const int nsnap = sfo_snapshot_rows(pb->step, snap_every);
     const int nrow = pb->step - 2;
     int status = 0;
+    double *cm_dinv = NULL, *cm_work = NULL;
+    if (pb->consistent) {
+        cm_dinv = (double *)calloc(N, sizeof(double));
+        cm_work = (double *)malloc(sizeof(double) * 4 * (size_t)N);
+        for (int i = 0; i < N; i++)
+            for (int k = M.p[i]; k < M.p[i + 1]; k++)
+                if (M.j[k] == i) cm_dinv[i] = M.x[k] != 0.0 ? 1.0 / M.x[k] : 0.0;
+    }
     const double t_loop = wall_s();
     for (int shot = 0; shot < pb->src_num && status == 0; shot++) {
         const int src = pb->src_node[shot];
@@ -858,6 +907,15 @@ int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,
                     R_(13)[i] = -dt * c2[i] * dyy[i] * e71[i] - dt * dy[i] * e35[i] + e35[i];
                 }
             }
+            /* consistent-mass solves (:664-680, 730-746): M x = rhs per field,
+             * from the previous values, without the Dirichlet zeroing */
+            if (pb->consistent) {
+                static const int dst[NRHS] = {U1n, U2n, U3n, Lx1, Lx2, Lx3, Lx4,
+                                              W1n, W2n, W3n, Ly1, Ly2, Ly3, Ly4};
+                for (int k = 0; k < NRHS && status == 0; k++)
+                    if (cg_mass(&M, cm_dinv, R_(k), S_(dst[k]), cm_work, N) != 0) status = 4;
+                if (status) break;
+            } else
             /* mass-lumped solve (:681-729): Dirichlet nodes -> 0; a zero lumped
              * mass leaves the previous values in place */
             {
@@ -911,7 +969,7 @@ int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,
 #undef E_
 #undef R_
     if (pb->timing) { pb->timing[0] = t_loop - t_start; pb->timing[1] = wall_s() - t_loop; }
-    free(st); free(eq); free(rh); free(mp); free(dir); free(mass_lump);
+    free(st); free(eq); free(rh); free(mp); free(dir); free(mass_lump); free(cm_dinv); free(cm_work);
     free(M.p); free(M.j); free(M.x);
     for (int k = 1; k <= 6; k++) { free(K[k].p); free(K[k].j); free(K[k].x); }
 #ifdef _OPENMP

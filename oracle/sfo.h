@@ -81,7 +81,8 @@ int sfo_node_location(int node_num, double edge_size, const double *x, const dou
  *     fall before it=2).  snap_every = 200 reproduces the reference.
  *   energy_u / energy_w: [src_num][step] (may be NULL)
  * Returns 0; 1 when the reference would exit(1) on the energy bound (the
- * run stops there, outputs keep what was written so far); 2 on bad input. */
+ * run stops there, outputs keep what was written so far); 2 on bad input;
+ * 4 when a consistent-mass solve did not converge. */
 typedef struct {
     int type_code, node_num, element_num, order;
     const int *element_node;
@@ -96,6 +97,10 @@ typedef struct {
     int snap_every;
     int nthreads;           /* OpenMP threads, <=0: library default */
     double *timing;         /* optional out: [0] set-up seconds, [1] time-loop seconds */
+    int consistent;         /* 0: solver "masslump"; 1: the consistent-mass branch (solver
+                               "pardiso" / "mgmres", elastic_wave.c:664-680, 730-746): the 14
+                               right-hand sides solved with M (Jacobi-preconditioned CG to a
+                               1e-12 relative residual, from the previous values) */
 } sfo_problem;
 
 int sfo_elastic_run(const sfo_problem *pb, double *seis_u, double *seis_w,

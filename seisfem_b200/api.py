@@ -17,8 +17,9 @@ from .problem import Problem
 
 LIBPATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libseisfem_b200.so")
 
-SFG_OK, SFG_ERR_BLOWUP = 0, 6
-PRECISIONS = {"fp32k": 0, "fp32": 1, "fp64": 2, "plain": 3}
+SFG_OK, SFG_ERR_BLOWUP, SFG_ERR_NOCONV = 0, 6, 12
+# "fp64cm": FP64 with the consistent mass matrix (solver "pardiso" / "mgmres")
+PRECISIONS = {"fp32k": 0, "fp32": 1, "fp64": 2, "plain": 3, "fp64cm": 4}
 
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")

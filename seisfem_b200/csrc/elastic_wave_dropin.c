@@ -17,11 +17,13 @@
  *   - fatal conditions exit(1) with the reference's messages: an unknown
  *     solver (:747-753) and the energy bound (:779-785; the rows computed
  *     before the failing step are written first).
- * Solver "masslump" is the GPU path; "pardiso" and "mgmres" (consistent-mass
- * solves) are not provided and exit(1) like an unknown solver.
- * Environment: SFG_DEVICE (CUDA device, default 0), SFG_PRECISION
- * (fp32k = FP32 with Kahan-compensated displacement, the default; fp32;
- * fp64).
+ * Solver "masslump" takes the lumped-mass GPU path; "pardiso" and "mgmres"
+ * take the consistent-mass path (SFG_FP64_CONSISTENT: the 14 systems of each
+ * step solved with M by preconditioned conjugate gradients on the GPU, FP64);
+ * any other string exits(1) like the reference.
+ * Environment: SFG_DEVICE (CUDA device, default 0), SFG_PRECISION for
+ * "masslump" (fp32k = FP32 with Kahan-compensated displacement, the default;
+ * fp32; fp64).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -65,7 +67,8 @@ void elastic_wave(char *type, int node_num, int element_num, int element_order, 
 {
     (void)nnz;
     (void)csr_p_size;
-    if (strcmp(solver, "masslump") != 0) {
+    const int consistent = strcmp(solver, "pardiso") == 0 || strcmp(solver, "mgmres") == 0;
+    if (strcmp(solver, "masslump") != 0 && !consistent) {
         fprintf(stderr, "\nELASTIC_MPML- Fatal error!\n  Solver type is not set = \"%s\".\n", solver);
         exit(1);
     }
@@ -111,6 +114,7 @@ void elastic_wave(char *type, int node_num, int element_num, int element_order, 
     const char *ps = getenv("SFG_PRECISION");
     if (ps && strcmp(ps, "fp64") == 0) precision = SFG_FP64;
     else if (ps && strcmp(ps, "fp32") == 0) precision = SFG_FP32;
+    if (consistent) precision = SFG_FP64_CONSISTENT;
 
     const int rows = step - 2, nsnap = sfg_snapshot_rows(step, 200);
     double *su = malloc(sizeof(double) * (size_t)src_num * rows * (rec_num > 0 ? rec_num : 1));

@@ -98,7 +98,8 @@ namespace {
 const char *kStatus[] = {"ok", "bad argument", "CUDA error", "device out of memory", "zero-area element",
                          "index out of range", "energy bound exceeded", "row too long",
                          "call out of order", "device wait timed out", "no usable CUDA device",
-                         "size above the fixed limit of a no-allocation entry point"};
+                         "size above the fixed limit of a no-allocation entry point",
+                         "consistent-mass solve did not converge"};
 
 int fail(sfg_ctx *c, int code, const std::string &msg)
 {
@@ -183,7 +184,7 @@ extern "C" {
 
 const char *sfg_error_string(int s)
 {
-    return (s >= 0 && s <= 11) ? kStatus[s] : "unknown status";
+    return (s >= 0 && s <= 12) ? kStatus[s] : "unknown status";
 }
 
 const char *sfg_last_error(const sfg_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
@@ -511,7 +512,7 @@ int sfg_lumped_mass_set(sfg_ctx *ctx, const double *mass_lump)
 namespace {
 
 struct LoopPlan {
-    int kind;            // SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH
+    int kind;            // SFG_FP32_KAHAN, SFG_FP32, SFG_FP64, SFG_FP32_PLAIN_PATH, SFG_FP64_CONSISTENT
     int S;               // shots advanced together (1, 32, 64, 128)
     int spl;             // shots per lane (batched)
     int threads;         // FP64 path: threads per block
@@ -522,6 +523,8 @@ struct LoopPlan {
 
 // The fused FP32 kernels run in the two-class node numbering.
 bool permuted(const LoopPlan &pl) { return pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN; }
+// The FP64 paths (lumped or consistent mass) share the FP64 state layout.
+bool fp64(const LoopPlan &pl) { return pl.kind == SFG_FP64 || pl.kind == SFG_FP64_CONSISTENT; }
 
 // Device buffers of one batch.
 struct BatchBufs {
@@ -541,7 +544,24 @@ struct BatchBufs {
     // one model per shot: the batch's coefficient streams and the row
     // records with the geometric mass matrix
     float *cmm = nullptr, *sig = nullptr, *rec_geo = nullptr;
+    // consistent-mass solves: B, X, R, Z, P, Q [N][14], 1/diag(M) [N],
+    // scalars; flags: converged, failed solves
+    double *cm = nullptr;
+    int *cmi = nullptr;
 };
+
+Cm64 cm_view(const DevProblem &P, const BatchBufs &b)
+{
+    Cm64 g;
+    const size_t n = (size_t)P.node_num, w = n * CM_COLS;
+    g.n = P.node_num; g.up = P.up; g.uj = P.uj; g.mx = P.ux;
+    g.B = b.cm; g.X = b.cm + w; g.R = b.cm + 2 * w; g.Z = b.cm + 3 * w; g.P = b.cm + 4 * w; g.Q = b.cm + 5 * w;
+    g.dinv = b.cm + 6 * w;
+    g.sc = b.cm + 6 * w + n;
+    g.done = b.cmi;
+    g.fails = b.cmi + 1;
+    return g;
+}
 
 // Buffers return to the context's pool; the caller has waited for every
 // stream that used them.
@@ -555,6 +575,7 @@ void free_bufs(sfg_ctx *ctx, BatchBufs &b)
     pfree(ctx, b.snap_u); pfree(ctx, b.snap_w); pfree(ctx, b.energy);
     pfree(ctx, b.pst); pfree(ctx, b.peq); pfree(ctx, b.prhs); pfree(ctx, b.panew);
     pfree(ctx, b.cmm); pfree(ctx, b.sig); pfree(ctx, b.rec_geo);
+    pfree(ctx, b.cm); pfree(ctx, b.cmi);
     b = BatchBufs();
 }
 
@@ -597,14 +618,22 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
         c.seis_row = it >= 3 ? it - 3 : -1;
         const int nxt = cur ^ 1;
         cudaError_t e;
-        if (pl.kind == SFG_FP64) {
+        if (fp64(pl)) {
             Step64 a;
             a.c = c; a.up = P.up; a.uj = P.uj; a.ux = P.ux; a.nnz = P.union_nnz; a.coef = P.coefd;
             a.Gin = (const double *)b.G[cur]; a.Gout = (double *)b.G[nxt];
             a.Pin = (const double *)b.Pv[cur]; a.Pout = (double *)b.Pv[nxt];
-            e = launch_step64(a, pl.threads, st);
-            if (e != cudaSuccess) return -1;
-            launches++;
+            if (pl.kind == SFG_FP64) {
+                e = launch_step64(a, pl.threads, st);
+                if (e != cudaSuccess) return -1;
+                launches++;
+            } else {
+                const Cm64 g = cm_view(P, b);
+                if (launch_cm_rhs(a, g, st) != cudaSuccess) return -1;
+                const int ns = queue_cm_solve(g, st);
+                if (ns < 0 || launch_cm_newmark(a, g, st) != cudaSuccess) return -1;
+                launches += 2 + ns;
+            }
         } else {
             Step2 a;
             a.c = c; a.na = P.na; a.S = S;
@@ -632,7 +661,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
         cur = nxt;
         if (nsnap > 0 && (it + 1) % snap_every == 0 && srow < nsnap) {
             const size_t off = (size_t)srow * N;
-            if (pl.kind == SFG_FP64)
+            if (fp64(pl))
                 e = launch_snapshot64((const double *)b.G[cur], N, b.snap_u + off, b.snap_w + off, st);
             else
                 e = launch_snapshot2({b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, N, P.na, S, P.perm, b.snap_u + off,
@@ -646,7 +675,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
     // the last state's receiver row
     c.it = last - 1;
     c.seis_row = last - 3;
-    cudaError_t e = pl.kind == SFG_FP64
+    cudaError_t e = fp64(pl)
                         ? launch_gather64(c, (const double *)b.G[cur], S, st)
                         : launch_gather2(c, P.na, {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, S, st);
     if (e != cudaSuccess) return -1;
@@ -657,7 +686,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
 int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int nsnap, BatchBufs &b)
 {
     const int N = ctx->N, S = pl.S, R = run->rec_num, rows = run->step - 2;
-    const size_t esz = pl.kind == SFG_FP64 ? sizeof(double) : sizeof(float);
+    const size_t esz = fp64(pl) ? sizeof(double) : sizeof(float);
     b.gbytes = (size_t)N * GREC * S * esz;
     b.pbytes = (size_t)N * PREC * S * esz;
     const int na = ctx->P.na, nz = N - na;
@@ -670,10 +699,16 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
         CK(palloc(ctx, &b.peq, sizeof(float) * 22 * (size_t)N));
         CK(palloc(ctx, &b.prhs, sizeof(float) * 14 * (size_t)N));
         CK(palloc(ctx, &b.panew, sizeof(float) * 6 * (size_t)N));
-    } else if (pl.kind == SFG_FP64) {
+    } else if (fp64(pl)) {
         for (int k = 0; k < 2; k++) {
             CK(palloc(ctx, &b.G[k], b.gbytes));
             CK(palloc(ctx, &b.Pv[k], b.pbytes));
+        }
+        if (pl.kind == SFG_FP64_CONSISTENT) {
+            CK(palloc(ctx, &b.cm, sizeof(double) * ((size_t)N * (6 * CM_COLS + 1) + cm_scalar_count())));
+            CK(palloc(ctx, &b.cmi, sizeof(int) * 2));
+            CK(cudaMemsetAsync(b.cmi, 0, sizeof(int) * 2, st));
+            CK(launch_cm_diag(cm_view(ctx->P, b), st));
         }
     } else {
         for (int k = 0; k < 2; k++) {
@@ -713,8 +748,11 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         z(b.pst, sizeof(float) * 36 * (size_t)N);
         z(b.panew, sizeof(float) * 6 * (size_t)N);
-    } else if (pl.kind == SFG_FP64) {
+    } else if (fp64(pl)) {
         for (int k = 0; k < 2; k++) { z(b.G[k], b.gbytes); z(b.Pv[k], b.pbytes); }
+        // the first guess of the first step's solves (later steps start from
+        // the previous solution, like the reference's GMRES calls)
+        z(b.cm ? b.cm + (size_t)N * CM_COLS : nullptr, sizeof(double) * (size_t)N * CM_COLS);
     } else {
         for (int k = 0; k < 2; k++) {
             z(b.Gc[k], b.gc_bytes); z(b.Pa[k], b.pa_bytes); z(b.Gs[k], b.gs_bytes); z(b.Ps[k], b.gs_bytes);
@@ -734,7 +772,7 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
 // objective).  The caller resets the state afterwards.
 int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
 {
-    if (pl.kind == SFG_FP64 || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
+    if (fp64(pl) || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
     const int kahan = pl.kind == SFG_FP32_KAHAN ? 1 : 0;
     const int si = pl.S == 1 ? 0 : (pl.S == 32 ? 1 : (pl.S == 64 ? 2 : 3));
     int *slot = ctx->tune.shape[si][kahan];
@@ -952,7 +990,10 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capt
     for (int r = 0; r < run->rec_num; r++)
         if (run->rec_node[r] < 0 || run->rec_node[r] >= N)
             return fail(ctx, SFG_ERR_BADINDEX, "receiver node out of range (node_location miss gives -1)");
-    if (run->precision < 0 || run->precision > 3) return fail(ctx, SFG_ERR_ARG, "bad precision");
+    if (run->precision < 0 || run->precision > 4) return fail(ctx, SFG_ERR_ARG, "bad precision");
+    // consistent mass: up to 3 + 3 * CM_MAXIT kernels per step, queued
+    // directly (most return at once) instead of captured
+    if (run->precision == SFG_FP64_CONSISTENT) capture = false;
     CK(cudaSetDevice(ctx->device));
     sfg_plan *p = new sfg_plan();
     p->ctx = ctx;
@@ -1085,6 +1126,13 @@ int plan_finish(sfg_plan *p, int batch, double *seis_u, double *seis_w, double *
     }
     if (status == SFG_ERR_BLOWUP)
         ctx->err = "energy exceeds maximum value at step " + std::to_string(ctx->stats.blowup_step);
+    if (status == SFG_OK && p->b.cmi) {
+        int fails = 0;
+        CK(cudaMemcpy(&fails, p->b.cmi + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        if (fails > 0)
+            status = fail(ctx, SFG_ERR_NOCONV, std::to_string(fails) + " consistent-mass solves stopped above 1e-12 "
+                                               "relative residual after " + std::to_string(CM_MAXIT) + " iterations");
+    }
     return status;
 }
 

@@ -33,10 +33,11 @@ __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, 
 // multiply-add contraction: per-product row sums from 0.0 in column order
 // (csr_matvec.c:10-16), right-hand sides as written at elastic_wave.c:585-591
 // and 651-657, division by the lumped mass (:709-722), Newmark (:757-776).
-__global__ void __launch_bounds__(128) step64_kernel(const Step64 a)
+
+// receiver gather of the step's input state (elastic_wave.c:787-795)
+__device__ __forceinline__ void gather_in64(const Step64 &a, int i)
 {
     const StepCommon &c = a.c;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (c.seis_row >= 0 && i < c.nrec) {
         long long node = c.rec[i];
         const double *g = a.Gin + node * GREC;
@@ -44,82 +45,292 @@ __global__ void __launch_bounds__(128) step64_kernel(const Step64 a)
         c.seis_u[o] = add(add(g[0], g[1]), g[2]);
         c.seis_w[o] = add(add(g[3], g[4]), g[5]);
     }
+}
+
+// the 32 distinct products of row i and its 14 right-hand sides
+// (elastic_wave.c:533-592, 599-658), source included
+__device__ __forceinline__ void rhs64(const Step64 &a, int i, double r[14])
+{
+    const StepCommon &c = a.c;
+    double kU[6], kW[6], m[20];
+    for (int k = 0; k < 6; k++) { kU[k] = 0.0; kW[k] = 0.0; }
+    for (int k = 0; k < 20; k++) m[k] = 0.0;
+    const long long nz = a.nnz;
+    for (int e = a.up[i]; e < a.up[i + 1]; e++) {
+        const int j = a.uj[e];
+        const double *g = a.Gin + (long long)j * GREC;
+        const double u = add(add(g[0], g[1]), g[2]);
+        const double w = add(add(g[3], g[4]), g[5]);
+        const double vm = a.ux[e];
+        for (int k = 0; k < 6; k++) {
+            const double kv = a.ux[(k + 1) * nz + e];
+            kU[k] = add(kU[k], mul(kv, u));
+            kW[k] = add(kW[k], mul(kv, w));
+        }
+        for (int v = 0; v < 20; v++) m[v] = add(m[v], mul(vm, g[v]));
+    }
+    const double *cf = a.coef + (size_t)i * CREC;
+    const double c0 = cf[0], c1 = cf[1], c2 = cf[2], c3 = cf[3];
+    const double dx = cf[4], dy = cf[5], dxx = cf[6], dyy = cf[7];
+    const double dxxp = cf[9], dyyp = cf[10];
+    const double dt = c.dt;
+    // m: 0..5 = M*U1..W3, 6..11 = M*V1..V6, 12..15 = M*Lx1..4, 16..19 = M*Ly1..4
+    r[0] = sub(sub(mul(-c0, kU[0]), mul(mul(2.0, dx), m[6])), mul(mul(dx, dx), m[0]));
+    r[0] = add(add(r[0], m[12]), m[13]);
+    r[1] = sub(sub(sub(sub(mul(-c1, kW[2]), mul(c3, kW[3])), mul(dx, m[7])), mul(dy, m[7])), mul(mul(dx, dy), m[1]));
+    r[2] = sub(sub(mul(-c3, kU[1]), mul(mul(2.0, dy), m[8])), mul(mul(dy, dy), m[2]));
+    r[2] = add(add(r[2], m[14]), m[15]);
+    r[3] = add(sub(mul(mul(mul(-dt, c0), dxx), kU[4]), mul(mul(dt, dx), m[12])), m[12]);
+    r[4] = add(sub(mul(mul(mul(-dt, c3), dyyp), kW[4]), mul(mul(dt, dy), m[13])), m[13]);
+    r[5] = add(sub(mul(mul(mul(-dt, c1), dxxp), kW[5]), mul(mul(dt, dx), m[14])), m[14]);
+    r[6] = add(sub(mul(mul(mul(-dt, c3), dyy), kU[5]), mul(mul(dt, dy), m[15])), m[15]);
+    r[7] = sub(sub(mul(-c3, kW[0]), mul(mul(2.0, dx), m[9])), mul(mul(dx, dx), m[3]));
+    r[7] = add(add(r[7], m[16]), m[17]);
+    r[8] = sub(sub(sub(sub(mul(-c3, kU[2]), mul(c1, kU[3])), mul(dx, m[10])), mul(dy, m[10])), mul(mul(dx, dy), m[4]));
+    r[9] = sub(sub(mul(-c2, kW[1]), mul(mul(2.0, dy), m[11])), mul(mul(dy, dy), m[5]));
+    r[9] = add(add(r[9], m[18]), m[19]);
+    r[10] = add(sub(mul(mul(mul(-dt, c3), dxx), kW[4]), mul(mul(dt, dx), m[16])), m[16]);
+    r[11] = add(sub(mul(mul(mul(-dt, c1), dyyp), kU[4]), mul(mul(dt, dy), m[17])), m[17]);
+    r[12] = add(sub(mul(mul(mul(-dt, c3), dxxp), kU[5]), mul(mul(dt, dx), m[18])), m[18]);
+    r[13] = add(sub(mul(mul(mul(-dt, c2), dyy), kW[5]), mul(mul(dt, dy), m[19])), m[19]);
+    if (i == c.src[0]) {
+        const double ps = c.amp[c.it];
+        r[0] = add(r[0], mul(ps, c.sin_af));
+        r[7] = add(r[7], mul(ps, c.cos_af));
+    }
+}
+
+// Newmark update of row i (elastic_wave.c:754-786) from the new
+// accelerations an (U1..W3) and memory variables L (Lx1..4, Ly1..4)
+__device__ __forceinline__ void newmark64(const Step64 &a, int i, const double an[6], const double L[8], double &eu,
+                                          double &ew)
+{
+    const double dt = a.c.dt;
+    const double *g = a.Gin + (size_t)i * GREC;
+    const double *pi = a.Pin + (size_t)i * PREC;
+    double *go = a.Gout + (size_t)i * GREC;
+    double *po = a.Pout + (size_t)i * PREC;
+    double U[6];
+    for (int k = 0; k < 6; k++) {
+        const double Uk = g[k], Vk = g[6 + k], Ak = pi[k];
+        const double X = add(mul(-0.5, Ak), an[k]);
+        U[k] = add(add(Uk, mul(Vk, dt)), mul(mul(X, dt), dt));
+        go[k] = U[k];
+        go[6 + k] = add(Vk, mul(add(mul(-0.5, Ak), mul(1.5, an[k])), dt));
+        po[k] = an[k];
+    }
+    for (int k = 0; k < 8; k++) go[12 + k] = L[k];
+    const double uu = add(add(U[0], U[1]), U[2]), ww = add(add(U[3], U[4]), U[5]);
+    eu = uu * uu;
+    ew = ww * ww;
+}
+
+// right-hand side k of each solved field: accelerations U1..W3, then Lx1..4, Ly1..4
+__constant__ int kAccRhs[6] = {0, 1, 2, 7, 8, 9};
+
+__global__ void __launch_bounds__(128) step64_kernel(const Step64 a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    gather_in64(a, i);
     double eu = 0.0, ew = 0.0;
-    if (i < c.n) {
-        double kU[6], kW[6], m[20];
-        for (int k = 0; k < 6; k++) { kU[k] = 0.0; kW[k] = 0.0; }
-        for (int k = 0; k < 20; k++) m[k] = 0.0;
-        const long long nz = a.nnz;
-        for (int e = a.up[i]; e < a.up[i + 1]; e++) {
-            const int j = a.uj[e];
-            const double *g = a.Gin + (long long)j * GREC;
-            const double u = add(add(g[0], g[1]), g[2]);
-            const double w = add(add(g[3], g[4]), g[5]);
-            const double vm = a.ux[e];
-            for (int k = 0; k < 6; k++) {
-                const double kv = a.ux[(k + 1) * nz + e];
-                kU[k] = add(kU[k], mul(kv, u));
-                kW[k] = add(kW[k], mul(kv, w));
-            }
-            for (int v = 0; v < 20; v++) m[v] = add(m[v], mul(vm, g[v]));
-        }
-        const double *cf = a.coef + (size_t)i * CREC;
-        const double c0 = cf[0], c1 = cf[1], c2 = cf[2], c3 = cf[3];
-        const double dx = cf[4], dy = cf[5], dxx = cf[6], dyy = cf[7];
-        const double dirichlet_or_zero = cf[8], dxxp = cf[9], dyyp = cf[10], mlump = cf[11];
-        const double dt = c.dt;
-        // m: 0..5 = M*U1..W3, 6..11 = M*V1..V6, 12..15 = M*Lx1..4, 16..19 = M*Ly1..4
+    if (i < a.c.n) {
         double r[14];
-        r[0] = sub(sub(mul(-c0, kU[0]), mul(mul(2.0, dx), m[6])), mul(mul(dx, dx), m[0]));
-        r[0] = add(add(r[0], m[12]), m[13]);
-        r[1] = sub(sub(sub(sub(mul(-c1, kW[2]), mul(c3, kW[3])), mul(dx, m[7])), mul(dy, m[7])), mul(mul(dx, dy), m[1]));
-        r[2] = sub(sub(mul(-c3, kU[1]), mul(mul(2.0, dy), m[8])), mul(mul(dy, dy), m[2]));
-        r[2] = add(add(r[2], m[14]), m[15]);
-        r[3] = add(sub(mul(mul(mul(-dt, c0), dxx), kU[4]), mul(mul(dt, dx), m[12])), m[12]);
-        r[4] = add(sub(mul(mul(mul(-dt, c3), dyyp), kW[4]), mul(mul(dt, dy), m[13])), m[13]);
-        r[5] = add(sub(mul(mul(mul(-dt, c1), dxxp), kW[5]), mul(mul(dt, dx), m[14])), m[14]);
-        r[6] = add(sub(mul(mul(mul(-dt, c3), dyy), kU[5]), mul(mul(dt, dy), m[15])), m[15]);
-        r[7] = sub(sub(mul(-c3, kW[0]), mul(mul(2.0, dx), m[9])), mul(mul(dx, dx), m[3]));
-        r[7] = add(add(r[7], m[16]), m[17]);
-        r[8] = sub(sub(sub(sub(mul(-c3, kU[2]), mul(c1, kU[3])), mul(dx, m[10])), mul(dy, m[10])), mul(mul(dx, dy), m[4]));
-        r[9] = sub(sub(mul(-c2, kW[1]), mul(mul(2.0, dy), m[11])), mul(mul(dy, dy), m[5]));
-        r[9] = add(add(r[9], m[18]), m[19]);
-        r[10] = add(sub(mul(mul(mul(-dt, c3), dxx), kW[4]), mul(mul(dt, dx), m[16])), m[16]);
-        r[11] = add(sub(mul(mul(mul(-dt, c1), dyyp), kU[4]), mul(mul(dt, dy), m[17])), m[17]);
-        r[12] = add(sub(mul(mul(mul(-dt, c3), dxxp), kU[5]), mul(mul(dt, dx), m[18])), m[18]);
-        r[13] = add(sub(mul(mul(mul(-dt, c2), dyy), kW[5]), mul(mul(dt, dy), m[19])), m[19]);
-        if (i == c.src[0]) {
-            const double ps = c.amp[c.it];
-            r[0] = add(r[0], mul(ps, c.sin_af));
-            r[7] = add(r[7], mul(ps, c.cos_af));
-        }
+        rhs64(a, i, r);
+        const double *cf = a.coef + (size_t)i * CREC;
+        const double dirichlet_or_zero = cf[8], mlump = cf[11];
         const bool zero = dirichlet_or_zero == 0.0;
         double an[6], L[8];
-        const int ia[6] = {0, 1, 2, 7, 8, 9};
-        for (int k = 0; k < 6; k++) an[k] = zero ? 0.0 : __ddiv_rn(r[ia[k]], mlump);
+        for (int k = 0; k < 6; k++) an[k] = zero ? 0.0 : __ddiv_rn(r[kAccRhs[k]], mlump);
         for (int k = 0; k < 4; k++) {
             L[k] = zero ? 0.0 : __ddiv_rn(r[3 + k], mlump);
             L[4 + k] = zero ? 0.0 : __ddiv_rn(r[10 + k], mlump);
         }
-        const double *g = a.Gin + (size_t)i * GREC;
-        const double *pi = a.Pin + (size_t)i * PREC;
-        double *go = a.Gout + (size_t)i * GREC;
-        double *po = a.Pout + (size_t)i * PREC;
-        double U[6];
-        for (int k = 0; k < 6; k++) {
-            const double Uk = g[k], Vk = g[6 + k], Ak = pi[k];
-            const double X = add(mul(-0.5, Ak), an[k]);
-            U[k] = add(add(Uk, mul(Vk, dt)), mul(mul(X, dt), dt));
-            go[k] = U[k];
-            go[6 + k] = add(Vk, mul(add(mul(-0.5, Ak), mul(1.5, an[k])), dt));
-            po[k] = an[k];
-        }
-        for (int k = 0; k < 8; k++) go[12 + k] = L[k];
-        const double uu = add(add(U[0], U[1]), U[2]), ww = add(add(U[3], U[4]), U[5]);
-        eu = uu * uu;
-        ew = ww * ww;
+        newmark64(a, i, an, L, eu, ew);
     }
-    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+    block_energy(a.c.energy ? a.c.energy + ((size_t)a.c.it) * 2 : nullptr, eu, ew);
+}
+
+// ------------------------------------------------ consistent-mass solves
+//
+// The reference solves M x = rhs for the 14 fields with PARDISO or with
+// restarted GMRES + ILU (tolerance 1e-8, the previous values as the first
+// guess; elastic_wave.c:664-680, 730-746).  Here: conjugate gradients with
+// the Jacobi preconditioner (M is symmetric positive definite), the 14
+// columns together so that M is streamed once per iteration for all of
+// them, started from the previous solution and stopped per column when
+// |r| <= 1e-12 |b|.  Each iteration is three kernels (q = M p with p.q;
+// x, r, z updates with r.z and r.r; the new directions); the block sums of
+// the dot products are added atomically into per-iteration slots.  CM_MAXIT
+// iterations are queued per step; once every column has converged the
+// remaining ones return at once.  Scalars sc[t]: [0] r.z, [1] b.b (t = 0),
+// [2] p.q, [3] r.r, each CM_COLS wide.
+
+constexpr int kCmThreads = 256;
+
+__device__ __forceinline__ void block_add_cols(double v[CM_COLS], double *out)
+{
+    __shared__ double sh[CM_COLS][kCmThreads / 32];
+#pragma unroll
+    for (int k = 0; k < CM_COLS; k++)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < CM_COLS; k++) sh[k][threadIdx.x >> 5] = v[k];
+    __syncthreads();
+    if (threadIdx.x < CM_COLS) {
+        double s = 0.0;
+        for (int w = 0; w < kCmThreads / 32; w++) s += sh[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, s);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void spmm_row(const Cm64 &g, int i, const double *__restrict__ V, double q[CM_COLS])
+{
+    for (int k = 0; k < CM_COLS; k++) q[k] = 0.0;
+    for (int e = g.up[i]; e < g.up[i + 1]; e++) {
+        const double m = g.mx[e];
+        const double *v = V + (size_t)g.uj[e] * CM_COLS;
+#pragma unroll
+        for (int k = 0; k < CM_COLS; k++) q[k] += m * v[k];
+    }
+}
+
+__device__ __forceinline__ const double *cm_sc(const Cm64 &g, int t, int which) { return g.sc + ((size_t)t * 4 + which) * CM_COLS; }
+
+__device__ __forceinline__ bool cm_conv(const Cm64 &g, int t, int k)
+{
+    const double rr = cm_sc(g, t, 3)[k], bb = cm_sc(g, 0, 1)[k];
+    return rr <= CM_TOL * CM_TOL * bb || rr <= 1e-200;
+}
+
+__global__ void cm_diag_kernel(const Cm64 g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    double d = 0.0;
+    for (int e = g.up[i]; e < g.up[i + 1]; e++)
+        if (g.uj[e] == i) d = g.mx[e];
+    g.dinv[i] = d != 0.0 ? 1.0 / d : 0.0;
+}
+
+__global__ void __launch_bounds__(128) cm_rhs_kernel(const Step64 a, const Cm64 g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    gather_in64(a, i);
+    if (i < a.c.n) {
+        double r[14];
+        rhs64(a, i, r);
+        for (int k = 0; k < CM_COLS; k++) g.B[(size_t)i * CM_COLS + k] = r[k];
+    }
+}
+
+// r = b - M x, z = D^-1 r, p = z; sums r.z, b.b, r.r
+__global__ void __launch_bounds__(kCmThreads) cm_init_kernel(const Cm64 g)
+{
+    const int i = blockIdx.x * kCmThreads + threadIdx.x;
+    double rz[CM_COLS], bb[CM_COLS], rr[CM_COLS];
+    for (int k = 0; k < CM_COLS; k++) { rz[k] = 0.0; bb[k] = 0.0; rr[k] = 0.0; }
+    if (i < g.n) {
+        double q[CM_COLS];
+        spmm_row(g, i, g.X, q);
+        const double di = g.dinv[i];
+        for (int k = 0; k < CM_COLS; k++) {
+            const size_t o = (size_t)i * CM_COLS + k;
+            const double b = g.B[o], r = b - q[k], z = r * di;
+            g.R[o] = r; g.Z[o] = z; g.P[o] = z;
+            rz[k] = r * z; bb[k] = b * b; rr[k] = r * r;
+        }
+    }
+    block_add_cols(rz, g.sc + 0 * CM_COLS);
+    block_add_cols(bb, g.sc + 1 * CM_COLS);
+    block_add_cols(rr, g.sc + 3 * CM_COLS);
+}
+
+// q = M p; sum p.q into iteration t
+__global__ void __launch_bounds__(kCmThreads) cm_spmm_kernel(const Cm64 g, int t)
+{
+    if (*g.done) return;
+    const int i = blockIdx.x * kCmThreads + threadIdx.x;
+    double pq[CM_COLS];
+    for (int k = 0; k < CM_COLS; k++) pq[k] = 0.0;
+    if (i < g.n) {
+        double q[CM_COLS];
+        spmm_row(g, i, g.P, q);
+        for (int k = 0; k < CM_COLS; k++) {
+            const size_t o = (size_t)i * CM_COLS + k;
+            g.Q[o] = q[k];
+            pq[k] = g.P[o] * q[k];
+        }
+    }
+    block_add_cols(pq, g.sc + ((size_t)t * 4 + 2) * CM_COLS);
+}
+
+// x += alpha p, r -= alpha q, z = D^-1 r; sums r.z and r.r into iteration t + 1
+__global__ void __launch_bounds__(kCmThreads) cm_update_kernel(const Cm64 g, int t)
+{
+    if (*g.done) return;
+    const int i = blockIdx.x * kCmThreads + threadIdx.x;
+    double rz[CM_COLS], rr[CM_COLS];
+    for (int k = 0; k < CM_COLS; k++) { rz[k] = 0.0; rr[k] = 0.0; }
+    if (i < g.n) {
+        const double di = g.dinv[i];
+        for (int k = 0; k < CM_COLS; k++) {
+            const size_t o = (size_t)i * CM_COLS + k;
+            double r = g.R[o];
+            if (!cm_conv(g, t, k)) {
+                const double alpha = cm_sc(g, t, 0)[k] / cm_sc(g, t, 2)[k];
+                g.X[o] += alpha * g.P[o];
+                r -= alpha * g.Q[o];
+                g.R[o] = r;
+                g.Z[o] = r * di;
+            }
+            rz[k] = r * g.Z[o];
+            rr[k] = r * r;
+        }
+    }
+    block_add_cols(rz, g.sc + ((size_t)(t + 1) * 4 + 0) * CM_COLS);
+    block_add_cols(rr, g.sc + ((size_t)(t + 1) * 4 + 3) * CM_COLS);
+}
+
+// p = z + beta p for the columns still running; the flag when none is
+__global__ void __launch_bounds__(kCmThreads) cm_direction_kernel(const Cm64 g, int t)
+{
+    if (*g.done) return;
+    const int i = blockIdx.x * kCmThreads + threadIdx.x;
+    bool all = true;
+    for (int k = 0; k < CM_COLS; k++) {
+        const bool c = cm_conv(g, t + 1, k);
+        all = all && c;
+        if (!c && i < g.n) {
+            const size_t o = (size_t)i * CM_COLS + k;
+            const double beta = cm_sc(g, t + 1, 0)[k] / cm_sc(g, t, 0)[k];
+            g.P[o] = g.Z[o] + beta * g.P[o];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && all) *g.done = 1;
+}
+
+// a solve that used every queued iteration without converging
+__global__ void cm_check_kernel(const Cm64 g)
+{
+    if (*g.done) return;
+    bool all = true;
+    for (int k = 0; k < CM_COLS; k++) all = all && cm_conv(g, CM_MAXIT, k);
+    if (!all) atomicAdd(g.fails, 1);
+}
+
+__global__ void __launch_bounds__(128) cm_newmark_kernel(const Step64 a, const Cm64 g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double eu = 0.0, ew = 0.0;
+    if (i < a.c.n) {
+        const double *x = g.X + (size_t)i * CM_COLS;
+        double an[6], L[8];
+        for (int k = 0; k < 6; k++) an[k] = x[kAccRhs[k]];
+        for (int k = 0; k < 4; k++) { L[k] = x[3 + k]; L[4 + k] = x[10 + k]; }
+        newmark64(a, i, an, L, eu, ew);
+    }
+    block_energy(a.c.energy ? a.c.energy + ((size_t)a.c.it) * 2 : nullptr, eu, ew);
 }
 
 // ------------------------------------------------ gathers, snapshots
@@ -283,6 +494,48 @@ cudaError_t launch_step64(const Step64 &a, int threads, cudaStream_t st)
 {
     int blocks = (a.c.n + threads - 1) / threads;
     step64_kernel<<<blocks, threads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+size_t cm_scalar_count() { return (size_t)(CM_MAXIT + 1) * 4 * CM_COLS; }
+
+cudaError_t launch_cm_diag(const Cm64 &g, cudaStream_t st)
+{
+    if (g.n > 0) cm_diag_kernel<<<(g.n + 255) / 256, 256, 0, st>>>(g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cm_rhs(const Step64 &a, const Cm64 &g, cudaStream_t st)
+{
+    const int n = std::max(a.c.n, a.c.seis_row >= 0 ? a.c.nrec : 0);
+    if (n > 0) cm_rhs_kernel<<<(n + 127) / 128, 128, 0, st>>>(a, g);
+    return cudaGetLastError();
+}
+
+int queue_cm_solve(const Cm64 &g, cudaStream_t st)
+{
+    if (cudaMemsetAsync(g.sc, 0, sizeof(double) * cm_scalar_count(), st) != cudaSuccess) return -1;
+    if (cudaMemsetAsync(g.done, 0, sizeof(int), st) != cudaSuccess) return -1;
+    const unsigned blocks = (unsigned)((g.n + kCmThreads - 1) / kCmThreads);
+    int launches = 0;
+    if (blocks) {
+        cm_init_kernel<<<blocks, kCmThreads, 0, st>>>(g);
+        launches++;
+        for (int t = 0; t < CM_MAXIT; t++) {
+            cm_spmm_kernel<<<blocks, kCmThreads, 0, st>>>(g, t);
+            cm_update_kernel<<<blocks, kCmThreads, 0, st>>>(g, t);
+            cm_direction_kernel<<<blocks, kCmThreads, 0, st>>>(g, t);
+            launches += 3;
+        }
+        cm_check_kernel<<<1, 1, 0, st>>>(g);
+        launches++;
+    }
+    return cudaGetLastError() == cudaSuccess ? launches : -1;
+}
+
+cudaError_t launch_cm_newmark(const Step64 &a, const Cm64 &g, cudaStream_t st)
+{
+    if (a.c.n > 0) cm_newmark_kernel<<<(a.c.n + 127) / 128, 128, 0, st>>>(a, g);
     return cudaGetLastError();
 }
 

@@ -49,6 +49,32 @@ struct Step64 {
 enum StepKind { STEP_FP32_KAHAN = 0, STEP_FP32 = 1, STEP_FP64 = 2 };
 
 cudaError_t launch_step64(const Step64 &a, int threads, cudaStream_t st);
+
+// Consistent-mass solves (elastic_wave.c:664-680, 730-746: solver "pardiso" /
+// "mgmres"): the 14 right-hand sides of a step are solved with M itself by a
+// Jacobi-preconditioned conjugate gradient over all 14 columns at once.
+constexpr int CM_COLS = 14;
+constexpr int CM_MAXIT = 64;          // iterations queued per step (later ones return at once)
+constexpr double CM_TOL = 1e-12;      // |r| <= CM_TOL |b| per column
+struct Cm64 {
+    int n;
+    const int *up, *uj;
+    const double *mx;                 // M on the union pattern (value stream 0)
+    double *dinv;                     // [n] 1 / M_ii
+    double *B, *X, *R, *Z, *P, *Q;    // [n][14]; X holds the previous step's solution
+    double *sc;                       // [CM_MAXIT + 1][4][14]: r.z, b.b, p.q, r.r
+    int *done;                        // all columns converged
+    int *fails;                       // steps whose solve did not converge (accumulated)
+};
+size_t cm_scalar_count();
+cudaError_t launch_cm_diag(const Cm64 &g, cudaStream_t st);
+// the products and right-hand sides of step64_kernel into g.B (and the
+// receiver gather of the step's input state)
+cudaError_t launch_cm_rhs(const Step64 &a, const Cm64 &g, cudaStream_t st);
+// M X = B; returns the number of kernels queued, or -1
+int queue_cm_solve(const Cm64 &g, cudaStream_t st);
+// Newmark update from the solved accelerations and memory variables
+cudaError_t launch_cm_newmark(const Step64 &a, const Cm64 &g, cudaStream_t st);
 // receiver gather of a finished state (after the last step), snapshots
 cudaError_t launch_gather64(const StepCommon &c, const double *G, int S, cudaStream_t st);
 cudaError_t launch_snapshot64(const double *G, int n, double *snap_u, double *snap_w, cudaStream_t st);

@@ -11,12 +11,16 @@ reference sources are available; the fixtures travel, the reference does not).
                   place by oracle/ref_acoustic_harness.c): u snapshots and
                   energy per step, with the seeded vp, the lumped mass of
                   density 1 and the canonical CSR of stiffness type 0
+  consistent_small.npz  small elastic_wave() runs of the reference's
+                  consistent-mass branch (solver "mgmres": restarted GMRES + ILU
+                  on M, solver/mgmres/mgmres.c), dt inside that scheme's
+                  stability limit
   examples.npz    subsets of the reference's committed EXAMPLE outputs
                   (example 2: Q4 internal mesh, snapshots; example 6: T3
                   exterior mesh with a free surface, seismograms) and the mesh
                   of example 6 (its input files)
 
-Usage: make -C oracle && python tests/golden/make_golden.py [acoustic]
+Usage: make -C oracle && python tests/golden/make_golden.py [acoustic|consistent]
 """
 from __future__ import annotations
 
@@ -101,6 +105,21 @@ def acoustic_small(R, RA):
     np.savez_compressed(os.path.join(HERE, "acoustic_small.npz"), **out)
 
 
+CONSISTENT_RUNS = [("Q4", 16, 402, 5e-4, 3, 5), ("T3", 14, 402, 5e-4, 3, 6)]
+
+
+def consistent_small(R):
+    out = {}
+    for t, n, step, dt, pml, seed in CONSISTENT_RUNS:
+        p = small_problem(t, n=n, step=step, pml=pml, seed=seed, dt=dt)
+        r = R.run(p, nthreads=4, solver="mgmres")
+        assert r["status"] == 0
+        key = f"{t}_{n}"
+        out[key + "_seis_u"], out[key + "_seis_w"] = r["seis_u"], r["seis_w"]
+        out[key + "_snap_u"], out[key + "_snap_w"] = r["snap_u"], r["snap_w"]
+    np.savez_compressed(os.path.join(HERE, "consistent_small.npz"), **out)
+
+
 def read_rows(path, stride=1, max_rows=None):
     rows = []
     with open(path) as f:
@@ -132,11 +151,14 @@ def examples():
 
 if __name__ == "__main__":
     R = Reference()
-    only_acoustic = sys.argv[1:] == ["acoustic"]
-    if not only_acoustic:
+    part = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if part == "all":
         csr_small(R)
         runs_small(R)
         examples()
-    acoustic_small(R, ReferenceAcoustic())
-    for f in ("csr_small.npz", "runs_small.npz", "examples.npz", "acoustic_small.npz"):
+    if part in ("all", "acoustic"):
+        acoustic_small(R, ReferenceAcoustic())
+    if part in ("all", "consistent"):
+        consistent_small(R)
+    for f in ("csr_small.npz", "runs_small.npz", "examples.npz", "acoustic_small.npz", "consistent_small.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
