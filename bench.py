@@ -51,6 +51,12 @@ def workload(name: str, rank: int = 0):
     elif name == "q4_200_grf_64shots":
         # the batched kernels on a smaller mesh (profiling case; state > L2)
         p = P.config_3a(n=200, step=500)
+    elif name == "q4_200_consistent":
+        # config 1's mesh and model through the consistent-mass branch (solver
+        # "mgmres"), at dt = 0.5 ms, inside that scheme's stability limit
+        p = P.config_1(step=2002)
+        p.dt = 5e-4
+        p.name = "config1_q4_200_consistent_mass_dt0.5ms"
     else:
         raise SystemExit(f"unknown workload {name}")
     if rank and len(p.src_node) == 1:
@@ -101,7 +107,7 @@ def clocks_stop(proc, f, path, device):
     return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(prob_name: str, seconds_budget: float = 30.0) -> dict:
+def cpu_baseline(prob_name: str, seconds_budget: float = 30.0, solver: str = "masslump", nsteps: int = 8) -> dict:
     """The reference's own CPU loop (oracle/_ref) on this host's cores, on a
     bounded sample: the full set-up plus a few time steps of the workload,
     each step timed from the reference's end-of-step output."""
@@ -109,21 +115,20 @@ def cpu_baseline(prob_name: str, seconds_budget: float = 30.0) -> dict:
     import oracle as O
     prob = workload(prob_name)
     cores = os.cpu_count() or 1
-    nsteps = 8
     prob.step = 2 + nsteps
     if os.path.exists(O.LIBREF):
         ref = O.Reference()
-        out = ref.run(prob, nthreads=cores, want_snapshots=False)
+        out = ref.run(prob, nthreads=cores, want_snapshots=False, solver=solver)
         t = out["step_end_times"]
         dts = np.diff(t)
         per_step = float(np.median(dts)) if len(dts) else float("nan")
         kind = "reference"
-        sample = (f"{prob.name}: reference elastic_wave() with step={prob.step} ({nsteps} time steps, "
+        sample = (f"{prob.name}: reference elastic_wave() solver {solver} with step={prob.step} ({nsteps} time steps, "
                   f"set-up {t[0] - (t[1] - t[0]) if len(t) > 1 else float('nan'):.1f} s excluded); "
                   f"median of per-step times from its end-of-step seismogram writes")
     else:
         orc = O.Oracle()
-        out = orc.run(prob, nthreads=cores)
+        out = orc.run(prob, nthreads=cores, solver=solver)
         per_step = out["loop_seconds"] / nsteps
         kind = "port"
         sample = f"{prob.name}: oracle port, {nsteps} time steps, loop time only"
@@ -143,7 +148,8 @@ def run_reference_arm(args):
     n = args.warmup + args.steps
     prob.step = 2 + n
     if os.path.exists(O.LIBREF):
-        out = O.Reference().run(prob, nthreads=cores, want_snapshots=False)
+        solver = "mgmres" if args.workload == "q4_200_consistent" else "masslump"
+        out = O.Reference().run(prob, nthreads=cores, want_snapshots=False, solver=solver)
         t = out["step_end_times"]
         dts = np.diff(np.concatenate([[t[0] - (t[1] - t[0])], t])) if len(t) > 1 else np.array([np.nan])
         timed = dts[args.warmup:args.warmup + args.steps]
@@ -260,6 +266,92 @@ def acoustic_reference(c, nsteps: int) -> dict:
     return {"value": N / per_step, "unit": "node-steps/s", "cores": cores, "kind": kind,
             "sample": f"{c.name}: {what}, {nsteps} time steps on {cores} host threads; median per-step time",
             "seconds_per_step": per_step}
+
+
+def consistent_bytes(N: int, union_nnz: int, steps: int, iterations: int) -> int:
+    """Algorithmic bytes of a consistent-mass run (FP64): per time step the
+    right-hand-side kernel (the union pattern with 7 FP64 values and its
+    column, the 20-value state record and 12 coefficients read, 14 values
+    written) and the Newmark kernel (14 solved values, 20 + 12 state values
+    read and written); per conjugate-gradient iteration q = M p (M's
+    column and value, p read and q written, 14 columns), the update (x, p,
+    q, r read; x, r, z written; 1/diag) and the new directions (z, p read,
+    p written)."""
+    per_step = union_nnz * (4 + 7 * 8) + N * 8 * (20 + 12 + 14) + N * 8 * (14 + 2 * (20 + 12))
+    per_iter = union_nnz * (4 + 8) + N * 8 * (14 * (2 + 7 + 3) + 1)
+    return steps * per_step + iterations * per_iter
+
+
+def run_consistent(args):
+    """The consistent-mass branch (SFG_FP64_CONSISTENT): one bench step = one
+    complete simulation of the workload, device-resident (CUDA events around
+    the plan's launch); e2e = sfg_setup + sfg_run from host arrays."""
+    import torch
+    from seisfem_b200.api import Context, Plan
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = 0
+    torch.cuda.set_device(dev)
+    prob = workload(args.workload)
+    N, steps = prob.mesh.node_num, prob.step - 2
+    ctx = Context(dev)
+    ctx.setup(prob)
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    plan = Plan(ctx, prob, precision="fp64cm", snap_every=0)
+    for _ in range(args.warmup):
+        plan.launch(0, sh)
+    torch.cuda.synchronize(dev)
+    plan.finish(0, stream=sh)
+    cpath = os.path.join(tempfile.gettempdir(), "sfg_clocks_cm.csv")
+    cproc, cf = clocks_start(cpath)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.launch(0, sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = clocks_stop(cproc, cf, cpath, dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    res = plan.finish(0, stream=sh)
+    st = ctx.stats()
+    iters = int(st["cm_iterations"])
+    launches = plan.launches
+    plan.close()
+    b_run = consistent_bytes(N, st["union_nnz"], steps, iters)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = b_run / (ms * 1e-3) / 1e9
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        c2 = Context(dev)
+        c2.setup(prob)
+        c2.run(prob, precision="fp64cm", snap_every=200)
+        times.append(time.perf_counter() - t0)
+        c2.close()
+    m, md = prob.mesh, prob.model
+    h2d = sum(a.nbytes for a in (m.element_node, m.x, m.y, md.rho, md.vp, md.vs, md.c))
+    ns = ctx.L.sfg_snapshot_rows(prob.step, 200)
+    d2h = 2 * 8 * steps * len(prob.rec_node) + 2 * 8 * ns * N
+    dof_steps = 2 * N * steps
+    line = {"metric": METRIC, "value": dof_steps / (ms * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": prob.name, "element": m.type_name, "nodes": N, "dof": prob.dof,
+                       "time_steps": steps, "dt": prob.dt, "solver": "consistent mass (pardiso / mgmres branch)",
+                       "cg_iterations_per_time_step": iters / steps, "union_nnz": st["union_nnz"],
+                       "l2": "CG vectors (6 x 14 doubles per node) + matrix: fits L2 at this size"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "algorithmic_bytes_per_run": b_run,
+                         "note": "whole run (step kernels + CG iterations) over its CUDA-event time"},
+            "e2e": {"value": dof_steps / float(min(times)), "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "cpu_baseline": None if args.no_cpu_baseline else cpu_baseline(args.workload, solver="mgmres", nsteps=4),
+            "clocks": clocks, "gpu_launches": launches * args.steps, "energy_status": int(res["status"])}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
 
 
 def run_surrogate(args):
@@ -520,6 +612,8 @@ def main():
         return run_reference_arm(args)
     if args.workload in ACOUSTIC_WORKLOADS:
         return run_acoustic(args)
+    if args.workload == "q4_200_consistent":
+        return run_consistent(args)
     if args.workload == "surrogate_q4_128":
         return run_surrogate(args)
     if args.workload == "q4_16meshes":

@@ -109,6 +109,8 @@ typedef struct {
     int pml_rows;              /* rows with a non-zero M-PML profile */
     int value_tuples;          /* distinct (M / rho, K1..K6) tuples the one-shot step kernels read
                                   from a dictionary; 0 when they stream full values per entry */
+    int cm_iterations;         /* SFG_FP64_CONSISTENT: conjugate-gradient iterations of the last
+                                  finished batch, all its steps together */
 } sfg_stats;
 
 /* ---------------------------------------------------------- context API */

@@ -53,7 +53,8 @@ class Stats_(C.Structure):
     _fields_ = [("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_ms", C.c_double),
                 ("dof_steps", C.c_longlong), ("union_nnz", C.c_longlong), ("csr_nnz", C.c_longlong * 7),
                 ("kernel_launches", C.c_int), ("rows_per_block", C.c_int), ("blowup_step", C.c_int),
-                ("interior_rows", C.c_int), ("pml_rows", C.c_int), ("value_tuples", C.c_int)]
+                ("interior_rows", C.c_int), ("pml_rows", C.c_int), ("value_tuples", C.c_int),
+                ("cm_iterations", C.c_int)]
 
 
 class AcousticDesc_(C.Structure):
@@ -344,6 +345,8 @@ class Plan:
 
     def launch(self, batch: int = 0, stream: int = 0):
         self.ctx._check(self.L.sfg_plan_launch(self.ptr, batch, stream or None))
+        # plans queued directly (consistent mass) count their kernels as they queue them
+        self.launches = self.L.sfg_plan_launches(self.ptr)
 
     def finish(self, batch: int = 0, out=None, stream: int = 0, raise_on_blowup: bool = True):
         """Wait for `batch`, copy its outputs into `out` (dict of host arrays;

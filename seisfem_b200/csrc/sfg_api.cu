@@ -560,6 +560,7 @@ Cm64 cm_view(const DevProblem &P, const BatchBufs &b)
     g.sc = b.cm + 6 * w + n;
     g.done = b.cmi;
     g.fails = b.cmi + 1;
+    g.iters = b.cmi + 2;
     return g;
 }
 
@@ -706,8 +707,8 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
         }
         if (pl.kind == SFG_FP64_CONSISTENT) {
             CK(palloc(ctx, &b.cm, sizeof(double) * ((size_t)N * (6 * CM_COLS + 1) + cm_scalar_count())));
-            CK(palloc(ctx, &b.cmi, sizeof(int) * 2));
-            CK(cudaMemsetAsync(b.cmi, 0, sizeof(int) * 2, st));
+            CK(palloc(ctx, &b.cmi, sizeof(int) * 3));
+            CK(cudaMemsetAsync(b.cmi, 0, sizeof(int) * 3, st));
             CK(launch_cm_diag(cm_view(ctx->P, b), st));
         }
     } else {
@@ -753,6 +754,7 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
         // the first guess of the first step's solves (later steps start from
         // the previous solution, like the reference's GMRES calls)
         z(b.cm ? b.cm + (size_t)N * CM_COLS : nullptr, sizeof(double) * (size_t)N * CM_COLS);
+        z(b.cmi ? b.cmi + 2 : nullptr, sizeof(int));   // iterations of this batch
     } else {
         for (int k = 0; k < 2; k++) {
             z(b.Gc[k], b.gc_bytes); z(b.Pa[k], b.pa_bytes); z(b.Gs[k], b.gs_bytes); z(b.Ps[k], b.gs_bytes);
@@ -1126,6 +1128,11 @@ int plan_finish(sfg_plan *p, int batch, double *seis_u, double *seis_w, double *
     }
     if (status == SFG_ERR_BLOWUP)
         ctx->err = "energy exceeds maximum value at step " + std::to_string(ctx->stats.blowup_step);
+    if (p->b.cmi) {
+        int iters = 0;
+        CK(cudaMemcpy(&iters, p->b.cmi + 2, sizeof(int), cudaMemcpyDeviceToHost));
+        ctx->stats.cm_iterations = iters;
+    }
     if (status == SFG_OK && p->b.cmi) {
         int fails = 0;
         CK(cudaMemcpy(&fails, p->b.cmi + 1, sizeof(int), cudaMemcpyDeviceToHost));

@@ -307,7 +307,10 @@ __global__ void __launch_bounds__(kCmThreads) cm_direction_kernel(const Cm64 g, 
             g.P[o] = g.Z[o] + beta * g.P[o];
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && all) *g.done = 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *g.iters += 1;
+        if (all) *g.done = 1;
+    }
 }
 
 // a solve that used every queued iteration without converging

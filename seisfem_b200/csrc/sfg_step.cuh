@@ -65,6 +65,7 @@ struct Cm64 {
     double *sc;                       // [CM_MAXIT + 1][4][14]: r.z, b.b, p.q, r.r
     int *done;                        // all columns converged
     int *fails;                       // steps whose solve did not converge (accumulated)
+    int *iters;                       // iterations run (accumulated)
 };
 size_t cm_scalar_count();
 cudaError_t launch_cm_diag(const Cm64 &g, cudaStream_t st);
