@@ -545,9 +545,12 @@ struct BatchBufs {
     // records with the geometric mass matrix
     float *cmm = nullptr, *sig = nullptr, *rec_geo = nullptr;
     // consistent-mass solves: B, X, R, Z, P, Q [N][14], 1/diag(M) [N],
-    // scalars; flags: converged, failed solves
+    // scalars; flags: converged, failed solves, iterations
     double *cm = nullptr;
     int *cmi = nullptr;
+    // the solve of one step (its buffers do not change from step to step),
+    // captured once: one graph launch per step instead of ~200 kernel launches
+    cudaGraphExec_t cm_exec = nullptr;
 };
 
 Cm64 cm_view(const DevProblem &P, const BatchBufs &b)
@@ -577,6 +580,7 @@ void free_bufs(sfg_ctx *ctx, BatchBufs &b)
     pfree(ctx, b.pst); pfree(ctx, b.peq); pfree(ctx, b.prhs); pfree(ctx, b.panew);
     pfree(ctx, b.cmm); pfree(ctx, b.sig); pfree(ctx, b.rec_geo);
     pfree(ctx, b.cm); pfree(ctx, b.cmi);
+    if (b.cm_exec) cudaGraphExecDestroy(b.cm_exec);
     b = BatchBufs();
 }
 
@@ -631,9 +635,9 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             } else {
                 const Cm64 g = cm_view(P, b);
                 if (launch_cm_rhs(a, g, st) != cudaSuccess) return -1;
-                const int ns = queue_cm_solve(g, st);
-                if (ns < 0 || launch_cm_newmark(a, g, st) != cudaSuccess) return -1;
-                launches += 2 + ns;
+                if (cudaGraphLaunch(b.cm_exec, st) != cudaSuccess) return -1;
+                if (launch_cm_newmark(a, g, st) != cudaSuccess) return -1;
+                launches += 2 + 2 + 3 * CM_MAXIT;
             }
         } else {
             Step2 a;
@@ -710,6 +714,18 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
             CK(palloc(ctx, &b.cmi, sizeof(int) * 3));
             CK(cudaMemsetAsync(b.cmi, 0, sizeof(int) * 3, st));
             CK(launch_cm_diag(cm_view(ctx->P, b), st));
+            CK(cudaStreamSynchronize(st));
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const int nq = queue_cm_solve(cm_view(ctx->P, b), st);
+            const cudaError_t ec = cudaStreamEndCapture(st, &g);
+            if (nq < 0 || ec != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return fail(ctx, SFG_ERR_CUDA, "capture of the consistent-mass solve failed");
+            }
+            const cudaError_t ei = cudaGraphInstantiate(&b.cm_exec, g, 0);
+            cudaGraphDestroy(g);
+            CK(ei);
         }
     } else {
         for (int k = 0; k < 2; k++) {
