@@ -227,14 +227,17 @@ __global__ void fill_value(double *p, int n, double v)
     if (i < n) p[i] = v;
 }
 
-// device buffers of one run, freed on every return path
+// device buffers of one run (from the device's stream-ordered pool), released
+// in stream order on every return path
 struct Bufs {
+    cudaStream_t st;
     std::vector<void *> ptrs;
-    ~Bufs() { for (void *p : ptrs) cudaFree(p); }
+    explicit Bufs(cudaStream_t s) : st(s) {}
+    ~Bufs() { for (void *p : ptrs) keep_free(p, st); }
     template <typename T>
     cudaError_t get(T **p, size_t n)
     {
-        cudaError_t e = cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(n, 1));
+        cudaError_t e = keep_alloc(p, sizeof(T) * std::max<size_t>(n, 1), st);
         if (e == cudaSuccess) ptrs.push_back(*p);
         return e;
     }
@@ -323,7 +326,7 @@ extern "C" int sfg_acoustic_run(sfg_ctx *ctx, const sfg_mesh *m, const double *v
     cudaStream_t st = ctx_stream(ctx);
     const auto t_setup = std::chrono::steady_clock::now();
     const int pml = d->pml ? 1 : 0, NV = pml ? 5 : 2;
-    Bufs B;
+    Bufs B(st);
 
     // element matrices: M (density 1) and K0, or M, K1, K5, K2, K6
     int *d_en, *d_flags, *d_ci, *d_cj;
@@ -357,7 +360,7 @@ extern "C" int sfg_acoustic_run(sfg_ctx *ctx, const sfg_mesh *m, const double *v
         ~CanonGuard()
         {
             canon_free(c, false, s);
-            cudaFree(c.up); cudaFree(c.uj); cudaFree(c.ux);
+            keep_free(c.up, s); keep_free(c.uj, s); keep_free(c.ux, s);
         }
     } guard{co, st};
     if (rc != SFG_OK) return ctx_fail(ctx, rc, "acoustic canonical CSR: " + err);

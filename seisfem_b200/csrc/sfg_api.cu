@@ -118,7 +118,7 @@ int fail(sfg_ctx *c, int code, const std::string &msg)
 template <typename T>
 cudaError_t upload(T **d, const T *h, size_t n, cudaStream_t st)
 {
-    cudaError_t e = cudaMalloc((void **)d, sizeof(T) * std::max<size_t>(n, 1));
+    cudaError_t e = keep_alloc(d, sizeof(T) * std::max<size_t>(n, 1), st);
     if (e != cudaSuccess) return e;
     if (n) e = cudaMemcpyAsync(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st);
     return e;
@@ -158,15 +158,17 @@ int type_code_of(const char *t)
     return -1;
 }
 
-void free_problem(DevProblem &P)
+// the set-up's arrays back to the pool, in stream order on st
+void free_problem(DevProblem &P, cudaStream_t st)
 {
-    cudaFree(P.up); cudaFree(P.uj); cudaFree(P.ux);
-    for (auto &c : P.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
-    cudaFree(P.mass_lump); cudaFree(P.mpml); cudaFree(P.coef64); cudaFree(P.dirichlet);
-    cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.perm); cudaFree(P.inv);
-    cudaFree(P.sellA); cudaFree(P.sellZ); cudaFree(P.sliceA); cudaFree(P.sliceZ); cudaFree(P.upp);
-    cudaFree(P.dict); cudaFree(P.sellAd); cudaFree(P.sellZd); cudaFree(P.rowrho);
-    cudaFree(P.recp); cudaFree(P.recA); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ); cudaFree(P.rho0);
+    for (void *p : {(void *)P.up, (void *)P.uj, (void *)P.ux}) keep_free(p, st);
+    for (auto &c : P.csr) { keep_free(c.p, st); keep_free(c.j, st); keep_free(c.x, st); c = DevCsr(); }
+    for (void *p : {(void *)P.mass_lump, (void *)P.mpml, (void *)P.coef64, (void *)P.dirichlet, (void *)P.coef32,
+                    (void *)P.coefd, (void *)P.perm, (void *)P.inv, (void *)P.sellA, (void *)P.sellZ,
+                    (void *)P.sliceA, (void *)P.sliceZ, (void *)P.upp, (void *)P.dict, (void *)P.sellAd,
+                    (void *)P.sellZd, (void *)P.rowrho, (void *)P.recp, (void *)P.recA, (void *)P.coefA,
+                    (void *)P.imA, (void *)P.coefZ, (void *)P.rho0})
+        keep_free(p, st);
     P = DevProblem();
 }
 
@@ -220,7 +222,8 @@ void sfg_destroy(sfg_ctx *c)
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    free_problem(c->P);
+    free_problem(c->P, c->stream);
+    cudaStreamSynchronize(c->stream);
     for (auto &p : c->plain_x) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->stream2) cudaStreamDestroy(c->stream2);
@@ -273,7 +276,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     auto t0 = std::chrono::steady_clock::now();
     CK(cudaSetDevice(ctx->device));
     ctx->ready = false;
-    free_problem(ctx->P);
+    free_problem(ctx->P, ctx->stream);
     const int tc = type_code_of(m->type);
     if (tc < 0) return fail(ctx, SFG_ERR_ARG, std::string("unknown element type ") + (m->type ? m->type : "(null)"));
     const int p = elem_order_host(tc);
@@ -301,7 +304,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(upload(&d_y, m->y, (size_t)N, st));
     CK(upload(&d_rho, md->rho, (size_t)N, st));
     CK(upload(&P.coef64, md->c, (size_t)4 * N, st));
-    CK(cudaMalloc(&d_flags, sizeof(int)));
+    CK(keep_alloc(&d_flags, sizeof(int), st));
     CK(cudaMemsetAsync(d_flags, 0, sizeof(int), st));
     // the COO streams are set-up temporaries: from the device's pool
     CK(tmp_alloc((void **)&d_ci, sizeof(int) * nnz, st));
@@ -317,7 +320,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (hflags & FLAG_ZERO_AREA) {
-        cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+        for (void *q : {(void *)d_en, (void *)d_x, (void *)d_y, (void *)d_rho, (void *)d_flags}) keep_free(q, st);
         cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
         return fail(ctx, SFG_ERR_ZERO_AREA, "an element has zero area");
     }
@@ -327,7 +330,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     tr.mark("setup: canonical CSR");
     if (rc != SFG_OK) {
         canon_free(co, false, st);
-        cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_rho); cudaFree(d_flags);
+        for (void *q : {(void *)co.up, (void *)co.uj, (void *)co.ux}) keep_free(q, st);
+        for (void *q : {(void *)d_en, (void *)d_x, (void *)d_y, (void *)d_rho, (void *)d_flags}) keep_free(q, st);
         cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
         return rc;
     }
@@ -335,8 +339,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     P.up = co.up; P.uj = co.uj; P.ux = co.ux; P.union_nnz = co.union_nnz; P.max_row_len = co.max_row_len;
 
     // lumped mass (mass_sparse_*.c, lumpflag = 1)
-    CK(cudaMalloc(&P.mass_lump, sizeof(double) * N));
-    CK(cudaMalloc(&d_scr, sizeof(double) * (2 * (size_t)E + 2)));
+    CK(keep_alloc(&P.mass_lump, sizeof(double) * N, st));
+    CK(keep_alloc(&d_scr, sizeof(double) * (2 * (size_t)E + 2), st));
     CK(launch_lumped_mass(tc, N, E, d_en, d_x, d_y, d_rho, co.row_start, co.bucket, d_cj, P.mass_lump, d_scr,
                           d_flags, st));
 
@@ -349,7 +353,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     const double d0x = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * tx);
     const double d0y = 3.0 * vp_max * std::log10(1.0 / Rcoef) / (2.0 * ty);
     tr.mark("setup: lumped mass");
-    CK(cudaMalloc(&P.mpml, sizeof(double) * 6 * (size_t)N));
+    CK(keep_alloc(&P.mpml, sizeof(double) * 6 * (size_t)N, st));
     CK(launch_mpml(N, d_x, d_y, co.row_start, d0x, d0y, tx, ty, m->xmin + tx, m->xmax - tx, m->ymin + ty,
                    m->ymax - ty, 1, 1 - m->free_surface, 1, 1, P.mpml, st));
 
@@ -403,7 +407,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
                                      &P.slotsZ, st));
             CK(build_row_density(N, d_rho, P.perm, &P.rowrho, st));
             CK(cudaStreamSynchronize(st));
-            cudaFree(tid);
+            keep_free(tid, st);
         } else {
             CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA,
                                 &P.slotsA, st));
@@ -417,8 +421,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(cudaStreamSynchronize(st));
     tr.mark("setup: SELL, records");
     canon_free(co, true, st);
-    cudaFree(d_en); cudaFree(d_x); cudaFree(d_y); cudaFree(d_flags);
-    cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st); cudaFree(d_scr);
+    for (void *q : {(void *)d_en, (void *)d_x, (void *)d_y, (void *)d_flags, (void *)d_scr}) keep_free(q, st);
+    cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
     P.rho0 = d_rho;
     P.h_rho0.assign(md->rho, md->rho + N);
     P.h_dir = std::move(dir);
@@ -497,7 +501,8 @@ int sfg_lumped_mass_set(sfg_ctx *ctx, const double *mass_lump)
     DevProblem &P = ctx->P;
     CK(cudaStreamSynchronize(ctx->stream));   // no queued work may still read the old values
     CK(cudaMemcpy(P.mass_lump, mass_lump, sizeof(double) * ctx->N, cudaMemcpyHostToDevice));
-    cudaFree(P.coef32); cudaFree(P.coefd); cudaFree(P.coefA); cudaFree(P.imA); cudaFree(P.coefZ);
+    for (void *q : {(void *)P.coef32, (void *)P.coefd, (void *)P.coefA, (void *)P.imA, (void *)P.coefZ})
+        keep_free(q, ctx->stream);
     P.coef32 = nullptr; P.coefd = nullptr; P.coefA = nullptr; P.imA = nullptr; P.coefZ = nullptr;
     CK(build_coef(ctx->N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, ctx->stream));
     CK(build_coef2(ctx->N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, ctx->stream));
@@ -914,9 +919,9 @@ void plan_free(sfg_plan *p)
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     free_bufs(p->ctx, p->b);
-    cudaFree(p->d_src_all);
-    cudaFree(p->d_cmm_all);
-    cudaFree(p->d_sig_all);
+    keep_free(p->d_src_all, p->ctx->stream);
+    keep_free(p->d_cmm_all, p->ctx->stream);
+    keep_free(p->d_sig_all, p->ctx->stream);
     delete p;
 }
 

@@ -540,7 +540,7 @@ __global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict_
 void canon_free(CanonOut &o, bool keep_csr, cudaStream_t st)
 {
     if (!keep_csr)
-        for (auto &c : o.csr) { cudaFree(c.p); cudaFree(c.j); cudaFree(c.x); c = DevCsr(); }
+        for (auto &c : o.csr) { keep_free(c.p, st); keep_free(c.j, st); keep_free(c.x, st); c = DevCsr(); }
     if (o.row_start) cudaFreeAsync(o.row_start, st);
     if (o.bucket) cudaFreeAsync(o.bucket, st);
     o.row_start = nullptr;
@@ -588,29 +588,29 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     // row pointers: union + each stream
     int *up = nullptr;
     if (want_union) {
-        SFG_TRY(cudaMalloc(&up, sizeof(int) * ((size_t)N + 1)));
+        SFG_TRY(keep_alloc(&up, sizeof(int) * ((size_t)N + 1), st));
         SFG_TRY(exclusive_scan_int(cu, up, N, st));
         int tot = 0;
         SFG_TRY(cudaMemcpyAsync(&tot, up + N, sizeof(int), cudaMemcpyDeviceToHost, st));
         SFG_TRY(cudaStreamSynchronize(st));
         out.union_nnz = tot;
         out.up = up;
-        SFG_TRY(cudaMalloc(&out.uj, sizeof(int) * std::max<size_t>(tot, 1)));
-        SFG_TRY(cudaMalloc(&out.ux, sizeof(double) * (size_t)nv * std::max<size_t>(tot, 1)));
+        SFG_TRY(keep_alloc(&out.uj, sizeof(int) * std::max<size_t>(tot, 1), st));
+        SFG_TRY(keep_alloc(&out.ux, sizeof(double) * (size_t)nv * std::max<size_t>(tot, 1), st));
     }
     int *dvp[8] = {nullptr}, *dvj[8] = {nullptr};
     double *dvx[8] = {nullptr};
     if (want_csr) {
         for (int s = 0; s < nv; s++) {
             DevCsr &c = out.csr[s];
-            SFG_TRY(cudaMalloc(&c.p, sizeof(int) * ((size_t)N + 1)));
+            SFG_TRY(keep_alloc(&c.p, sizeof(int) * ((size_t)N + 1), st));
             SFG_TRY(exclusive_scan_int(cv + (size_t)s * N, c.p, N, st));
             int tot = 0;
             SFG_TRY(cudaMemcpyAsync(&tot, c.p + N, sizeof(int), cudaMemcpyDeviceToHost, st));
             SFG_TRY(cudaStreamSynchronize(st));
             c.nnz = tot;
-            SFG_TRY(cudaMalloc(&c.j, sizeof(int) * std::max<size_t>(tot, 1)));
-            SFG_TRY(cudaMalloc(&c.x, sizeof(double) * std::max<size_t>(tot, 1)));
+            SFG_TRY(keep_alloc(&c.j, sizeof(int) * std::max<size_t>(tot, 1), st));
+            SFG_TRY(keep_alloc(&c.x, sizeof(double) * std::max<size_t>(tot, 1), st));
             dvp[s] = c.p; dvj[s] = c.j; dvx[s] = c.x;
         }
     }

@@ -258,8 +258,8 @@ int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, 
         if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, &s->bad, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e == cudaSuccess && !bad) {
-            e = cudaMalloc(d_table, sizeof(float4) * 2 * (size_t)count);
-            if (e == cudaSuccess) e = cudaMalloc(d_tid, sizeof(int) * std::max<long long>(nnz, 1));
+            e = keep_alloc(d_table, sizeof(float4) * 2 * (size_t)count, st);
+            if (e == cudaSuccess) e = keep_alloc(d_tid, sizeof(int) * std::max<long long>(nnz, 1), st);
             if (e == cudaSuccess) {
                 dict_compact<<<1, 1024, 0, st>>>(s, *d_table);
                 dict_ids<<<(unsigned)((nnz + 255) / 256), 256, 0, st>>>(nnz, s, slot_of, *d_tid);
@@ -273,8 +273,8 @@ int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, 
         }
     }
     if (T < 0) {   // not applicable (too many tuples, a collision) or an error
-        cudaFree(*d_tid);
-        cudaFree(*d_table);
+        keep_free(*d_tid, st);
+        keep_free(*d_table, st);
         *d_tid = nullptr;
         *d_table = nullptr;
     }
@@ -293,14 +293,14 @@ cudaError_t build_sell_range_dict(int r0, int r1, const int *d_up, const int *d_
     int *len = nullptr;
     cudaError_t e;
     if ((e = cudaMallocAsync((void **)&len, sizeof(int) * ((size_t)nsl + 1), st)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_slice, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_slice, sizeof(int) * ((size_t)nsl + 1), st)) != cudaSuccess) return e;
     if ((e = launch_range_slice_len(r0, r1, d_up, d_perm, len, st)) != cudaSuccess) return e;
     if ((e = exclusive_scan_int(len, *d_slice, nsl, st)) != cudaSuccess) return e;
     int tot = 0;
     cudaMemcpyAsync(&tot, *d_slice + nsl, sizeof(int), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     *slots = tot;
-    if ((e = cudaMalloc(d_sell, sizeof(int2) * 32 * std::max<size_t>(tot, 1))) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_sell, sizeof(int2) * 32 * std::max<size_t>(tot, 1), st)) != cudaSuccess) return e;
     if (nsl) range_sell_fill_dict<<<nsl, 32, 0, st>>>(r0, r1, d_up, d_uj, d_tid, zero_id, *d_slice, d_perm, d_inv, *d_sell);
     e = cudaGetLastError();
     cudaFreeAsync(len, st);
@@ -309,7 +309,7 @@ cudaError_t build_sell_range_dict(int r0, int r1, const int *d_up, const int *d_
 
 cudaError_t build_row_density(int n, const double *d_rho, const int *d_perm, float **d_out, cudaStream_t st)
 {
-    cudaError_t e = cudaMalloc(d_out, sizeof(float) * std::max(n, 1));
+    cudaError_t e = keep_alloc(d_out, sizeof(float) * std::max(n, 1), st);
     if (e == cudaSuccess && n > 0) {
         row_density<<<(n + 255) / 256, 256, 0, st>>>(n, d_rho, d_perm, *d_out);
         e = cudaGetLastError();

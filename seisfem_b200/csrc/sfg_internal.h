@@ -124,6 +124,21 @@ inline cudaError_t tmp_alloc(void **p, size_t bytes, cudaStream_t st)
     if (!pool) return cudaErrorMemoryAllocation;
     return cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, st);
 }
+// The long-lived arrays of a set-up (DevProblem) and of plans come from the
+// same pool, which keeps released blocks mapped: allocating and releasing the
+// ~1-2 GB of a large set-up then costs microseconds, where cudaMalloc and
+// cudaFree map and unmap the pages of every block (up to ~300 ms per set-up
+// and release of a 641,601-node Q9 problem).  Usable from any stream once
+// `st` has reached the allocation; released in stream order on `st`.
+template <typename T>
+inline cudaError_t keep_alloc(T **p, size_t bytes, cudaStream_t st)
+{
+    return tmp_alloc((void **)p, bytes, st);
+}
+inline void keep_free(void *p, cudaStream_t st)
+{
+    if (p) cudaFreeAsync(p, st);
+}
 
 // ---- step data and kernels (sfg_step.cu) ---------------------------------
 int build_step_data(DevProblem &P, const double *d_c, double dt_unused, std::string &err,

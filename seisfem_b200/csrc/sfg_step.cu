@@ -617,7 +617,7 @@ cudaError_t launch_plain_gather(const Plain32 &a, cudaStream_t st)
 
 cudaError_t permute_rows(int n, int width, const float *d_src, const int *d_perm, float **d_dst, cudaStream_t st)
 {
-    cudaError_t e = cudaMalloc(d_dst, sizeof(float) * width * std::max(n, 1));
+    cudaError_t e = keep_alloc(d_dst, sizeof(float) * width * std::max(n, 1), st);
     if (e != cudaSuccess) return e;
     long long tot = (long long)n * width;
     if (tot) permute_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, width, d_src, d_perm, *d_dst);
@@ -628,8 +628,8 @@ cudaError_t build_coef(int n, const double *d_c, const double *d_mpml, const dou
                        const unsigned char *d_dir, float **d_coef32, double **d_coef64, cudaStream_t st)
 {
     cudaError_t e;
-    if ((e = cudaMalloc(d_coef32, sizeof(float) * CREC * std::max(n, 1))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_coef64, sizeof(double) * CREC * std::max(n, 1))) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_coef32, sizeof(float) * CREC * std::max(n, 1), st)) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_coef64, sizeof(double) * CREC * std::max(n, 1), st)) != cudaSuccess) return e;
     coef_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, d_c, d_mpml, d_mass, d_dir, *d_coef32, *d_coef64);
     return cudaGetLastError();
 }

@@ -1447,26 +1447,26 @@ cudaError_t build_sell_range(int r0, int r1, const int *d_up, const int *d_uj, c
     const int n = r1 - r0, nsl = (n + 31) / 32;
     int *len = nullptr;
     cudaError_t e;
-    if ((e = cudaMalloc(&len, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_slice, sizeof(int) * ((size_t)nsl + 1))) != cudaSuccess) return e;
+    if ((e = tmp_alloc((void **)&len, sizeof(int) * ((size_t)nsl + 1), st)) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_slice, sizeof(int) * ((size_t)nsl + 1), st)) != cudaSuccess) return e;
     if (nsl) range_slice_len<<<(nsl + 127) / 128, 128, 0, st>>>(r0, r1, d_up, d_perm, len);
     if ((e = exclusive_scan_int(len, *d_slice, nsl, st)) != cudaSuccess) return e;
     int tot = 0;
     cudaMemcpyAsync(&tot, *d_slice + nsl, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     *slots = tot;
-    if ((e = cudaMalloc(d_sell, sizeof(float) * planes * 32 * std::max<size_t>(tot, 1))) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_sell, sizeof(float) * planes * 32 * std::max<size_t>(tot, 1), st)) != cudaSuccess) return e;
     if (nsl) range_sell_fill<<<nsl, 32, 0, st>>>(r0, r1, d_up, d_uj, d_ux, nnz, *d_slice, d_perm, d_inv, planes, *d_sell);
     e = cudaGetLastError();
     cudaStreamSynchronize(st);
-    cudaFree(len);
+    cudaFreeAsync(len, st);
     return e;
 }
 
 cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double *d_ux, long long nnz,
                            const int *d_perm, const int *d_inv, const int *d_upp, float **d_rec, cudaStream_t st)
 {
-    cudaError_t e = cudaMalloc(d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1));
+    cudaError_t e = keep_alloc(d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1), st);
     if (e != cudaSuccess) return e;
     if (n) rec_perm_fill<<<(n + 127) / 128, 128, 0, st>>>(n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, *d_rec);
     return cudaGetLastError();
@@ -1479,7 +1479,7 @@ cudaError_t build_rec_fold(int n, int na, const int *d_up, const int *d_uj, cons
     int nnz_a = 0;
     cudaError_t e = cudaMemcpyAsync(&nnz_a, d_upp + na, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaMalloc(d_rec, sizeof(float) * 8 * std::max(nnz_a, 1));
+    if (e == cudaSuccess) e = keep_alloc(d_rec, sizeof(float) * 8 * std::max(nnz_a, 1), st);
     if (e == cudaSuccess && na > 0) {
         rec_fold_fill<<<(na + 127) / 128, 128, 0, st>>>(na, n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, d_c, *d_rec);
         e = cudaGetLastError();
@@ -1491,9 +1491,9 @@ cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm,
                         float **d_coefZ, cudaStream_t st)
 {
     cudaError_t e;
-    if ((e = cudaMalloc(d_coefA, sizeof(float4) * std::max(na, 1))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_imA, sizeof(float) * std::max(na, 1))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(d_coefZ, sizeof(float) * CREC * std::max(n - na, 1))) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_coefA, sizeof(float4) * std::max(na, 1), st)) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_imA, sizeof(float) * std::max(na, 1), st)) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_coefZ, sizeof(float) * CREC * std::max(n - na, 1), st)) != cudaSuccess) return e;
     if (n) coef2_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, na, d_coef32, d_perm, *d_coefA, *d_imA, *d_coefZ);
     return cudaGetLastError();
 }
@@ -1512,9 +1512,9 @@ cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double 
     A((void **)&isA, sizeof(int) * n); A((void **)&isZ, sizeof(int) * n);
     A((void **)&posA, sizeof(int) * (n + 1)); A((void **)&posZ, sizeof(int) * (n + 1));
     A((void **)&perm0, sizeof(int) * n); A((void **)&lenp, sizeof(int) * n); A((void **)&cnt, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(d_perm, sizeof(int) * std::max(n, 1));
-    if (e == cudaSuccess) e = cudaMalloc(d_inv, sizeof(int) * std::max(n, 1));
-    if (e == cudaSuccess) e = cudaMalloc(d_upp, sizeof(int) * (n + 1));
+    if (e == cudaSuccess) e = keep_alloc(d_perm, sizeof(int) * std::max(n, 1), st);
+    if (e == cudaSuccess) e = keep_alloc(d_inv, sizeof(int) * std::max(n, 1), st);
+    if (e == cudaSuccess) e = keep_alloc(d_upp, sizeof(int) * (n + 1), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(int), st);
     const int g = (n + 255) / 256;
     int na = 0, npml = 0;
