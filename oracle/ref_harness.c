@@ -19,8 +19,9 @@
  *   exit           returns to the harness with status 1 (energy bound,
  *                  elastic_wave.c:779-785);
  *   printf         silenced unless SFR_VERBOSE is set.
- * PARDISO / MGMRES are not on the masslump path; their entry points are
- * stubs that return to the harness with status 3.
+ * PARDISO (a proprietary library, absent) is a stub that returns to the
+ * harness with status 3; solver "mgmres" runs the reference's own
+ * solver/mgmres/mgmres.c (the consistent-mass branch).
  */
 #include <math.h>
 #include <omp.h>
