@@ -93,7 +93,8 @@ def structured_mesh(type_name: str, nelemx: int, nelemy: int, xmin: float, xmax:
 
     Q4/T3 nodes: mesh/mesh_xy_q4.c:40-47 (``((n-i)*min + i*max)/(1.0*n)``);
     Q9/T6 nodes: mesh/mesh_xy_q9.c:44-51 (``i*(max-min)/(2.0*n)``, no offset);
-    connectivity: mesh/mesh_element_{q4,t3,q9,t6}.c.
+    Q16/T10 nodes: mesh/mesh_xy_q16.c (``i*(max-min)/(3.0*n)``, no offset);
+    connectivity: mesh/mesh_element_{q4,t3,q9,t6,q16,t10}.c.
     """
     nx, ny = nelemx, nelemy
     if type_name in ("Q4", "T3"):
@@ -134,6 +135,26 @@ def structured_mesh(type_name: str, nelemx: int, nelemy: int, xmin: float, xmax:
         else:
             en = np.stack([np.stack([sw, se, nw, s, c, w], 1), np.stack([ne, nw, se, n, c, e], 1)],
                           axis=1).reshape(-1, 6)
+    elif type_name in ("Q16", "T10"):
+        # cubic elements on the (3nx+1) x (3ny+1) node grid:
+        # mesh/mesh_xy_{q16,t10}.c (``i*(max-min)/(3.0*n)``, no offset),
+        # mesh/mesh_element_{q16,t10}.c (element base node, then rows of 4)
+        row = 3 * nx + 1
+        i = np.arange(row)
+        j = np.arange(3 * ny + 1)
+        xs = i * (xmax - xmin) / (3.0 * nx)
+        ys = j * (ymax - ymin) / (3.0 * ny)
+        X = np.tile(xs, 3 * ny + 1)
+        Y = np.repeat(ys, row)
+        jj, ii = np.meshgrid(np.arange(1, ny + 1), np.arange(1, nx + 1), indexing="ij")
+        b = ((jj - 1) * 3 * row + 3 * ii - 2).ravel()
+        g = lambda r, c: b + r * row + c          # node in grid row r, column c of the element
+        if type_name == "Q16":
+            en = np.stack([g(r, c) for r in range(4) for c in range(4)], axis=1)
+        else:
+            lower = [g(0, 0), g(0, 1), g(0, 2), g(0, 3), g(1, 2), g(2, 1), g(3, 0), g(2, 0), g(1, 0), g(1, 1)]
+            upper = [g(3, 3), g(3, 2), g(3, 1), g(3, 0), g(2, 1), g(1, 2), g(0, 3), g(1, 3), g(2, 3), g(2, 2)]
+            en = np.stack([np.stack(lower, 1), np.stack(upper, 1)], axis=1).reshape(-1, 10)
     else:
         raise NotImplementedError(f"structured {type_name} meshes are not generated here")
     return Mesh(type_name, np.ascontiguousarray(en.ravel(), np.int32),

@@ -16,7 +16,7 @@ FP32_TOL = 1e-4      # seismogram / snapshot rel-L2 vs the FP64 oracle
 FP64_TOL = 1e-10
 
 
-@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6"])
+@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6", "T10", "Q16"])
 def test_csr_bit_exact(ctx, oracle, etype):
     p = small_problem(etype, n=9, step=10, pml=2, seed=3)
     ctx.setup(p)
@@ -30,7 +30,7 @@ def test_csr_bit_exact(ctx, oracle, etype):
         assert np.array_equal(gx, Bx), (etype, k)
 
 
-@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6"])
+@pytest.mark.parametrize("etype", ["Q4", "Q9", "T3", "T6", "T10", "Q16"])
 def test_lumped_mass_and_mpml(ctx, oracle, etype):
     p = small_problem(etype, n=9, step=10, pml=2, seed=5)
     ctx.setup(p)
@@ -62,6 +62,24 @@ def test_fp64_run_matches_oracle(ctx, oracle, etype, n, step, dt):
     out = ctx.run(p, precision="fp64")
     for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
         assert np.array_equal(out[k], ref[k]), (k, rel_l2(out[k], ref[k]))
+
+
+@pytest.mark.parametrize("etype", ["T10", "Q16"])
+def test_cubic_fp64_identical_until_the_energy_bound(ctx, oracle, etype):
+    """Cubic elements: with the oracle's lumped mass the FP64 loop reproduces
+    the oracle (itself identical to the reference) up to the step at which
+    the reference's energy bound ends the run, and stops at that step."""
+    from seisfem_b200.api import SFG_ERR_BLOWUP
+    p = small_problem(etype, n=8, step=202, pml=2, seed=3, dt=5e-4)
+    ref = oracle.run(p, energy=True)
+    assert ref["status"] == 1
+    stop = int(np.nonzero(ref["energy_u"][0])[0].max())     # the step whose energy passed the bound
+    ctx.setup(p)
+    ctx.set_lumped_mass(oracle.mass_lumped(p.mesh, p.model.rho))
+    out = ctx.run(p, precision="fp64", raise_on_blowup=False)
+    assert out["status"] == SFG_ERR_BLOWUP and out["stats"]["blowup_step"] == stop
+    for k in ("seis_u", "seis_w"):
+        assert np.array_equal(out[k][:, :stop - 2], ref[k][:, :stop - 2]), k
 
 
 @pytest.mark.parametrize("precision", ["fp32k", "fp32", "plain"])
