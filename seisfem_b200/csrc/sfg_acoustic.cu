@@ -22,7 +22,9 @@
 // (mesh order), slot k of row i at [(sbase[i/32] + k) * 32 + i%32]; columns as
 // int32 and the NV matrix values of a slot as NV doubles, each plane of 32
 // lanes contiguous, so a warp's loads of one slot are fully coalesced.  Rows
-// loop to their own length: padding slots are never read.  State vectors are
+// loop to their own length: padding slots are never read.  Streams read once
+// per step (slots, per-node coefficients) load with the evict-first hint,
+// leaving L1 to the neighbour gathers.  State vectors are
 // FP64 [N]: u_old / u_now / u_new rotate through three buffers (acoustic.c),
 // u1 and u2 likewise, p1, p2 and u through two (acoustic_pml.c).
 #include <cuda_runtime.h>
@@ -85,18 +87,18 @@ __global__ void __launch_bounds__(kThreads) acoustic_step(const AcStep a)
         const int *cp = a.col + (size_t)base * 32 + lane;
         const double *vq = a.val + (size_t)base * 2 * 32 + lane;
         double y1 = 0.0, y2 = 0.0, y3 = 0.0;   // K u_now, M u_now, M u_old
-        int jn = len > 0 ? __ldg(cp) : 0;       // the next slot's column, one slot ahead
+        int jn = len > 0 ? __ldcs(cp) : 0;      // the next slot's column, one slot ahead
         for (int k = 0; k < len; k++) {
             const int j = jn;
-            jn = k + 1 < len ? __ldg(cp + (size_t)(k + 1) * 32) : 0;
-            const double mv = __ldg(vq + (size_t)k * 64), kv = __ldg(vq + (size_t)k * 64 + 32);
+            jn = k + 1 < len ? __ldcs(cp + (size_t)(k + 1) * 32) : 0;
+            const double mv = __ldcs(vq + (size_t)k * 64), kv = __ldcs(vq + (size_t)k * 64 + 32);
             const double b = __ldg(a.u1n + j), o = __ldg(a.u1o + j);
             y1 = y1 + kv * b;
             y2 = y2 + mv * b;
             y3 = y3 + mv * o;
         }
-        const double rhs = (double)(i == a.src) * a.ps - __ldg(a.cv + i) * y1 + 2.0 * y2 - y3;
-        const double m = __ldg(a.m + i);
+        const double rhs = (double)(i == a.src) * a.ps - __ldcs(a.cv + i) * y1 + 2.0 * y2 - y3;
+        const double m = __ldcs(a.m + i);
         const double u = m != 0.0 ? rhs / (1.0 * m) : __ldg(a.u1n + i);
         a.u1w[i] = u;
         if (a.snap) a.snap[i] = u;
@@ -113,8 +115,8 @@ struct PmlSums {
     double z1 = 0.0, z2 = 0.0, z3 = 0.0, z4 = 0.0, z5 = 0.0;
     __device__ __forceinline__ void add(const AcStep &a, int j, const double *v)
     {
-        const double mv = __ldg(v), k1 = __ldg(v + 32), k5 = __ldg(v + 64), k2 = __ldg(v + 96),
-                     k6 = __ldg(v + 128);
+        const double mv = __ldcs(v), k1 = __ldcs(v + 32), k5 = __ldcs(v + 64), k2 = __ldcs(v + 96),
+                     k6 = __ldcs(v + 128);
         const double u = __ldg(a.un + j);
         x1 = x1 + mv * __ldg(a.u1n + j);
         x2 = x2 + mv * __ldg(a.u1o + j);
@@ -143,17 +145,17 @@ __global__ void __launch_bounds__(kThreads) acoustic_pml_step(const AcStep a)
         const int *cp = a.col + (size_t)base * 32 + lane;
         const double *vq = a.val + (size_t)base * 5 * 32 + lane;
         PmlSums s;
-        int jn = len > 0 ? __ldg(cp) : 0;
+        int jn = len > 0 ? __ldcs(cp) : 0;
         for (int k = 0; k < len; k++) {
             const int j = jn;
-            jn = k + 1 < len ? __ldg(cp + (size_t)(k + 1) * 32) : 0;
+            jn = k + 1 < len ? __ldcs(cp + (size_t)(k + 1) * 32) : 0;
             s.add(a, j, vq + (size_t)k * 160);
         }
         const double x1 = s.x1, x2 = s.x2, x3 = s.x3, x4 = s.x4, x5 = s.x5;
         const double z1 = s.z1, z2 = s.z2, z3 = s.z3, z4 = s.z4, z5 = s.z5;
-        const double dt = a.dt, cv = __ldg(a.cv + i);
-        const double dx = __ldg(a.pdx + i), dy = __ldg(a.pdy + i);
-        const double dxx = __ldg(a.pdxx + i), dyy = __ldg(a.pdyy + i);
+        const double dt = a.dt, cv = __ldcs(a.cv + i);
+        const double dx = __ldcs(a.pdx + i), dy = __ldcs(a.pdy + i);
+        const double dxx = __ldcs(a.pdxx + i), dyy = __ldcs(a.pdyy + i);
         // the M p products of equations 2 and 4 repeat those of 1 and 3 (same
         // rows, same order, same operands): x3, z3
         const double rhs1 = 2.0 * x1 - x2 - 2.0 * dt * dx * x1 + 2 * dt * dx * x2 - dt * dt * dx * dx * x1 +
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kThreads) acoustic_pml_step(const AcStep a)
         const double rhs3 = 2.0 * z1 - z2 - 2.0 * dt * dy * z1 + 2 * dt * dy * z2 - dt * dt * dy * dy * z1 +
                             cv * z4 + cv * z3;
         const double rhs4 = z3 - dt * dy * z3 - dt * dyy * z5;
-        const double m = __ldg(a.m + i);
+        const double m = __ldcs(a.m + i);
         double u1, p1, u2, p2;
         if (m != 0.0) {
             u1 = rhs1 / (1.0 * m);
