@@ -137,16 +137,45 @@ def cpu_baseline(prob_name: str, seconds_budget: float = 30.0, solver: str = "ma
             "seconds_per_step": per_step}
 
 
+def bench_config(prob, shots_per_rank: int, world: int) -> dict:
+    """The workload's description, shared by both arms so that their config
+    objects are identical: what is simulated, not how."""
+    return {"workload": prob.name, "element": prob.mesh.type_name, "nodes": prob.mesh.node_num,
+            "dof": prob.dof, "shots_per_rank": shots_per_rank, "time_steps": prob.step - 2,
+            "l2": "per-step working set (matrix + state) > 126 MB L2; no flush needed",
+            "parallelism": f"shots over {world} GPU(s)"}
+
+
+def mapped_repo_libraries() -> list:
+    """Shared objects of this repository mapped into this process."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            f = line.split()
+            if len(f) >= 6 and f[-1].endswith(".so") and f[-1].startswith(ROOT):
+                out.add(os.path.relpath(f[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference_arm(args):
+    """The reference's own elastic_wave() (oracle/_ref, compiled from the
+    reference sources; else the oracle port) on the host cores.  Its problem
+    is built with the numpy node scan, so this process never loads
+    libseisfem_b200.so (checked below)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    P.use_scan_locator()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     prob = workload(args.workload)
+    cfg = bench_config(prob, len(prob.src_node), args.gpus)
     cores = os.cpu_count() or 1
     n = args.warmup + args.steps
     prob.step = 2 + n
+    prob.src_node = prob.src_node[:1]
     if os.path.exists(O.LIBREF):
         solver = "mgmres" if args.workload == "q4_200_consistent" else "masslump"
         out = O.Reference().run(prob, nthreads=cores, want_snapshots=False, solver=solver)
@@ -159,14 +188,18 @@ def run_reference_arm(args):
         timed = np.full(args.steps, out["loop_seconds"] / n)
         kind = "port"
     ms = float(np.sum(timed)) * 1e3
+    # every shot of the workload costs the same per time step; one is timed
     value = 2 * prob.mesh.node_num * args.steps / (ms / 1e3)
-    sample = (f"{prob.name}: {n} time steps of the reference elastic_wave() loop on {cores} host threads; "
-              f"bench step = one time step; the first {args.warmup} are warm-up")
+    sample = (f"{prob.name}: {n} time steps of one shot of the reference elastic_wave() loop on {cores} host "
+              f"threads; bench step = one time step; the first {args.warmup} are warm-up")
+    libs = mapped_repo_libraries()
+    assert "seisfem_b200.api" not in sys.modules and not any(l.startswith("seisfem_b200") for l in libs), libs
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": prob.name, "nodes": prob.mesh.node_num, "dof": prob.dof, "element": "Q9",
-                       "time_steps_per_bench_step": 1},
+            "config": cfg,
+            "run": {"precision": "fp64 (the reference's own C)", "time_steps_per_bench_step": 1,
+                    "repo_libraries_loaded": libs},
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -767,12 +800,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64",
                 "data": "synthetic",
-                "config": {"workload": prob.name, "element": prob.mesh.type_name, "nodes": prob.mesh.node_num,
-                           "dof": prob.dof, "shots_per_rank": S, "time_steps": prob.step - 2,
-                           "precision": args.precision, "union_nnz": st["union_nnz"],
-                           "setup_ms": round(st["setup_ms"], 1),
-                           "l2": "per-step working set (matrix + state) > 126 MB L2; no flush needed",
-                           "parallelism": f"shots over {world} GPU(s)"},
+                "config": bench_config(prob, S, world),
+                "run": {"precision": args.precision, "union_nnz": st["union_nnz"],
+                        "setup_ms": round(st["setup_ms"], 1), "repo_libraries_loaded": mapped_repo_libraries()},
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches,
                 "launch_shape": launch_shape(st["rows_per_block"], S),

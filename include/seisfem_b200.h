@@ -247,17 +247,23 @@ int sfg_node_location(int node_num, double edge_size, const double *x, const dou
  *
  * d_element_node (1-based), d_x, d_y: device arrays; d_out6: device
  * [6][node_num] = dx, dy, dxx, dyy, dxx*pyx, dyy*pxy; nodes of no element keep
- * their values.  The work runs on `stream` (a cudaStream_t, NULL = legacy
- * default stream) and the call returns after it has finished.
+ * their values.  The work runs on `stream` (a cudaStream_t) and the call
+ * returns after it has finished.  Use a stream created with
+ * cudaStreamNonBlocking: NULL (the legacy default stream) is accepted, but it
+ * waits for, and holds up, every blocking stream of the device, which defeats
+ * running next to other work.
  *
  * Scratch: a fixed device array of SFG_NOALLOC_MAX_NODES + 256 bytes inside
- * the library; the call clears what it uses itself, so nothing has to start
- * at zero.  node_num above SFG_NOALLOC_MAX_NODES returns SFG_ERR_LIMIT.
- * The first call on each device looks up the scratch address; make it
- * before any stream capture.  Calls that overlap in time on one device (two
- * host threads, or two streams) share the scratch and race: serialise them.
- * Returns SFG_ERR_BADINDEX when an element_node entry is outside
- * 1..node_num (those entries are skipped). */
+ * the library (every device that loads the library holds it until exit); the
+ * call clears what it uses itself, so nothing has to start at zero.
+ * node_num above SFG_NOALLOC_MAX_NODES returns SFG_ERR_LIMIT.  Each call
+ * looks up the scratch address in the current context (the first call on a
+ * device loads it); make that first call before any stream capture.  The call
+ * waits for its stream to read back an error word, so a stream that is being
+ * captured is refused with SFG_ERR_ARG.  Calls that overlap in time on one
+ * device (two host threads, or two streams) share the scratch and race:
+ * serialise them.  Returns SFG_ERR_BADINDEX, with d_out6 untouched, when an
+ * element_node entry is outside 1..node_num. */
 #define SFG_NOALLOC_MAX_NODES (1 << 22)
 int sfg_abc_mpml_device_noalloc(int node_num, int element_num, int element_order, const int *d_element_node,
                                 const double *d_x, const double *d_y, int mpml_nx, int mpml_ny, double h,

@@ -12,7 +12,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 
 #include "../../include/seisfem_b200.h"
 #include "sfg_mpml.cuh"
@@ -23,10 +22,6 @@ constexpr int kErrOffset = 0;      // int: set to 1 when an element_node entry i
 constexpr int kFlagOffset = 256;   // node_num bytes: 1 = referenced by some element
 
 __device__ __align__(256) unsigned char g_mpml_scratch[kFlagOffset + SFG_NOALLOC_MAX_NODES];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char *g_addr[kMaxDevices];   // scratch address per device, looked up once
 
 // Clears the error word and the first n flags (every call starts from zero;
 // a previous call may have marked more nodes).
@@ -75,21 +70,29 @@ __global__ void noalloc_mpml(int n, const double *__restrict__ xa, const double 
 
 int status_of(cudaError_t e) { return e == cudaSuccess ? SFG_OK : SFG_ERR_CUDA; }
 
-// Address of the scratch array on the current device: one symbol lookup per
-// device, made with that device current.
+// Address of the scratch array in the current context, looked up on every
+// call: a context that the caller reset and re-created reloads the module at
+// another address, so a cached address could point at freed memory.  The
+// lookup allocates nothing.
 int scratch_address(unsigned char **out)
 {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SFG_ERR_NODEVICE;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_mpml_scratch);
-        if (e != cudaSuccess || !p) return e == cudaErrorNoKernelImageForDevice ? SFG_ERR_NODEVICE : SFG_ERR_CUDA;
-        g_addr[dev] = static_cast<unsigned char *>(p);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_mpml_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return e == cudaErrorNoKernelImageForDevice || e == cudaErrorNoDevice ? SFG_ERR_NODEVICE : SFG_ERR_CUDA;
     }
-    *out = g_addr[dev];
+    *out = static_cast<unsigned char *>(p);
     return SFG_OK;
+}
+
+// Reads the error word back (pageable host memory: the copy completes before
+// the call returns) and waits for the stream.
+int read_error_word(const unsigned char *scr, cudaStream_t st, int *bad)
+{
+    int rc = status_of(cudaMemcpyAsync(bad, scr + kErrOffset, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (rc) return rc;
+    return status_of(cudaStreamSynchronize(st));
 }
 
 }  // namespace
@@ -105,10 +108,16 @@ int sfg_abc_mpml_device_noalloc(int node_num, int element_num, int element_order
     if (node_num <= 0 || element_num < 0 || element_order <= 0 || !d_element_node || !d_x || !d_y || !d_out6)
         return SFG_ERR_ARG;
     if (node_num > SFG_NOALLOC_MAX_NODES) return SFG_ERR_LIMIT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call waits for its stream (it reads the error word back), which a
+    // stream that is being captured does not allow: refuse rather than
+    // invalidate the caller's capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) { cudaGetLastError(); return SFG_ERR_ARG; }
+    if (cap != cudaStreamCaptureStatusNone) return SFG_ERR_ARG;
     unsigned char *scr = nullptr;
     int rc = scratch_address(&scr);
     if (rc) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // abc_mpml.c:57-61 on the host (log10 of the host library)
     const double Rcoef = 0.0001;
     const double tx = h * mpml_nx, ty = h * mpml_ny;
@@ -119,14 +128,16 @@ int sfg_abc_mpml_device_noalloc(int node_num, int element_num, int element_order
     noalloc_clear<<<(node_num + 16 * 256 - 1) / (16 * 256), 256, 0, st>>>(scr, node_num);
     if (cnt > 0) noalloc_mark<<<(unsigned)std::min<long long>((cnt + 255) / 256, 148 * 16), 256, 0, st>>>(
         d_element_node, cnt, node_num, scr);
+    if ((rc = status_of(cudaGetLastError()))) return rc;
+    // like sfg_abc_mpml, a bad element_node entry leaves d_out6 untouched
+    int bad = 0;
+    if ((rc = read_error_word(scr, st, &bad))) return rc;
+    if (bad) return SFG_ERR_BADINDEX;
     noalloc_mpml<<<nblk, 256, 0, st>>>(node_num, d_x, d_y, scr, d0x, d0y, tx, ty, xmin + tx, xmax - tx, ymin + ty,
                                        ymax - ty, use_mpml_xmin, use_mpml_xmax, use_mpml_ymin, use_mpml_ymax,
                                        d_out6);
     if ((rc = status_of(cudaGetLastError()))) return rc;
-    int bad = 0;
-    if ((rc = status_of(cudaMemcpyAsync(&bad, scr + kErrOffset, sizeof(int), cudaMemcpyDeviceToHost, st)))) return rc;
-    if ((rc = status_of(cudaStreamSynchronize(st)))) return rc;
-    return bad ? SFG_ERR_BADINDEX : SFG_OK;
+    return status_of(cudaStreamSynchronize(st));
 }
 
 }  // extern "C"

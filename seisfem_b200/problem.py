@@ -230,12 +230,27 @@ def line_points(n, first, last):
              first[1] + i * (last[1] - first[1]) / (1.0 * (n - 1))) for i in range(n)]
 
 
+_SCAN_LOCATOR = False
+
+
+def use_scan_locator(on: bool = True) -> None:
+    """Make ``locate`` use the numpy scan (``node_location``) instead of the
+    library's grid locator.  A process that times the reference's own code
+    builds its problems this way, so it never loads libseisfem_b200.so; both
+    locators return the same nodes (the last-match rule)."""
+    global _SCAN_LOCATOR
+    _SCAN_LOCATOR = bool(on)
+
+
 def locate(mesh, edge_size, pts):
     """Node indices of points (sfg_node_location: the reference's rule with a
     grid instead of a scan per point)."""
-    from .api import node_location as locate_all
     pts = np.asarray(pts, np.float64).reshape(-1, 2)
-    out = locate_all(mesh.x, mesh.y, edge_size, pts[:, 0], pts[:, 1])
+    if _SCAN_LOCATOR:
+        out = np.array([node_location(mesh, edge_size, px, py) for px, py in pts], np.int32)
+    else:
+        from .api import node_location as locate_all
+        out = locate_all(mesh.x, mesh.y, edge_size, pts[:, 0], pts[:, 1])
     if (out < 0).any():
         raise ValueError("a source or receiver lies outside the mesh")
     return out

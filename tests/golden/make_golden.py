@@ -20,7 +20,8 @@ reference sources are available; the fixtures travel, the reference does not).
                   exterior mesh with a free surface, seismograms) and the mesh
                   of example 6 (its input files)
 
-Usage: make -C oracle && python tests/golden/make_golden.py [acoustic|consistent]
+Usage: SEISFEM_REFERENCE=<reference tree> make -C oracle &&
+       SEISFEM_REFERENCE=<reference tree> python tests/golden/make_golden.py [acoustic|consistent]
 """
 from __future__ import annotations
 
@@ -34,7 +35,11 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-REF = os.environ.get("SEISFEM_REFERENCE", "/root/reference")
+REF = os.environ.get("SEISFEM_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "time_evolution")):
+    raise SystemExit("set SEISFEM_REFERENCE to the reference source tree (the directory holding "
+                     "time_evolution/, assemble/, EXAMPLE/, ...) and build oracle/_ref with "
+                     "`make -C oracle REF=$SEISFEM_REFERENCE` first")
 
 from oracle import Reference, ReferenceAcoustic  # noqa: E402
 from seisfem_b200.problem import small_problem, structured_mesh  # noqa: E402
