@@ -36,9 +36,10 @@ METRIC = "DOF-steps/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "step_kernel_traffic.txt")
 T6_STABLE_STEPS = 602
+DEFAULT_WORKLOAD = "q9_400_layered"
 
 
-def workload(name: str, rank: int = 0):
+def workload(name: str, shots: int = 1):
     if name == "q9_400_layered":
         p = P.config_2()
     elif name == "q4_200_homog":
@@ -59,11 +60,11 @@ def workload(name: str, rank: int = 0):
         p.name = "config1_q4_200_consistent_mass_dt0.5ms"
     else:
         raise SystemExit(f"unknown workload {name}")
-    if rank and len(p.src_node) == 1:
-        # each rank runs its own shot: the source moves one element per rank
+    if shots > 1 and len(p.src_node) == 1:
+        # a shot list for several ranks: the source moves one element per shot
         m = p.mesh
         x0, y0 = m.x[p.src_node[0]], m.y[p.src_node[0]]
-        p.src_node = P.locate(m, p.edge_size, [(x0, y0 + p.edge_size * rank)])
+        p.src_node = P.locate(m, p.edge_size, [(x0, y0 + p.edge_size * k) for k in range(shots)])
     return p
 
 
@@ -485,19 +486,30 @@ def run_group(args):
         c.setup(p)
         ctxs.append(c)
         plans.append(Plan(c, p, precision=args.precision, snap_every=0))
-    grp = Group(plans)
-    for _ in range(args.warmup):
-        grp.launch(sh)
-    torch.cuda.synchronize(dev)
-    for pl in plans:
-        pl.finish(0, stream=sh)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        grp.launch(sh)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / args.steps
+
+    def time_group(g):
+        for _ in range(args.warmup):
+            g.launch(sh)
+        torch.cuda.synchronize(dev)
+        for pl in plans:
+            pl.finish(0, stream=sh)
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.launch(sh)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / args.steps
+
+    # the plans' own graphs side by side (the comparison), then the fused group
+    os.environ["SFG_GROUP_CHILD_GRAPHS"] = "1"
+    child = Group(plans)
+    del os.environ["SFG_GROUP_CHILD_GRAPHS"]
+    ms_child = time_group(child)
+    child_launches = child.launches
+    child.close()
+    grp = Group(plans)
+    ms = time_group(grp)
     e0.record(stream)
     for pl in plans:
         pl.launch(0, sh)
@@ -519,7 +531,12 @@ def run_group(args):
                        "nodes_total": sum(p.mesh.node_num for p in probs), "time_steps": steps,
                        "precision": args.precision, "shots_per_mesh": 1,
                        "l2": "per-step working set of all meshes > 126 MB L2"},
+            "group_mode": "multi-mesh kernels (2 launches per time step)" if grp.fused else "child graphs",
+            "group_launch_shapes": grp.shapes,
+            "launches_per_time_step": grp.launches / steps,
             "sequential_ms": ms_seq, "group_over_sequential": ms_seq / ms,
+            "child_graphs_ms": ms_child, "child_graphs_launches_per_time_step": child_launches / steps,
+            "group_over_child_graphs": ms_child / ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "algorithmic_bytes_per_step": b_step},
             "launch_shapes": shapes, "gpu_launches": grp.launches * args.steps, "e2e": None, "cpu_baseline": None}
@@ -612,10 +629,14 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="q9_400_layered")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", default="fp32k", choices=["fp32k", "fp32", "fp64", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the config-3a batched-vs-plain section of the default workload's line")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the FP64 run that the rel_l2 field compares the timed run's outputs with")
     ap.add_argument("--compare-plain", action="store_true",
                     help="also time the unfused path (one SpMV launch per product) on one shot")
     ap.add_argument("--train-shots", type=int, default=4096)
@@ -668,8 +689,14 @@ def main():
                                 device_id=torch.device("cuda", local))
     dev = local
     torch.cuda.set_device(dev)
-    prob = workload(args.workload, rank)
+    from seisfem_b200.shots import gather_seismograms_device, shard_problem
+    # the job's shot list (one shot per rank for one-source workloads),
+    # sharded over the ranks; each rank advances its block with no
+    # communication inside the time loop
+    prob_all = workload(args.workload, world)
+    prob = shard_problem(prob_all, rank, world)
     S = len(prob.src_node)
+    S_all = len(prob_all.src_node)
     ctx = Context(dev)
     ctx.setup(prob)
     st = ctx.stats()
@@ -711,7 +738,29 @@ def main():
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
     dof_steps_rank = 2 * prob.mesh.node_num * S * (prob.step - 2)
-    value = dof_steps_rank * world * args.steps / (ms_max / 1e3)
+    dof_steps_job = 2 * prob.mesh.node_num * S_all * (prob.step - 2)
+    value = dof_steps_job * args.steps / (ms_max / 1e3)
+
+    # the job's seismograms, collected once after the loop: this rank's block
+    # copied device to device, then one all_gather over NCCL (outside the
+    # timed region; there is no collective inside the time loop)
+    gathered = None
+    if world > 1:
+        rows_, R_ = prob.step - 2, len(prob.rec_node)
+        su = torch.empty((S, rows_, R_), dtype=torch.float64, device=f"cuda:{dev}")
+        sw = torch.empty_like(su)
+        plan_g = Plan(ctx, prob, precision=args.precision, snap_every=0)
+        plan_g.launch(0, sh)
+        plan_g.finish_device(0, su.data_ptr(), sw.data_ptr(), sh)
+        plan_g.close()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        full_u = gather_seismograms_device(su, S_all, rank, world)
+        full_w = gather_seismograms_device(sw, S_all, rank, world)
+        torch.cuda.synchronize(dev)
+        gathered = {"shots": S_all, "bytes": 2 * full_u.numel() * 8, "ms": (time.perf_counter() - t0) * 1e3,
+                    "how": "all_gather_into_tensor of device tensors (NCCL)",
+                    "finite": bool(torch.isfinite(full_u).all() and torch.isfinite(full_w).all())}
 
     # roofline: the fused step kernel alone (a plan without snapshot copies),
     # average launch time = loop time / time steps, on the launching stream
@@ -765,7 +814,7 @@ def main():
         t_e2e = torch.tensor([statistics.median(times[1:])], dtype=torch.float64, device=f"cuda:{dev}")
         if world > 1:
             dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-        e2e = {"value": dof_steps_rank * world / float(t_e2e.item()), "unit": METRIC,
+        e2e = {"value": dof_steps_job / float(t_e2e.item()), "unit": METRIC,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "seconds_per_step": float(t_e2e.item()),
                "note": "one elastic_wave()-equivalent call per step: sfg_setup (GPU assembly from host arrays) + "
@@ -791,6 +840,14 @@ def main():
                  "ratio_batched_over_plain_per_shot_cost": value / (world * per_shot_plain)}
         pp.close()
 
+    parity = None
+    if not args.no_parity and args.precision != "fp64":
+        parity = fused_parity(ctx, prob, res)
+
+    batched = None
+    if world == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_batched:
+        batched = batched_section(dev, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload)
@@ -800,19 +857,139 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64",
                 "data": "synthetic",
-                "config": bench_config(prob, S, world),
+                "config": bench_config(prob_all, S_all // world if S_all % world == 0 else S_all / world, world),
                 "run": {"precision": args.precision, "union_nnz": st["union_nnz"],
                         "setup_ms": round(st["setup_ms"], 1), "repo_libraries_loaded": mapped_repo_libraries()},
                 "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches,
                 "launch_shape": launch_shape(st["rows_per_block"], S),
                 "vs_plain_path": plain,
+                "rel_l2": parity,
+                "batched": batched,
+                "gathered_seismograms": gathered,
                 "energy_status": int(res["status"])}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     ctx.close()
     return 0
+
+
+def rel_l2(a, b) -> float:
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
+
+
+REFERENCE_FIXTURES = {"config1_q4_200": "config1", "config2_q9_400": "config2"}
+
+
+def fused_parity(ctx, prob, res, shots=(0, -1)) -> dict:
+    """Relative L2 errors (||a - b|| / ||b|| over each whole output array) of
+    the timed run's seismograms and 200-step snapshots: against the FP64 GPU
+    path (the reference's operation order) run once here on the same inputs,
+    outside the timed region, and, where a committed fixture of the
+    reference's own FP64 run of this workload exists, against its values (a
+    subset: every few receivers, snapshots on a coarse node grid).  Batches
+    compare their first and last shot."""
+    S = len(prob.src_node)
+    pick = sorted({s % S for s in shots})
+    keys = [k for k in ("seis_u", "seis_w", "snap_u", "snap_w") if k in res]
+    t0 = time.perf_counter()
+    out = {"bound": 1e-4, "against": "FP64 GPU path, same inputs, every receiver and snapshot node",
+           "shots_compared": pick}
+    ref = {k: [] for k in keys}
+    for s in pick:
+        r = ctx.run(prob, precision="fp64", snap_every=200 if "snap_u" in res else 0,
+                    src_node=prob.src_node[[s]], want_snapshots="snap_u" in res)
+        for k in keys:
+            ref[k].append(r[k][0])
+    for k in keys:
+        out[k] = max(rel_l2(res[k][s], ref[k][i]) for i, s in enumerate(pick))
+    out["max"] = max(out[k] for k in keys)
+    out["fp64_seconds"] = round(time.perf_counter() - t0, 2)
+    name = REFERENCE_FIXTURES.get(prob.name)
+    path = os.path.join(ROOT, "tests", "golden", f"{name}_reference.npz") if name else None
+    if path and os.path.exists(path) and S == 1:
+        f = np.load(path)
+        rec, nodes = f["rec"], f["nodes"]
+        sub = {"seis_u": res["seis_u"][0][:, rec], "seis_w": res["seis_w"][0][:, rec]}
+        if "snap_u" in res:
+            sub["snap_u"], sub["snap_w"] = res["snap_u"][0][:, nodes], res["snap_w"][0][:, nodes]
+        fx = {k: rel_l2(v, f[k]) for k, v in sub.items()}
+        fx64 = {k: rel_l2(ref[k][0][:, rec] if k.startswith("seis") else ref[k][0][:, nodes], f[k]) for k in sub}
+        out["vs_reference_run"] = {
+            "fixture": os.path.relpath(path, ROOT),
+            "what": f"the reference's own FP64 elastic_wave() run of this workload: receivers every "
+                    f"{int(rec[1] - rec[0])}, snapshot nodes on every {int(nodes[1] - nodes[0])}th grid line",
+            "fp32": fx, "fp64_gpu": fx64, "max": max(fx.values())}
+    return out
+
+
+def batched_section(dev: int, stream, steps: int = 3, warmup: int = 3) -> dict:
+    """The metric's own comparison on config 3a (Q4 400x400 GRF, 64 shots,
+    2000 time steps): the 64-shot batch advanced as one SpMM-shaped fused
+    step per time step, against the plain single-shot FP32 path (one
+    csr_matvec launch per product, as elastic_wave.c structures the step) on
+    one of its shots; DOF-steps/s, the fused kernels' roofline, and the
+    batch's first and last shot against FP64 single-shot runs."""
+    import torch
+    from seisfem_b200.api import Context, Plan
+    prob = workload("q4_400_grf_64shots")
+    S, N, T = len(prob.src_node), prob.mesh.node_num, prob.step - 2
+    sh = stream.cuda_stream
+    ctx = Context(dev)
+    ctx.setup(prob)
+    plan = Plan(ctx, prob, precision="fp32k", snap_every=0)
+    for _ in range(warmup):
+        plan.launch(0, sh)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.launch(0, sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    res = plan.finish(0, stream=sh)
+    launches = plan.launches
+    plan.close()
+    value = 2 * N * S * T / (ms * 1e-3)
+    b_step = step_bytes(ctx, prob, S)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = b_step * T / (ms * 1e-3) / 1e9
+    # the plain single-shot FP32 path on the batch's first shot
+    pp = Plan(ctx, prob, precision="plain", snap_every=0, src_node=prob.src_node[:1])
+    pp.launch(0, sh)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    pp.launch(0, sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    pms = e0.elapsed_time(e1)
+    plain_rate = 2 * N * T / (pms * 1e-3)
+    plain_launches = pp.launches / T
+    pp.close()
+    parity = fused_parity(ctx, prob, res)
+    st = ctx.stats()
+    ctx.close()
+    return {"config": {"workload": prob.name, "element": "Q4", "nodes": N, "shots": S, "time_steps": T,
+                       "precision": "fp32k", "union_nnz": st["union_nnz"],
+                       "l2": "per-step working set > 126 MB L2; no flush needed"},
+            "value": value, "unit": METRIC, "ms_per_run": ms, "runs_timed": steps, "warmup": warmup,
+            "gpu_launches_per_run": launches,
+            "launch_shape": launch_shape(st["rows_per_block"], S),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": b_step,
+                         "avg_step_us": round(ms * 1e3 / T, 3),
+                         "kernel": "stepA/stepZ batched fused step, 64 shots innermost",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                         else "fallback"},
+            "vs_plain_path": {"plain_single_shot_dof_steps_per_s": plain_rate, "plain_ms_per_shot": pms,
+                              "plain_launches_per_time_step": plain_launches,
+                              "batched_per_shot_dof_steps_per_s": value / S,
+                              "ratio_batched_over_plain_per_shot_cost": value / plain_rate},
+            "rel_l2": parity, "energy_status": int(res["status"])}
 
 
 def launch_shape(code, S):

@@ -184,18 +184,26 @@ int sfg_plan_create_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_mode
 int sfg_run_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *models, double *seis_u,
                    double *seis_w, double *snap_u, double *snap_w);
 
-/* Plan groups (no counterpart in the reference): the captured time loops of
- * several single-batch plans -- independent meshes of any sizes, each with
- * the launch shapes its own autotuning picked -- as one CUDA graph with no
- * dependencies between them, so one launch advances all of them side by
- * side.  Results are read per plan with sfg_plan_finish(plan, 0, ...) after
- * the group's stream has finished.  A group uses its plans' buffers: do not
+/* Plan groups: several single-batch plans -- independent problems on meshes
+ * of any sizes, which the reference runs one after another
+ * (time_evolution/elastic_wave.c:446-518 loops over shots; its callers over
+ * meshes) -- advanced by one CUDA-graph launch.  When every plan is a
+ * one-shot fused FP32 plan (SFG_FP32_KAHAN or SFG_FP32) with the same step
+ * count and all or none of the meshes carry a value dictionary, the group's
+ * graph issues one class-A and one class-Z kernel per time step for all
+ * meshes together (each block finds its mesh in a block map), with the
+ * launch shapes the largest mesh's autotuning picked; other groups compose
+ * the plans' own graphs side by side (SFG_GROUP_CHILD_GRAPHS=1 forces that).
+ * Results are read per plan with sfg_plan_finish(plan, 0, ...) after the
+ * group's stream has finished.  A group uses its plans' buffers: do not
  * launch a member plan while the group runs; destroy the group before its
  * plans.  All plans must live on one device. */
 typedef struct sfg_group sfg_group;
 int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **group);
 int sfg_group_launch(sfg_group *group, void *stream);
 int sfg_group_launches(const sfg_group *group);   /* kernels one launch runs */
+/* 0: child graphs; else 1 + the multi-mesh kernels' launch shapes (class A * 16 + class Z) */
+int sfg_group_fused(const sfg_group *group);
 void sfg_group_destroy(sfg_group *group);
 int sfg_sync(sfg_ctx *ctx);
 

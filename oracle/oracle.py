@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import shutil
 import tempfile
 
 import numpy as np
@@ -253,9 +254,11 @@ class ReferenceAcoustic:
             self.lib.sfa_set_step_times(None, 0)
         # seconds of each completed time step (from its energy.dat write)
         step_seconds = np.diff(stamps[1:ne.value]) if ne.value > 2 else np.zeros(0)
+        if workdir is None:
+            shutil.rmtree(tmp, ignore_errors=True)
         return {"snap": snap.reshape(rows, N)[:ns.value // N], "energy": energy[:ne.value],
                 "energy_values": ne.value, "status": rc, "seconds": secs.value, "step_seconds": step_seconds,
-                "workdir": tmp}
+                "workdir": workdir}
 
 
 class Reference:
@@ -363,5 +366,9 @@ class Reference:
         nst = int(np.count_nonzero(step_t))
         out["step_end_times"] = step_t[:nst] - t_call     # seconds since the call began
         out["seconds"] = secs.value
-        out["workdir"] = tmp
+        if workdir is None:
+            # the text files were read back through the harness; a temporary
+            # directory made here goes (a caller's own directory stays)
+            shutil.rmtree(tmp, ignore_errors=True)
+        out["workdir"] = workdir
         return out

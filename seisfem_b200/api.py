@@ -76,7 +76,7 @@ EXPORTS = ["sfg_create", "sfg_destroy", "sfg_error_string", "sfg_last_error", "s
            "sfg_plan_launches", "sfg_plan_launch", "sfg_plan_finish", "sfg_plan_destroy", "elastic_wave", "sfg_mass_sparse_all",
            "sfg_stif_sparse_all", "sfg_coo2csr_canonical", "sfg_abc_mpml", "sfg_csr_matvec", "sfg_node_location",
            "sfg_abc_mpml_device_noalloc", "sfg_plan_create_models", "sfg_run_models", "sfg_group_create", "sfg_group_launch", "sfg_group_launches",
-           "sfg_group_destroy",
+           "sfg_group_fused", "sfg_group_destroy",
            # scalar acoustic solvers (include/seisfem_acoustic.h)
            "sfg_acoustic_snapshot_rows", "sfg_acoustic_run", "acoustic", "acoustic_pml",
            # learned surrogate (include/seisfem_fno.h)
@@ -118,6 +118,7 @@ def lib(path: str = LIBPATH):
     L.sfg_group_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     L.sfg_group_launch.argtypes = [C.c_void_p, C.c_void_p]
     L.sfg_group_launches.argtypes = [C.c_void_p]
+    L.sfg_group_fused.argtypes = [C.c_void_p]
     L.sfg_group_destroy.argtypes = [C.c_void_p]
     L.sfg_plan_launches.argtypes = [C.c_void_p]
     L.sfg_plan_launch.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -364,6 +365,15 @@ class Plan:
         out["status"] = rc
         return out
 
+    def finish_device(self, batch: int, d_seis_u: int, d_seis_w: int, stream: int = 0,
+                      raise_on_blowup: bool = True) -> int:
+        """Wait for `batch` and copy its seismograms into device buffers
+        (the full [src_num][step-2][rec] layout, this batch's shots at their
+        offset); no host copies of outputs."""
+        rc = self.L.sfg_plan_finish(self.ptr, batch, d_seis_u, d_seis_w, None, None, stream or None)
+        self.ctx._check(rc, allow=() if raise_on_blowup else (SFG_ERR_BLOWUP,))
+        return rc
+
     def close(self):
         if self.ptr:
             self.L.sfg_plan_destroy(self.ptr)
@@ -376,9 +386,36 @@ class Plan:
             pass
 
 
+def device_runner(ctx: "Context", precision: str = "fp32k", stream=None):
+    """A runner for shots.run_sharded: advances a (sub-)problem's shots on
+    the context's device with a Plan and returns its seismograms as CUDA
+    tensors [shots][step-2][rec] (torch owns the output memory)."""
+    import torch
+
+    def run(sub):
+        S, R, rows = len(sub.src_node), len(sub.rec_node), sub.step - 2
+        dev = torch.device("cuda", torch.cuda.current_device())
+        su = torch.empty((S, rows, R), dtype=torch.float64, device=dev)
+        sw = torch.empty((S, rows, R), dtype=torch.float64, device=dev)
+        if S == 0:                 # a rank with no shots still joins the gather
+            return su, sw
+        sh = stream.cuda_stream if stream is not None else 0
+        plan = Plan(ctx, sub, precision=precision, snap_every=0)
+        try:
+            for b in range(plan.batches):
+                plan.launch(b, sh)
+                plan.finish_device(b, su.data_ptr(), sw.data_ptr(), sh)
+        finally:
+            plan.close()
+        return su, sw
+    return run
+
+
 class Group:
     """Several single-batch plans (independent meshes) as one CUDA-graph
-    launch (sfg_group_*); results are read per plan with Plan.finish()."""
+    launch (sfg_group_*); results are read per plan with Plan.finish().
+    ``fused``: the graph runs one class-A and one class-Z kernel per time
+    step for all meshes (otherwise the plans' own graphs side by side)."""
 
     def __init__(self, plans):
         self.plans = list(plans)
@@ -390,6 +427,9 @@ class Group:
             raise SfgError(rc, "sfg_group_create")
         self.ptr = h
         self.launches = self.L.sfg_group_launches(h)
+        f = self.L.sfg_group_fused(h)
+        self.fused = f > 0
+        self.shapes = {"variant_A": (f - 1) // 16, "variant_Z": (f - 1) % 16} if f > 0 else None
 
     def launch(self, stream: int = 0):
         rc = self.L.sfg_group_launch(self.ptr, stream or None)

@@ -589,6 +589,39 @@ void free_bufs(sfg_ctx *ctx, BatchBufs &b)
     b = BatchBufs();
 }
 
+// Fields of the step argument block shared by every step of a batch (the
+// time index and receiver row are set per step).
+StepCommon step_common(const DevProblem &P, const LoopPlan &pl, const sfg_run_desc *run, const BatchBufs &b)
+{
+    StepCommon c;
+    c.n = P.node_num; c.dt = run->dt; c.amp = b.amp;
+    const double pi_af = 3.1415926535898;                 // elastic_wave.c:66-67
+    c.sin_af = std::sin(90.0 * pi_af / 180.0);
+    c.cos_af = std::cos(90.0 * pi_af / 180.0);
+    c.src = b.src; c.nshot = pl.S; c.rec = b.rec; c.nrec = run->rec_num; c.seis_rows = run->step - 2;
+    c.seis_u = b.seis_u; c.seis_w = b.seis_w; c.energy = b.energy; c.nsteps = run->step;
+    c.it = 2;
+    c.seis_row = -1;
+    return c;
+}
+
+// The fused FP32 step's argument block reading state buffer `cur` and
+// writing `cur ^ 1`.
+Step2 step2_args(const DevProblem &P, const LoopPlan &pl, const StepCommon &c, const BatchBufs &b, int cur)
+{
+    const int nxt = cur ^ 1;
+    Step2 a;
+    a.c = c; a.na = P.na; a.S = pl.S;
+    a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
+    a.sellAd = P.sellAd; a.sellZd = P.sellZd; a.dict = P.dict; a.dict_n = P.dict_n; a.rowrho = P.rowrho;
+    a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.recA = P.recA; a.coefA = P.coefA; a.imA = P.imA;
+    a.coefZ = P.coefZ;
+    a.cmm = b.cmm; a.sig = b.sig;
+    a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
+    a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
+    return a;
+}
+
 // Queue the whole time loop of one batch on `st` (captured into a graph by
 // the caller).  Returns the number of kernels queued, or -1 on a launch error.
 int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b, int snap_every,
@@ -597,13 +630,8 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
     const DevProblem &P = ctx->P;
     const int N = P.node_num, S = pl.S, R = run->rec_num, rows = run->step - 2;
     int launches = 0;
-    StepCommon c;
-    c.n = N; c.dt = run->dt; c.amp = b.amp;
-    const double pi_af = 3.1415926535898;                 // elastic_wave.c:66-67
-    c.sin_af = std::sin(90.0 * pi_af / 180.0);
-    c.cos_af = std::cos(90.0 * pi_af / 180.0);
-    c.src = b.src; c.nshot = S; c.rec = b.rec; c.nrec = R; c.seis_rows = rows;
-    c.seis_u = b.seis_u; c.seis_w = b.seis_w; c.energy = b.energy; c.nsteps = run->step;
+    StepCommon c = step_common(P, pl, run, b);
+    (void)R; (void)rows;
     int cur = 0, srow = 1;
     const int last = 2 + steps_to_run;   // exclusive
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
@@ -645,14 +673,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
                 launches += 2 + 2 + 3 * CM_MAXIT;
             }
         } else {
-            Step2 a;
-            a.c = c; a.na = P.na; a.S = S;
-            a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
-            a.sellAd = P.sellAd; a.sellZd = P.sellZd; a.dict = P.dict; a.dict_n = P.dict_n; a.rowrho = P.rowrho;
-            a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.recA = P.recA; a.coefA = P.coefA; a.imA = P.imA; a.coefZ = P.coefZ;
-            a.cmm = b.cmm; a.sig = b.sig;
-            a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
-            a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
+            const Step2 a = step2_args(P, pl, c, b, cur);
             const bool comp = pl.kind == SFG_FP32_KAHAN;
             // fork: the class-Z kernel on the second stream, class A here; join
             if (cudaEventRecord(ctx->ev_fork, st) != cudaSuccess) return -1;
@@ -1293,14 +1314,225 @@ void sfg_plan_destroy(sfg_plan *plan)
     plan_free(plan);
 }
 
+}  // extern "C"
+
 // ------------------------------------------------------------ plan groups
+//
+// A group advances several single-batch plans -- independent problems on
+// meshes of different sizes, the reference's serial loop over meshes and
+// shots (elastic_wave.c:446-518) -- with one graph launch.  When every plan
+// is a one-shot fused FP32 plan with the same precision and step count, the
+// group's graph issues ONE class-A and ONE class-Z kernel per time step for
+// all meshes together (stepA_multi / stepZ_multi: each block looks up its
+// mesh and block in a map and reads that mesh's step descriptor), so small
+// meshes share the SMs instead of each launch idling most of the GPU.  Other
+// groups compose the plans' own graphs as child graphs.
 
 struct sfg_group {
     int device = 0;
     int launches = 0;
+    bool fused = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    Step2 *d_desc = nullptr;     // [2][nplans]: step descriptors of both state parities
+    int2 *d_map = nullptr;       // [nblkA + nblkZ]: (mesh, block of that mesh)
+    int shapes = 0;              // one-shot launch shapes of the multi-mesh kernels: A * 16 + Z
 };
+
+namespace {
+
+void group_free(sfg_group *g)
+{
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->d_desc) cudaFree(g->d_desc);
+    if (g->d_map) cudaFree(g->d_map);
+    delete g;
+}
+
+// Plans whose loops can share the multi-mesh kernels: one batch of one shot,
+// the fused FP32 kinds, one precision and one step count, all with or all
+// without a value dictionary.
+bool group_fusable(sfg_plan *const *plans, int nplans)
+{
+    for (int i = 0; i < nplans; i++) {
+        const sfg_plan *p = plans[i];
+        if (p->pl.S != 1 || !permuted(p->pl) || p->d_cmm_all) return false;
+        if (p->pl.kind != plans[0]->pl.kind || p->run.step != plans[0]->run.step) return false;
+        if ((p->ctx->P.dict_n > 0) != (plans[0]->ctx->P.dict_n > 0)) return false;
+    }
+    return true;
+}
+
+// Capture the group's loop: every plan's state reset, then per time step one
+// class-Z launch (second stream) and one class-A launch for all meshes,
+// snapshots and the last receiver row per plan.  Returns kernels per run.
+int group_capture(sfg_group *g, sfg_plan *const *plans, int nplans, int shapeA, int shapeZ, int nblkA, int nblkZ)
+{
+    sfg_ctx *ctx0 = plans[0]->ctx;
+    cudaStream_t st = ctx0->stream, st2 = ctx0->stream2;
+    const int step = plans[0]->run.step, last = step;   // it = 2 .. step - 1
+    const bool comp = plans[0]->pl.kind == SFG_FP32_KAHAN;
+    const bool dict = ctx0->P.dict_n > 0;
+    int dict_max = 0;
+    for (int i = 0; i < nplans; i++) dict_max = std::max(dict_max, plans[i]->ctx->P.dict_n);
+    int launches = 0;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1;
+    bool ok = true;
+    for (int i = 0; i < nplans && ok; i++) {
+        sfg_plan *p = plans[i];
+        ok = queue_reset(p->pl, p->ctx->N, step, p->nsnap, p->b, st) == cudaSuccess;
+    }
+    int cur = 0;
+    std::vector<int> srow(nplans, 1);
+    for (int it = 2; it < last && ok; it++) {
+        const Step2 *descs = g->d_desc + (size_t)cur * nplans;
+        ok = cudaEventRecord(ctx0->ev_fork, st) == cudaSuccess &&
+             cudaStreamWaitEvent(st2, ctx0->ev_fork, 0) == cudaSuccess &&
+             (nblkZ == 0 ||
+              launch_stepZ_multi(descs, g->d_map + nblkA, nblkZ, dict, dict_max, comp, shapeZ, it, st2) == cudaSuccess) &&
+             launch_stepA_multi(descs, g->d_map, nblkA, dict, dict_max, comp, shapeA, it, st) == cudaSuccess &&
+             cudaEventRecord(ctx0->ev_join, st2) == cudaSuccess &&
+             cudaStreamWaitEvent(st, ctx0->ev_join, 0) == cudaSuccess;
+        launches += 1 + (nblkZ > 0);
+        cur ^= 1;
+        for (int i = 0; i < nplans && ok; i++) {
+            sfg_plan *p = plans[i];
+            const int se = p->run.snap_every;
+            if (p->nsnap > 0 && se > 0 && (it + 1) % se == 0 && srow[i] < p->nsnap) {
+                const BatchBufs &b = p->b;
+                const int N = p->ctx->N;
+                const size_t off = (size_t)srow[i] * N;
+                ok = launch_snapshot2({b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, N, p->ctx->P.na, 1, p->ctx->P.perm,
+                                      b.snap_u + off, b.snap_w + off, (long long)p->nsnap * N, st) == cudaSuccess;
+                launches++;
+                srow[i]++;
+            }
+        }
+    }
+    for (int i = 0; i < nplans && ok; i++) {
+        sfg_plan *p = plans[i];
+        StepCommon c = step_common(p->ctx->P, p->pl, &p->run, p->b);
+        c.it = last - 1;
+        c.seis_row = last - 3;
+        const BatchBufs &b = p->b;
+        ok = launch_gather2(c, p->ctx->P.na, {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]}, 1, st) == cudaSuccess;
+        launches++;
+    }
+    const cudaError_t e = cudaStreamEndCapture(st, &g->graph);
+    return ok && e == cudaSuccess ? launches : -1;
+}
+
+// Block map for launch shapes with tA / tZ threads per block: class-A blocks
+// (which also carry the receiver gather on their first nrec threads) of every
+// mesh, then class-Z blocks.
+void group_map(sfg_plan *const *plans, int nplans, int tA, int tZ, std::vector<int2> &map, int &nblkA, int &nblkZ)
+{
+    map.clear();
+    for (int i = 0; i < nplans; i++) {
+        const DevProblem &P = plans[i]->ctx->P;
+        const int na = std::max(P.na, plans[i]->run.rec_num);
+        for (int k = 0; k < (na + tA - 1) / tA; k++) map.push_back(make_int2(i, k));
+    }
+    nblkA = (int)map.size();
+    for (int i = 0; i < nplans; i++) {
+        const DevProblem &P = plans[i]->ctx->P;
+        const int nz = P.node_num - P.na;
+        for (int k = 0; k < (nz + tZ - 1) / tZ; k++) map.push_back(make_int2(i, k));
+    }
+    nblkZ = (int)map.size() - nblkA;
+}
+
+int group_create_fused(sfg_plan *const *plans, int nplans, sfg_group *g)
+{
+    sfg_ctx *ctx0 = plans[0]->ctx;
+    cudaStream_t st = ctx0->stream, st2 = ctx0->stream2;
+    const bool comp = plans[0]->pl.kind == SFG_FP32_KAHAN;
+    const bool dict = ctx0->P.dict_n > 0;
+    int dict_max = 0;
+    for (int i = 0; i < nplans; i++) dict_max = std::max(dict_max, plans[i]->ctx->P.dict_n);
+    std::vector<Step2> desc(2 * (size_t)nplans);
+    size_t most = 0;
+    for (int i = 0; i < nplans; i++) {
+        const sfg_plan *p = plans[i];
+        const DevProblem &P = p->ctx->P;
+        const StepCommon c = step_common(P, p->pl, &p->run, p->b);
+        for (int par = 0; par < 2; par++) desc[(size_t)par * nplans + i] = step2_args(P, p->pl, c, p->b, par);
+        most += (size_t)(P.node_num / 32 + 2);
+    }
+    if (cudaMalloc((void **)&g->d_desc, sizeof(Step2) * desc.size()) != cudaSuccess) return SFG_ERR_OOM;
+    // room for the block map of the smallest blocks (64 threads)
+    if (cudaMalloc((void **)&g->d_map, sizeof(int2) * 2 * most) != cudaSuccess) return SFG_ERR_OOM;
+    if (cudaMemcpy(g->d_desc, desc.data(), sizeof(Step2) * desc.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return SFG_ERR_CUDA;
+    std::vector<int2> map;
+    int nblkA = 0, nblkZ = 0;
+    auto use_shapes = [&](int sa, int sz) -> bool {
+        group_map(plans, nplans, step2_threads(sa), step2_threads(sz), map, nblkA, nblkZ);
+        return map.size() <= 2 * most &&
+               cudaMemcpy(g->d_map, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    // launch shapes: SFG_SHAPE_A / SFG_SHAPE_Z pin them; otherwise time a
+    // few steps of each one-shot shape for both classes, then the class-Z
+    // shape with the class-A shape fixed (the plans' own state buffers are
+    // scratch here: the group's graph resets them at every launch)
+    int shapeA = plans[0]->pl.shapeA, shapeZ = plans[0]->pl.shapeZ;
+    const char *fa = std::getenv("SFG_SHAPE_A"), *fz = std::getenv("SFG_SHAPE_Z");
+    if (fa && fz) {
+        shapeA = std::atoi(fa);
+        shapeZ = std::atoi(fz);
+    } else {
+        const int probe = std::min(12, plans[0]->run.step - 2);
+        cudaEvent_t e0, e1;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return SFG_ERR_CUDA;
+        auto time_shapes = [&](int sa, int sz, float &ms) -> bool {
+            if (!use_shapes(sa, sz)) return false;
+            bool ok = true;
+            for (int rep = 0; rep < 2 && ok; rep++) {   // the first pass warms up
+                ok = cudaEventRecord(e0, st) == cudaSuccess;
+                for (int it = 2; it < 2 + probe && ok; it++) {
+                    const Step2 *d = g->d_desc + (size_t)(it & 1) * nplans;
+                    ok = cudaEventRecord(ctx0->ev_fork, st) == cudaSuccess &&
+                         cudaStreamWaitEvent(st2, ctx0->ev_fork, 0) == cudaSuccess &&
+                         (nblkZ == 0 || launch_stepZ_multi(d, g->d_map + nblkA, nblkZ, dict, dict_max, comp, sz, it,
+                                                           st2) == cudaSuccess) &&
+                         launch_stepA_multi(d, g->d_map, nblkA, dict, dict_max, comp, sa, it, st) == cudaSuccess &&
+                         cudaEventRecord(ctx0->ev_join, st2) == cudaSuccess &&
+                         cudaStreamWaitEvent(st, ctx0->ev_join, 0) == cudaSuccess;
+                }
+                ok = ok && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+                     cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            }
+            return ok;
+        };
+        float best = 1e30f, ms = 0.f;
+        bool ok = true;
+        for (int v = 0; v < step2_variants() && ok; v++) {
+            ok = time_shapes(v, v, ms);
+            if (ok && ms < best) { best = ms; shapeA = v; shapeZ = v; }
+        }
+        for (int v = 0; v < step2_variants() && ok; v++) {
+            if (v == shapeA) continue;
+            ok = time_shapes(shapeA, v, ms);
+            if (ok && ms < best) { best = ms; shapeZ = v; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (!ok) return SFG_ERR_CUDA;
+    }
+    if (!use_shapes(shapeA, shapeZ)) return SFG_ERR_CUDA;
+    if (nblkA == 0) return SFG_ERR_ARG;
+    const int n = group_capture(g, plans, nplans, shapeA, shapeZ, nblkA, nblkZ);
+    if (n < 0) return SFG_ERR_CUDA;
+    g->launches = n;
+    g->shapes = shapeA * 16 + shapeZ;
+    g->fused = true;
+    return SFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **out)
 {
@@ -1312,21 +1544,23 @@ int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **out)
     if (cudaSetDevice(dev) != cudaSuccess) return SFG_ERR_CUDA;
     sfg_group *g = new sfg_group();
     g->device = dev;
-    auto bail = [&](int code) {
-        if (g->exec) cudaGraphExecDestroy(g->exec);
-        if (g->graph) cudaGraphDestroy(g->graph);
-        delete g;
-        return code;
-    };
-    if (cudaGraphCreate(&g->graph, 0) != cudaSuccess) return bail(SFG_ERR_CUDA);
-    for (int i = 0; i < nplans; i++) {
-        // no dependencies: the meshes' time loops run side by side
-        cudaGraphNode_t node;
-        if (cudaGraphAddChildGraphNode(&node, g->graph, nullptr, 0, plans[i]->graph) != cudaSuccess)
-            return bail(SFG_ERR_CUDA);
-        g->launches += plans[i]->launches;
+    const char *env = std::getenv("SFG_GROUP_CHILD_GRAPHS");
+    if (group_fusable(plans, nplans) && !(env && env[0] == '1')) {
+        const int rc = group_create_fused(plans, nplans, g);
+        if (rc != SFG_OK) { group_free(g); return rc; }
+    } else {
+        if (cudaGraphCreate(&g->graph, 0) != cudaSuccess) { group_free(g); return SFG_ERR_CUDA; }
+        for (int i = 0; i < nplans; i++) {
+            // no dependencies: the meshes' time loops run side by side
+            cudaGraphNode_t node;
+            if (cudaGraphAddChildGraphNode(&node, g->graph, nullptr, 0, plans[i]->graph) != cudaSuccess) {
+                group_free(g);
+                return SFG_ERR_CUDA;
+            }
+            g->launches += plans[i]->launches;
+        }
     }
-    if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) return bail(SFG_ERR_CUDA);
+    if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) { group_free(g); return SFG_ERR_CUDA; }
     *out = g;
     return SFG_OK;
 }
@@ -1340,14 +1574,14 @@ int sfg_group_launch(sfg_group *g, void *stream)
 
 int sfg_group_launches(const sfg_group *g) { return g ? g->launches : 0; }
 
+int sfg_group_fused(const sfg_group *g) { return g && g->fused ? 1 + g->shapes : 0; }
+
 void sfg_group_destroy(sfg_group *g)
 {
     if (!g) return;
     cudaSetDevice(g->device);
     cudaDeviceSynchronize();
-    if (g->exec) cudaGraphExecDestroy(g->exec);
-    if (g->graph) cudaGraphDestroy(g->graph);
-    delete g;
+    group_free(g);
 }
 
 int sfg_sync(sfg_ctx *ctx)

@@ -89,8 +89,8 @@ template <bool COMP>
 __device__ __forceinline__ void finish_A(float su, float sw, const float *mL, float im, double dt, double src_u,
                                          double src_w, float *g, float *p, float &uu, float &ww)
 {
-    float Uh = g[0], Wh = g[1], Vu = g[10], Vw = g[11];
-    float Au = p[0], Aw = p[1], lou = p[2], low = p[3];
+    float Uh = g[0], Wh = g[1], lou = g[10], low = g[11];
+    float Au = p[0], Aw = p[1], Vu = p[2], Vw = p[3];
     const float au = im * (su + ((mL[0] + mL[1]) + (mL[2] + mL[3])) + (float)src_u);
     const float aw = im * (sw + ((mL[4] + mL[5]) + (mL[6] + mL[7])) + (float)src_w);
     if (COMP) {
@@ -106,9 +106,9 @@ __device__ __forceinline__ void finish_A(float su, float sw, const float *mL, fl
     g[1] = Wh;
 #pragma unroll
     for (int k = 0; k < 8; k++) g[2 + k] = im * mL[k];
-    g[10] = Vu;
-    g[11] = Vw;
-    p[0] = Au; p[1] = Aw; p[2] = lou; p[3] = low;
+    g[10] = lou;
+    g[11] = low;
+    p[0] = Au; p[1] = Aw; p[2] = Vu; p[3] = Vw;
 }
 
 template <typename T>
@@ -162,14 +162,20 @@ __device__ __forceinline__ void finish_Z(const float *kU, const float *kW, const
         for (int k = 0; k < 6; k++) newmark_kahan(gs[k], ps[6 + k], gs[6 + k], ps[k], r.a[k], (float)dt);
         // the totals from the compensated split fields (each hi + lo) in FP64:
         // inside the M-PML the split fields are far larger than their sum
-        su = (float)((((double)gs[0] + ps[6]) + ((double)gs[1] + ps[7])) + ((double)gs[2] + ps[8]));
-        sw = (float)((((double)gs[3] + ps[9]) + ((double)gs[4] + ps[10])) + ((double)gs[5] + ps[11]));
+        const double su64 = (((double)gs[0] + ps[6]) + ((double)gs[1] + ps[7])) + ((double)gs[2] + ps[8]);
+        const double sw64 = (((double)gs[3] + ps[9]) + ((double)gs[4] + ps[10])) + ((double)gs[5] + ps[11]);
+        su = (float)su64;
+        sw = (float)sw64;
+        gc[10] = (float)(su64 - (double)su);
+        gc[11] = (float)(sw64 - (double)sw);
     } else {
         float Ut[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) { Ut[k] = newmark_plain(gs[k], gs[6 + k], ps[k], r.a[k], (float)dt); ps[6 + k] = 0.f; }
         su = (Ut[0] + Ut[1]) + Ut[2];
         sw = (Ut[3] + Ut[4]) + Ut[5];
+        gc[10] = 0.f;
+        gc[11] = 0.f;
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) { L[k] = r.lx[k]; L[4 + k] = r.ly[k]; }
@@ -179,8 +185,6 @@ __device__ __forceinline__ void finish_Z(const float *kU, const float *kW, const
     gc[1] = sw;
 #pragma unroll
     for (int k = 0; k < 8; k++) gc[2 + k] = L[k];
-    gc[10] = 0.f;
-    gc[11] = 0.f;
 }
 
 __device__ __forceinline__ bool is_pml_row(float4 c1)
@@ -193,8 +197,8 @@ __device__ __forceinline__ bool is_pml_row(float4 c1)
 __device__ __forceinline__ void total_uw(const State32 &st, int na, int S, long long node, int s, double &u, double &w)
 {
     if (node < na) {
-        u = (double)st.Gc[(node * GC + 0) * S + s] + (double)st.Pa[(node * PA + 2) * S + s];
-        w = (double)st.Gc[(node * GC + 1) * S + s] + (double)st.Pa[(node * PA + 3) * S + s];
+        u = (double)st.Gc[(node * GC + 0) * S + s] + (double)st.Gc[(node * GC + 10) * S + s];
+        w = (double)st.Gc[(node * GC + 1) * S + s] + (double)st.Gc[(node * GC + 11) * S + s];
     } else {
         const long long z = node - na;
         u = 0.0;
@@ -208,13 +212,14 @@ __device__ __forceinline__ void total_uw(const State32 &st, int na, int S, long 
 }
 
 // Receiver gather (elastic_wave.c:787-795) of the step's input state.
-__device__ __forceinline__ void gather2_one(const StepCommon &c, int na, const State32 &st, int S, int t)
+__device__ __forceinline__ void gather2_one(const StepCommon &c, int na, const State32 &st, int S, int t,
+                                            int seis_row)
 {
-    if (c.seis_row < 0 || t >= c.nrec * S) return;
+    if (seis_row < 0 || t >= c.nrec * S) return;
     const int s = t / c.nrec, r = t - s * c.nrec;
     double u, w;
     total_uw(st, na, S, c.rec[r], s, u, w);
-    const size_t o = ((size_t)s * c.seis_rows + c.seis_row) * c.nrec + r;
+    const size_t o = ((size_t)s * c.seis_rows + seis_row) * c.nrec + r;
     c.seis_u[o] = u;
     c.seis_w[o] = w;
 }
@@ -257,14 +262,13 @@ __device__ __forceinline__ void load_dict(const Step2 &a, float4 *stab)
     __syncthreads();
 }
 
-template <bool COMP, int THREADS, int MINB, bool DICT>
-__global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
+// Class-A rows of block `bid` of one mesh (the tuples already in stab).
+template <bool COMP, int THREADS, bool DICT>
+__device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4 *stab, int it, int seis_row)
 {
-    extern __shared__ float4 stab[];
-    if (DICT) load_dict<THREADS>(a, stab);
     const StepCommon &c = a.c;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
-    gather2_one(c, a.na, a.in, 1, i);
+    const int i = bid * THREADS + threadIdx.x;
+    gather2_one(c, a.na, a.in, 1, i, seis_row);
     double eu = 0.0, ew = 0.0;
     if (i < a.na) {
         const int lane = i & 31, slice = i >> 5;
@@ -274,12 +278,18 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
 #pragma unroll
         for (int k = 0; k < 8; k++) mL[k] = 0.f;
         const int s0 = __ldg(a.sliceA + slice), s1 = __ldg(a.sliceA + slice + 1);
+        // own displacements (hi, lo): every row of K1..K6 sums to zero, so
+        // K U = sum_j K_ij (U_j - U_i), and the differences of the hi and lo
+        // parts keep the products free of the cancellation that FP32 sums
+        // of K_ij U_j suffer on smooth fields
+        const float4 *gi = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
+        const float4 own0 = __ldg(gi), own2 = __ldg(gi + 2);
         auto acc = [&](int j, float vm, const float *kv) {
             const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
-            const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+            const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
-            for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+            for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
             mL[0] += vm * q0.z; mL[1] += vm * q0.w; mL[2] += vm * q1.x; mL[3] += vm * q1.y;
             mL[4] += vm * q1.z; mL[5] += vm * q1.w; mL[6] += vm * q2.x; mL[7] += vm * q2.y;
         };
@@ -310,17 +320,15 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
         const float im = __ldcs(a.imA + i);
         double src_u = 0.0, src_w = 0.0;
         if (i == c.src[0]) {
-            const double ps = c.amp[c.it];
+            const double ps = c.amp[it];
             src_u = ps * c.sin_af;
             src_w = ps * c.cos_af;
         }
         float g[GC], p[PA];
-        const float4 *gi = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const float4 v = __ldg(gi + k);
-            g[4 * k] = v.x; g[4 * k + 1] = v.y; g[4 * k + 2] = v.z; g[4 * k + 3] = v.w;
-        }
+        const float4 own1 = __ldg(gi + 1);
+        g[0] = own0.x; g[1] = own0.y; g[2] = own0.z; g[3] = own0.w;
+        g[4] = own1.x; g[5] = own1.y; g[6] = own1.z; g[7] = own1.w;
+        g[8] = own2.x; g[9] = own2.y; g[10] = own2.z; g[11] = own2.w;
         const float4 pv = __ldcs(reinterpret_cast<const float4 *>(a.in.Pa) + i);
         p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
         float uu, ww, su, sw;
@@ -333,17 +341,24 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
         eu = (double)uu * uu;
         ew = (double)ww * ww;
     }
-    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+    block_energy(c.energy ? c.energy + ((size_t)it) * 2 : nullptr, eu, ew);
 }
 
 template <bool COMP, int THREADS, int MINB, bool DICT>
-__global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
+__global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
 {
     extern __shared__ float4 stab[];
     if (DICT) load_dict<THREADS>(a, stab);
+    stepA_body<COMP, THREADS, DICT>(a, blockIdx.x, stab, a.c.it, a.c.seis_row);
+}
+
+// Class-Z rows of block `bid` of one mesh (the tuples already in stab).
+template <bool COMP, int THREADS, bool DICT>
+__device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4 *stab, int it)
+{
     const StepCommon &c = a.c;
     const int nz = c.n - a.na;
-    const int local = blockIdx.x * THREADS + threadIdx.x;
+    const int local = bid * THREADS + threadIdx.x;
     const int i = a.na + local;
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
     if (local < nz) {
@@ -360,6 +375,9 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
 #pragma unroll
         for (int k = 0; k < 20; k++) m[k] = 0.f;
         const int s0 = __ldg(a.sliceZ + slice), s1 = __ldg(a.sliceZ + slice + 1);
+        // own totals (hi, lo) for the stiffness products in difference form
+        const float4 *gci = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
+        const float4 own0 = __ldg(gci), own2 = __ldg(gci + 2);
         const float *sd = DICT ? nullptr : a.sellZ + (size_t)s0 * 256 + lane;
         DictSlots ss;
         if (DICT) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
@@ -386,8 +404,8 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
                 float vm, kv[6];
                 slot(j, vm, kv, 6);
                 const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
-                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+                const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
                 // split fields exist for class-Z columns; rows outside the
                 // M-PML that share the warp see zeros for class-A columns (their
                 // damping coefficients are zero, so those products are unused)
@@ -397,7 +415,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
                     z0 = __ldg(sj); z1 = __ldg(sj + 1); z2 = __ldg(sj + 2);
                 }
 #pragma unroll
-                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
                 m[0] += vm * z0.x;  m[1] += vm * z0.y;  m[2] += vm * z0.z;  m[3] += vm * z0.w;
                 m[4] += vm * z1.x;  m[5] += vm * z1.y;  m[6] += vm * z1.z;  m[7] += vm * z1.w;
                 m[8] += vm * z2.x;  m[9] += vm * z2.y;  m[10] += vm * z2.z; m[11] += vm * z2.w;
@@ -411,10 +429,10 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
                 float vm, kv[4];
                 slot(j, vm, kv, 4);
                 const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1);
-                const float2 q2 = __ldg(reinterpret_cast<const float2 *>(gj + 2));
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+                const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
-                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * q0.x; kW[k] += kv[k] * q0.y; }
+                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
                 m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
                 m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
             }
@@ -426,7 +444,7 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
         }
         double src_u = 0.0, src_w = 0.0;
         if (i == c.src[0]) {
-            const double ps = c.amp[c.it];
+            const double ps = c.amp[it];
             src_u = ps * c.sin_af;
             src_w = ps * c.cos_af;
         }
@@ -453,7 +471,45 @@ __global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
         eu = (double)uu * uu;
         ew = (double)ww * ww;
     }
-    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+    block_energy(c.energy ? c.energy + ((size_t)it) * 2 : nullptr, eu, ew);
+}
+
+template <bool COMP, int THREADS, int MINB, bool DICT>
+__global__ void __launch_bounds__(THREADS, MINB) stepZ_kernel(const Step2 a)
+{
+    extern __shared__ float4 stab[];
+    if (DICT) load_dict<THREADS>(a, stab);
+    stepZ_body<COMP, THREADS, DICT>(a, blockIdx.x, stab, a.c.it);
+}
+
+// ------------------------------------------------ several meshes per launch
+//
+// One launch per class and time step for a group of independent one-shot
+// problems (meshes of different sizes): block b works on block map[b].y of
+// mesh map[b].x and reads that mesh's step descriptor (the in/out state of
+// this step's parity) in place; `it` gives the time index and receiver row,
+// which the per-mesh launches carry in their descriptors.
+
+template <bool COMP, int THREADS, int MINB, bool DICT>
+__global__ void __launch_bounds__(THREADS, MINB) stepA_multi(const Step2 *__restrict__ descs,
+                                                             const int2 *__restrict__ map, int it)
+{
+    extern __shared__ float4 stab[];
+    const int2 mb = __ldg(map + blockIdx.x);
+    const Step2 &a = descs[mb.x];
+    if (DICT) load_dict<THREADS>(a, stab);
+    stepA_body<COMP, THREADS, DICT>(a, mb.y, stab, it, it >= 3 ? it - 3 : -1);
+}
+
+template <bool COMP, int THREADS, int MINB, bool DICT>
+__global__ void __launch_bounds__(THREADS, MINB) stepZ_multi(const Step2 *__restrict__ descs,
+                                                             const int2 *__restrict__ map, int it)
+{
+    extern __shared__ float4 stab[];
+    const int2 mb = __ldg(map + blockIdx.x);
+    const Step2 &a = descs[mb.x];
+    if (DICT) load_dict<THREADS>(a, stab);
+    stepZ_body<COMP, THREADS, DICT>(a, mb.y, stab, it);
 }
 
 // --------------------------------------------------------- batched kernels
@@ -587,7 +643,7 @@ __global__ void __launch_bounds__(SPL == 2 && !MM ? 128 : 256, SPL == 1 ? 3 : (S
     constexpr int nch = S / (32 * SPL);
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
+    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t, c.seis_row);
     if (c.energy) energy_zero(se, S);
     const int warp = gtid >> 5, warps_total = (gridDim.x * blockDim.x) >> 5;
     const int s_base = (warp % nch) * 32 * SPL + lane * SPL;
@@ -726,7 +782,7 @@ __global__ void __launch_bounds__(256, 1) stepA_staged(const Step2 a)
     const StepCommon &c = a.c;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t);
+    for (int t = gtid; t < c.nrec * S; t += gridDim.x * blockDim.x) gather2_one(c, a.na, a.in, S, t, c.seis_row);
     if (c.energy) energy_zero(se, S);
     const int warp = gtid >> 5, warps_total = (gridDim.x * blockDim.x) >> 5;
     const int s_base = lane * SPL;
@@ -1032,7 +1088,7 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
 
 __global__ void gather2_kernel(const StepCommon c, int na, const State32 st, int S)
 {
-    gather2_one(c, na, st, S, blockIdx.x * blockDim.x + threadIdx.x);
+    gather2_one(c, na, st, S, blockIdx.x * blockDim.x + threadIdx.x, c.seis_row);
 }
 
 __global__ void snapshot2_kernel(const State32 st, int n, int na, int S, const int *perm, double *su, double *sw,
@@ -1327,6 +1383,46 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
     if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
         return cudaErrorInvalidValue;
     SFG_SHAPES(stepZ_kernel, a.c.n - a.na);
+    return cudaGetLastError();
+}
+#undef SFG_ONE
+
+int step2_threads(int variant)
+{
+    switch (variant) {
+    case 0: case 1: return 128;
+    case 2: return 256;
+    case 4: return 64;
+    case 5: return 512;
+    default: return 256;
+    }
+}
+
+#define SFG_ONE(KERNEL, T, M, COUNT)                                                           \
+    do {                                                                                       \
+        const size_t smem = sizeof(float4) * 2 * (size_t)dict_max;                             \
+        if (dict) {                                                                            \
+            if (comp) KERNEL<true, T, M, true><<<(COUNT), T, smem, st>>>(descs, map, it);      \
+            else KERNEL<false, T, M, true><<<(COUNT), T, smem, st>>>(descs, map, it);          \
+        } else {                                                                               \
+            if (comp) KERNEL<true, T, M, false><<<(COUNT), T, 0, st>>>(descs, map, it);        \
+            else KERNEL<false, T, M, false><<<(COUNT), T, 0, st>>>(descs, map, it);            \
+        }                                                                                      \
+    } while (0)
+
+cudaError_t launch_stepA_multi(const Step2 *descs, const int2 *map, int nblocks, bool dict, int dict_max, bool comp,
+                               int variant, int it, cudaStream_t st)
+{
+    if (dict_max > kDictMax || (dict && dict_max <= 0)) return cudaErrorInvalidValue;
+    SFG_SHAPES(stepA_multi, nblocks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stepZ_multi(const Step2 *descs, const int2 *map, int nblocks, bool dict, int dict_max, bool comp,
+                               int variant, int it, cudaStream_t st)
+{
+    if (dict_max > kDictMax || (dict && dict_max <= 0)) return cudaErrorInvalidValue;
+    SFG_SHAPES(stepZ_multi, nblocks);
     return cudaGetLastError();
 }
 #undef SFG_ONE

@@ -16,9 +16,12 @@
 //
 // State records (node-major, shot index innermost for batches of S shots):
 //   Gc[n][12]   gathered by every row: U W Lx1 Lx2 | Lx3 Lx4 Ly1 Ly2 | Ly3 Ly4
-//               Vu Vw   (U, W: FP32 value of the total; Vu, Vw: total
-//               velocities of class-A rows, 0 in class Z)
-//   Pa[na][4]   class A, private: Au Aw lo_u lo_w
+//               lo_u lo_w   (the totals as FP32 pairs U + lo_u, W + lo_w: in
+//               class A the compensated displacement itself, in class Z the
+//               FP64 sum of the split pairs split into two floats; the
+//               one-shot kernels form K U as sum_j K_ij (U_j - U_i) from both
+//               parts, since every row of K1..K6 sums to zero)
+//   Pa[na][4]   class A, private: Au Aw Vu Vw (total accelerations, velocities)
 //   Gs[nz][12]  class Z, gathered by M-PML rows: U1 U2 U3 W1 W2 W3 (high FP32
 //               part) | V1..V6
 //   Ps[nz][12]  class Z, private: A1..A6 | lo1..lo6
@@ -80,6 +83,17 @@ struct Step2 {
 int step2_variants();
 cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st);
 cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st);
+// threads per block of one-shot launch shape `variant`
+int step2_threads(int variant);
+// several one-shot problems per launch: descs[m] the step descriptor of mesh
+// m for this step's parity (it and the receiver row are set from `it`);
+// map[b] = (mesh, block of that mesh) for each of the nblocks blocks, blocks
+// of step2_threads(variant) rows; dict: every mesh has a value dictionary,
+// dict_max its largest tuple count
+cudaError_t launch_stepA_multi(const Step2 *descs, const int2 *map, int nblocks, bool dict, int dict_max, bool comp,
+                               int variant, int it, cudaStream_t st);
+cudaError_t launch_stepZ_multi(const Step2 *descs, const int2 *map, int nblocks, bool dict, int dict_max, bool comp,
+                               int variant, int it, cudaStream_t st);
 // S = a.S shots, a multiple of 32 * spl; a warp advances 32 * spl shots of
 // one row (spl per lane); warps per block a multiple of S / (32 * spl)
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);

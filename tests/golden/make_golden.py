@@ -15,13 +15,19 @@ reference sources are available; the fixtures travel, the reference does not).
                   consistent-mass branch (solver "mgmres": restarted GMRES + ILU
                   on M, solver/mgmres/mgmres.c), dt inside that scheme's
                   stability limit
+  config1_reference.npz, config2_reference.npz  the reference's FP64 runs of
+                  the two benchmark configurations at full size and length
+                  (Q4 200x200, 1000 steps; Q9 400x400 layered, 3000 steps):
+                  every 4th / 10th receiver over all time steps, and the
+                  200-step snapshots on a coarse grid of nodes (every 8th /
+                  16th grid line), with checksums of the inputs they belong to
   examples.npz    subsets of the reference's committed EXAMPLE outputs
                   (example 2: Q4 internal mesh, snapshots; example 6: T3
                   exterior mesh with a free surface, seismograms) and the mesh
                   of example 6 (its input files)
 
 Usage: SEISFEM_REFERENCE=<reference tree> make -C oracle &&
-       SEISFEM_REFERENCE=<reference tree> python tests/golden/make_golden.py [acoustic|consistent]
+       SEISFEM_REFERENCE=<reference tree> python tests/golden/make_golden.py [acoustic|consistent|config1|config2]
 """
 from __future__ import annotations
 
@@ -42,6 +48,8 @@ if not REF or not os.path.isdir(os.path.join(REF, "time_evolution")):
                      "`make -C oracle REF=$SEISFEM_REFERENCE` first")
 
 from oracle import Reference, ReferenceAcoustic  # noqa: E402
+from fixture_keys import FULL_CONFIG_STRIDES, full_config_subset, input_checksum  # noqa: E402
+from seisfem_b200 import problem as P  # noqa: E402
 from seisfem_b200.problem import small_problem, structured_mesh  # noqa: E402
 
 
@@ -125,6 +133,26 @@ def consistent_small(R):
     np.savez_compressed(os.path.join(HERE, "consistent_small.npz"), **out)
 
 
+FULL_CONFIGS = {"config1": P.config_1, "config2": P.config_2}
+
+
+def full_config(R, name):
+    build = FULL_CONFIGS[name]
+    rec_stride, grid_stride = FULL_CONFIG_STRIDES[name]
+    P.use_scan_locator()
+    prob = build()
+    rec, nodes = full_config_subset(prob, rec_stride, grid_stride)
+    r = R.run(prob, nthreads=os.cpu_count() or 1)
+    assert r["status"] == 0, r["status"]
+    out = {"checksum": input_checksum(prob), "rec": rec, "nodes": nodes, "seconds": np.float64(r["seconds"]),
+           "seis_u": r["seis_u"][0][:, rec], "seis_w": r["seis_w"][0][:, rec],
+           "snap_u": r["snap_u"][0][:, nodes], "snap_w": r["snap_w"][0][:, nodes],
+           # norms of the full outputs, so that a subset's error can be scaled
+           "norm_seis_u": np.linalg.norm(r["seis_u"]), "norm_seis_w": np.linalg.norm(r["seis_w"]),
+           "norm_snap_u": np.linalg.norm(r["snap_u"]), "norm_snap_w": np.linalg.norm(r["snap_w"])}
+    np.savez_compressed(os.path.join(HERE, f"{name}_reference.npz"), **out)
+
+
 def read_rows(path, stride=1, max_rows=None):
     rows = []
     with open(path) as f:
@@ -165,5 +193,11 @@ if __name__ == "__main__":
         acoustic_small(R, ReferenceAcoustic())
     if part in ("all", "consistent"):
         consistent_small(R)
-    for f in ("csr_small.npz", "runs_small.npz", "examples.npz", "acoustic_small.npz", "consistent_small.npz"):
+    for name in FULL_CONFIGS:
+        if part in ("all", name):
+            full_config(R, name)
+    for f in ("csr_small.npz", "runs_small.npz", "examples.npz", "acoustic_small.npz", "consistent_small.npz",
+              "config1_reference.npz", "config2_reference.npz"):
+        if not os.path.exists(os.path.join(HERE, f)):
+            continue
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

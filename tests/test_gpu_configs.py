@@ -44,8 +44,15 @@ def test_config4_t6_energy_bound_trips_like_the_reference(ctx, oracle):
     assert 200 < b64 < 400 and abs(b32 - b64) <= 3, (b64, b32)
 
 
-def test_group_launch_matches_separate_plans(oracle):
+@pytest.mark.parametrize("mode", ["fused", "child_graphs"])
+def test_group_launch_matches_separate_plans(oracle, mode, monkeypatch):
+    """Uneven meshes in one graph launch -- one class-A and one class-Z
+    kernel per time step for all meshes ("fused"), or the plans' own graphs
+    side by side -- give each plan's own results bit for bit, on repeated
+    launches."""
     from seisfem_b200.api import Context, Group, Plan
+    if mode == "child_graphs":
+        monkeypatch.setenv("SFG_GROUP_CHILD_GRAPHS", "1")
     probs = config_3b(count=3, lo=20, hi=50, step=202, pml=4)
     assert len({p.mesh.node_num for p in probs}) == 3
     ctxs = [Context(0) for _ in probs]
@@ -57,7 +64,14 @@ def test_group_launch_matches_separate_plans(oracle):
         pl.launch(0)
         alone.append(pl.finish(0))
     grp = Group(plans)
-    assert grp.launches == sum(pl.launches for pl in plans)
+    assert grp.fused == (mode == "fused")
+    steps = probs[0].step - 2
+    if grp.fused:
+        # two kernels per time step for all meshes, plus per mesh one
+        # snapshot (step 199) and the last receiver row
+        assert grp.launches == 2 * steps + 2 * len(plans), grp.launches
+    else:
+        assert grp.launches == sum(pl.launches for pl in plans)
     for _ in range(2):       # twice: every launch starts from the zero state
         grp.launch()
         for c in ctxs:
@@ -70,6 +84,37 @@ def test_group_launch_matches_separate_plans(oracle):
     got = plans[1].finish(0)
     for k in ("seis_u", "seis_w"):
         assert rel_l2(got[k], ref[k]) < FP32_TOL, k
+    grp.close()
+    for pl in plans:
+        pl.close()
+    for c in ctxs:
+        c.close()
+
+
+def test_group_of_mixed_plans_composes_child_graphs():
+    """A group with a batched plan cannot share the one-shot multi-mesh
+    kernels: it falls back to the plans' own graphs, still bit for bit."""
+    from seisfem_b200.api import Context, Group, Plan
+    from seisfem_b200.problem import small_problem
+    probs = [small_problem("Q4", n=24, step=122, pml=4, seed=2),
+             small_problem("Q4", n=30, step=122, pml=4, seed=3, shots=32)]
+    ctxs = [Context(0) for _ in probs]
+    for c, p in zip(ctxs, probs):
+        c.setup(p)
+    plans = [Plan(c, p, precision="fp32k", snap_every=0, shots_per_batch=len(p.src_node)) for c, p in zip(ctxs, probs)]
+    alone = []
+    for pl in plans:
+        pl.launch(0)
+        alone.append(pl.finish(0))
+    grp = Group(plans)
+    assert not grp.fused
+    grp.launch()
+    for c in ctxs:
+        c.L.sfg_sync(c.ptr)
+    for pl, a in zip(plans, alone):
+        out = pl.finish(0)
+        for k in ("seis_u", "seis_w"):
+            assert np.array_equal(out[k], a[k]), k
     grp.close()
     for pl in plans:
         pl.close()

@@ -1,7 +1,9 @@
 """Multi-rank shot sharding on CPU (gloo, world size 2): every rank advances
 its own block of shots with no communication inside the time loop, and the
-seismograms are gathered once on rank 0.  The per-rank compute here is the
-CPU oracle; on GPUs it is the same code path with sfg_run per rank."""
+seismograms are collected once with one all_gather of tensors.  The ranks
+run the same code as bench.py --gpus N (shots.run_sharded with a runner per
+rank); here the runner is the CPU oracle, on GPUs it is api.device_runner
+(a Plan on the rank's device) and the collective goes over NCCL."""
 import os
 import socket
 
@@ -29,38 +31,47 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, out_path):
+def _oracle_runner(sub):
+    import torch
+    from oracle import Oracle
+    out = Oracle().run(sub, nthreads=1)
+    return torch.from_numpy(out["seis_u"]), torch.from_numpy(out["seis_w"])
+
+
+def _worker(rank, world, port, out_path, shots):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path[:0] = [root, os.path.join(root, "oracle")]
     import datetime
     import torch.distributed as dist
-    from oracle import Oracle
     from seisfem_b200.problem import small_problem
-    from seisfem_b200.shots import gather_seismograms, shard as shard_
+    from seisfem_b200.shots import gather_seismograms, run_sharded, shard_problem
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
-    p = small_problem("Q4", n=12, step=120, pml=2, seed=3, shots=5)
-    mine = shard_(len(p.src_node), rank, world)
-    p.src_node = p.src_node[mine]
-    local = Oracle().run(p, nthreads=1)["seis_u"]
-    full = gather_seismograms(local, 5, rank, world)
+    p = small_problem("Q4", n=12, step=120, pml=2, seed=3, shots=shots)
+    su, sw = run_sharded(p, rank, world, _oracle_runner)
+    # the host-array gather agrees with the tensor gather
+    host = gather_seismograms(_oracle_runner(shard_problem(p, rank, world))[0].numpy(), shots, rank, world)
     if rank == 0:
-        np.save(out_path, full)
+        assert np.array_equal(host, su.numpy())
+        np.savez(out_path, seis_u=su.numpy(), seis_w=sw.numpy())
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_ranks_match_single_process(tmp_path, oracle):
+@pytest.mark.parametrize("shots", [5, 1])
+def test_two_ranks_match_single_process(tmp_path, oracle, shots):
+    """5 shots (3 + 2: uneven shards) and 1 shot (one rank has none)."""
     import torch.multiprocessing as mp
     from seisfem_b200.problem import small_problem
-    out = str(tmp_path / "gathered.npy")
-    mp.start_processes(_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    out = str(tmp_path / "gathered.npz")
+    mp.start_processes(_worker, args=(2, _free_port(), out, shots), nprocs=2, join=True, start_method="spawn")
     gathered = np.load(out)
-    ref = oracle.run(small_problem("Q4", n=12, step=120, pml=2, seed=3, shots=5), nthreads=1)["seis_u"]
-    assert gathered.shape == ref.shape
-    assert np.array_equal(gathered, ref)
+    ref = oracle.run(small_problem("Q4", n=12, step=120, pml=2, seed=3, shots=shots), nthreads=1)
+    for k in ("seis_u", "seis_w"):
+        assert gathered[k].shape == ref[k].shape
+        assert np.array_equal(gathered[k], ref[k])
 
 
 # ---------------------------------------------------------------- surrogate
