@@ -56,16 +56,20 @@ struct RunCache {
 };
 
 // Launch shapes already tuned in this process, keyed by the mesh signature
-// (rows, union nonzeros, interior rows, element type) and device, so that a
-// new context on the same mesh does not tune again.
+// (rows, union nonzeros, interior rows, element type), the one-shot slot
+// layout (0: full values, 1: value dictionary, 2: dictionary and
+// staged-gather tiles) and device, so that a new context on the same mesh
+// and layout does not tune again.
 struct TuneKey {
     int device, N, na, type;
     long long nnz;
+    int layout;
     bool operator<(const TuneKey &o) const
     {
-        return std::tie(device, N, na, type, nnz) < std::tie(o.device, o.N, o.na, o.type, o.nnz);
+        return std::tie(device, N, na, type, nnz, layout) < std::tie(o.device, o.N, o.na, o.type, o.nnz, o.layout);
     }
 };
+static int slot_layout(const sfg::DevProblem &P) { return P.dict_n <= 0 ? 0 : (P.tileA_off ? 2 : 1); }
 static std::map<TuneKey, RunCache> g_tuned;
 static std::mutex g_tuned_mu;
 
@@ -167,7 +171,8 @@ void free_problem(DevProblem &P, cudaStream_t st)
                     (void *)P.coefd, (void *)P.perm, (void *)P.inv, (void *)P.sellA, (void *)P.sellZ,
                     (void *)P.sliceA, (void *)P.sliceZ, (void *)P.upp, (void *)P.dict, (void *)P.sellAd,
                     (void *)P.sellZd, (void *)P.rowrho, (void *)P.recp, (void *)P.recA, (void *)P.coefA,
-                    (void *)P.imA, (void *)P.coefZ, (void *)P.rho0})
+                    (void *)P.imA, (void *)P.coefZ, (void *)P.rho0, (void *)P.sellAt, (void *)P.sellZt,
+                    (void *)P.tileA_off, (void *)P.tileA_ext, (void *)P.tileZ_off, (void *)P.tileZ_ext})
         keep_free(p, st);
     P = DevProblem();
 }
@@ -370,13 +375,38 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
 
     // step data: coefficients, SELL-32 slices (single shot), row records (batched)
     CK(build_coef(N, P.coef64, P.mpml, P.mass_lump, P.dirichlet, &P.coef32, &P.coefd, st));
+    // The one-shot kernels' matrix slots: (column, tuple id) when the union
+    // entries reduce to a small value dictionary (meshes of congruent
+    // elements), else column + M + K1..K4 (class A) or K1..K6 (class Z).
+    // SFG_NO_VALUE_DICT=1 keeps the full-value slots (to compare the two).
+    // The dictionary is found first: with one, the numbering below orders
+    // each class spatially and cuts it into tiles for the staged-gather
+    // kernels (SFG_NO_TILES=1 keeps the mesh order and no tiles).
+    int *tid = nullptr, zero_id = 0;
+    {
+        const char *nd = std::getenv("SFG_NO_VALUE_DICT");
+        const int T = (nd && *nd && *nd != '0')
+                          ? 0
+                          : build_value_dict(N, P.up, P.ux, P.union_nnz, d_rho, &tid, &P.dict, &zero_id, st);
+        if (T < 0) return fail(ctx, SFG_ERR_CUDA, "value dictionary");
+        P.dict_n = T;
+        ctx->stats.value_tuples = T;
+    }
+    const char *nt = std::getenv("SFG_NO_TILES"), *mo = std::getenv("SFG_MORTON");
+    const bool tiles = P.dict_n > 0 && !(nt && *nt && *nt != '0');
+    // the spatial (Morton) order inside the classes: SFG_MORTON=1 (with tiles)
+    const bool morton = tiles && mo && *mo == '1';
     // two-class numbering of the fused FP32 step (sfg_step32.cuh): class Z =
     // rows inside the M-PML and every column they reference; class A = the
-    // rest.  Inside each class, windows of 2048 rows are ordered by (M-PML
-    // flag, decreasing length) so that 32-row SELL slices need no padding.
+    // rest.  Inside each class, windows of rows are ordered by (M-PML flag,
+    // decreasing length) so that 32-row SELL slices need no padding; with
+    // tiles the class is first put in Morton order of the node coordinates
+    // and the windows are the tiles.
     {
         int na = 0, npml = 0;
-        CK(build_classes(N, P.up, P.uj, P.mpml, P.max_row_len, &P.perm, &P.inv, &P.upp, &na, &npml, st));
+        CK(build_classes(N, P.up, P.uj, P.mpml, P.max_row_len, &P.perm, &P.inv, &P.upp, &na, &npml, st,
+                         tiles ? kTileRows : 0, morton ? d_x : nullptr, morton ? d_y : nullptr, m->xmin, m->xmax,
+                         m->ymin, m->ymax));
         std::vector<int> perm(N), inv(N);
         CK(cudaMemcpyAsync(perm.data(), P.perm, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(inv.data(), P.inv, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
@@ -388,33 +418,36 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         ctx->stats.pml_rows = npml;
     }
     tr.mark("setup: M-PML, coef, classes");
-    // The one-shot kernels' matrix slots: (column, tuple id) when the union
-    // entries reduce to a small value dictionary (meshes of congruent
-    // elements), else column + M + K1..K4 (class A) or K1..K6 (class Z).
-    // SFG_NO_VALUE_DICT=1 keeps the full-value slots (to compare the two).
-    {
-        const char *nd = std::getenv("SFG_NO_VALUE_DICT");
-        int *tid = nullptr, zero_id = 0;
-        const int T = (nd && *nd && *nd != '0')
-                          ? 0
-                          : build_value_dict(N, P.up, P.ux, P.union_nnz, d_rho, &tid, &P.dict, &zero_id, st);
-        if (T < 0) return fail(ctx, SFG_ERR_CUDA, "value dictionary");
-        P.dict_n = T;
-        if (T > 0) {
-            CK(build_sell_range_dict(0, P.na, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellAd, &P.sliceA,
-                                     &P.slotsA, st));
-            CK(build_sell_range_dict(P.na, N, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellZd, &P.sliceZ,
-                                     &P.slotsZ, st));
-            CK(build_row_density(N, d_rho, P.perm, &P.rowrho, st));
-            CK(cudaStreamSynchronize(st));
-            keep_free(tid, st);
-        } else {
-            CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA,
-                                &P.slotsA, st));
-            CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ,
-                                &P.slotsZ, st));
+    if (P.dict_n > 0) {
+        CK(build_sell_range_dict(0, P.na, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellAd, &P.sliceA, &P.slotsA,
+                                 st));
+        CK(build_sell_range_dict(P.na, N, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellZd, &P.sliceZ, &P.slotsZ,
+                                 st));
+        CK(build_row_density(N, d_rho, P.perm, &P.rowrho, st));
+        if (tiles) {
+            int ha = 0, hz = 0;
+            CK(build_tiles(0, P.na, P.up, P.uj, tid, zero_id, P.perm, P.inv, P.sliceA, P.slotsA, &P.tileA_off,
+                           &P.tileA_ext, &P.sellAt, &ha, &P.slotsA_max, st));
+            CK(build_tiles(P.na, N, P.up, P.uj, tid, zero_id, P.perm, P.inv, P.sliceZ, P.slotsZ, &P.tileZ_off,
+                           &P.tileZ_ext, &P.sellZt, &hz, &P.slotsZ_max, st));
+            if (ha < 0 || hz < 0 || !P.tileA_off || !P.tileZ_off) {   // a tile reaches too far: no tiles
+                for (void *q : {(void *)P.tileA_off, (void *)P.tileA_ext, (void *)P.sellAt, (void *)P.tileZ_off,
+                                (void *)P.tileZ_ext, (void *)P.sellZt})
+                    keep_free(q, st);
+                P.tileA_off = P.tileA_ext = P.tileZ_off = P.tileZ_ext = nullptr;
+                P.sellAt = P.sellZt = nullptr;
+                ha = hz = 0;
+            }
+            P.haloA_max = ha;
+            P.haloZ_max = hz;
         }
-        ctx->stats.value_tuples = T;
+        CK(cudaStreamSynchronize(st));
+        keep_free(tid, st);
+    } else {
+        CK(build_sell_range(0, P.na, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 6, &P.sellA, &P.sliceA,
+                            &P.slotsA, st));
+        CK(build_sell_range(P.na, N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, 8, &P.sellZ, &P.sliceZ,
+                            &P.slotsZ, st));
     }
     CK(build_rec_perm(N, P.up, P.uj, P.ux, P.union_nnz, P.perm, P.inv, P.upp, &P.recp, st));
     CK(build_coef2(N, P.na, P.coef32, P.perm, &P.coefA, &P.imA, &P.coefZ, st));
@@ -429,7 +462,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     for (auto &px : ctx->plain_x) { cudaFree(px); px = nullptr; }
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
-        auto it = g_tuned.find({ctx->device, N, P.na, tc, P.union_nnz});
+        auto it = g_tuned.find({ctx->device, N, P.na, tc, P.union_nnz, slot_layout(P)});
         ctx->tune = it != g_tuned.end() ? it->second : RunCache();
     }
     ctx->ready = true;
@@ -619,6 +652,11 @@ Step2 step2_args(const DevProblem &P, const LoopPlan &pl, const StepCommon &c, c
     a.cmm = b.cmm; a.sig = b.sig;
     a.in = {b.Gc[cur], b.Pa[cur], b.Gs[cur], b.Ps[cur]};
     a.out = {b.Gc[nxt], b.Pa[nxt], b.Gs[nxt], b.Ps[nxt]};
+    a.sellAt = P.sellAt; a.sellZt = P.sellZt;
+    a.tileA_off = P.tileA_off; a.tileA_ext = P.tileA_ext; a.tileZ_off = P.tileZ_off; a.tileZ_ext = P.tileZ_ext;
+    a.haloA_max = P.haloA_max; a.haloZ_max = P.haloZ_max;
+    a.slotsA_max = P.slotsA_max; a.slotsZ_max = P.slotsZ_max;
+    a.max_row_len = P.max_row_len;
     return a;
 }
 
@@ -823,6 +861,10 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     std::vector<int> cand;
     if (pl.S == 1) {
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
+        // the staged-gather tile kernels, where the set-up built tiles, and
+        // the staged slot streams, where there is a value dictionary
+        if (ctx->P.tileA_off && ctx->P.tileZ_off && !b.cmm) cand.push_back(kTileShape);
+        if (ctx->P.dict_n > 0 && !b.cmm) cand.push_back(kSlotStageShape);
     } else {
         for (int spl : {1, 2, 4})
             if (pl.S % (32 * spl) == 0)
@@ -894,7 +936,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     pl.shapeZ = pick_z;
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
-        g_tuned[{ctx->device, ctx->N, ctx->P.na, ctx->P.type_code, ctx->P.union_nnz}] = ctx->tune;
+        g_tuned[{ctx->device, ctx->N, ctx->P.na, ctx->P.type_code, ctx->P.union_nnz, slot_layout(ctx->P)}] = ctx->tune;
     }
     return SFG_OK;
 }

@@ -69,6 +69,10 @@ struct DevProblem {
     float4 *dict = nullptr;          // [2 dict_n]
     int2 *sellAd = nullptr, *sellZd = nullptr;   // SELL-32 slots (column, tuple id)
     float *rowrho = nullptr;         // [N] row density, permuted
+    // staged-gather tiles (sfg_step32.cuh: Step2::tile*); tileA_off == nullptr without them
+    unsigned *sellAt = nullptr, *sellZt = nullptr;
+    int *tileA_off = nullptr, *tileA_ext = nullptr, *tileZ_off = nullptr, *tileZ_ext = nullptr;
+    int haloA_max = 0, haloZ_max = 0, slotsA_max = 0, slotsZ_max = 0;
     float4 *coefA = nullptr;         // [na]
     float *imA = nullptr;            // [na]
     float *coefZ = nullptr;          // [N - na][12]

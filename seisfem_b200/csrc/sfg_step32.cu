@@ -14,7 +14,10 @@
 // and forms the class-Z totals U1+U2+U3, W1+W2+W3 from those pairs in FP64.
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
+#include <vector>
 
 #include "sfg_dev.cuh"
 #include "sfg_internal.h"
@@ -263,8 +266,9 @@ __device__ __forceinline__ void load_dict(const Step2 &a, float4 *stab)
 }
 
 // Class-A rows of block `bid` of one mesh (the tuples already in stab).
-template <bool COMP, int THREADS, bool DICT>
-__device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4 *stab, int it, int seis_row)
+template <bool COMP, int THREADS, bool DICT, bool STG = false>
+__device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4 *stab, int it, int seis_row,
+                                           const int2 *stg = nullptr, int slb = 0)
 {
     const StepCommon &c = a.c;
     const int i = bid * THREADS + threadIdx.x;
@@ -295,10 +299,10 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
         };
         if (DICT) {
             DictSlots ss;
-            ss.init(a.sellAd + (size_t)s0 * 32 + lane, s1 - s0);
+            if (!STG) ss.init(a.sellAd + (size_t)s0 * 32 + lane, s1 - s0);
 #pragma unroll 2
             for (int g = s0; g < s1; ++g) {
-                const int2 cv = ss.next();
+                const int2 cv = STG ? stg[(g - slb) * 32 + lane] : ss.next();
                 const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
                 const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
                 acc(cv.x, t0.x, kv);
@@ -353,8 +357,9 @@ __global__ void __launch_bounds__(THREADS, MINB) stepA_kernel(const Step2 a)
 }
 
 // Class-Z rows of block `bid` of one mesh (the tuples already in stab).
-template <bool COMP, int THREADS, bool DICT>
-__device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4 *stab, int it)
+template <bool COMP, int THREADS, bool DICT, bool STG = false>
+__device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4 *stab, int it,
+                                           const int2 *stg = nullptr, int slb = 0)
 {
     const StepCommon &c = a.c;
     const int nz = c.n - a.na;
@@ -380,11 +385,12 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
         const float4 own0 = __ldg(gci), own2 = __ldg(gci + 2);
         const float *sd = DICT ? nullptr : a.sellZ + (size_t)s0 * 256 + lane;
         DictSlots ss;
-        if (DICT) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
+        if (DICT && !STG) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
+        int gs_next = s0 - slb;   // staged slots: the next slot row in shared memory
         // slot g's column, M and K1..K(NK): from the dictionary or the full-value planes
         auto slot = [&](int &j, float &vm, float *kv, int nk) {
             if (DICT) {
-                const int2 cv = ss.next();
+                const int2 cv = STG ? stg[(gs_next++) * 32 + lane] : ss.next();
                 const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
                 j = cv.x;
                 vm = t0.x;
@@ -1084,6 +1090,308 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
     if (c.energy) energy_flush<SPL>(c, se, S, s_base, eu, ew);
 }
 
+// ------------------------------------------ staged-gather tile kernels
+//
+// One block of kTileRows threads per tile: a window of kTileRows consecutive
+// rows of one class, which the set-up's Morton order makes a compact patch
+// of the mesh.  The block first copies every record its rows gather -- its
+// own rows' and its halo's (the rows outside the tile that its rows
+// reference) -- from global memory into shared memory with cp.async, all
+// copies in flight at once, and then runs the arithmetic of stepA_kernel /
+// stepZ_kernel (value dictionary) with every neighbour read served from
+// shared memory.  Slots are 4 bytes: (halo position << 16 | tuple id).  The
+// staged records are planes of float4 (plane k holds bytes 16k..16k+15 of
+// each record), so a warp reading one plane touches distinct banks when its
+// columns are distinct.
+
+// Copies the 48-byte records rows[k] (k < nr: row w0 + k; else ext[k - nr])
+// of `base` into planes P, P + H, P + 2H of shared memory.
+__device__ __forceinline__ void tile_stage(const float *__restrict__ base, int w0, int nr,
+                                           const int *__restrict__ ext, int ne, float4 *P, int H)
+{
+    const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(P);
+    for (int k = threadIdx.x; k < nr + ne; k += blockDim.x) {
+        const int g = k < nr ? w0 + k : __ldg(ext + k - nr);
+        const float *src = base + (size_t)g * 12;
+        cp_async16(s0 + 16u * (uint32_t)k, src);
+        cp_async16(s0 + 16u * (uint32_t)(H + k), src + 4);
+        cp_async16(s0 + 16u * (uint32_t)(2 * H + k), src + 8);
+    }
+}
+
+// Copies n float4 from global src to shared dst (all threads, 16-byte cp.async).
+__device__ __forceinline__ void tile_copy(float4 *dst, const float4 *__restrict__ src, int n)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) cp_async16(d + 16u * (uint32_t)k, src + k);
+}
+
+template <bool COMP>
+__global__ void __launch_bounds__(kTileRows, 3) stepAT_kernel(const Step2 a)
+{
+    // shared memory (float4 units): the halo's three planes [3H], the
+    // dictionary [2D], the tile's slots [8 SM], Pa [kTileRows], c [kTileRows]
+    extern __shared__ float4 tsm[];
+    const int H = a.haloA_max, SM = a.slotsA_max;
+    const float4 *P0 = tsm, *P1 = tsm + H, *P2 = tsm + 2 * H;
+    float4 *stab = tsm + 3 * H;
+    float4 *SL = stab + 2 * a.dict_n;
+    float4 *PAs = SL + 8 * SM;
+    float4 *CFs = PAs + kTileRows;
+    const StepCommon &c = a.c;
+    const int t = blockIdx.x, tx = threadIdx.x;
+    const int i = t * kTileRows + tx;
+    gather2_one(c, a.na, a.in, 1, i, c.seis_row);
+    const int w0 = t * kTileRows;
+    const int nr = max(0, min(a.na - w0, kTileRows));
+    for (int k = tx; k < 2 * a.dict_n; k += kTileRows) stab[k] = __ldg(a.dict + k);
+    int slb = 0;   // the tile's first slot row
+    if (nr > 0) {
+        const int e0 = __ldg(a.tileA_off + t), ne = __ldg(a.tileA_off + t + 1) - e0;
+        slb = __ldg(a.sliceA + w0 / 32);
+        const int sle = __ldg(a.sliceA + (w0 + nr + 31) / 32);
+        tile_copy(SL, reinterpret_cast<const float4 *>(a.sellAt) + (size_t)slb * 8, (sle - slb) * 8);
+        tile_copy(PAs, reinterpret_cast<const float4 *>(a.in.Pa) + w0, nr);
+        tile_copy(CFs, a.coefA + w0, nr);
+        tile_stage(a.in.Gc, w0, nr, a.tileA_ext + e0, ne, tsm, H);
+    }
+    const float im = tx < nr ? __ldcs(a.imA + i) : 0.f;
+    const float rho = tx < nr ? __ldcs(a.rowrho + i) : 0.f;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    double eu = 0.0, ew = 0.0;
+    if (tx < nr) {
+        const int lane = i & 31, slice = i >> 5;
+        float kU[4], kW[4], mL[8];
+#pragma unroll
+        for (int k = 0; k < 4; k++) { kU[k] = 0.f; kW[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 8; k++) mL[k] = 0.f;
+        const int sl0 = __ldg(a.sliceA + slice), sl1 = __ldg(a.sliceA + slice + 1);
+        // own (hi, lo) displacements: K U = sum_j K_ij (U_j - U_i)
+        const float4 own0 = P0[tx], own2 = P2[tx];
+        const unsigned *sv = reinterpret_cast<const unsigned *>(SL) + lane;
+#pragma unroll 2
+        for (int g = sl0; g < sl1; ++g) {
+            const unsigned v = sv[(g - slb) * 32];
+            const int loc = (int)(v >> 16), id = (int)(v & 0xFFFFu);
+            const float4 t0 = stab[2 * id], t1 = stab[2 * id + 1];
+            const float4 q0 = P0[loc], q1 = P1[loc], q2 = P2[loc];
+            const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
+            const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
+            const float vm = t0.x;
+#pragma unroll
+            for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
+            mL[0] += vm * q0.z; mL[1] += vm * q0.w; mL[2] += vm * q1.x; mL[3] += vm * q1.y;
+            mL[4] += vm * q1.z; mL[5] += vm * q1.w; mL[6] += vm * q2.x; mL[7] += vm * q2.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) mL[k] *= rho;
+        const float4 cf = CFs[tx];
+        double src_u = 0.0, src_w = 0.0;
+        if (i == c.src[0]) {
+            const double ps = c.amp[c.it];
+            src_u = ps * c.sin_af;
+            src_w = ps * c.cos_af;
+        }
+        float g[GC], p[PA];
+        const float4 own1 = P1[tx];
+        g[0] = own0.x; g[1] = own0.y; g[2] = own0.z; g[3] = own0.w;
+        g[4] = own1.x; g[5] = own1.y; g[6] = own1.z; g[7] = own1.w;
+        g[8] = own2.x; g[9] = own2.y; g[10] = own2.z; g[11] = own2.w;
+        const float4 pv = PAs[tx];
+        p[0] = pv.x; p[1] = pv.y; p[2] = pv.z; p[3] = pv.w;
+        float uu, ww, su, sw;
+        stiff_sums(kU, kW, cf, su, sw);
+        finish_A<COMP>(su, sw, mL, im, c.dt, src_u, src_w, g, p, uu, ww);
+        float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+#pragma unroll
+        for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+        reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
+        eu = (double)uu * uu;
+        ew = (double)ww * ww;
+    }
+    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+}
+
+template <bool COMP>
+__global__ void __launch_bounds__(kTileRows, 2) stepZT_kernel(const Step2 a)
+{
+    // shared memory (float4 units): the halo's Gc planes [3H] and Gs planes
+    // [3H], the dictionary [2D], the tile's slots [8 SM], Ps [3 kTileRows],
+    // coefficients [3 kTileRows]
+    extern __shared__ float4 tsm[];
+    const int H = a.haloZ_max, SM = a.slotsZ_max;
+    const float4 *P0 = tsm, *P1 = tsm + H, *P2 = tsm + 2 * H;       // Gc records
+    float4 *Q = tsm + 3 * H;                                       // Gs records
+    const float4 *Q0 = Q, *Q1 = Q + H, *Q2 = Q + 2 * H;
+    float4 *stab = tsm + 6 * H;
+    float4 *SL = stab + 2 * a.dict_n;
+    float4 *PSs = SL + 8 * SM;
+    float4 *CFs = PSs + 3 * kTileRows;
+    const StepCommon &c = a.c;
+    const int nz = c.n - a.na;
+    const int t = blockIdx.x, tx = threadIdx.x;
+    const int local = t * kTileRows + tx;
+    const int i = a.na + local;
+    const int w0 = a.na + t * kTileRows;
+    const int nr = max(0, min(nz - t * kTileRows, kTileRows));
+    for (int k = tx; k < 2 * a.dict_n; k += kTileRows) stab[k] = __ldg(a.dict + k);
+    const int e0 = __ldg(a.tileZ_off + t), ne = __ldg(a.tileZ_off + t + 1) - e0;
+    const int *ext = a.tileZ_ext + e0;
+    const int lb = t * kTileRows;                                  // the tile's first class-Z row
+    const int slb = __ldg(a.sliceZ + lb / 32), sle = __ldg(a.sliceZ + (lb + nr + 31) / 32);
+    tile_copy(SL, reinterpret_cast<const float4 *>(a.sellZt) + (size_t)slb * 8, (sle - slb) * 8);
+    tile_copy(PSs, reinterpret_cast<const float4 *>(a.in.Ps) + (size_t)lb * 3, 3 * nr);
+    tile_copy(CFs, reinterpret_cast<const float4 *>(a.coefZ) + (size_t)lb * 3, 3 * nr);
+    const float rho = tx < nr ? __ldcs(a.rowrho + i) : 0.f;
+    tile_stage(a.in.Gc, w0, nr, ext, ne, tsm, H);
+    {
+        // split-field records of the staged rows (class Z only; zeros for
+        // class-A columns, whose split fields no row uses)
+        const uint32_t q0 = (uint32_t)__cvta_generic_to_shared(Q);
+        for (int k = tx; k < nr + ne; k += kTileRows) {
+            const int g = k < nr ? w0 + k : __ldg(ext + k - nr);
+            if (g >= a.na) {
+                const float *src = a.in.Gs + (size_t)(g - a.na) * GS;
+                cp_async16(q0 + 16u * (uint32_t)k, src);
+                cp_async16(q0 + 16u * (uint32_t)(H + k), src + 4);
+                cp_async16(q0 + 16u * (uint32_t)(2 * H + k), src + 8);
+            } else {
+                const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+                Q[k] = z;
+                Q[H + k] = z;
+                Q[2 * H + k] = z;
+            }
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
+    if (tx < nr) {
+        c0 = CFs[3 * tx]; c1 = CFs[3 * tx + 1]; c2 = CFs[3 * tx + 2];
+    }
+    const bool full = __any_sync(0xffffffffu, tx < nr && is_pml_row(c1));
+    double eu = 0.0, ew = 0.0;
+    if (tx < nr) {
+        const int lane = local & 31, slice = local >> 5;
+        float kU[6], kW[6], m[20];
+#pragma unroll
+        for (int k = 0; k < 6; k++) { kU[k] = 0.f; kW[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 20; k++) m[k] = 0.f;
+        const int sl0 = __ldg(a.sliceZ + slice), sl1 = __ldg(a.sliceZ + slice + 1);
+        const float4 own0 = P0[tx], own2 = P2[tx];
+        const unsigned *sv = reinterpret_cast<const unsigned *>(SL) + lane;
+        if (full) {
+#pragma unroll 2
+            for (int g = sl0; g < sl1; ++g) {
+                const unsigned v = sv[(g - slb) * 32];
+                const int loc = (int)(v >> 16), id = (int)(v & 0xFFFFu);
+                const float4 t0 = stab[2 * id], t1 = stab[2 * id + 1];
+                const float kv[6] = {t0.y, t0.z, t0.w, t1.x, t1.y, t1.z};
+                const float vm = t0.x;
+                const float4 q0 = P0[loc], q1 = P1[loc], q2 = P2[loc];
+                const float4 z0 = Q0[loc], z1 = Q1[loc], z2 = Q2[loc];
+                const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
+#pragma unroll
+                for (int k = 0; k < 6; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
+                m[0] += vm * z0.x;  m[1] += vm * z0.y;  m[2] += vm * z0.z;  m[3] += vm * z0.w;
+                m[4] += vm * z1.x;  m[5] += vm * z1.y;  m[6] += vm * z1.z;  m[7] += vm * z1.w;
+                m[8] += vm * z2.x;  m[9] += vm * z2.y;  m[10] += vm * z2.z; m[11] += vm * z2.w;
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
+        } else {
+#pragma unroll 2
+            for (int g = sl0; g < sl1; ++g) {
+                const unsigned v = sv[(g - slb) * 32];
+                const int loc = (int)(v >> 16), id = (int)(v & 0xFFFFu);
+                const float4 t0 = stab[2 * id], t1 = stab[2 * id + 1];
+                const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
+                const float vm = t0.x;
+                const float4 q0 = P0[loc], q1 = P1[loc], q2 = P2[loc];
+                const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
+#pragma unroll
+                for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
+                m[12] += vm * q0.z; m[13] += vm * q0.w; m[14] += vm * q1.x; m[15] += vm * q1.y;
+                m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 20; k++) m[k] *= rho;
+        double src_u = 0.0, src_w = 0.0;
+        if (i == c.src[0]) {
+            const double ps = c.amp[c.it];
+            src_u = ps * c.sin_af;
+            src_w = ps * c.cos_af;
+        }
+        float gs[GS], ps_[PS], gc[GC];
+        const float4 sq[3] = {Q0[tx], Q1[tx], Q2[tx]};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float4 w = PSs[3 * tx + k];
+            gs[4 * k] = sq[k].x; gs[4 * k + 1] = sq[k].y; gs[4 * k + 2] = sq[k].z; gs[4 * k + 3] = sq[k].w;
+            ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
+        }
+        float uu, ww;
+        finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, uu, ww);
+        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+        float4 *so = reinterpret_cast<float4 *>(a.out.Gs + (size_t)local * GS);
+        float4 *po = reinterpret_cast<float4 *>(a.out.Ps + (size_t)local * PS);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            gco[k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
+            so[k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
+            po[k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
+        }
+        eu = (double)uu * uu;
+        ew = (double)ww * ww;
+    }
+    block_energy(c.energy ? c.energy + ((size_t)c.it) * 2 : nullptr, eu, ew);
+}
+
+// ------------------------------- one-shot kernels with staged slot streams
+//
+// Launch shape kSlotStageShape: blocks of 128 rows copy all the SELL slots of
+// their 4 slices (value dictionary: 8-byte (column, tuple id) pairs) into
+// shared memory with cp.async before their rows start, so that no row waits
+// for its slot stream; the neighbour gathers stay global (L1/L2), in the
+// mesh-order numbering where a slice's gathers are contiguous.
+constexpr int kStgThreads = 128;
+
+template <bool COMP>
+__global__ void __launch_bounds__(kStgThreads, 4) stepA_kernel_stg(const Step2 a)
+{
+    extern __shared__ float4 stab[];            // dictionary [2D], then the slot rows
+    int2 *slt = reinterpret_cast<int2 *>(stab + 2 * a.dict_n);
+    const int nsl = (a.na + 31) / 32;
+    const int sa = min(nsl, (int)blockIdx.x * (kStgThreads / 32)), sb = min(nsl, sa + kStgThreads / 32);
+    const int slb = sa < nsl ? __ldg(a.sliceA + sa) : 0, sle = sa < nsl ? __ldg(a.sliceA + sb) : 0;
+    tile_copy(reinterpret_cast<float4 *>(slt), reinterpret_cast<const float4 *>(a.sellAd + (size_t)slb * 32),
+              (sle - slb) * 16);
+    for (int t = threadIdx.x; t < 2 * a.dict_n; t += kStgThreads) stab[t] = __ldg(a.dict + t);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    stepA_body<COMP, kStgThreads, true, true>(a, blockIdx.x, stab, a.c.it, a.c.seis_row, slt, slb);
+}
+
+template <bool COMP>
+__global__ void __launch_bounds__(kStgThreads, 4) stepZ_kernel_stg(const Step2 a)
+{
+    extern __shared__ float4 stab[];
+    int2 *slt = reinterpret_cast<int2 *>(stab + 2 * a.dict_n);
+    const int nsl = (a.c.n - a.na + 31) / 32;
+    const int sa = min(nsl, (int)blockIdx.x * (kStgThreads / 32)), sb = min(nsl, sa + kStgThreads / 32);
+    const int slb = sa < nsl ? __ldg(a.sliceZ + sa) : 0, sle = sa < nsl ? __ldg(a.sliceZ + sb) : 0;
+    tile_copy(reinterpret_cast<float4 *>(slt), reinterpret_cast<const float4 *>(a.sellZd + (size_t)slb * 32),
+              (sle - slb) * 16);
+    for (int t = threadIdx.x; t < 2 * a.dict_n; t += kStgThreads) stab[t] = __ldg(a.dict + t);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    stepZ_body<COMP, kStgThreads, true, true>(a, blockIdx.x, stab, a.c.it, slt, slb);
+}
+
 // --------------------------------------------------- gathers, snapshots
 
 __global__ void gather2_kernel(const StepCommon c, int na, const State32 st, int S)
@@ -1256,17 +1564,42 @@ __global__ void class_scatter(int n, const unsigned char *__restrict__ zone, con
     perm0[zone[r] ? na + posZ[r] : posA[r]] = r;
 }
 
-// One block per window of 2048 rows (windows restart at the class boundary):
-// a stable sort by (M-PML flag, decreasing row length) -- a bitonic sort of
-// keys that carry the position in the window as their low 11 bits.
+// Morton key (bits of the two quantised coordinates interleaved) of the
+// mesh node of every entry of perm0, for the spatial order inside a class.
+__device__ __forceinline__ unsigned spread16(unsigned v)
+{
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__global__ void class_morton(int n, const int *__restrict__ perm0, const double *__restrict__ x,
+                             const double *__restrict__ y, double x0, double sx, double y0, double sy,
+                             unsigned *__restrict__ key)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = perm0[i];
+    const double qx = fmin(fmax((x[r] - x0) * sx, 0.0), 65535.0);
+    const double qy = fmin(fmax((y[r] - y0) * sy, 0.0), 65535.0);
+    key[i] = (spread16((unsigned)qy) << 1) | spread16((unsigned)qx);
+}
+
+// One block per window of W rows (a power of two <= 2048; windows restart at
+// the class boundary): a stable sort by (M-PML flag, decreasing row length)
+// -- a bitonic sort of keys that carry the position in the window as their
+// low 11 bits.
 __global__ void __launch_bounds__(1024) class_windows(int n, int na, int maxlen, const int *__restrict__ up,
                                                       const unsigned char *__restrict__ pml,
-                                                      const int *__restrict__ perm0, int *__restrict__ perm)
+                                                      const int *__restrict__ perm0, int *__restrict__ perm, int W)
 {
-    constexpr int W = 2048;
-    __shared__ unsigned key[W];
+    __shared__ unsigned key[2048];
     const int wa = (na + W - 1) / W;
     const int w = blockIdx.x;
+    // (W is uniform across the block)
     const int w0 = w < wa ? w * W : na + (w - wa) * W;
     const int w1 = w < wa ? min(na, w0 + W) : min(n, w0 + W);
     for (int i = threadIdx.x; i < W; i += blockDim.x) {
@@ -1369,8 +1702,97 @@ cudaError_t launch_range_slice_len(int r0, int r1, const int *d_up, const int *d
         }                                                                                      \
     } while (0)
 
+// dynamic shared memory a tile kernel may use, raised per device as needed
+template <typename K>
+static cudaError_t allow_smem(K kernel, size_t smem, int *cache)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) return e != cudaSuccess ? e : cudaErrorInvalidDevice;
+    if ((size_t)cache[dev] >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cache[dev] = (int)smem;
+    return e;
+}
+
+cudaError_t launch_stepA_tile(const Step2 &a, bool comp, cudaStream_t st)
+{
+    static int cache[2][64];
+    if (!a.tileA_off || a.dict_n <= 0 || a.dict_n > kDictMax || a.haloA_max <= 0 || a.haloA_max > kTileHaloMax)
+        return cudaErrorInvalidValue;
+    // the fused receiver gather runs on the first nrec threads
+    const int rows = std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0);
+    if (rows <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((rows + kTileRows - 1) / kTileRows);
+    const size_t smem = sizeof(float4) * (3 * (size_t)a.haloA_max + 2 * (size_t)a.dict_n + 8 * (size_t)a.slotsA_max +
+                                          2 * (size_t)kTileRows);
+    cudaError_t e;
+    if (comp) {
+        if ((e = allow_smem(stepAT_kernel<true>, smem, cache[1])) != cudaSuccess) return e;
+        stepAT_kernel<true><<<blocks, kTileRows, smem, st>>>(a);
+    } else {
+        if ((e = allow_smem(stepAT_kernel<false>, smem, cache[0])) != cudaSuccess) return e;
+        stepAT_kernel<false><<<blocks, kTileRows, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stepZ_tile(const Step2 &a, bool comp, cudaStream_t st)
+{
+    static int cache[2][64];
+    if (!a.tileZ_off || a.dict_n <= 0 || a.dict_n > kDictMax || a.haloZ_max <= 0 || a.haloZ_max > kTileHaloMax)
+        return cudaErrorInvalidValue;
+    const int nz = a.c.n - a.na;
+    if (nz <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((nz + kTileRows - 1) / kTileRows);
+    const size_t smem = sizeof(float4) * (6 * (size_t)a.haloZ_max + 2 * (size_t)a.dict_n + 8 * (size_t)a.slotsZ_max +
+                                          6 * (size_t)kTileRows);
+    cudaError_t e;
+    if (comp) {
+        if ((e = allow_smem(stepZT_kernel<true>, smem, cache[1])) != cudaSuccess) return e;
+        stepZT_kernel<true><<<blocks, kTileRows, smem, st>>>(a);
+    } else {
+        if ((e = allow_smem(stepZT_kernel<false>, smem, cache[0])) != cudaSuccess) return e;
+        stepZT_kernel<false><<<blocks, kTileRows, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+// staged slot streams (launch shape kSlotStageShape; value dictionary only)
+static cudaError_t launch_stg(const Step2 &a, bool comp, bool classA, cudaStream_t st)
+{
+    static int cache[4][64];
+    if (a.dict_n <= 0 || a.dict_n > kDictMax || a.max_row_len <= 0 || !a.dict) return cudaErrorInvalidValue;
+    const int rows = classA ? std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0) : a.c.n - a.na;
+    if (rows <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((rows + kStgThreads - 1) / kStgThreads);
+    // slot rows of a block: at most (kStgThreads / 32) slices of max_row_len
+    const size_t smem = sizeof(float4) * (2 * (size_t)a.dict_n + 16 * (size_t)(kStgThreads / 32) * a.max_row_len);
+    cudaError_t e;
+    if (classA) {
+        if (comp) {
+            if ((e = allow_smem(stepA_kernel_stg<true>, smem, cache[0])) != cudaSuccess) return e;
+            stepA_kernel_stg<true><<<blocks, kStgThreads, smem, st>>>(a);
+        } else {
+            if ((e = allow_smem(stepA_kernel_stg<false>, smem, cache[1])) != cudaSuccess) return e;
+            stepA_kernel_stg<false><<<blocks, kStgThreads, smem, st>>>(a);
+        }
+    } else {
+        if (comp) {
+            if ((e = allow_smem(stepZ_kernel_stg<true>, smem, cache[2])) != cudaSuccess) return e;
+            stepZ_kernel_stg<true><<<blocks, kStgThreads, smem, st>>>(a);
+        } else {
+            if ((e = allow_smem(stepZ_kernel_stg<false>, smem, cache[3])) != cudaSuccess) return e;
+            stepZ_kernel_stg<false><<<blocks, kStgThreads, smem, st>>>(a);
+        }
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st)
 {
+    if (variant == kTileShape) return launch_stepA_tile(a, comp, st);
+    if (variant == kSlotStageShape) return launch_stg(a, comp, true, st);
     if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
         return cudaErrorInvalidValue;
     // the fused receiver gather runs on the first nrec threads
@@ -1380,6 +1802,8 @@ cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st
 
 cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st)
 {
+    if (variant == kTileShape) return launch_stepZ_tile(a, comp, st);
+    if (variant == kSlotStageShape) return launch_stg(a, comp, false, st);
     if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
         return cudaErrorInvalidValue;
     SFG_SHAPES(stepZ_kernel, a.c.n - a.na);
@@ -1595,10 +2019,49 @@ cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm,
 }
 
 
+// Reorders perm0 inside class A ([0, na)) and inside class Z by the Morton
+// key of the nodes' coordinates (stable: equal keys keep mesh order), so that
+// windows of consecutive rows are compact patches of the mesh.
+static cudaError_t morton_order(int n, int na, int *perm0, const double *d_x, const double *d_y, double x0,
+                                double x1, double y0, double y1, cudaStream_t st)
+{
+    const double sx = x1 > x0 ? 65535.0 / (x1 - x0) : 0.0, sy = y1 > y0 ? 65535.0 / (y1 - y0) : 0.0;
+    unsigned *key = nullptr, *key2 = nullptr;
+    int *val2 = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cudaMallocAsync((void **)&key, sizeof(unsigned) * n, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&key2, sizeof(unsigned) * n, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&val2, sizeof(int) * n, st);
+    if (e == cudaSuccess) {
+        class_morton<<<(n + 255) / 256, 256, 0, st>>>(n, perm0, d_x, d_y, x0, sx, y0, sy, key);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key2, perm0, val2, std::max(na, n - na), 0, 32,
+                                            st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&tmp, std::max<size_t>(tmp_bytes, 16), st);
+    // the two classes one after the other (radix sort is stable)
+    const int seg[2][2] = {{0, na}, {na, n}};
+    for (int c = 0; c < 2 && e == cudaSuccess; c++) {
+        const int b = seg[c][0], m = seg[c][1] - seg[c][0];
+        if (m <= 1) continue;
+        size_t tb = tmp_bytes;
+        e = cub::DeviceRadixSort::SortPairs(tmp, tb, key + b, key2 + b, perm0 + b, val2 + b, m, 0, 32, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(perm0 + b, val2 + b, sizeof(int) * m, cudaMemcpyDeviceToDevice, st);
+    }
+    for (void *p : {(void *)key, (void *)key2, (void *)val2, tmp})
+        if (p) cudaFreeAsync(p, st);
+    return e;
+}
+
 cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double *d_mpml, int maxlen, int **d_perm,
-                          int **d_inv, int **d_upp, int *na_out, int *npml_out, cudaStream_t st)
+                          int **d_inv, int **d_upp, int *na_out, int *npml_out, cudaStream_t st, int tile_rows,
+                          const double *d_x, const double *d_y, double x0, double x1, double y0, double y1)
 {
     if (maxlen < 0 || maxlen >= (1 << 19)) return cudaErrorInvalidValue;
+    const int W = tile_rows > 0 ? tile_rows : 2048;
+    if (W > 2048 || (W & (W - 1))) return cudaErrorInvalidValue;
     unsigned char *pml = nullptr, *zone = nullptr;
     int *isA = nullptr, *isZ = nullptr, *posA = nullptr, *posZ = nullptr, *perm0 = nullptr, *lenp = nullptr,
         *cnt = nullptr;
@@ -1628,9 +2091,10 @@ cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double 
         if (e == cudaSuccess) e = cudaMemcpyAsync(&na, posA + n, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&npml, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && d_x && d_y) e = morton_order(n, na, perm0, d_x, d_y, x0, x1, y0, y1, st);
         if (e == cudaSuccess) {
-            const int windows = (na + 2047) / 2048 + (n - na + 2047) / 2048;
-            class_windows<<<windows, 1024, 0, st>>>(n, na, maxlen, d_up, pml, perm0, *d_perm);
+            const int windows = (na + W - 1) / W + (n - na + W - 1) / W;
+            class_windows<<<windows, std::min(W, 1024), 0, st>>>(n, na, maxlen, d_up, pml, perm0, *d_perm, W);
             class_inverse<<<g, 256, 0, st>>>(n, *d_perm, d_up, *d_inv, lenp);
             e = cudaGetLastError();
         }
@@ -1644,6 +2108,184 @@ cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double 
     return e;
 }
 
+
+// ------------------------------------------------ staged-gather tiles
+
+namespace {
+
+constexpr int kTileCand = 4096;   // references outside a tile collected before removing repeats
+
+// Bitonic sort of P keys (a power of two) in shared memory by the block.
+__device__ void block_bitonic(unsigned *key, int P)
+{
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const bool asc = (i & k) == 0;
+                    const unsigned a = key[i], b = key[ixj];
+                    if ((a > b) == asc) { key[i] = b; key[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// Tile t of permuted rows [r0, r1): the distinct rows outside the tile that
+// its rows reference, ascending.  ext == nullptr: their count into cnt[t]
+// (kTileHaloMax + 1 when more references than fit); else written to
+// ext[off[t] ...].
+__global__ void __launch_bounds__(256) tile_halo(int r0, int r1, const int *__restrict__ up,
+                                                 const int *__restrict__ uj, const int *__restrict__ perm,
+                                                 const int *__restrict__ inv, int *__restrict__ cnt,
+                                                 const int *__restrict__ off, int *__restrict__ ext)
+{
+    __shared__ unsigned cand[kTileCand];
+    __shared__ int ncand, part[257];
+    const int t = blockIdx.x;
+    const int w0 = r0 + t * kTileRows, w1 = min(r1, w0 + kTileRows);
+    if (threadIdx.x == 0) ncand = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < w1 - w0; k += blockDim.x) {
+        const int r = perm[w0 + k];
+        for (int e = up[r]; e < up[r + 1]; e++) {
+            const int c = inv[uj[e]];
+            if (c < w0 || c >= w1) {
+                const int p = atomicAdd(&ncand, 1);
+                if (p < kTileCand) cand[p] = (unsigned)c;
+            }
+        }
+    }
+    __syncthreads();
+    const int m = ncand;
+    if (m > kTileCand) {
+        if (threadIdx.x == 0 && !ext) cnt[t] = kTileHaloMax + 1;
+        return;
+    }
+    int P = 1;
+    while (P < m) P <<= 1;
+    for (int k = m + threadIdx.x; k < P; k += blockDim.x) cand[k] = 0xFFFFFFFFu;
+    __syncthreads();
+    block_bitonic(cand, P);
+    // first entry of each run of equal rows: count per thread chunk, scan
+    const int chunk = (P + blockDim.x - 1) / blockDim.x;
+    const int k0 = threadIdx.x * chunk, k1 = min(m, k0 + chunk);
+    int mine = 0;
+    for (int k = k0; k < k1; k++) mine += (k == 0 || cand[k] != cand[k - 1]);
+    part[threadIdx.x + 1] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        part[0] = 0;
+        for (int i = 1; i <= (int)blockDim.x; i++) part[i] += part[i - 1];
+    }
+    __syncthreads();
+    if (!ext) {
+        if (threadIdx.x == 0) cnt[t] = part[blockDim.x];
+        return;
+    }
+    int o = off[t] + part[threadIdx.x];
+    for (int k = k0; k < k1; k++)
+        if (k == 0 || cand[k] != cand[k - 1]) ext[o++] = (int)cand[k];
+}
+
+// Packed slots (halo position << 16 | tuple id) of the rows of [r0, r1) in
+// the SELL-32 slices sp; padding slots name the row itself with the zero tuple.
+__global__ void tile_sell_fill(int r0, int r1, const int *__restrict__ up, const int *__restrict__ uj,
+                               const int *__restrict__ tid, int zero_id, const int *__restrict__ sp,
+                               const int *__restrict__ perm, const int *__restrict__ inv, const int *__restrict__ off,
+                               const int *__restrict__ ext, unsigned *__restrict__ sell)
+{
+    const int s = blockIdx.x, lane = threadIdx.x;
+    const int n = r1 - r0, r = s * 32 + lane;
+    const int t = (s * 32) / kTileRows;
+    const int w0 = r0 + t * kTileRows, w1 = min(r1, w0 + kTileRows);
+    const int *ex = ext + off[t];
+    const int ne = off[t + 1] - off[t];
+    const int s0 = sp[s], s1 = sp[s + 1];
+    const int o = r < n ? perm[r0 + r] : 0;
+    const int a0 = r < n ? up[o] : 0, len = r < n ? up[o + 1] - a0 : 0;
+    const unsigned own = r < n ? (unsigned)(r0 + r - w0) : 0u;
+    for (int k = 0; k < s1 - s0; k++) {
+        unsigned loc = own, id = (unsigned)zero_id;
+        if (k < len) {
+            const int c = inv[uj[a0 + k]];
+            if (c >= w0 && c < w1) {
+                loc = (unsigned)(c - w0);
+            } else {
+                int lo = 0, hi = ne;          // first external entry >= c (present by construction)
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (ex[mid] < c) lo = mid + 1;
+                    else hi = mid;
+                }
+                loc = (unsigned)(w1 - w0 + lo);
+            }
+            id = (unsigned)tid[a0 + k];
+        }
+        sell[(size_t)(s0 + k) * 32 + lane] = (loc << 16) | id;
+    }
+}
+
+}  // namespace
+
+cudaError_t build_tiles(int r0, int r1, const int *d_up, const int *d_uj, const int *d_tid, int zero_id,
+                        const int *d_perm, const int *d_inv, const int *d_slice, long long slots, int **d_off,
+                        int **d_ext, unsigned **d_sell, int *halo_max, int *slots_max, cudaStream_t st)
+{
+    *d_off = nullptr;
+    *d_ext = nullptr;
+    *d_sell = nullptr;
+    *halo_max = 0;
+    *slots_max = 0;
+    const int n = r1 - r0;
+    if (n <= 0) return cudaSuccess;
+    const int ntiles = (n + kTileRows - 1) / kTileRows, nsl = (n + 31) / 32;
+    {
+        // slot rows per tile, from the slice pointers
+        std::vector<int> sp(nsl + 1);
+        cudaError_t e0 = cudaMemcpyAsync(sp.data(), d_slice, sizeof(int) * (nsl + 1), cudaMemcpyDeviceToHost, st);
+        if (e0 == cudaSuccess) e0 = cudaStreamSynchronize(st);
+        if (e0 != cudaSuccess) return e0;
+        constexpr int per = kTileRows / 32;
+        for (int t = 0; t < ntiles; t++) *slots_max = std::max(*slots_max, sp[std::min(nsl, (t + 1) * per)] - sp[t * per]);
+    }
+    int *cnt = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&cnt, sizeof(int) * (ntiles + 1), st);
+    if (e != cudaSuccess) return e;
+    tile_halo<<<ntiles, 256, 0, st>>>(r0, r1, d_up, d_uj, d_perm, d_inv, cnt, nullptr, nullptr);
+    e = cudaGetLastError();
+    std::vector<int> h(ntiles);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), cnt, sizeof(int) * ntiles, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    int hmax = 0;
+    for (int t = 0; t < ntiles && e == cudaSuccess; t++)
+        hmax = std::max(hmax, std::min(kTileRows, n - t * kTileRows) + h[t]);
+    if (e != cudaSuccess || hmax > kTileHaloMax) {
+        cudaFreeAsync(cnt, st);
+        *halo_max = e == cudaSuccess ? -1 : 0;
+        return e;
+    }
+    e = keep_alloc(d_off, sizeof(int) * (ntiles + 1), st);
+    if (e == cudaSuccess) e = exclusive_scan_int(cnt, *d_off, ntiles, st);
+    int tot = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot, *d_off + ntiles, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = keep_alloc(d_ext, sizeof(int) * std::max(tot, 1), st);
+    if (e == cudaSuccess) {
+        tile_halo<<<ntiles, 256, 0, st>>>(r0, r1, d_up, d_uj, d_perm, d_inv, cnt, *d_off, *d_ext);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = keep_alloc(d_sell, sizeof(unsigned) * 32 * std::max<long long>(slots, 1), st);
+    if (e == cudaSuccess) {
+        tile_sell_fill<<<nsl, 32, 0, st>>>(r0, r1, d_up, d_uj, d_tid, zero_id, d_slice, d_perm, d_inv, *d_off,
+                                           *d_ext, *d_sell);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(cnt, st);
+    *halo_max = hmax;
+    return e;
+}
 
 cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long nnz, const int *d_perm,
                           const int *d_upp, const double *d_rho0, const float *d_recp, float **d_rec, cudaStream_t st)

@@ -77,7 +77,24 @@ struct Step2 {
     const float *sig;
     State32 in;
     State32W out;
+    // staged-gather tiles of the one-shot kernels (value dictionary only;
+    // tileA_off == nullptr without them): each class is cut into windows of
+    // kTileRows consecutive rows; tile t's halo is its own rows followed by
+    // the rows tile?_ext[tile?_off[t] .. tile?_off[t + 1]) (sorted) that
+    // its rows reference outside it; the SELL-32 slots (same slices as
+    // sellAd / sellZd) hold (halo position << 16 | tuple id)
+    const unsigned *sellAt, *sellZt;
+    const int *tileA_off, *tileA_ext, *tileZ_off, *tileZ_ext;
+    int haloA_max, haloZ_max;  // largest halo of a tile of each class (rows)
+    int slotsA_max, slotsZ_max;  // most SELL slot rows (32 slots each) of a tile of each class
+    int max_row_len;           // longest union row (slot rows of one slice at most)
 };
+
+// rows per staged-gather tile (one block of as many threads per tile)
+constexpr int kTileRows = 256;
+// largest halo a tile may have (own rows included); a mesh whose tiles reach
+// further keeps the unstaged kernels
+constexpr int kTileHaloMax = 2048;
 
 // single shot (thread per row); variant = launch shape 0..step2_variants()-1
 int step2_variants();
@@ -94,6 +111,15 @@ cudaError_t launch_stepA_multi(const Step2 *descs, const int2 *map, int nblocks,
                                int variant, int it, cudaStream_t st);
 cudaError_t launch_stepZ_multi(const Step2 *descs, const int2 *map, int nblocks, bool dict, int dict_max, bool comp,
                                int variant, int it, cudaStream_t st);
+// staged-gather tiles (launch shape kTileShape of launch_stepA / launch_stepZ):
+// the tile's own records and its halo are copied into shared memory with
+// cp.async, and every gather of the step reads shared memory
+constexpr int kTileShape = 6;
+// one-shot kernels whose 128-row blocks copy their slot streams into shared
+// memory before their rows start (value dictionary; gathers stay global)
+constexpr int kSlotStageShape = 7;
+cudaError_t launch_stepA_tile(const Step2 &a, bool comp, cudaStream_t st);
+cudaError_t launch_stepZ_tile(const Step2 &a, bool comp, cudaStream_t st);
 // S = a.S shots, a multiple of 32 * spl; a warp advances 32 * spl shots of
 // one row (spl per lane); warps per block a multiple of S / (32 * spl)
 cudaError_t launch_stepA_batched(const Step2 &a, bool comp, int spl, int warps, cudaStream_t st);
@@ -118,8 +144,22 @@ cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double
 // the two-class numbering on the device: perm (class A, then class Z; windows
 // of 2048 rows stably sorted by M-PML flag and decreasing length), its
 // inverse and the permuted row pointers; na = class-A rows, npml = M-PML rows
+// tile_rows > 0: windows of tile_rows rows (a power of two <= 2048) instead
+// of 2048; d_x, d_y given: rows inside each class in Morton order of the node
+// coordinates (over [x0, x1] x [y0, y1]) before the windows, else mesh order
 cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double *d_mpml, int maxlen, int **d_perm,
-                          int **d_inv, int **d_upp, int *na, int *npml, cudaStream_t st);
+                          int **d_inv, int **d_upp, int *na, int *npml, cudaStream_t st, int tile_rows = 0,
+                          const double *d_x = nullptr, const double *d_y = nullptr, double x0 = 0, double x1 = 1,
+                          double y0 = 0, double y1 = 1);
+// staged-gather tiles of permuted rows [r0, r1) (windows of kTileRows): the
+// external halo rows per tile (d_off [ntiles + 1], d_ext) and the packed
+// SELL-32 slots over the slices of d_slice (build_sell_range_dict's);
+// *halo_max = the largest halo (own rows included), or -1 when a tile's
+// halo passes kTileHaloMax (no tile data is then kept); *slots_max = the most
+// slot rows (32 slots each) of a tile
+cudaError_t build_tiles(int r0, int r1, const int *d_up, const int *d_uj, const int *d_tid, int zero_id,
+                        const int *d_perm, const int *d_inv, const int *d_slice, long long slots, int **d_off,
+                        int **d_ext, unsigned **d_sell, int *halo_max, int *slots_max, cudaStream_t st);
 // one model per shot: row records with M_geo = M / rho0(row) in plane 1
 // (stream-ordered allocation), and the row sums of M_geo in mesh order
 cudaError_t build_rec_geo(int n, const int *d_up, const double *d_ux, long long nnz, const int *d_perm,

@@ -464,6 +464,48 @@ def target(seis_u: np.ndarray, seis_w: np.ndarray) -> np.ndarray:
     return np.stack([seis_u.T, seis_w.T]).astype(np.float32)
 
 
+def moveout_samples(seeds, speed: float = 3000.0, **cfg) -> np.ndarray:
+    """Per shot and receiver [n][W]: the whole samples |y_rec - y_src| / speed
+    / dt of a wave at `speed` from the source to each receiver (config-5
+    geometry; no FEM run)."""
+    from .problem import config_5
+    out = []
+    for s in seeds:
+        p = config_5(int(s), **cfg)
+        m = p.mesh
+        off = np.abs(m.y[p.rec_node] - m.y[p.src_node[0]])
+        out.append(np.floor(off / speed / p.dt).astype(np.int32))
+    return np.stack(out)
+
+
+def to_reduced_time(y: np.ndarray, shift: np.ndarray) -> np.ndarray:
+    """y[n][c][W][T] -> the traces advanced by their moveout: r[..., w, tau] =
+    y[..., w, tau + shift[n, w]] (zeros past the end).  Exact inverse
+    from_reduced_time for every sample at or after the shift; the samples
+    before it (ahead of the first arrival at that speed) are dropped."""
+    out = np.zeros_like(y)
+    T = y.shape[-1]
+    for n in range(y.shape[0]):
+        for w in range(y.shape[2]):
+            s = int(shift[n, w])
+            if s < T:
+                out[n, :, w, :T - s] = y[n, :, w, s:]
+    return out
+
+
+def from_reduced_time(r: np.ndarray, shift: np.ndarray) -> np.ndarray:
+    """Inverse of to_reduced_time: y[..., w, t] = r[..., w, t - shift[n, w]]
+    for t >= shift, zero before."""
+    out = np.zeros_like(r)
+    T = r.shape[-1]
+    for n in range(r.shape[0]):
+        for w in range(r.shape[2]):
+            s = int(shift[n, w])
+            if s < T:
+                out[n, :, w, s:] = r[n, :, w, :T - s]
+    return out
+
+
 def generate(seeds, device: int = 0, D: int = 128, batch: int = 64, **cfg):
     """FEM shots for `seeds` (config_5; one mesh, each shot its own model and
     source): inputs [n][4][D][W], gathers [n][2][W][T] and the FEM's wall

@@ -306,3 +306,21 @@ def test_trained_surrogate_beats_untrained_on_held_out_fem_shots():
     assert e1 < 0.8 * e0 and e1 < 1.0, (e0, e1)
     # a larger inference batch: the same per-shot arithmetic
     assert _rel(sg.predict(xte, batch=16), pred) < 1e-5
+
+
+def test_reduced_time_round_trip():
+    """The surrogate's reduced-time targets: every sample at or after a
+    trace's moveout comes back exactly; earlier samples (ahead of the first
+    arrival at that speed) are zero."""
+    from seisfem_b200.surrogate import from_reduced_time, moveout_samples, to_reduced_time
+    rng = np.random.default_rng(3)
+    y = rng.standard_normal((4, 2, 6, 50)).astype(np.float32)
+    sh = rng.integers(0, 60, (4, 6))          # shifts past the trace's end included
+    z = from_reduced_time(to_reduced_time(y, sh), sh)
+    for n in range(4):
+        for w in range(6):
+            s = sh[n, w]
+            assert np.array_equal(z[n, :, w, s:], y[n, :, w, s:])
+            assert not z[n, :, w, :s].any()
+    m = moveout_samples([5000, 5001], samples=100, nrec=16)
+    assert m.shape == (2, 16) and (m >= 0).all() and m.max() < 500

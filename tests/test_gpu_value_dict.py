@@ -55,3 +55,68 @@ def test_distinct_elements_keep_full_value_slots(oracle, monkeypatch):
     ref = oracle.run(p)
     for k in ("seis_u", "seis_w"):
         assert rel_l2(out[k], ref[k]) < FP32_TOL, k
+
+
+def _run_shape(p, monkeypatch, shape_a, shape_z, no_tiles=False, morton=False):
+    from seisfem_b200.api import Context
+    monkeypatch.delenv("SFG_NO_VALUE_DICT", raising=False)
+    monkeypatch.setenv("SFG_MORTON", "1" if morton else "0")
+    if no_tiles:
+        monkeypatch.setenv("SFG_NO_TILES", "1")
+    else:
+        monkeypatch.delenv("SFG_NO_TILES", raising=False)
+    monkeypatch.setenv("SFG_SHAPE_A", str(shape_a))
+    monkeypatch.setenv("SFG_SHAPE_Z", str(shape_z))
+    ctx = Context(0)
+    try:
+        ctx.setup(p)
+        out = ctx.run(p, precision="fp32k")
+        out["rows_per_block"] = ctx.stats()["rows_per_block"]
+    finally:
+        ctx.close()
+    return out
+
+
+TILE = 6           # the staged-gather tile kernels' launch shape
+STAGED_SLOTS = 7   # one-shot kernels with their slot streams staged in shared memory
+
+
+@pytest.mark.parametrize("make", [lambda: config_2(n=40, step=402, pml=6),
+                                  lambda: small_problem("Q4", n=48, step=302, pml=6, seed=11),
+                                  lambda: small_problem("T6", n=24, step=102, pml=4, seed=5, dt=2.5e-4)],
+                         ids=["q9_layered", "q4_smooth_model", "t6"])
+@pytest.mark.parametrize("morton", [False, True], ids=["mesh_order", "morton_order"])
+def test_staged_tiles_match_unstaged_kernels_and_oracle(oracle, monkeypatch, make, morton):
+    """The staged-gather tile kernels (halo in shared memory, 4-byte slots)
+    against the unstaged dictionary kernels on the same numbering (mesh order
+    or Morton order inside the classes), and both against the FP64 oracle;
+    also with one class staged and the other not, and with staged slot
+    streams."""
+    p = make()
+    tiles = _run_shape(p, monkeypatch, TILE, TILE, morton=morton)
+    assert tiles["rows_per_block"] == TILE * 16 + TILE
+    plain = _run_shape(p, monkeypatch, 0, 0, morton=morton)
+    mixed = _run_shape(p, monkeypatch, TILE, 0, morton=morton)
+    staged = _run_shape(p, monkeypatch, STAGED_SLOTS, STAGED_SLOTS, morton=morton)
+    ref = oracle.run(p)
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert rel_l2(tiles[k], plain[k]) < 1e-6, (k, rel_l2(tiles[k], plain[k]))
+        assert rel_l2(mixed[k], plain[k]) < 1e-6, (k, rel_l2(mixed[k], plain[k]))
+        # the staged slot streams change nothing in the arithmetic
+        assert np.array_equal(staged[k], plain[k]), (k, rel_l2(staged[k], plain[k]))
+        assert rel_l2(tiles[k], ref[k]) < FP32_TOL, (k, rel_l2(tiles[k], ref[k]))
+
+
+def test_mesh_order_without_tiles_matches(oracle, monkeypatch):
+    """SFG_NO_TILES=1 keeps the mesh order inside the classes (no Morton
+    order, no tiles); a pinned tile shape is then refused."""
+    from seisfem_b200.api import SfgError
+    p = config_2(n=30, step=302, pml=5)
+    a = _run_shape(p, monkeypatch, 0, 0, no_tiles=True)
+    ref = oracle.run(p)
+    b = _run_shape(p, monkeypatch, STAGED_SLOTS, STAGED_SLOTS, no_tiles=True)
+    for k in ("seis_u", "seis_w"):
+        assert rel_l2(a[k], ref[k]) < FP32_TOL, k
+        assert np.array_equal(a[k], b[k]), k
+    with pytest.raises(SfgError):
+        _run_shape(p, monkeypatch, TILE, TILE, no_tiles=True)
