@@ -396,6 +396,7 @@ def run_surrogate(args):
     import torch
     from seisfem_b200.surrogate import (Surrogate, from_reduced_time, generate, moveout_samples, rel_l2,
                                         to_reduced_time)
+    from seisfem_b200.surrogate import hybrid as hybrid_run
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     ntr, nte = args.train_shots, args.test_shots
@@ -459,11 +460,11 @@ def run_surrogate(args):
     fem_rate = 1.0 / float(fem_tr[-1])
     sur_rate = B / (fwd_ms * 1e-3)
     # hybrid pipeline: every shot runs the surrogate; shots over the bound run the FEM too
-    hybrid = nte / (nte / sur_rate + fallback.sum() / fem_rate)
+    hybrid = hybrid_run(err, 1e-2, 1.0 / sur_rate, 1.0 / fem_rate)["shots_per_s"]
     for bound in (1e-2, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5):
-        fb = err > bound
-        hybrid_by_bound.append({"bound": bound, "fallback_fraction": float(fb.mean()),
-                                "hybrid_shots_per_s": nte / (nte / sur_rate + fb.sum() / fem_rate)})
+        h = hybrid_run(err, bound, 1.0 / sur_rate, 1.0 / fem_rate)
+        hybrid_by_bound.append({"bound": bound, "fallback_fraction": h["fallback_fraction"],
+                                "hybrid_shots_per_s": h["shots_per_s"]})
     met = [h["bound"] for h in hybrid_by_bound if h["fallback_fraction"] <= 0.1]
     line = {"metric": "surrogate shots/s", "value": sur_rate, "unit": "shots/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": fwd_ms, "higher_is_better": True,
@@ -666,7 +667,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--infer-batch", type=int, default=64, help="surrogate shots per inference pass")
-    ap.add_argument("--moveout-speed", type=float, default=3000.0,
+    ap.add_argument("--moveout-speed", type=float, default=0.0,
                     help="surrogate: train on traces advanced by their moveout at this speed (m/s); 0 = raw time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -379,9 +379,12 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     // entries reduce to a small value dictionary (meshes of congruent
     // elements), else column + M + K1..K4 (class A) or K1..K6 (class Z).
     // SFG_NO_VALUE_DICT=1 keeps the full-value slots (to compare the two).
-    // The dictionary is found first: with one, the numbering below orders
-    // each class spatially and cuts it into tiles for the staged-gather
-    // kernels (SFG_NO_TILES=1 keeps the mesh order and no tiles).
+    // The dictionary is found first: with one and SFG_MORTON=1, the
+    // numbering below orders each class spatially (Morton order) and cuts it
+    // into tiles for the staged-gather kernels (launch shape kTileShape);
+    // otherwise the classes keep the mesh order in windows of 2048 rows, the
+    // faster numbering for the other one-shot kernels on the structured
+    // meshes measured (SFG_NO_TILES=1 also turns tiles off).
     int *tid = nullptr, zero_id = 0;
     {
         const char *nd = std::getenv("SFG_NO_VALUE_DICT");
@@ -393,9 +396,8 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         ctx->stats.value_tuples = T;
     }
     const char *nt = std::getenv("SFG_NO_TILES"), *mo = std::getenv("SFG_MORTON");
-    const bool tiles = P.dict_n > 0 && !(nt && *nt && *nt != '0');
-    // the spatial (Morton) order inside the classes: SFG_MORTON=1 (with tiles)
-    const bool morton = tiles && mo && *mo == '1';
+    const bool morton = P.dict_n > 0 && mo && *mo == '1' && !(nt && *nt && *nt != '0');
+    const bool tiles = morton;
     // two-class numbering of the fused FP32 step (sfg_step32.cuh): class Z =
     // rows inside the M-PML and every column they reference; class A = the
     // rest.  Inside each class, windows of rows are ordered by (M-PML flag,
@@ -861,10 +863,10 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     std::vector<int> cand;
     if (pl.S == 1) {
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
-        // the staged-gather tile kernels, where the set-up built tiles, and
-        // the staged slot streams, where there is a value dictionary
+        // the staged-gather tile kernels, where the set-up built tiles (the
+        // staged slot streams, kSlotStageShape, measured slower on every
+        // mesh tried: pinned with SFG_SHAPE_A/Z only)
         if (ctx->P.tileA_off && ctx->P.tileZ_off && !b.cmm) cand.push_back(kTileShape);
-        if (ctx->P.dict_n > 0 && !b.cmm) cand.push_back(kSlotStageShape);
     } else {
         for (int spl : {1, 2, 4})
             if (pl.S % (32 * spl) == 0)

@@ -532,6 +532,17 @@ def generate(seeds, device: int = 0, D: int = 128, batch: int = 64, **cfg):
     return xs, np.stack(ys), secs
 
 
+def hybrid(err: np.ndarray, bound: float, sur_seconds_per_shot: float, fem_seconds_per_shot: float) -> dict:
+    """The surrogate with the FEM as its fallback: every shot runs the
+    surrogate, and the shots whose error passes `bound` run the FEM too (an
+    exact error judge: the fraction is the best case of any estimate of the
+    error).  Returns the fallback fraction and shots per second."""
+    fb = np.asarray(err) > bound
+    n = len(fb)
+    t = n * sur_seconds_per_shot + int(fb.sum()) * fem_seconds_per_shot
+    return {"bound": float(bound), "fallback_fraction": float(fb.mean()), "shots_per_s": n / t if t > 0 else 0.0}
+
+
 def rel_l2(pred: np.ndarray, ref: np.ndarray) -> np.ndarray:
     """Per-shot relative L2 error over the whole gather."""
     B = ref.shape[0]

@@ -308,6 +308,39 @@ def test_trained_surrogate_beats_untrained_on_held_out_fem_shots():
     assert _rel(sg.predict(xte, batch=16), pred) < 1e-5
 
 
+@pytest.mark.gpu
+def test_hybrid_beats_the_fem_at_the_error_it_meets():
+    """The surrogate with the FEM as fallback, at a stated error: trained on
+    128 FEM shots (config-5 mesh, 200 samples, reduced time), judged on 32
+    held out.  At the bound the held-out median meets (half the shots fall
+    back) the hybrid's shots/s -- surrogate on every shot, FEM on the
+    fallen-back ones, per-shot times measured here -- is above the FEM's
+    alone; at 1e-2 every shot falls back and the hybrid is slower."""
+    import time
+    import torch
+    from seisfem_b200.surrogate import (Surrogate, from_reduced_time, generate, hybrid, moveout_samples, rel_l2,
+                                        to_reduced_time)
+    cfg = dict(samples=200)
+    xtr, ytr, fem_tr = generate(range(5000, 5128), **cfg)
+    xte, yte, _ = generate(range(9000, 9032), **cfg)
+    sh_tr, sh_te = moveout_samples(range(5000, 5128), **cfg), moveout_samples(range(9000, 9032), **cfg)
+    sg = Surrogate(B=16, T=200, seed=0)
+    sg.fit(xtr, to_reduced_time(ytr, sh_tr), epochs=30, lr=2e-3)
+    sg.predict(xte)                              # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pred = from_reduced_time(sg.predict(xte), sh_te)
+    torch.cuda.synchronize()
+    t_sur = (time.perf_counter() - t0) / len(xte)
+    t_fem = float(fem_tr[-1])
+    err = rel_l2(pred, yte)
+    bound = float(np.median(err))
+    h = hybrid(err, bound, t_sur, t_fem)
+    assert h["fallback_fraction"] <= 0.5 and h["shots_per_s"] > 1.0 / t_fem, (bound, h, 1.0 / t_fem)
+    h1 = hybrid(err, 1e-2, t_sur, t_fem)
+    assert h1["fallback_fraction"] == 1.0 and h1["shots_per_s"] < 1.0 / t_fem
+
+
 def test_reduced_time_round_trip():
     """The surrogate's reduced-time targets: every sample at or after a
     trace's moveout comes back exactly; earlier samples (ahead of the first

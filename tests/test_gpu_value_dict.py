@@ -85,14 +85,14 @@ STAGED_SLOTS = 7   # one-shot kernels with their slot streams staged in shared m
                                   lambda: small_problem("Q4", n=48, step=302, pml=6, seed=11),
                                   lambda: small_problem("T6", n=24, step=102, pml=4, seed=5, dt=2.5e-4)],
                          ids=["q9_layered", "q4_smooth_model", "t6"])
-@pytest.mark.parametrize("morton", [False, True], ids=["mesh_order", "morton_order"])
-def test_staged_tiles_match_unstaged_kernels_and_oracle(oracle, monkeypatch, make, morton):
-    """The staged-gather tile kernels (halo in shared memory, 4-byte slots)
-    against the unstaged dictionary kernels on the same numbering (mesh order
-    or Morton order inside the classes), and both against the FP64 oracle;
-    also with one class staged and the other not, and with staged slot
-    streams."""
+def test_staged_tiles_match_unstaged_kernels_and_oracle(oracle, monkeypatch, make):
+    """The staged-gather tile kernels (halo in shared memory, 4-byte slots;
+    Morton order inside the classes, SFG_MORTON=1) against the unstaged
+    dictionary kernels on the same numbering, and both against the FP64
+    oracle; also with one class staged and the other not, and with staged
+    slot streams."""
     p = make()
+    morton = True
     tiles = _run_shape(p, monkeypatch, TILE, TILE, morton=morton)
     assert tiles["rows_per_block"] == TILE * 16 + TILE
     plain = _run_shape(p, monkeypatch, 0, 0, morton=morton)
@@ -108,8 +108,9 @@ def test_staged_tiles_match_unstaged_kernels_and_oracle(oracle, monkeypatch, mak
 
 
 def test_mesh_order_without_tiles_matches(oracle, monkeypatch):
-    """SFG_NO_TILES=1 keeps the mesh order inside the classes (no Morton
-    order, no tiles); a pinned tile shape is then refused."""
+    """Without SFG_MORTON=1 (here also SFG_NO_TILES=1) the classes keep the
+    mesh order and no tiles are built: the staged slot streams still work,
+    bit for bit, and a pinned tile shape is refused."""
     from seisfem_b200.api import SfgError
     p = config_2(n=30, step=302, pml=5)
     a = _run_shape(p, monkeypatch, 0, 0, no_tiles=True)
