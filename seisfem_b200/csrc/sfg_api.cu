@@ -761,9 +761,10 @@ int alloc_bufs(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, int ns
     b.gbytes = (size_t)N * GREC * S * esz;
     b.pbytes = (size_t)N * PREC * S * esz;
     const int na = ctx->P.na, nz = N - na;
-    b.gc_bytes = (size_t)N * GC * S * sizeof(float);
+    // Gc, Gs, Ps hold whole blocks of 32 rows (the one-shot block layout)
+    b.gc_bytes = (size_t)blk_rows(N) * GC * S * sizeof(float);
     b.pa_bytes = (size_t)std::max(na, 1) * PA * S * sizeof(float);
-    b.gs_bytes = (size_t)std::max(nz, 1) * GS * S * sizeof(float);
+    b.gs_bytes = (size_t)blk_rows(std::max(nz, 1)) * GS * S * sizeof(float);
     cudaStream_t st = ctx->stream;
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         CK(palloc(ctx, &b.pst, sizeof(float) * 36 * (size_t)N));

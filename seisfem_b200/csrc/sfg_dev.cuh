@@ -5,6 +5,14 @@
 
 namespace sfg {
 
+// Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch, sm_90+):
+// one instruction puts a whole contiguous stream in flight without holding
+// registers.  p 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+    if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Block-wide sum of (a, b) into dst[0], dst[1] (one atomic pair per block).
 __device__ __forceinline__ void block_energy(double *dst, double a, double b)
 {

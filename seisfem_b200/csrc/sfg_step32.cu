@@ -197,19 +197,26 @@ __device__ __forceinline__ bool is_pml_row(float4 c1)
 
 // Displacement of permuted row `node` of shot `s` in a finished state:
 // class A: hi + lo of the totals; class Z: sum of the split pairs (FP64).
+// Value k of row r's 12-float record in a state array: the one-shot block
+// layout (blk4) when S = 1, else [row][value][S].
+__device__ __forceinline__ double rec_val(const float *base, long long r, int k, int S, int s)
+{
+    return (double)(S == 1 ? base[4 * blk4(r, k >> 2, 3) + (k & 3)] : base[(r * 12 + k) * S + s]);
+}
+
 __device__ __forceinline__ void total_uw(const State32 &st, int na, int S, long long node, int s, double &u, double &w)
 {
     if (node < na) {
-        u = (double)st.Gc[(node * GC + 0) * S + s] + (double)st.Gc[(node * GC + 10) * S + s];
-        w = (double)st.Gc[(node * GC + 1) * S + s] + (double)st.Gc[(node * GC + 11) * S + s];
+        u = rec_val(st.Gc, node, 0, S, s) + rec_val(st.Gc, node, 10, S, s);
+        w = rec_val(st.Gc, node, 1, S, s) + rec_val(st.Gc, node, 11, S, s);
     } else {
         const long long z = node - na;
         u = 0.0;
         w = 0.0;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            u += (double)st.Gs[(z * GS + k) * S + s] + (double)st.Ps[(z * PS + 6 + k) * S + s];
-            w += (double)st.Gs[(z * GS + 3 + k) * S + s] + (double)st.Ps[(z * PS + 9 + k) * S + s];
+            u += rec_val(st.Gs, z, k, S, s) + rec_val(st.Ps, z, 6 + k, S, s);
+            w += rec_val(st.Gs, z, 3 + k, S, s) + rec_val(st.Ps, z, 9 + k, S, s);
         }
     }
 }
@@ -282,15 +289,27 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
 #pragma unroll
         for (int k = 0; k < 8; k++) mL[k] = 0.f;
         const int s0 = __ldg(a.sliceA + slice), s1 = __ldg(a.sliceA + slice + 1);
+        if (DICT && !STG && lane == 0) {
+            // the slice's slot rows and the private streams of its rows (read
+            // once, after the gathers) into L2 ahead of use: the whole slice
+            // is in flight at once instead of the two slot rows the registers
+            // hold
+            const int r0 = slice * 32, nr = min(32, a.na - r0);
+            prefetch_l2(a.sellAd + (size_t)s0 * 32, (unsigned)(s1 - s0) * 256u);
+            prefetch_l2(reinterpret_cast<const float4 *>(a.in.Pa) + r0, 16u * nr);
+            prefetch_l2(a.coefA + r0, 16u * nr);
+            prefetch_l2(a.imA + r0, (4u * nr) & ~15u);
+            prefetch_l2(a.rowrho + r0, (4u * nr) & ~15u);
+        }
         // own displacements (hi, lo): every row of K1..K6 sums to zero, so
         // K U = sum_j K_ij (U_j - U_i), and the differences of the hi and lo
         // parts keep the products free of the cancellation that FP32 sums
         // of K_ij U_j suffer on smooth fields
-        const float4 *gi = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
-        const float4 own0 = __ldg(gi), own2 = __ldg(gi + 2);
+        const float4 *G4 = reinterpret_cast<const float4 *>(a.in.Gc);
+        const float4 own0 = __ldg(G4 + blk4(i, 0, 3)), own2 = __ldg(G4 + blk4(i, 2, 3));
         auto acc = [&](int j, float vm, const float *kv) {
-            const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+            const float4 *gj = G4 + blk4(j, 0, 3);
+            const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
             const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
             for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
@@ -329,7 +348,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
             src_w = ps * c.cos_af;
         }
         float g[GC], p[PA];
-        const float4 own1 = __ldg(gi + 1);
+        const float4 own1 = __ldg(G4 + blk4(i, 1, 3));
         g[0] = own0.x; g[1] = own0.y; g[2] = own0.z; g[3] = own0.w;
         g[4] = own1.x; g[5] = own1.y; g[6] = own1.z; g[7] = own1.w;
         g[8] = own2.x; g[9] = own2.y; g[10] = own2.z; g[11] = own2.w;
@@ -338,9 +357,9 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
         float uu, ww, su, sw;
         stiff_sums(kU, kW, cf, su, sw);
         finish_A<COMP>(su, sw, mL, im, c.dt, src_u, src_w, g, p, uu, ww);
-        float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+        float4 *go = reinterpret_cast<float4 *>(a.out.Gc) + blk4(i, 0, 3);
 #pragma unroll
-        for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+        for (int k = 0; k < 3; k++) go[32 * k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
         reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
         eu = (double)uu * uu;
         ew = (double)ww * ww;
@@ -367,8 +386,8 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
     const int i = a.na + local;
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
     if (local < nz) {
-        const float4 *cf = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
-        c0 = __ldcs(cf); c1 = __ldcs(cf + 1); c2 = __ldcs(cf + 2);
+        const float4 *cf = reinterpret_cast<const float4 *>(a.coefZ) + blk4(local, 0, 3);
+        c0 = __ldcs(cf); c1 = __ldcs(cf + 32); c2 = __ldcs(cf + 64);
     }
     const bool full = __any_sync(0xffffffffu, local < nz && is_pml_row(c1));
     double eu = 0.0, ew = 0.0;
@@ -380,9 +399,17 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
 #pragma unroll
         for (int k = 0; k < 20; k++) m[k] = 0.f;
         const int s0 = __ldg(a.sliceZ + slice), s1 = __ldg(a.sliceZ + slice + 1);
+        if (DICT && !STG && lane == 0) {
+            // the slice's slot rows and its rows' private records into L2
+            const int r0 = slice * 32;
+            prefetch_l2(a.sellZd + (size_t)s0 * 32, (unsigned)(s1 - s0) * 256u);
+            prefetch_l2(reinterpret_cast<const float4 *>(a.in.Ps) + blk4(r0, 0, 3), 1536u);
+            prefetch_l2(reinterpret_cast<const float4 *>(a.in.Gs) + blk4(r0, 0, 3), 1536u);
+        }
         // own totals (hi, lo) for the stiffness products in difference form
-        const float4 *gci = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)i * GC);
-        const float4 own0 = __ldg(gci), own2 = __ldg(gci + 2);
+        const float4 *G4 = reinterpret_cast<const float4 *>(a.in.Gc);
+        const float4 *S4 = reinterpret_cast<const float4 *>(a.in.Gs);
+        const float4 own0 = __ldg(G4 + blk4(i, 0, 3)), own2 = __ldg(G4 + blk4(i, 2, 3));
         const float *sd = DICT ? nullptr : a.sellZ + (size_t)s0 * 256 + lane;
         DictSlots ss;
         if (DICT && !STG) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
@@ -409,16 +436,16 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
                 int j;
                 float vm, kv[6];
                 slot(j, vm, kv, 6);
-                const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+                const float4 *gj = G4 + blk4(j, 0, 3);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
                 const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
                 // split fields exist for class-Z columns; rows outside the
                 // M-PML that share the warp see zeros for class-A columns (their
                 // damping coefficients are zero, so those products are unused)
                 float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0, z2 = z0;
                 if (j >= a.na) {
-                    const float4 *sj = reinterpret_cast<const float4 *>(a.in.Gs + (size_t)(j - a.na) * GS);
-                    z0 = __ldg(sj); z1 = __ldg(sj + 1); z2 = __ldg(sj + 2);
+                    const float4 *sj = S4 + blk4(j - a.na, 0, 3);
+                    z0 = __ldg(sj); z1 = __ldg(sj + 32); z2 = __ldg(sj + 64);
                 }
 #pragma unroll
                 for (int k = 0; k < 6; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
@@ -434,8 +461,8 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
                 int j;
                 float vm, kv[4];
                 slot(j, vm, kv, 4);
-                const float4 *gj = reinterpret_cast<const float4 *>(a.in.Gc + (size_t)j * GC);
-                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 1), q2 = __ldg(gj + 2);
+                const float4 *gj = G4 + blk4(j, 0, 3);
+                const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
                 const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
                 for (int k = 0; k < 4; k++) { kU[k] += kv[k] * du; kW[k] += kv[k] * dw; }
@@ -455,24 +482,24 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
             src_w = ps * c.cos_af;
         }
         float gs[GS], ps_[PS], gc[GC];
-        const float4 *si = reinterpret_cast<const float4 *>(a.in.Gs + (size_t)local * GS);
-        const float4 *pi = reinterpret_cast<const float4 *>(a.in.Ps + (size_t)local * PS);
+        const float4 *si = S4 + blk4(local, 0, 3);
+        const float4 *pi = reinterpret_cast<const float4 *>(a.in.Ps) + blk4(local, 0, 3);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const float4 v = __ldg(si + k), w = __ldcs(pi + k);
+            const float4 v = __ldg(si + 32 * k), w = __ldcs(pi + 32 * k);
             gs[4 * k] = v.x; gs[4 * k + 1] = v.y; gs[4 * k + 2] = v.z; gs[4 * k + 3] = v.w;
             ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
         }
         float uu, ww;
         finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, uu, ww);
-        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
-        float4 *so = reinterpret_cast<float4 *>(a.out.Gs + (size_t)local * GS);
-        float4 *po = reinterpret_cast<float4 *>(a.out.Ps + (size_t)local * PS);
+        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc) + blk4(i, 0, 3);
+        float4 *so = reinterpret_cast<float4 *>(a.out.Gs) + blk4(local, 0, 3);
+        float4 *po = reinterpret_cast<float4 *>(a.out.Ps) + blk4(local, 0, 3);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            gco[k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
-            so[k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
-            po[k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
+            gco[32 * k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
+            so[32 * k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
+            po[32 * k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
         }
         eu = (double)uu * uu;
         ew = (double)ww * ww;
@@ -1026,8 +1053,8 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
     for (long long task = warp; task < tasks; task += warps_total) {
         const int local = (int)(task / nch);
         const int i = a.na + local;
-        const float4 *cfp = reinterpret_cast<const float4 *>(a.coefZ) + (size_t)local * 3;
-        const float4 c0 = __ldg(cfp), c1 = __ldg(cfp + 1), c2 = __ldg(cfp + 2);
+        const float4 *cfp = reinterpret_cast<const float4 *>(a.coefZ) + blk4(local, 0, 3);
+        const float4 c0 = __ldg(cfp), c1 = __ldg(cfp + 32), c2 = __ldg(cfp + 64);
         float kU[6][SPL], kW[6][SPL], m[20][SPL];
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
@@ -1105,17 +1132,19 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
 // columns are distinct.
 
 // Copies the 48-byte records rows[k] (k < nr: row w0 + k; else ext[k - nr])
-// of `base` into planes P, P + H, P + 2H of shared memory.
+// of `base` (one-shot block layout, blk4) into planes P, P + H, P + 2H of
+// shared memory.
 __device__ __forceinline__ void tile_stage(const float *__restrict__ base, int w0, int nr,
                                            const int *__restrict__ ext, int ne, float4 *P, int H)
 {
     const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(P);
+    const float4 *b4 = reinterpret_cast<const float4 *>(base);
     for (int k = threadIdx.x; k < nr + ne; k += blockDim.x) {
         const int g = k < nr ? w0 + k : __ldg(ext + k - nr);
-        const float *src = base + (size_t)g * 12;
+        const float4 *src = b4 + blk4(g, 0, 3);
         cp_async16(s0 + 16u * (uint32_t)k, src);
-        cp_async16(s0 + 16u * (uint32_t)(H + k), src + 4);
-        cp_async16(s0 + 16u * (uint32_t)(2 * H + k), src + 8);
+        cp_async16(s0 + 16u * (uint32_t)(H + k), src + 32);
+        cp_async16(s0 + 16u * (uint32_t)(2 * H + k), src + 64);
     }
 }
 
@@ -1204,9 +1233,9 @@ __global__ void __launch_bounds__(kTileRows, 3) stepAT_kernel(const Step2 a)
         float uu, ww, su, sw;
         stiff_sums(kU, kW, cf, su, sw);
         finish_A<COMP>(su, sw, mL, im, c.dt, src_u, src_w, g, p, uu, ww);
-        float4 *go = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
+        float4 *go = reinterpret_cast<float4 *>(a.out.Gc) + blk4(i, 0, 3);
 #pragma unroll
-        for (int k = 0; k < 3; k++) go[k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+        for (int k = 0; k < 3; k++) go[32 * k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
         reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
         eu = (double)uu * uu;
         ew = (double)ww * ww;
@@ -1242,8 +1271,10 @@ __global__ void __launch_bounds__(kTileRows, 2) stepZT_kernel(const Step2 a)
     const int lb = t * kTileRows;                                  // the tile's first class-Z row
     const int slb = __ldg(a.sliceZ + lb / 32), sle = __ldg(a.sliceZ + (lb + nr + 31) / 32);
     tile_copy(SL, reinterpret_cast<const float4 *>(a.sellZt) + (size_t)slb * 8, (sle - slb) * 8);
-    tile_copy(PSs, reinterpret_cast<const float4 *>(a.in.Ps) + (size_t)lb * 3, 3 * nr);
-    tile_copy(CFs, reinterpret_cast<const float4 *>(a.coefZ) + (size_t)lb * 3, 3 * nr);
+    // the tile's Ps records and coefficients: whole blocks of the block
+    // layout (lb is a multiple of 32), read back with blk4(tx, k, 3)
+    tile_copy(PSs, reinterpret_cast<const float4 *>(a.in.Ps) + (size_t)lb * 3, 3 * (int)blk_rows(nr));
+    tile_copy(CFs, reinterpret_cast<const float4 *>(a.coefZ) + (size_t)lb * 3, 3 * (int)blk_rows(nr));
     const float rho = tx < nr ? __ldcs(a.rowrho + i) : 0.f;
     tile_stage(a.in.Gc, w0, nr, ext, ne, tsm, H);
     {
@@ -1253,10 +1284,10 @@ __global__ void __launch_bounds__(kTileRows, 2) stepZT_kernel(const Step2 a)
         for (int k = tx; k < nr + ne; k += kTileRows) {
             const int g = k < nr ? w0 + k : __ldg(ext + k - nr);
             if (g >= a.na) {
-                const float *src = a.in.Gs + (size_t)(g - a.na) * GS;
+                const float4 *src = reinterpret_cast<const float4 *>(a.in.Gs) + blk4(g - a.na, 0, 3);
                 cp_async16(q0 + 16u * (uint32_t)k, src);
-                cp_async16(q0 + 16u * (uint32_t)(H + k), src + 4);
-                cp_async16(q0 + 16u * (uint32_t)(2 * H + k), src + 8);
+                cp_async16(q0 + 16u * (uint32_t)(H + k), src + 32);
+                cp_async16(q0 + 16u * (uint32_t)(2 * H + k), src + 64);
             } else {
                 const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
                 Q[k] = z;
@@ -1269,7 +1300,7 @@ __global__ void __launch_bounds__(kTileRows, 2) stepZT_kernel(const Step2 a)
     __syncthreads();
     float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, c2 = c0;
     if (tx < nr) {
-        c0 = CFs[3 * tx]; c1 = CFs[3 * tx + 1]; c2 = CFs[3 * tx + 2];
+        c0 = CFs[blk4(tx, 0, 3)]; c1 = CFs[blk4(tx, 1, 3)]; c2 = CFs[blk4(tx, 2, 3)];
     }
     const bool full = __any_sync(0xffffffffu, tx < nr && is_pml_row(c1));
     double eu = 0.0, ew = 0.0;
@@ -1330,20 +1361,20 @@ __global__ void __launch_bounds__(kTileRows, 2) stepZT_kernel(const Step2 a)
         const float4 sq[3] = {Q0[tx], Q1[tx], Q2[tx]};
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const float4 w = PSs[3 * tx + k];
+            const float4 w = PSs[blk4(tx, k, 3)];
             gs[4 * k] = sq[k].x; gs[4 * k + 1] = sq[k].y; gs[4 * k + 2] = sq[k].z; gs[4 * k + 3] = sq[k].w;
             ps_[4 * k] = w.x; ps_[4 * k + 1] = w.y; ps_[4 * k + 2] = w.z; ps_[4 * k + 3] = w.w;
         }
         float uu, ww;
         finish_Z<COMP>(kU, kW, m, c0, c1, c2, c.dt, src_u, src_w, gs, ps_, gc, uu, ww);
-        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc + (size_t)i * GC);
-        float4 *so = reinterpret_cast<float4 *>(a.out.Gs + (size_t)local * GS);
-        float4 *po = reinterpret_cast<float4 *>(a.out.Ps + (size_t)local * PS);
+        float4 *gco = reinterpret_cast<float4 *>(a.out.Gc) + blk4(i, 0, 3);
+        float4 *so = reinterpret_cast<float4 *>(a.out.Gs) + blk4(local, 0, 3);
+        float4 *po = reinterpret_cast<float4 *>(a.out.Ps) + blk4(local, 0, 3);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            gco[k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
-            so[k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
-            po[k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
+            gco[32 * k] = make_float4(gc[4 * k], gc[4 * k + 1], gc[4 * k + 2], gc[4 * k + 3]);
+            so[32 * k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
+            po[32 * k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
         }
         eu = (double)uu * uu;
         ew = (double)ww * ww;
@@ -1514,8 +1545,8 @@ __global__ void coef2_kernel(int n, int na, const float *__restrict__ coef, cons
         coefA[r] = make_float4(src[0], src[1], src[2], src[3]);
         imA[r] = src[8];
     } else {
-        float *d = coefZ + (size_t)(r - na) * CREC;
-        for (int k = 0; k < CREC; k++) d[k] = src[k];
+        // the block layout of the one-shot records (blk4), 12 floats per row
+        for (int k = 0; k < CREC; k++) coefZ[4 * blk4(r - na, k >> 2, 3) + (k & 3)] = src[k];
     }
 }
 
@@ -2013,7 +2044,10 @@ cudaError_t build_coef2(int n, int na, const float *d_coef32, const int *d_perm,
     cudaError_t e;
     if ((e = keep_alloc(d_coefA, sizeof(float4) * std::max(na, 1), st)) != cudaSuccess) return e;
     if ((e = keep_alloc(d_imA, sizeof(float) * std::max(na, 1), st)) != cudaSuccess) return e;
-    if ((e = keep_alloc(d_coefZ, sizeof(float) * CREC * std::max(n - na, 1), st)) != cudaSuccess) return e;
+    if ((e = keep_alloc(d_coefZ, sizeof(float) * CREC * blk_rows(std::max(n - na, 1)), st)) != cudaSuccess) return e;
+    // rows past the last class-Z row of the last block stay zero
+    if ((e = cudaMemsetAsync(*d_coefZ, 0, sizeof(float) * CREC * blk_rows(std::max(n - na, 1)), st)) != cudaSuccess)
+        return e;
     if (n) coef2_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, na, d_coef32, d_perm, *d_coefA, *d_imA, *d_coefZ);
     return cudaGetLastError();
 }

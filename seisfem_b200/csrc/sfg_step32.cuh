@@ -37,6 +37,20 @@ namespace sfg {
 
 constexpr int GC = 12, PA = 4, GS = 12, PS = 12;
 
+// One-shot layout (S = 1) of the 48-byte records Gc, Gs, Ps and the class-Z
+// coefficients: rows in blocks of 32, block b holding float4 q of its rows
+// 32 b .. 32 b + 31 contiguously (q = 0 .. nq - 1).  The 32 rows of a SELL
+// slice gather neighbours that are mostly consecutive rows, so one float4
+// load of the warp touches 4-5 128-byte lines instead of the 12 of records
+// laid end to end.  Arrays in this layout hold whole blocks (rows rounded up
+// to 32).  Batches (S > 1) keep [row][value][S].
+__host__ __device__ __forceinline__ long long blk4(long long r, int q, int nq)
+{
+    return (((r >> 5) * nq + q) << 5) | (r & 31);
+}
+// rows rounded up to whole blocks of 32
+__host__ __device__ __forceinline__ long long blk_rows(long long n) { return (n + 31) & ~31LL; }
+
 struct State32 {
     const float *Gc, *Pa, *Gs, *Ps;
 };
