@@ -203,8 +203,9 @@ __global__ void dict_ids(long long nnz, const DictScratch *s, const int *__restr
 }
 
 // SELL slots of rows [r0, r1) (slice pointers sp as build_sell_range): the
-// permuted column and the tuple id; padding slots point at the row itself
-// with the zero tuple
+// float4 index blk4(column, 0, 3) of the permuted column's state record and
+// twice the tuple id (the tuple's first float4 in the kernels' table);
+// padding slots point at the row itself with the zero tuple
 __global__ void range_sell_fill_dict(int r0, int r1, const int *__restrict__ up, const int *__restrict__ uj,
                                      const int *__restrict__ tid, int zero_id, const int *__restrict__ sp,
                                      const int *__restrict__ perm, const int *__restrict__ inv, int2 *__restrict__ sell)
@@ -216,8 +217,8 @@ __global__ void range_sell_fill_dict(int r0, int r1, const int *__restrict__ up,
     const int a0 = r < n ? up[o] : 0, len = r < n ? up[o + 1] - a0 : 0;
     for (int k = 0; k < s1 - s0; k++) {
         int2 v;
-        if (k < len) v = make_int2(inv[uj[a0 + k]], tid[a0 + k]);
-        else v = make_int2(r < n ? r0 + r : r0, zero_id);
+        if (k < len) v = make_int2((int)blk4(inv[uj[a0 + k]], 0, 3), 2 * tid[a0 + k]);
+        else v = make_int2((int)blk4(r < n ? r0 + r : r0, 0, 3), 2 * zero_id);
         sell[(size_t)(s0 + k) * 32 + lane] = v;
     }
 }

@@ -307,8 +307,9 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
         // of K_ij U_j suffer on smooth fields
         const float4 *G4 = reinterpret_cast<const float4 *>(a.in.Gc);
         const float4 own0 = __ldg(G4 + blk4(i, 0, 3)), own2 = __ldg(G4 + blk4(i, 2, 3));
-        auto acc = [&](int j, float vm, const float *kv) {
-            const float4 *gj = G4 + blk4(j, 0, 3);
+        // jq: the float4 index blk4(j, 0, 3) of neighbour j's record
+        auto acc = [&](int jq, float vm, const float *kv) {
+            const float4 *gj = G4 + jq;
             const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
             const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
@@ -322,7 +323,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
 #pragma unroll 2
             for (int g = s0; g < s1; ++g) {
                 const int2 cv = STG ? stg[(g - slb) * 32 + lane] : ss.next();
-                const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
+                const float4 t0 = stab[cv.y], t1 = stab[cv.y + 1];
                 const float kv[4] = {t0.y, t0.z, t0.w, t1.x};
                 acc(cv.x, t0.x, kv);
             }
@@ -336,7 +337,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
                 float kv[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++) kv[k] = ldgf(sd + 64 + 32 * k);
-                acc(__float_as_int(ldgf(sd)), ldgf(sd + 32), kv);
+                acc((int)blk4(__float_as_int(ldgf(sd)), 0, 3), ldgf(sd + 32), kv);
             }
         }
         const float4 cf = __ldcs(a.coefA + i);
@@ -414,17 +415,20 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
         DictSlots ss;
         if (DICT && !STG) ss.init(a.sellZd + (size_t)s0 * 32 + lane, s1 - s0);
         int gs_next = s0 - slb;   // staged slots: the next slot row in shared memory
-        // slot g's column, M and K1..K(NK): from the dictionary or the full-value planes
+        // slot g's record index jq = blk4(column, 0, 3), M and K1..K(NK): from
+        // the dictionary or the full-value planes.  With na a multiple of 32,
+        // a class-Z column's split-field record is Gs float4 jq - 3 na.
+        const int zq = 3 * a.na;
         auto slot = [&](int &j, float &vm, float *kv, int nk) {
             if (DICT) {
                 const int2 cv = STG ? stg[(gs_next++) * 32 + lane] : ss.next();
-                const float4 t0 = stab[2 * cv.y], t1 = stab[2 * cv.y + 1];
+                const float4 t0 = stab[cv.y], t1 = stab[cv.y + 1];
                 j = cv.x;
                 vm = t0.x;
                 kv[0] = t0.y; kv[1] = t0.z; kv[2] = t0.w; kv[3] = t1.x;
                 if (nk == 6) { kv[4] = t1.y; kv[5] = t1.z; }
             } else {
-                j = __float_as_int(ldgf(sd));
+                j = (int)blk4(__float_as_int(ldgf(sd)), 0, 3);
                 vm = ldgf(sd + 32);
                 for (int k = 0; k < nk; k++) kv[k] = ldgf(sd + 64 + 32 * k);
                 sd += 256;
@@ -436,15 +440,15 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
                 int j;
                 float vm, kv[6];
                 slot(j, vm, kv, 6);
-                const float4 *gj = G4 + blk4(j, 0, 3);
+                const float4 *gj = G4 + j;
                 const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
                 const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
                 // split fields exist for class-Z columns; rows outside the
                 // M-PML that share the warp see zeros for class-A columns (their
                 // damping coefficients are zero, so those products are unused)
                 float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0, z2 = z0;
-                if (j >= a.na) {
-                    const float4 *sj = S4 + blk4(j - a.na, 0, 3);
+                if (j >= zq) {
+                    const float4 *sj = S4 + (j - zq);
                     z0 = __ldg(sj); z1 = __ldg(sj + 32); z2 = __ldg(sj + 64);
                 }
 #pragma unroll
@@ -461,7 +465,7 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
                 int j;
                 float vm, kv[4];
                 slot(j, vm, kv, 4);
-                const float4 *gj = G4 + blk4(j, 0, 3);
+                const float4 *gj = G4 + j;
                 const float4 q0 = __ldg(gj), q1 = __ldg(gj + 32), q2 = __ldg(gj + 64);
                 const float du = (q0.x - own0.x) + (q2.z - own2.z), dw = (q0.y - own0.y) + (q2.w - own2.w);
 #pragma unroll
@@ -1585,6 +1589,15 @@ __global__ void class_split(int n, const unsigned char *__restrict__ zone, int *
     isZ[r] = zone[r] ? 1 : 0;
 }
 
+// the last `k` class-A rows (mesh order) join class Z, so that the class-A
+// row count is a multiple of 32 (posA: exclusive scan of the class-A flags)
+__global__ void class_align(int n, int k, const int *__restrict__ posA, unsigned char *__restrict__ zone)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n || zone[r]) return;
+    if (posA[r] >= posA[n] - k) zone[r] = 1;
+}
+
 // class A rows first, then class Z, each in mesh order
 __global__ void class_scatter(int n, const unsigned char *__restrict__ zone, const int *__restrict__ posA,
                               const int *__restrict__ posZ, int *__restrict__ perm0)
@@ -1708,11 +1721,15 @@ cudaError_t launch_range_slice_len(int r0, int r1, const int *d_up, const int *d
     return cudaGetLastError();
 }
 
-#define SFG_SHAPES(KERNEL, COUNT)                                                              \
+// (threads per block, minimum resident blocks) of the one-shot launch
+// shapes; shape 0 of the class-A kernel asks for 7 resident blocks of 128
+// threads (72 registers, 28 warps per SM), of the class-Z kernel for 4
+// (128 registers: its 32 products per M-PML slot stay in registers)
+#define SFG_SHAPES(KERNEL, COUNT, MINB0)                                                       \
     do {                                                                                       \
         if ((COUNT) <= 0) return cudaSuccess;                                                  \
         switch (variant) {                                                                     \
-        case 0: SFG_ONE(KERNEL, 128, 4, COUNT); break;                                         \
+        case 0: SFG_ONE(KERNEL, 128, MINB0, COUNT); break;                                     \
         case 1: SFG_ONE(KERNEL, 128, 6, COUNT); break;                                         \
         case 2: SFG_ONE(KERNEL, 256, 3, COUNT); break;                                         \
         case 4: SFG_ONE(KERNEL, 64, 16, COUNT); break;                                         \
@@ -1827,7 +1844,7 @@ cudaError_t launch_stepA(const Step2 &a, bool comp, int variant, cudaStream_t st
     if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
         return cudaErrorInvalidValue;
     // the fused receiver gather runs on the first nrec threads
-    SFG_SHAPES(stepA_kernel, std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0));
+    SFG_SHAPES(stepA_kernel, std::max(a.na, a.c.seis_row >= 0 ? a.c.nrec : 0), 7);
     return cudaGetLastError();
 }
 
@@ -1837,7 +1854,7 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
     if (variant == kSlotStageShape) return launch_stg(a, comp, false, st);
     if (a.dict_n > kDictMax || (a.dict_n > 0 && (!a.dict || !a.sellAd || !a.sellZd || !a.rowrho)))
         return cudaErrorInvalidValue;
-    SFG_SHAPES(stepZ_kernel, a.c.n - a.na);
+    SFG_SHAPES(stepZ_kernel, a.c.n - a.na, 4);
     return cudaGetLastError();
 }
 #undef SFG_ONE
@@ -1869,7 +1886,7 @@ cudaError_t launch_stepA_multi(const Step2 *descs, const int2 *map, int nblocks,
                                int variant, int it, cudaStream_t st)
 {
     if (dict_max > kDictMax || (dict && dict_max <= 0)) return cudaErrorInvalidValue;
-    SFG_SHAPES(stepA_multi, nblocks);
+    SFG_SHAPES(stepA_multi, nblocks, 7);
     return cudaGetLastError();
 }
 
@@ -1877,7 +1894,7 @@ cudaError_t launch_stepZ_multi(const Step2 *descs, const int2 *map, int nblocks,
                                int variant, int it, cudaStream_t st)
 {
     if (dict_max > kDictMax || (dict && dict_max <= 0)) return cudaErrorInvalidValue;
-    SFG_SHAPES(stepZ_multi, nblocks);
+    SFG_SHAPES(stepZ_multi, nblocks, 4);
     return cudaGetLastError();
 }
 #undef SFG_ONE
@@ -2116,6 +2133,19 @@ cudaError_t build_classes(int n, const int *d_up, const int *d_uj, const double 
         class_zone<<<g, 256, 0, st>>>(n, d_up, d_uj, pml, zone);
         class_split<<<g, 256, 0, st>>>(n, zone, isA, isZ);
         e = cudaGetLastError();
+        // a class-A row count that is a multiple of 32: the one-shot state
+        // blocks of the two classes then line up (blk4(i - na) = blk4(i) -
+        // 3 na), and the last few class-A rows carry split fields instead,
+        // which the class-Z step handles like any row outside the M-PML
+        int na0 = 0;
+        if (e == cudaSuccess) e = exclusive_scan_int(isA, posA, n, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&na0, posA + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && na0 % 32) {
+            class_align<<<g, 256, 0, st>>>(n, na0 % 32, posA, zone);
+            class_split<<<g, 256, 0, st>>>(n, zone, isA, isZ);
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess) e = exclusive_scan_int(isA, posA, n, st);
         if (e == cudaSuccess) e = exclusive_scan_int(isZ, posZ, n, st);
         if (e == cudaSuccess) {

@@ -10,9 +10,10 @@
 //      fields, so they carry only the totals U = U1+U2+U3, W = W1+W2+W3 (the
 //      Newmark update, elastic_wave.c:757-768, is linear: the totals follow
 //      the same recursion with the summed accelerations).
-// Numbering: rows [0, na) are class A, rows [na, n) class Z; inside each
-// class, windows of 2048 rows are sorted by (M-PML flag, row length) so that
-// 32-row SELL slices need no padding.  perm[r'] is the mesh node of row r'.
+// Numbering: rows [0, na) are class A, rows [na, n) class Z, na a multiple
+// of 32 (the last few rows of A join Z); inside each class, windows of 2048
+// rows are sorted by (M-PML flag, row length) so that 32-row SELL slices need
+// no padding.  perm[r'] is the mesh node of row r'.
 //
 // State records (node-major, shot index innermost for batches of S shots):
 //   Gc[n][12]   gathered by every row: U W Lx1 Lx2 | Lx3 Lx4 Ly1 Ly2 | Ly3 Ly4
@@ -67,9 +68,10 @@ struct Step2 {
     const float *sellZ;        // SELL-32 over rows [na, n): planes col, M, K1..K6
     const int *sliceZ;
     // value dictionary (sfg_dict.cu; dict_n = 0 without one): the one-shot
-    // kernels then read SELL-32 slots (column, tuple id) from sellAd / sellZd
-    // (same slices as sellA / sellZ), the tuple (M / rho_row, K1..K6) from
-    // dict[2 id], dict[2 id + 1], and scale the mass products by rowrho
+    // kernels then read SELL-32 slots (q, d) from sellAd / sellZd (same
+    // slices as sellA / sellZ): q = blk4(column, 0, 3), the float4 index of
+    // the column's Gc record, and d = 2 id, the tuple (M / rho_row, K1..K6)
+    // being dict[d], dict[d + 1]; the mass products are scaled by rowrho
     const int2 *sellAd;
     const int2 *sellZd;
     const float4 *dict;
