@@ -51,8 +51,10 @@ cudaMemPool_t device_pool(int device)
 
 struct RunCache {
     // launch shapes picked by the autotuner (stored + 1; 0 = not tuned):
-    // [shots: 1, 32, 64, 128][plain FP32, compensated][class A, class Z]
-    int shape[4][2][2] = {};
+    // [shots: 1, 32, 64, 128][plain FP32, compensated][one model, one model
+    // per shot][class A, class Z] (the kernels of the two model kinds take
+    // different launch shapes)
+    int shape[4][2][2][2] = {};
 };
 
 // Launch shapes already tuned in this process, keyed by the mesh signature
@@ -860,7 +862,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     if (fp64(pl) || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
     const int kahan = pl.kind == SFG_FP32_KAHAN ? 1 : 0;
     const int si = pl.S == 1 ? 0 : (pl.S == 32 ? 1 : (pl.S == 64 ? 2 : 3));
-    int *slot = ctx->tune.shape[si][kahan];
+    int *slot = ctx->tune.shape[si][kahan][b.cmm ? 1 : 0];
     std::vector<int> cand;
     if (pl.S == 1) {
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
@@ -885,7 +887,12 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
         pl.shapeZ = std::atoi(fz);
         return SFG_OK;
     }
-    if (slot[0] > 0 && slot[1] > 0) {   // cached choice
+    // class-A shapes outside the kernel's launch bounds are skipped; the
+    // class-Z kernel ignores the staged flag
+    auto valid_a = [&](int s) {
+        return pl.S == 1 || (s & 0x100) || (s & 15) <= stepA_batched_max_warps((s >> 4) & 15, b.cmm != nullptr);
+    };
+    if (slot[0] > 0 && slot[1] > 0 && valid_a(slot[0] - 1)) {   // cached choice
         pl.shapeA = slot[0] - 1;
         pl.shapeZ = slot[1] - 1;
         return SFG_OK;
@@ -908,11 +915,6 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
         CK(cudaEventSynchronize(e1));
         CK(cudaEventElapsedTime(&ms, e0, e1));
         return SFG_OK;
-    };
-    // class-A shapes outside the kernel's launch bounds are skipped; the
-    // class-Z kernel ignores the staged flag
-    auto valid_a = [&](int s) {
-        return pl.S == 1 || (s & 0x100) || (s & 15) <= stepA_batched_max_warps((s >> 4) & 15, b.cmm != nullptr);
     };
     float best = 1e30f;
     int pick_a = -1, pick_z = cand[0];
