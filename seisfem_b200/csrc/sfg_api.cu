@@ -395,6 +395,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
                           : build_value_dict(N, P.up, P.ux, P.union_nnz, d_rho, &tid, &P.dict, &zero_id, st);
         if (T < 0) return fail(ctx, SFG_ERR_CUDA, "value dictionary");
         P.dict_n = T;
+        P.h_dict.assign(2 * (size_t)T, float4{});
+        if (T > 0) CK(cudaMemcpyAsync(P.h_dict.data(), P.dict, sizeof(float4) * 2 * T, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
         ctx->stats.value_tuples = T;
     }
     const char *nt = std::getenv("SFG_NO_TILES"), *mo = std::getenv("SFG_MORTON");
@@ -651,6 +654,7 @@ Step2 step2_args(const DevProblem &P, const LoopPlan &pl, const StepCommon &c, c
     a.c = c; a.na = P.na; a.S = pl.S;
     a.sellA = P.sellA; a.sliceA = P.sliceA; a.sellZ = P.sellZ; a.sliceZ = P.sliceZ;
     a.sellAd = P.sellAd; a.sellZd = P.sellZd; a.dict = P.dict; a.dict_n = P.dict_n; a.rowrho = P.rowrho;
+    a.h_dict = P.h_dict.empty() ? nullptr : P.h_dict.data();
     a.up = P.upp; a.rec = b.rec_geo ? b.rec_geo : P.recp; a.recA = P.recA; a.coefA = P.coefA; a.imA = P.imA;
     a.coefZ = P.coefZ;
     a.cmm = b.cmm; a.sig = b.sig;

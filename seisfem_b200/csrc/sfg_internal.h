@@ -69,6 +69,7 @@ struct DevProblem {
     float4 *dict = nullptr;          // [2 dict_n]
     int2 *sellAd = nullptr, *sellZd = nullptr;   // SELL-32 slots (column, tuple id)
     float *rowrho = nullptr;         // [N] row density, permuted
+    std::vector<float4> h_dict;      // host copy of dict
     // staged-gather tiles (sfg_step32.cuh: Step2::tile*); tileA_off == nullptr without them
     unsigned *sellAt = nullptr, *sellZt = nullptr;
     int *tileA_off = nullptr, *tileA_ext = nullptr, *tileZ_off = nullptr, *tileZ_ext = nullptr;

@@ -77,6 +77,8 @@ struct Step2 {
     const float4 *dict;
     int dict_n;
     const float *rowrho;       // [n] row density, permuted numbering
+    const float4 *h_dict;      // host copy of dict[0 .. 2 dict_n), or nullptr: the one-shot launches
+                               // of at most kParamTuples tuples pass it in the kernel's parameters
     const int *up;             // row-major union records in the permuted numbering
     const float *rec;          //   [nnz][8]: col, M, K1..K6
     const float *recA;         // class-A rows, one model: [upp[na]][8] col, M and the
@@ -186,6 +188,9 @@ cudaError_t mass_row_sums_geo(int n, const int *d_up, const double *d_ux, const 
 // value dictionary of the one-shot kernels (sfg_dict.cu): at most kDictMax
 // tuples of (M / rho_row, K1..K6), two float4 each in shared memory
 constexpr int kDictMax = 512;
+// tuples the one-shot launches pass in the kernel's parameters (2 float4
+// each: 4 KB)
+constexpr int kParamTuples = 128;
 // tuples found (0: not applicable, the kernels keep full-value slots; -1 on a
 // CUDA error); d_tid[nnz] the tuple id of every union entry, d_table[2 T]
 int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, const double *d_rho, int **d_tid,

@@ -121,3 +121,23 @@ def test_mesh_order_without_tiles_matches(oracle, monkeypatch):
         assert np.array_equal(a[k], b[k]), k
     with pytest.raises(SfgError):
         _run_shape(p, monkeypatch, TILE, TILE, no_tiles=True)
+
+
+def test_class_a_rows_are_a_multiple_of_32(oracle):
+    """The set-up moves the last few class-A rows into class Z so that the
+    class-A row count is a multiple of 32 (the one-shot state blocks of the
+    two classes line up); the moved rows run the split-field step and the
+    results stay within the FP32 tolerance of the oracle."""
+    from seisfem_b200.api import Context
+    for p in (config_2(n=30, step=202, pml=5), small_problem("Q4", n=37, step=202, pml=3, seed=4)):
+        ctx = Context(0)
+        try:
+            ctx.setup(p)
+            out = ctx.run(p, precision="fp32k", want_snapshots=True)
+            st = ctx.stats()
+        finally:
+            ctx.close()
+        assert st["interior_rows"] % 32 == 0 and st["interior_rows"] > 0
+        ref = oracle.run(p)
+        for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+            assert rel_l2(out[k], ref[k]) < FP32_TOL, k
