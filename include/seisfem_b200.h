@@ -187,13 +187,14 @@ int sfg_run_models(sfg_ctx *ctx, const sfg_run_desc *run, const sfg_model *model
 /* Plan groups: several single-batch plans -- independent problems on meshes
  * of any sizes, which the reference runs one after another
  * (time_evolution/elastic_wave.c:446-518 loops over shots; its callers over
- * meshes) -- advanced by one CUDA-graph launch.  When every plan is a
+ * meshes) -- advanced by one CUDA-graph launch.  The group's graph composes
+ * the plans' own graphs side by side: every mesh advances on its own, with no
+ * per-step join across meshes.  With SFG_GROUP_FUSED=1, when every plan is a
  * one-shot fused FP32 plan (SFG_FP32_KAHAN or SFG_FP32) with the same step
- * count and all or none of the meshes carry a value dictionary, the group's
- * graph issues one class-A and one class-Z kernel per time step for all
- * meshes together (each block finds its mesh in a block map), with the
- * launch shapes the largest mesh's autotuning picked; other groups compose
- * the plans' own graphs side by side (SFG_GROUP_CHILD_GRAPHS=1 forces that).
+ * count and all or none of the meshes carry a value dictionary, the graph
+ * instead issues one class-A and one class-Z kernel per time step for all
+ * meshes together (each block finds its mesh in a block map; measured slower
+ * on B200).
  * Results are read per plan with sfg_plan_finish(plan, 0, ...) after the
  * group's stream has finished.  A group uses its plans' buffers: do not
  * launch a member plan while the group runs; destroy the group before its

@@ -1595,8 +1595,12 @@ int sfg_group_create(sfg_plan *const *plans, int nplans, sfg_group **out)
     if (cudaSetDevice(dev) != cudaSuccess) return SFG_ERR_CUDA;
     sfg_group *g = new sfg_group();
     g->device = dev;
-    const char *env = std::getenv("SFG_GROUP_CHILD_GRAPHS");
-    if (group_fusable(plans, nplans) && !(env && env[0] == '1')) {
+    // the plans' own graphs side by side by default: each mesh advances
+    // independently, with no per-step join across meshes, which measured
+    // faster on B200 than the multi-mesh kernels (config 3b: 351-362 against
+    // 379-395 ms); SFG_GROUP_FUSED=1 asks for the multi-mesh kernels
+    const char *env = std::getenv("SFG_GROUP_FUSED");
+    if (group_fusable(plans, nplans) && env && env[0] == '1') {
         const int rc = group_create_fused(plans, nplans, g);
         if (rc != SFG_OK) { group_free(g); return rc; }
     } else {

@@ -51,8 +51,10 @@ def test_group_launch_matches_separate_plans(oracle, mode, monkeypatch):
     side by side -- give each plan's own results bit for bit, on repeated
     launches."""
     from seisfem_b200.api import Context, Group, Plan
-    if mode == "child_graphs":
-        monkeypatch.setenv("SFG_GROUP_CHILD_GRAPHS", "1")
+    if mode == "fused":
+        monkeypatch.setenv("SFG_GROUP_FUSED", "1")
+    else:
+        monkeypatch.delenv("SFG_GROUP_FUSED", raising=False)
     probs = config_3b(count=3, lo=20, hi=50, step=202, pml=4)
     assert len({p.mesh.node_num for p in probs}) == 3
     ctxs = [Context(0) for _ in probs]
