@@ -870,6 +870,7 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
     std::vector<int> cand;
     if (pl.S == 1) {
         for (int v = 0; v < step2_variants(); v++) cand.push_back(v);
+        cand.push_back(8);   // 128 threads, 5 resident blocks (class Z within 102 registers)
         // the staged-gather tile kernels, where the set-up built tiles (the
         // staged slot streams, kSlotStageShape, measured slower on every
         // mesh tried: pinned with SFG_SHAPE_A/Z only)

@@ -1759,6 +1759,7 @@ cudaError_t launch_range_slice_len(int r0, int r1, const int *d_up, const int *d
         case 2: SFG_ONE(KERNEL, 256, 3, COUNT); break;                                         \
         case 4: SFG_ONE(KERNEL, 64, 16, COUNT); break;                                         \
         case 5: SFG_ONE(KERNEL, 512, 2, COUNT); break;                                         \
+        case 8: SFG_ONE(KERNEL, 128, 5, COUNT); break;                                         \
         default: SFG_ONE(KERNEL, 256, 4, COUNT); break;                                        \
         }                                                                                      \
     } while (0)
@@ -1893,7 +1894,7 @@ cudaError_t launch_stepZ(const Step2 &a, bool comp, int variant, cudaStream_t st
 int step2_threads(int variant)
 {
     switch (variant) {
-    case 0: case 1: return 128;
+    case 0: case 1: case 8: return 128;
     case 2: return 256;
     case 4: return 64;
     case 5: return 512;
