@@ -14,6 +14,33 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
 }
 
 // Block-wide sum of (a, b) into dst[0], dst[1] (one atomic pair per block).
+// The FP32 overload sums a block's squared displacements in FP32 (the
+// blow-up test compares the step's total with 1e7; a block holds at most
+// 512 rows) and adds the block's sums to the FP64 totals.
+__device__ __forceinline__ void block_energy(double *dst, float a, float b)
+{
+    __shared__ float sa[32], sb[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sa[w] = a; sb[w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        a = l < nw ? sa[l] : 0.f;
+        b = l < nw ? sb[l] : 0.f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0 && dst) { atomicAdd(dst, (double)a); atomicAdd(dst + 1, (double)b); }
+    }
+}
+
 __device__ __forceinline__ void block_energy(double *dst, double a, double b)
 {
     __shared__ double sa[32], sb[32];

@@ -281,7 +281,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
     const StepCommon &c = a.c;
     const int i = bid * THREADS + threadIdx.x;
     gather2_one(c, a.na, a.in, 1, i, seis_row);
-    double eu = 0.0, ew = 0.0;
+    float eu = 0.f, ew = 0.f;
     if (i < a.na) {
         const int lane = i & 31, slice = i >> 5;
         float kU[4], kW[4], mL[8];
@@ -363,8 +363,8 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
 #pragma unroll
         for (int k = 0; k < 3; k++) go[32 * k] = make_float4(g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
         reinterpret_cast<float4 *>(a.out.Pa)[i] = make_float4(p[0], p[1], p[2], p[3]);
-        eu = (double)uu * uu;
-        ew = (double)ww * ww;
+        eu = uu * uu;
+        ew = ww * ww;
     }
     block_energy(c.energy ? c.energy + ((size_t)it) * 2 : nullptr, eu, ew);
 }
@@ -392,7 +392,7 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
         c0 = __ldcs(cf); c1 = __ldcs(cf + 32); c2 = __ldcs(cf + 64);
     }
     const bool full = __any_sync(0xffffffffu, local < nz && is_pml_row(c1));
-    double eu = 0.0, ew = 0.0;
+    float eu = 0.f, ew = 0.f;
     if (local < nz) {
         const int lane = local & 31, slice = local >> 5;
         float kU[6], kW[6], m[20];
@@ -506,8 +506,8 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
             so[32 * k] = make_float4(gs[4 * k], gs[4 * k + 1], gs[4 * k + 2], gs[4 * k + 3]);
             po[32 * k] = make_float4(ps_[4 * k], ps_[4 * k + 1], ps_[4 * k + 2], ps_[4 * k + 3]);
         }
-        eu = (double)uu * uu;
-        ew = (double)ww * ww;
+        eu = uu * uu;
+        ew = ww * ww;
     }
     block_energy(c.energy ? c.energy + ((size_t)it) * 2 : nullptr, eu, ew);
 }
