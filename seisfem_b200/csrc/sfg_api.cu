@@ -395,9 +395,16 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
                           : build_value_dict(N, P.up, P.ux, P.union_nnz, d_rho, &tid, &P.dict, &zero_id, st);
         if (T < 0) return fail(ctx, SFG_ERR_CUDA, "value dictionary");
         P.dict_n = T;
-        P.h_dict.assign(2 * (size_t)T, float4{});
-        if (T > 0) CK(cudaMemcpyAsync(P.h_dict.data(), P.dict, sizeof(float4) * 2 * T, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        // a host copy for the launches that pass the table in the kernels'
+        // parameters (SFG_TABLE_SMEM=1 keeps every launch on the shared-memory
+        // table, to compare the two)
+        const char *ts = std::getenv("SFG_TABLE_SMEM");
+        P.h_dict.clear();
+        if (T > 0 && !(ts && *ts == '1')) {
+            P.h_dict.assign(2 * (size_t)T, float4{});
+            CK(cudaMemcpyAsync(P.h_dict.data(), P.dict, sizeof(float4) * 2 * T, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
         ctx->stats.value_tuples = T;
     }
     const char *nt = std::getenv("SFG_NO_TILES"), *mo = std::getenv("SFG_MORTON");

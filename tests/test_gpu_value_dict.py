@@ -141,3 +141,17 @@ def test_class_a_rows_are_a_multiple_of_32(oracle):
         ref = oracle.run(p)
         for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
             assert rel_l2(out[k], ref[k]) < FP32_TOL, k
+
+
+def test_tuple_table_in_parameters_matches_shared_memory(monkeypatch):
+    """The one-shot kernels read the tuple table from their parameters (at
+    most 128 tuples) or from shared memory (more tuples, the multi-mesh
+    kernels, SFG_TABLE_SMEM=1): the same values, so the same results bit for
+    bit."""
+    p = config_2(n=40, step=302, pml=6)
+    monkeypatch.delenv("SFG_TABLE_SMEM", raising=False)
+    a = _run_shape(p, monkeypatch, 0, 0, no_tiles=True)
+    monkeypatch.setenv("SFG_TABLE_SMEM", "1")
+    b = _run_shape(p, monkeypatch, 0, 0, no_tiles=True)
+    for k in ("seis_u", "seis_w", "snap_u", "snap_w"):
+        assert np.array_equal(a[k], b[k]), (k, rel_l2(a[k], b[k]))
