@@ -831,10 +831,10 @@ def main():
         h2d = sum(a.nbytes for a in (m.element_node, m.x, m.y, md.rho, md.vp, md.vs, md.c)) + 8 * S + 4 * len(prob.rec_node)
         ns = ctx.L.sfg_snapshot_rows(prob.step, 200)
         d2h = 2 * 8 * S * (prob.step - 2) * len(prob.rec_node) + 2 * 8 * S * ns * m.node_num
-        # two untimed calls, then the median of five: single calls on a shared
-        # host vary by up to ~0.5 s (context creation, set-up allocations)
+        # two untimed calls, then the median of seven: single calls on a
+        # shared host vary by up to ~1 s (context creation, set-up)
         times = []
-        for k in range(2 + 5):
+        for k in range(2 + 7):
             barrier()
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
@@ -852,7 +852,7 @@ def main():
                "seconds_per_step": float(t_e2e.item()),
                "seconds_timed_calls": [round(t, 4) for t in times[2:]],
                "note": "one elastic_wave()-equivalent call per step: sfg_setup (GPU assembly from host arrays) + "
-                       "sfg_run (loop, seismograms and 200-step snapshots copied back); median of 5 calls after 2"}
+                       "sfg_run (loop, seismograms and 200-step snapshots copied back); median of 7 calls after 2"}
 
     plain = None
     if args.compare_plain:
