@@ -722,6 +722,21 @@ __global__ void __launch_bounds__(SPL == 2 && !MM ? 128 : 256, SPL == 1 ? 3 : (S
     const long long tasks = (long long)a.na * nch;
     for (long long task = warp; task < tasks; task += warps_total) {
         const int i = (int)(task / nch);
+        if (lane == 0 && task % nch == 0) {
+            // into L2 while the row's gathers run: the row's own values that
+            // its update reads afterwards (U, W and their lo parts, Pa), and
+            // the next task's row records
+            prefetch_l2(a.in.Gc + (size_t)i * GC * S, 2u * S * 4u);
+            prefetch_l2(a.in.Gc + ((size_t)i * GC + 10) * S, 2u * S * 4u);
+            prefetch_l2(a.in.Pa + (size_t)i * PA * S, (unsigned)PA * S * 4u);
+            if (MM) prefetch_l2(a.cmm + (size_t)i * 6 * S, 6u * S * 4u);
+            const long long nt = task + warps_total;
+            if (nt < tasks) {
+                const int i2 = (int)(nt / nch);
+                const int f0 = __ldg(a.up + i2), f1 = __ldg(a.up + i2 + 1);
+                prefetch_l2(rec + 2 * (size_t)f0, 32u * (unsigned)(f1 - f0));
+            }
+        }
         float kU[NK][SPL], kW[NK][SPL], mL[8][SPL];
 #pragma unroll
         for (int q = 0; q < SPL; q++) {
@@ -1016,6 +1031,7 @@ __device__ __forceinline__ void row_split(const Step2 &a, const float4 *rec, int
         const int cnt = min(32, e1 - base);
         float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
         if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
+
         int k = 0;
         // two entries in flight with 64 shots per warp, one with 32
         for (; SPL > 1 && k + 1 < cnt; k += 2) {
@@ -1082,6 +1098,20 @@ __global__ void __launch_bounds__(256, SPL == 1 ? 2 : 1) stepZ_batched(const Ste
     for (long long task = warp; task < tasks; task += warps_total) {
         const int local = (int)(task / nch);
         const int i = a.na + local;
+        if (lane == 0 && task % nch == 0) {
+            // into L2 while the row's gathers run: its own split fields and
+            // private values (read by its update afterwards), and the next
+            // task's row records
+            prefetch_l2(a.in.Gs + (size_t)local * GS * S, (unsigned)GS * S * 4u);
+            prefetch_l2(a.in.Ps + (size_t)local * PS * S, (unsigned)PS * S * 4u);
+            if (MM) prefetch_l2(a.cmm + (size_t)i * 6 * S, 6u * S * 4u);
+            const long long nt = task + warps_total;
+            if (nt < tasks) {
+                const int i2 = a.na + (int)(nt / nch);
+                const int f0 = __ldg(a.up + i2), f1 = __ldg(a.up + i2 + 1);
+                prefetch_l2(rec + 2 * (size_t)f0, 32u * (unsigned)(f1 - f0));
+            }
+        }
         const float4 *cfp = reinterpret_cast<const float4 *>(a.coefZ) + blk4(local, 0, 3);
         const float4 c0 = __ldg(cfp), c1 = __ldg(cfp + 32), c2 = __ldg(cfp + 64);
         float kU[6][SPL], kW[6][SPL], m[20][SPL];
