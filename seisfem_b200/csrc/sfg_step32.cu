@@ -1031,7 +1031,6 @@ __device__ __forceinline__ void row_split(const Step2 &a, const float4 *rec, int
         const int cnt = min(32, e1 - base);
         float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
         if (lane < cnt) { r0 = __ldg(rec + 2 * (size_t)(base + lane)); r1 = __ldg(rec + 2 * (size_t)(base + lane) + 1); }
-
         int k = 0;
         // two entries in flight with 64 shots per warp, one with 32
         for (; SPL > 1 && k + 1 < cnt; k += 2) {
