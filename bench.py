@@ -974,6 +974,7 @@ def batched_section(dev: int, stream, steps: int = 3, warmup: int = 3) -> dict:
     ctx = Context(dev)
     ctx.setup(prob)
     plan = Plan(ctx, prob, precision="fp32k", snap_every=0)
+    shape_code = ctx.stats()["rows_per_block"]   # the batch plan's pick (later plans overwrite the stats)
     for _ in range(warmup):
         plan.launch(0, sh)
     torch.cuda.synchronize(dev)
@@ -1012,7 +1013,7 @@ def batched_section(dev: int, stream, steps: int = 3, warmup: int = 3) -> dict:
                        "l2": "per-step working set > 126 MB L2; no flush needed"},
             "value": value, "unit": METRIC, "ms_per_run": ms, "runs_timed": steps, "warmup": warmup,
             "gpu_launches_per_run": launches,
-            "launch_shape": launch_shape(st["rows_per_block"], S),
+            "launch_shape": launch_shape(shape_code, S),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": b_step,
                          "avg_step_us": round(ms * 1e3 / T, 3),
