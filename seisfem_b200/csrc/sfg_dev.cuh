@@ -5,6 +5,12 @@
 
 namespace sfg {
 
+// The line holding p into L1 (this thread's prefetch; no data returned).
+__device__ __forceinline__ void prefetch_l1(const void *p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch, sm_90+):
 // one instruction puts a whole contiguous stream in flight without holding
 // registers.  p 16-byte aligned, bytes a multiple of 16.

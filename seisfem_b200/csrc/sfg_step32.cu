@@ -308,6 +308,12 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
         // of K_ij U_j suffer on smooth fields
         const float4 *G4 = reinterpret_cast<const float4 *>(a.in.Gc);
         const float4 own0 = __ldg(G4 + blk4(i, 0, 3)), own2 = __ldg(G4 + blk4(i, 2, 3));
+        // the values the row's update reads after the slot loop, into L1
+        prefetch_l1(G4 + blk4(i, 1, 3));
+        prefetch_l1(reinterpret_cast<const float4 *>(a.in.Pa) + i);
+        prefetch_l1(a.coefA + i);
+        prefetch_l1(a.imA + i);
+        if (DICT) prefetch_l1(a.rowrho + i);
         // jq: the float4 index blk4(j, 0, 3) of neighbour j's record
         auto acc = [&](int jq, float vm, const float *kv) {
             const float4 *gj = G4 + jq;
