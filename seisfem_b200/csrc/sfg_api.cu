@@ -1191,6 +1191,8 @@ int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaE
     const int N = ctx->N;
     if (queue_reset(p->pl, N, p->run.step, p->nsnap, p->b, st) != cudaSuccess)
         return fail(ctx, SFG_ERR_CUDA, "state reset failed");
+    // snapshot row 0 (the initial, zero state) is final once the reset ran
+    if (snap_done && !snap_done->empty()) CK(cudaEventRecord((*snap_done)[0], st));
     const int n = queue_loop(ctx, p->pl, &p->run, p->b, p->run.snap_every, p->nsnap, p->run.step - 2, st, snap_done);
     if (n < 0) return fail(ctx, SFG_ERR_CUDA, "launch of the time loop failed");
     p->launches = n;
