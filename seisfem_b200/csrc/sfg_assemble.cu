@@ -202,6 +202,76 @@ __global__ void element_coo_shared(int tc, int p, int E, int EB, const int *__re
     }
 }
 
+// The same entries for the set-up's seven matrices (consistent mass, then
+// stiffness types 1..6) with the element type known at compile time: the
+// quadrature and matrix loops unroll, and the shape table sits in shared
+// memory.  Every term and sum is the one element_coo_shared forms, in the
+// same order (this file is compiled without FMA contraction), so the bits
+// are the same.
+template <int TC>
+__global__ void __launch_bounds__(256) element_coo_std7(int E, int EB, const int *__restrict__ en,
+                                                        const double *__restrict__ x, const double *__restrict__ y,
+                                                        const double *__restrict__ rho,
+                                                        const double *__restrict__ tab, int *__restrict__ ci,
+                                                        int *__restrict__ cj, double *__restrict__ cx, int *flags)
+{
+    constexpr int P = elem_order(TC), PP = P * P, NQ = quad_count(TC);
+    __shared__ double stab[NQ * 48];
+    extern __shared__ double geo[];   // [EB][NQ][5]: drdx drdy dsdx dsdy area*w
+    for (int k = threadIdx.x; k < NQ * 48; k += blockDim.x) stab[k] = tab[k];
+    const int e0 = blockIdx.x * EB;
+    const int ne = min(EB, E - e0);
+    for (int k = threadIdx.x; k < ne * NQ; k += blockDim.x) {
+        const int le = k / NQ, q = k - le * NQ, e = e0 + le;
+        ElemGeom g;
+        elem_geom(TC, en + (long long)e * P, x, y, g);
+        if (g.area == 0.0 && q == 0) atomicOr(flags, FLAG_ZERO_AREA);
+        double r, s, w;
+        quad_point(TC, q, r, s, w);
+        double *o = geo + (size_t)k * 5;
+        map_point(TC, g, r, s, o[0], o[1], o[2], o[3]);
+        o[4] = g.area * w;
+    }
+    __syncthreads();
+    const long long nnz = (long long)E * PP;
+    for (int k = threadIdx.x; k < ne * PP; k += blockDim.x) {
+        const int le = k / PP, rem = k - le * PP, iq = rem / P, jq = rem - iq * P;
+        const int e = e0 + le;
+        const long long t = (long long)e * PP + rem;
+        const int *enE = en + (long long)e * P;
+        const int ip = enE[iq] - 1, jp = enE[jq] - 1;
+        const double rho_ip = rho[ip];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0, a6 = 0.0;
+        const double *gq = geo + (size_t)le * NQ * 5;
+#pragma unroll 4
+        for (int q = 0; q < NQ; q++, gq += 5) {
+            const double drdx = gq[0], drdy = gq[1], dsdx = gq[2], dsdy = gq[3], aw = gq[4];
+            const double *t0 = stab + 3 * q * 16, *t1 = t0 + 16, *t2 = t0 + 32;
+            const double phi_i = t0[iq], phi_j = t0[jq];
+            const double dxi = t1[iq] * drdx + t2[iq] * dsdx;
+            const double dyi = t1[iq] * drdy + t2[iq] * dsdy;
+            const double dxj = t1[jq] * drdx + t2[jq] * dsdx;
+            const double dyj = t1[jq] * drdy + t2[jq] * dsdy;
+            a0 = a0 + aw * rho_ip * phi_i * phi_j;
+            a1 = a1 + aw * (dxi * dxj);
+            a2 = a2 + aw * (dyi * dyj);
+            a3 = a3 + aw * (dxi * dyj);
+            a4 = a4 + aw * (dyi * dxj);
+            a5 = a5 + aw * (phi_i * dxj);
+            a6 = a6 + aw * (phi_i * dyj);
+        }
+        ci[t] = ip;
+        cj[t] = jp;
+        cx[t] = a0;
+        cx[nnz + t] = a1;
+        cx[2 * nnz + t] = a2;
+        cx[3 * nnz + t] = a3;
+        cx[4 * nnz + t] = a4;
+        cx[5 * nnz + t] = a5;
+        cx[6 * nnz + t] = a6;
+    }
+}
+
 cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x, const double *d_y,
                                const double *d_rho, int nmat, const int *mats, int *d_ci, int *d_cj,
                                double *d_cx, int *d_flags, cudaStream_t st)
@@ -218,7 +288,17 @@ cudaError_t launch_element_coo(int tc, int E, const int *d_en, const double *d_x
     const int EB = std::max(1, threads / pp);
     const long long blocks = ((long long)E + EB - 1) / EB;
     const size_t smem = sizeof(double) * 5 * (size_t)EB * nq;
-    if (blocks > 0)
+    const bool std7 = nmat == 7 && d_rho && d_ci && d_cj && mats[0] == -1 && mats[1] == 1 && mats[2] == 2 &&
+                      mats[3] == 3 && mats[4] == 4 && mats[5] == 5 && mats[6] == 6;
+    if (blocks > 0 && std7) {
+        switch (tc) {
+#define SFG_STD7(T) case T: element_coo_std7<T><<<(unsigned)blocks, threads, smem, st>>>(E, EB, d_en, d_x, d_y, \
+                        d_rho, tab, d_ci, d_cj, d_cx, d_flags); break;
+        SFG_STD7(T3) SFG_STD7(T6) SFG_STD7(T10) SFG_STD7(Q4) SFG_STD7(Q9) SFG_STD7(Q16)
+#undef SFG_STD7
+        default: break;
+        }
+    } else if (blocks > 0)
         element_coo_shared<<<(unsigned)blocks, threads, smem, st>>>(tc, p, E, EB, d_en, d_x, d_y, d_rho, nmat,
                                                                      ml, tab, d_ci, d_cj, d_cx, d_flags);
     e = cudaGetLastError();
@@ -451,14 +531,12 @@ __device__ bool iargsort_dev(int *vec, int *map, int n)
     return true;
 }
 
-// Pass 1 per row: restore COO order inside the row (the bucket was filled
-// with atomics), replay the Fortran sort, and count the union entries and
-// the surviving (nonzero-sum) entries of each value stream.
-__global__ void canon_pass1(int N, int nv, long long nnz, const int *__restrict__ row_start,
-                            int *__restrict__ bucket, const int *__restrict__ cj,
-                            const double *__restrict__ cx, int *__restrict__ vec,
-                            int *__restrict__ map, int *__restrict__ cnt_union,
-                            int *__restrict__ cnt_v, int *maxlen, int *flags)
+// Pass 1, one thread per row: restore COO order inside the row (the bucket
+// was filled with atomics) and replay the Fortran sort (vec = column + 1,
+// map = the permutation of the row's entries).
+__global__ void canon_pass1(int N, long long nnz, const int *__restrict__ row_start, int *__restrict__ bucket,
+                            const int *__restrict__ cj, int *__restrict__ vec, int *__restrict__ map, int *maxlen,
+                            int *flags)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= N) return;
@@ -473,61 +551,88 @@ __global__ void canon_pass1(int N, int nv, long long nnz, const int *__restrict_
     for (int i = 0; i < l; i++) { v[i] = cj[b[i]] + 1; m[i] = i; }
     if (!iargsort_dev(v, m, l)) { atomicOr(flags, FLAG_SORT_STACK); return; }
     atomicMax(maxlen, l);
-    int nu = 0;
-    int nz[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int k = 0;
-    while (k < l) {
-        int col = v[k];
-        double xs[8];
-        for (int s = 0; s < nv; s++) xs[s] = cx[(long long)s * nnz + b[m[k]]];
-        k++;
-        while (k < l && v[k] == col) {
-            for (int s = 0; s < nv; s++) xs[s] = xs[s] + cx[(long long)s * nnz + b[m[k]]];
-            k++;
-        }
-        nu++;
-        for (int s = 0; s < nv; s++) nz[s] += (xs[s] != 0.0);
-    }
-    cnt_union[r] = nu;
-    for (int s = 0; s < nv; s++) cnt_v[(long long)s * N + r] = nz[s];
 }
 
-// Pass 2 per row: write the union pattern and every stream's canonical CSR.
+// Pass 2, one warp per row: each run of equal columns in the sorted row is
+// one union entry u, summed by the lane that holds the run's first position,
+// in the sorted order (coo2csr_lib.f90's accumulation, so the sums round the
+// same).  The sums go to row-local scratch (tx[s][row_start + u], tc), and
+// the row's union length and per-stream nonzero counts to cnt_union, cnt_v.
+__global__ void canon_sums(int N, int nv, long long nnz, const int *__restrict__ row_start,
+                           const int *__restrict__ bucket, const double *__restrict__ cx,
+                           const int *__restrict__ vec, const int *__restrict__ map, int *__restrict__ tc,
+                           double *__restrict__ tx, int *__restrict__ cnt_union, int *__restrict__ cnt_v)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wr >= N) return;
+    const int r = (int)wr;
+    const int r1 = row_start[r], l = row_start[r + 1] - r1;
+    const int *b = bucket + r1, *v = vec + r1, *m = map + r1;
+    int base = 0;
+    int nz[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k0 = 0; k0 < l; k0 += 32) {
+        const int k = k0 + lane;
+        const int col = k < l ? v[k] : 0;
+        const bool start = k < l && (k == 0 || v[k - 1] != col);
+        const unsigned mask = __ballot_sync(0xffffffffu, start);
+        if (start) {
+            const int u = base + __popc(mask & ((1u << lane) - 1u));
+            double xs[8];
+            for (int s = 0; s < nv; s++) xs[s] = cx[(long long)s * nnz + b[m[k]]];
+            for (int kk = k + 1; kk < l && v[kk] == col; kk++)
+                for (int s = 0; s < nv; s++) xs[s] = xs[s] + cx[(long long)s * nnz + b[m[kk]]];
+            tc[r1 + u] = col - 1;
+            for (int s = 0; s < nv; s++) {
+                tx[(long long)s * nnz + r1 + u] = xs[s];
+                nz[s] += (xs[s] != 0.0);
+            }
+        }
+        base += __popc(mask);
+    }
+    for (int s = 0; s < nv; s++) {
+        int c = nz[s];
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt_v[(long long)s * N + r] = c;
+    }
+    if (lane == 0) cnt_union[r] = base;
+}
+
+// Pass 3, one warp per row: the union pattern and every stream's canonical
+// CSR (its nonzero sums, in column order) from the row-local scratch.
 __global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict__ row_start,
-                            const int *__restrict__ bucket, const double *__restrict__ cx,
-                            const int *__restrict__ vec, const int *__restrict__ map,
-                            const int *__restrict__ up, int *__restrict__ uj, double *__restrict__ ux,
-                            long long union_nnz, int *const *__restrict__ vp_,
+                            const int *__restrict__ tc, const double *__restrict__ tx,
+                            const int *__restrict__ cnt_union, const int *__restrict__ up, int *__restrict__ uj,
+                            double *__restrict__ ux, long long union_nnz, int *const *__restrict__ vp_,
                             int *const *__restrict__ vj_, double *const *__restrict__ vx_)
 {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= N) return;
-    int r1 = row_start[r], r2 = row_start[r + 1], l = r2 - r1;
-    const int *b = bucket + r1, *v = vec + r1, *m = map + r1;
-    long long uo = up ? up[r] : 0;
-    int vo[8];
-    for (int s = 0; s < nv; s++) vo[s] = vp_[s] ? vp_[s][r] : 0;
-    int k = 0;
-    while (k < l) {
-        int col = v[k];
-        double xs[8];
-        for (int s = 0; s < nv; s++) xs[s] = cx[(long long)s * nnz + b[m[k]]];
-        k++;
-        while (k < l && v[k] == col) {
-            for (int s = 0; s < nv; s++) xs[s] = xs[s] + cx[(long long)s * nnz + b[m[k]]];
-            k++;
+    const int lane = threadIdx.x & 31;
+    const long long wr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wr >= N) return;
+    const int r = (int)wr;
+    const int r1 = row_start[r], nu = cnt_union[r];
+    if (uj) {
+        const long long uo = up[r];
+        for (int u = lane; u < nu; u += 32) {
+            uj[uo + u] = tc[r1 + u];
+            for (int s = 0; s < nv; s++) ux[(long long)s * union_nnz + uo + u] = tx[(long long)s * nnz + r1 + u];
         }
-        if (uj) {
-            uj[uo] = col - 1;
-            for (int s = 0; s < nv; s++) ux[(long long)s * union_nnz + uo] = xs[s];
-            uo++;
-        }
-        for (int s = 0; s < nv; s++)
-            if (vj_[s] && xs[s] != 0.0) {
-                vj_[s][vo[s]] = col - 1;
-                vx_[s][vo[s]] = xs[s];
-                vo[s]++;
+    }
+    for (int s = 0; s < nv; s++) {
+        if (!vj_[s]) continue;
+        int vo = vp_[s][r];
+        for (int u0 = 0; u0 < nu; u0 += 32) {
+            const int u = u0 + lane;
+            const double x = u < nu ? tx[(long long)s * nnz + r1 + u] : 0.0;
+            const bool keep = u < nu && x != 0.0;
+            const unsigned mask = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int o = vo + __popc(mask & ((1u << lane) - 1u));
+                vj_[s][o] = tc[r1 + u];
+                vx_[s][o] = x;
             }
+            vo += __popc(mask);
+        }
     }
 }
 
@@ -553,8 +658,10 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
 {
     if (nv < 1 || nv > 8 || nnz >= (1LL << 31) || N < 0) { err = "canonicalize: bad sizes"; return SFG_ERR_ARG; }
     int *cnt = nullptr, *cursor = nullptr, *vec = nullptr, *map = nullptr, *cu = nullptr,
-        *cv = nullptr, *maxlen = nullptr;
+        *cv = nullptr, *maxlen = nullptr, *tc = nullptr;
+    double *tx = nullptr;
     size_t nn = (size_t)std::max<long long>(nnz, 1);
+    const bool sums = want_union || want_csr;
     // temporaries (row buckets included) come from the device's pool
     SFG_TRY(tmp_alloc((void **)&cnt, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(tmp_alloc((void **)&cursor, sizeof(int) * ((size_t)N + 1), st));
@@ -565,6 +672,10 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     SFG_TRY(tmp_alloc((void **)&cu, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(tmp_alloc((void **)&cv, sizeof(int) * (size_t)nv * ((size_t)N + 1), st));
     SFG_TRY(tmp_alloc((void **)&maxlen, sizeof(int), st));
+    if (sums) {
+        SFG_TRY(tmp_alloc((void **)&tc, sizeof(int) * nn, st));
+        SFG_TRY(tmp_alloc((void **)&tx, sizeof(double) * (size_t)nv * nn, st));
+    }
     SFG_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(cudaMemsetAsync(cursor, 0, sizeof(int) * ((size_t)N + 1), st));
     SFG_TRY(cudaMemsetAsync(maxlen, 0, sizeof(int), st));
@@ -574,16 +685,22 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     SFG_TRY(exclusive_scan_int(cnt, out.row_start, N, st));
     if (gb) row_fill_kernel<<<gb, tb, 0, st>>>(d_ci, nnz, N, out.row_start, cursor, out.bucket);
     unsigned gr = (unsigned)((N + 127) / 128);
-    if (gr)
-        canon_pass1<<<gr, 128, 0, st>>>(N, nv, nnz, out.row_start, out.bucket, d_cj, d_cx, vec, map, cu,
-                                        cv, maxlen, d_flags);
+    const unsigned gw = (unsigned)(((long long)N * 32 + 255) / 256);   // one warp per row
+    if (gr) canon_pass1<<<gr, 128, 0, st>>>(N, nnz, out.row_start, out.bucket, d_cj, vec, map, maxlen, d_flags);
+    if (gw && sums)
+        canon_sums<<<gw, 256, 0, st>>>(N, nv, nnz, out.row_start, out.bucket, d_cx, vec, map, tc, tx, cu, cv);
     SFG_TRY(cudaGetLastError());
     int hflags = 0;
     SFG_TRY(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
     SFG_TRY(cudaMemcpyAsync(&out.max_row_len, maxlen, sizeof(int), cudaMemcpyDeviceToHost, st));
     SFG_TRY(cudaStreamSynchronize(st));
-    if (hflags & FLAG_BADINDEX) { err = "COO row index out of range"; return SFG_ERR_BADINDEX; }
-    if (hflags & FLAG_SORT_STACK) { err = "row too long for the device sorter"; return SFG_ERR_ROWLEN; }
+    auto free_tmp = [&]() {
+        for (void *t : {(void *)cnt, (void *)cursor, (void *)vec, (void *)map, (void *)cu, (void *)cv,
+                        (void *)maxlen, (void *)tc, (void *)tx})
+            if (t) cudaFreeAsync(t, st);
+    };
+    if (hflags & FLAG_BADINDEX) { free_tmp(); err = "COO row index out of range"; return SFG_ERR_BADINDEX; }
+    if (hflags & FLAG_SORT_STACK) { free_tmp(); err = "row too long for the device sorter"; return SFG_ERR_ROWLEN; }
 
     // row pointers: union + each stream
     int *up = nullptr;
@@ -619,15 +736,13 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     void *htab[24];
     for (int s = 0; s < 8; s++) { htab[s] = dvp[s]; htab[8 + s] = dvj[s]; htab[16 + s] = dvx[s]; }
     SFG_TRY(cudaMemcpyAsync(d_tab, htab, sizeof(htab), cudaMemcpyHostToDevice, st));
-    if (gr)
-        canon_pass2<<<gr, 128, 0, st>>>(N, nv, nnz, out.row_start, out.bucket, d_cx, vec, map, out.up,
-                                        out.uj, out.ux, out.union_nnz, d_tab, d_tab + 8,
-                                        (double *const *)(d_tab + 16));
+    if (gw && sums)
+        canon_pass2<<<gw, 256, 0, st>>>(N, nv, nnz, out.row_start, tc, tx, cu, out.up, out.uj, out.ux,
+                                        out.union_nnz, d_tab, d_tab + 8, (double *const *)(d_tab + 16));
     SFG_TRY(cudaGetLastError());
     SFG_TRY(cudaStreamSynchronize(st));
-    for (void *t : {(void *)d_tab, (void *)cnt, (void *)cursor, (void *)vec, (void *)map, (void *)cu, (void *)cv,
-                    (void *)maxlen})
-        cudaFreeAsync(t, st);
+    cudaFreeAsync(d_tab, st);
+    free_tmp();
     return SFG_OK;
 }
 

@@ -11,7 +11,7 @@ namespace sfg {
 
 enum ElemType { T3 = 1, T6 = 2, T10 = 3, Q4 = 4, Q9 = 5, Q16 = 6 };
 
-__host__ __device__ inline int elem_order(int tc)
+__host__ __device__ constexpr int elem_order(int tc)
 {
     // mesh/mesh_element_order.c:2-57
     switch (tc) {
@@ -25,7 +25,7 @@ __host__ __device__ inline int elem_order(int tc)
     }
 }
 
-__host__ __device__ inline bool elem_is_quad(int tc) { return tc == Q4 || tc == Q9 || tc == Q16; }
+__host__ __device__ constexpr bool elem_is_quad(int tc) { return tc == Q4 || tc == Q9 || tc == Q16; }
 
 // Local positions of the nodes that define the element map
 // (mass_sparse_q4.c:176-179; q16 corners 0,3,15,12: mass_sparse_q16.c:179-182;
@@ -67,7 +67,7 @@ __device__ __forceinline__ int quad_point(int tc, int q, double &r, double &s, d
     return 12;
 }
 
-__host__ __device__ inline int quad_count(int tc) { return elem_is_quad(tc) ? 36 : 12; }
+__host__ __device__ constexpr int quad_count(int tc) { return elem_is_quad(tc) ? 36 : 12; }
 
 // Shape functions (shape/shape_*.c), products grouped left to right exactly as
 // the reference writes them.
