@@ -375,8 +375,13 @@ __global__ void node_lumped_mass(int tc, int p, int N, const int *__restrict__ e
     int pp = p * p;
     double m = 0.0;
     int nq = quad_count(tc);
-    for (int k = row_start[r]; k < row_start[r + 1]; k++) {
-        int c = bucket[k];
+    // the row's COO entries ascend, in runs of p: row iq of each element
+    // that holds node r (entries e pp + iq p + j, j = 0 .. p-1); its
+    // diagonal entry is the run's iq-th
+    for (int k = row_start[r]; k < row_start[r + 1]; k += p) {
+        const int c0 = bucket[k];
+        const int e0 = c0 / pp, iq0 = (c0 - e0 * pp) / p;
+        const int c = c0 + iq0;
         if (cj[c] != r) continue;
         int e = c / pp, rem = c - e * pp, iq = rem / p, jq = rem - iq * p;
         const int *enE = en + (long long)e * p;

@@ -57,19 +57,29 @@ __device__ __forceinline__ int row_of(const int *__restrict__ up, int n, long lo
 }
 
 // one thread per union entry (coalesced reads of the value planes)
-__global__ void dict_scale(int n, const int *__restrict__ up, const double *__restrict__ ux, long long nnz,
-                           const double *__restrict__ rho, DictScratch *s)
+// Largest magnitude per matrix: each thread strides over the union entries,
+// the block reduces, and one atomic per block and matrix merges the blocks
+// (a few hundred blocks, so the seven addresses see few atomics).
+__global__ void __launch_bounds__(256) dict_scale(int n, const int *__restrict__ up, const double *__restrict__ ux,
+                                                  long long nnz, const double *__restrict__ rho, DictScratch *s)
 {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double red[8][7];
     double m[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (e < nnz) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
         const double rr = rho[row_of(up, n, e)];
-        for (int k = 0; k < 7; k++) m[k] = fabs(entry_value(ux, nnz, e, k, rr));
+        for (int k = 0; k < 7; k++) m[k] = fmax(m[k], fabs(entry_value(ux, nnz, e, k, rr)));
     }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int k = 0; k < 7; k++) {
         double v = m[k];
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(&s->scale[k], (unsigned long long)__double_as_longlong(v));
+        if (lane == 0) red[w][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double v = 0.0;
+        for (int j = 0; j < (int)(blockDim.x >> 5); j++) v = fmax(v, red[j][threadIdx.x]);
+        if (v > 0.0) atomicMax(&s->scale[threadIdx.x], (unsigned long long)__double_as_longlong(v));
     }
 }
 
@@ -245,7 +255,7 @@ int build_value_dict(int n, const int *d_up, const double *d_ux, long long nnz, 
     if (e == cudaSuccess) e = cudaMemsetAsync(s, 0, sizeof(DictScratch), st);
     const unsigned g = (unsigned)((nnz + 255) / 256);
     if (e == cudaSuccess && n > 0 && nnz > 0) {
-        dict_scale<<<g, 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s);
+        dict_scale<<<std::min(g, 148u * 8u), 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s);
         dict_insert_zero<<<1, 1, 0, st>>>(s, zslot);
         dict_insert_entries<<<g, 256, 0, st>>>(n, d_up, d_ux, nnz, d_rho, s, slot_of);
         e = cudaGetLastError();

@@ -1549,19 +1549,25 @@ __global__ void range_sell_fill(int r0, int r1, const int *__restrict__ up, cons
     }
 }
 
+// One warp per permuted row: its union entries as 8-float records (column
+// in the permuted numbering, then M, K1..K6 rounded to FP32), two float4
+// stores per entry, consecutive entries on consecutive lanes.
 __global__ void rec_perm_fill(int n, const int *__restrict__ up, const int *__restrict__ uj,
                               const double *__restrict__ ux, long long nnz, const int *__restrict__ perm,
                               const int *__restrict__ inv, const int *__restrict__ upp, float *__restrict__ rec)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
+    const long long wr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wr >= n) return;
+    const int r = (int)wr, lane = threadIdx.x & 31;
     const int o = perm[r];
     const int a0 = up[o], len = up[o + 1] - a0;
     const long long d0 = upp[r];
-    for (int k = 0; k < len; k++) {
-        const long long e = a0 + k, d = d0 + k;
-        rec[d * 8] = __int_as_float(inv[uj[e]]);
-        for (int m = 0; m < 7; m++) rec[d * 8 + 1 + m] = (float)ux[m * nnz + e];
+    for (int k = lane; k < len; k += 32) {
+        const long long e = a0 + k;
+        float4 *d = reinterpret_cast<float4 *>(rec + (d0 + k) * 8);
+        d[0] = make_float4(__int_as_float(inv[uj[e]]), (float)ux[e], (float)ux[nnz + e], (float)ux[2 * nnz + e]);
+        d[1] = make_float4((float)ux[3 * nnz + e], (float)ux[4 * nnz + e], (float)ux[5 * nnz + e],
+                           (float)ux[6 * nnz + e]);
     }
 }
 
@@ -2103,7 +2109,9 @@ cudaError_t build_rec_perm(int n, const int *d_up, const int *d_uj, const double
 {
     cudaError_t e = keep_alloc(d_rec, sizeof(float) * 8 * std::max<long long>(nnz, 1), st);
     if (e != cudaSuccess) return e;
-    if (n) rec_perm_fill<<<(n + 127) / 128, 128, 0, st>>>(n, d_up, d_uj, d_ux, nnz, d_perm, d_inv, d_upp, *d_rec);
+    if (n)
+        rec_perm_fill<<<(unsigned)(((long long)n * 32 + 255) / 256), 256, 0, st>>>(n, d_up, d_uj, d_ux, nnz, d_perm,
+                                                                                    d_inv, d_upp, *d_rec);
     return cudaGetLastError();
 }
 
