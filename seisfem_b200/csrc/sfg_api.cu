@@ -284,6 +284,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     CK(cudaSetDevice(ctx->device));
     ctx->ready = false;
     free_problem(ctx->P, ctx->stream);
+    PhaseTrace tr(ctx->stream);
     const int tc = type_code_of(m->type);
     if (tc < 0) return fail(ctx, SFG_ERR_ARG, std::string("unknown element type ") + (m->type ? m->type : "(null)"));
     const int p = elem_order_host(tc);
@@ -296,6 +297,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     for (long long k = 0; k < (long long)E * p; k++)
         if (m->element_node[k] < 1 || m->element_node[k] > N)
             return fail(ctx, SFG_ERR_BADINDEX, "element_node entry out of range at " + std::to_string(k));
+    tr.mark("setup: checks");
     cudaStream_t st = ctx->stream;
     DevProblem &P = ctx->P;
     P.type_code = tc; P.order = p; P.node_num = N; P.element_num = E; P.coo_nnz = nnz;
@@ -320,7 +322,6 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
 
     // element matrices: consistent mass (with rho) and stiffness types 1..6
     const int mats[7] = {-1, 1, 2, 3, 4, 5, 6};
-    PhaseTrace tr(st);
     tr.mark("setup: uploads");
     CK(launch_element_coo(tc, E, d_en, d_x, d_y, d_rho, 7, mats, d_ci, d_cj, d_cx, d_flags, st));
     int hflags = 0;
@@ -333,7 +334,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     }
     CanonOut co;
     tr.mark("setup: element matrices");
-    int rc = canonicalize(N, nnz, d_ci, d_cj, d_cx, 7, true, true, co, d_flags, st, ctx->err);
+    // the union pattern and values; each matrix's own CSR is built from them
+    // on first use (csr_ensure)
+    int rc = canonicalize(N, nnz, d_ci, d_cj, d_cx, 7, true, false, co, d_flags, st, ctx->err);
     tr.mark("setup: canonical CSR");
     if (rc != SFG_OK) {
         canon_free(co, false, st);
@@ -342,7 +345,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         cudaFreeAsync(d_ci, st); cudaFreeAsync(d_cj, st); cudaFreeAsync(d_cx, st);
         return rc;
     }
-    for (int k = 0; k < 7; k++) P.csr[k] = co.csr[k];
+    for (int k = 0; k < 7; k++) P.csr_nnz[k] = co.nnz_v[k];
     P.up = co.up; P.uj = co.uj; P.ux = co.ux; P.union_nnz = co.union_nnz; P.max_row_len = co.max_row_len;
 
     // lumped mass (mass_sparse_*.c, lumpflag = 1)
@@ -407,6 +410,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         }
         ctx->stats.value_tuples = T;
     }
+    tr.mark("setup: M-PML, coef, dictionary");
     const char *nt = std::getenv("SFG_NO_TILES"), *mo = std::getenv("SFG_MORTON");
     const bool morton = P.dict_n > 0 && mo && *mo == '1' && !(nt && *nt && *nt != '0');
     const bool tiles = morton;
@@ -431,7 +435,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
         ctx->stats.interior_rows = na;
         ctx->stats.pml_rows = npml;
     }
-    tr.mark("setup: M-PML, coef, classes");
+    tr.mark("setup: classes");
     if (P.dict_n > 0) {
         CK(build_sell_range_dict(0, P.na, P.up, P.uj, tid, zero_id, P.perm, P.inv, &P.sellAd, &P.sliceA, &P.slotsA,
                                  st));
@@ -481,7 +485,7 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     }
     ctx->ready = true;
     ctx->stats.union_nnz = P.union_nnz;
-    for (int k = 0; k < 7; k++) ctx->stats.csr_nnz[k] = P.csr[k].nnz;
+    for (int k = 0; k < 7; k++) ctx->stats.csr_nnz[k] = P.csr_nnz[k];
     ctx->stats.setup_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SFG_OK;
@@ -491,7 +495,18 @@ int sfg_csr_nnz(sfg_ctx *ctx, int matrix, int *nnz)
 {
     if (!ctx || !nnz || matrix < 0 || matrix > 6) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
-    *nnz = (int)ctx->P.csr[matrix].nnz;
+    *nnz = (int)ctx->P.csr_nnz[matrix];
+    return SFG_OK;
+}
+
+// The canonical CSR of M, K1..K6 (coo2csr_lib.f90), from the union pattern.
+static int csr_ensure(sfg_ctx *ctx)
+{
+    DevProblem &P = ctx->P;
+    if (P.csr[0].p) return SFG_OK;
+    CK(cudaSetDevice(ctx->device));
+    const int rc = csr_from_union(ctx->N, 7, P.up, P.uj, P.ux, P.union_nnz, P.csr, ctx->stream, ctx->err);
+    if (rc != SFG_OK) return fail(ctx, rc, "canonical CSR: " + ctx->err);
     return SFG_OK;
 }
 
@@ -500,6 +515,8 @@ int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x)
     if (!ctx || matrix < 0 || matrix > 6) return SFG_ERR_ARG;
     if (!ctx->ready) return fail(ctx, SFG_ERR_STATE, "sfg_setup first");
     CK(cudaSetDevice(ctx->device));
+    const int rc = csr_ensure(ctx);
+    if (rc != SFG_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     const DevCsr &c = ctx->P.csr[matrix];
     if (p) CK(cudaMemcpy(p, c.p, sizeof(int) * ((size_t)ctx->N + 1), cudaMemcpyDeviceToHost));
@@ -961,6 +978,8 @@ int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
 int ensure_plain_matrices(sfg_ctx *ctx)
 {
     if (ctx->plain_x[0]) return SFG_OK;
+    const int rc = csr_ensure(ctx);
+    if (rc != SFG_OK) return rc;
     for (int k = 0; k < 7; k++) {
         const DevCsr &c = ctx->P.csr[k];
         std::vector<double> h(std::max<long long>(c.nnz, 1));

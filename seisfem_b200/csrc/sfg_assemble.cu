@@ -641,6 +641,69 @@ __global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict_
     }
 }
 
+// Nonzeros of each stream: block s sums cnt_v[s][0 .. N).
+__global__ void __launch_bounds__(256) count_totals(int N, const int *__restrict__ cnt_v, long long *__restrict__ tot)
+{
+    __shared__ long long red[8];
+    const int s = blockIdx.x;
+    long long c = 0;
+    for (int r = threadIdx.x; r < N; r += blockDim.x) c += cnt_v[(long long)s * N + r];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        tot[s] = t;
+    }
+}
+
+// One warp per row: the nonzero union entries of every stream.
+__global__ void union_nz_count(int N, int nv, const int *__restrict__ up, const double *__restrict__ ux,
+                               long long union_nnz, int *__restrict__ cnt_v)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wr >= N) return;
+    const int r = (int)wr;
+    const long long u0 = up[r];
+    const int nu = up[r + 1] - (int)u0;
+    for (int s = 0; s < nv; s++) {
+        int c = 0;
+        for (int u = lane; u < nu; u += 32) c += ux[(long long)s * union_nnz + u0 + u] != 0.0;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt_v[(long long)s * N + r] = c;
+    }
+}
+
+// One warp per row: each stream's CSR row, its nonzero union entries in order.
+__global__ void union_to_csr(int N, int nv, const int *__restrict__ up, const int *__restrict__ uj,
+                             const double *__restrict__ ux, long long union_nnz, int *const *__restrict__ vp_,
+                             int *const *__restrict__ vj_, double *const *__restrict__ vx_)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wr >= N) return;
+    const int r = (int)wr;
+    const long long u0 = up[r];
+    const int nu = up[r + 1] - (int)u0;
+    for (int s = 0; s < nv; s++) {
+        int vo = vp_[s][r];
+        for (int k0 = 0; k0 < nu; k0 += 32) {
+            const int u = k0 + lane;
+            const double x = u < nu ? ux[(long long)s * union_nnz + u0 + u] : 0.0;
+            const bool keep = u < nu && x != 0.0;
+            const unsigned mask = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int o = vo + __popc(mask & ((1u << lane) - 1u));
+                vj_[s][o] = uj[u0 + u];
+                vx_[s][o] = x;
+            }
+            vo += __popc(mask);
+        }
+    }
+}
+
 #define SFG_TRY(call)                                                              \
     do {                                                                           \
         cudaError_t e_ = (call);                                                   \
@@ -707,6 +770,14 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     if (hflags & FLAG_BADINDEX) { free_tmp(); err = "COO row index out of range"; return SFG_ERR_BADINDEX; }
     if (hflags & FLAG_SORT_STACK) { free_tmp(); err = "row too long for the device sorter"; return SFG_ERR_ROWLEN; }
 
+    // nonzeros of each stream (the CSR arrays themselves only with want_csr)
+    long long *d_tot = nullptr;
+    if (sums && !want_csr) {
+        SFG_TRY(tmp_alloc((void **)&d_tot, sizeof(long long) * 8, st));
+        count_totals<<<nv, 256, 0, st>>>(N, cv, d_tot);
+        SFG_TRY(cudaGetLastError());
+        SFG_TRY(cudaMemcpyAsync(out.nnz_v, d_tot, sizeof(long long) * nv, cudaMemcpyDeviceToHost, st));
+    }
     // row pointers: union + each stream
     int *up = nullptr;
     if (want_union) {
@@ -731,6 +802,7 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
             SFG_TRY(cudaMemcpyAsync(&tot, c.p + N, sizeof(int), cudaMemcpyDeviceToHost, st));
             SFG_TRY(cudaStreamSynchronize(st));
             c.nnz = tot;
+            out.nnz_v[s] = tot;
             SFG_TRY(keep_alloc(&c.j, sizeof(int) * std::max<size_t>(tot, 1), st));
             SFG_TRY(keep_alloc(&c.x, sizeof(double) * std::max<size_t>(tot, 1), st));
             dvp[s] = c.p; dvj[s] = c.j; dvx[s] = c.x;
@@ -747,7 +819,45 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     SFG_TRY(cudaGetLastError());
     SFG_TRY(cudaStreamSynchronize(st));
     cudaFreeAsync(d_tab, st);
+    if (d_tot) cudaFreeAsync(d_tot, st);
     free_tmp();
+    return SFG_OK;
+}
+
+int csr_from_union(int N, int nv, const int *d_up, const int *d_uj, const double *d_ux, long long union_nnz,
+                   DevCsr *out, cudaStream_t st, std::string &err)
+{
+    if (nv < 1 || nv > 8 || N < 0) { err = "csr_from_union: bad sizes"; return SFG_ERR_ARG; }
+    int *cv = nullptr, **d_tab = nullptr;
+    long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    SFG_TRY(tmp_alloc((void **)&cv, sizeof(int) * (size_t)nv * ((size_t)N + 1), st));
+    const unsigned gw = (unsigned)(((long long)N * 32 + 255) / 256);
+    if (gw) union_nz_count<<<gw, 256, 0, st>>>(N, nv, d_up, d_ux, union_nnz, cv);
+    SFG_TRY(cudaGetLastError());
+    for (int s = 0; s < nv; s++) {
+        SFG_TRY(keep_alloc(&out[s].p, sizeof(int) * ((size_t)N + 1), st));
+        SFG_TRY(exclusive_scan_int(cv + (size_t)s * N, out[s].p, N, st));
+    }
+    int htot[8];
+    for (int s = 0; s < nv; s++)
+        SFG_TRY(cudaMemcpyAsync(&htot[s], out[s].p + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SFG_TRY(cudaStreamSynchronize(st));
+    void *htab[24] = {nullptr};
+    for (int s = 0; s < nv; s++) {
+        tot[s] = htot[s];
+        out[s].nnz = tot[s];
+        SFG_TRY(keep_alloc(&out[s].j, sizeof(int) * std::max<long long>(tot[s], 1), st));
+        SFG_TRY(keep_alloc(&out[s].x, sizeof(double) * std::max<long long>(tot[s], 1), st));
+        htab[s] = out[s].p; htab[8 + s] = out[s].j; htab[16 + s] = out[s].x;
+    }
+    SFG_TRY(tmp_alloc((void **)&d_tab, sizeof(void *) * 24, st));
+    SFG_TRY(cudaMemcpyAsync(d_tab, htab, sizeof(htab), cudaMemcpyHostToDevice, st));
+    if (gw) union_to_csr<<<gw, 256, 0, st>>>(N, nv, d_up, d_uj, d_ux, union_nnz, d_tab, d_tab + 8,
+                                             (double *const *)(d_tab + 16));
+    SFG_TRY(cudaGetLastError());
+    SFG_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(d_tab, st);
+    cudaFreeAsync(cv, st);
     return SFG_OK;
 }
 

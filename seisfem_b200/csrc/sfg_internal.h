@@ -46,7 +46,10 @@ struct DevProblem {
     double *ux = nullptr;
     long long union_nnz = 0;
     int max_row_len = 0;
+    // the canonical CSR of each matrix, built from the union on first use
+    // (csr_ensure); their nonzero counts from set-up
     DevCsr csr[7];
+    long long csr_nnz[7] = {0, 0, 0, 0, 0, 0, 0};
     double *mass_lump = nullptr;     // [N]
     double *mpml = nullptr;          // [6][N]: dx, dy, dxx, dyy, dxx_pyx, dyy_pxy
     double *coef64 = nullptr;        // [4][N] c11, c13, c33, c44
@@ -110,7 +113,13 @@ struct CanonOut {
     int max_row_len = 0;
     int *row_start = nullptr;   // COO bucket offsets [N+1] (kept for the lumped mass)
     int *bucket = nullptr;      // COO indices per row, ascending [nnz]
+    long long nnz_v[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // nonzeros of each stream's CSR (also without want_csr)
 };
+// The canonical CSR of each of the nv streams from the union pattern and
+// values (the union entries whose value is nonzero, in column order): the
+// same arrays canonicalize's want_csr gives.
+int csr_from_union(int N, int nv, const int *d_up, const int *d_uj, const double *d_ux, long long union_nnz,
+                   DevCsr *out, cudaStream_t st, std::string &err);
 int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const double *d_cx, int nv,
                  bool want_union, bool want_csr, CanonOut &out, int *d_flags, cudaStream_t st,
                  std::string &err);
