@@ -294,10 +294,6 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     const int N = m->node_num, E = m->element_num;
     const long long nnz = (long long)E * p * p;
     if (nnz >= (1LL << 31)) return fail(ctx, SFG_ERR_ARG, "COO size exceeds 2^31");
-    for (long long k = 0; k < (long long)E * p; k++)
-        if (m->element_node[k] < 1 || m->element_node[k] > N)
-            return fail(ctx, SFG_ERR_BADINDEX, "element_node entry out of range at " + std::to_string(k));
-    tr.mark("setup: checks");
     cudaStream_t st = ctx->stream;
     DevProblem &P = ctx->P;
     P.type_code = tc; P.order = p; P.node_num = N; P.element_num = E; P.coo_nnz = nnz;
@@ -309,10 +305,20 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     int *d_en = nullptr, *d_flags = nullptr, *d_ci = nullptr, *d_cj = nullptr;
     double *d_x = nullptr, *d_y = nullptr, *d_rho = nullptr, *d_cx = nullptr, *d_scr = nullptr;
     CK(upload(&d_en, m->element_node, (size_t)E * p, st));
+    {
+        // every element_node entry names a node (1 .. N) before any kernel
+        // reads node data through it
+        long long bad = -1;
+        CK(check_element_nodes(d_en, (long long)E * p, N, &bad, st));
+        if (bad >= 0) {
+            keep_free(d_en, st);
+            return fail(ctx, SFG_ERR_BADINDEX, "element_node entry out of range at " + std::to_string(bad));
+        }
+    }
+    tr.mark("setup: checks");
     CK(upload(&d_x, m->x, (size_t)N, st));
     CK(upload(&d_y, m->y, (size_t)N, st));
     CK(upload(&d_rho, md->rho, (size_t)N, st));
-    CK(upload(&P.coef64, md->c, (size_t)4 * N, st));
     CK(keep_alloc(&d_flags, sizeof(int), st));
     CK(cudaMemsetAsync(d_flags, 0, sizeof(int), st));
     // the COO streams are set-up temporaries: from the device's pool
@@ -324,6 +330,9 @@ int sfg_setup(sfg_ctx *ctx, const sfg_mesh *m, const sfg_model *md)
     const int mats[7] = {-1, 1, 2, 3, 4, 5, 6};
     tr.mark("setup: uploads");
     CK(launch_element_coo(tc, E, d_en, d_x, d_y, d_rho, 7, mats, d_ci, d_cj, d_cx, d_flags, st));
+    // the elastic constants, staged from host memory while the element
+    // matrices are formed
+    CK(upload(&P.coef64, md->c, (size_t)4 * N, st));
     int hflags = 0;
     CK(cudaMemcpyAsync(&hflags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

@@ -109,6 +109,32 @@ cudaError_t exclusive_scan_int(const int *d_in, int *d_out, int n, cudaStream_t 
     return e;
 }
 
+// Lowest position k of an element_node entry outside [1, N] (atomicMin on
+// *first, which the caller sets to all ones).
+__global__ void element_node_check(const int *__restrict__ en, long long cnt, int N, unsigned long long *first)
+{
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (long long)gridDim.x * blockDim.x)
+        if (en[k] < 1 || en[k] > N) atomicMin(first, (unsigned long long)k);
+}
+
+cudaError_t check_element_nodes(const int *d_en, long long cnt, int N, long long *first_bad, cudaStream_t st)
+{
+    *first_bad = -1;
+    unsigned long long *d_first = nullptr, h = ~0ull;
+    cudaError_t e = tmp_alloc((void **)&d_first, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_first, 0xff, sizeof(unsigned long long), st);
+    if (e == cudaSuccess && cnt > 0) {
+        element_node_check<<<(unsigned)std::min<long long>((cnt + 255) / 256, 148 * 16), 256, 0, st>>>(d_en, cnt, N,
+                                                                                                        d_first);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d_first, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (d_first) cudaFreeAsync(d_first, st);
+    if (e == cudaSuccess && h != ~0ull) *first_bad = (long long)h;
+    return e;
+}
+
 // ------------------------------------------------------- element matrices
 
 struct MatList { int m[8]; };   // -1: consistent mass (rho), 0..6: stiffness type

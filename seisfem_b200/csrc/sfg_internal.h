@@ -120,6 +120,9 @@ struct CanonOut {
 // same arrays canonicalize's want_csr gives.
 int csr_from_union(int N, int nv, const int *d_up, const int *d_uj, const double *d_ux, long long union_nnz,
                    DevCsr *out, cudaStream_t st, std::string &err);
+// The lowest position of an element_node entry (1-based) outside [1, N] in
+// d_en[0 .. cnt), or -1 in *first_bad.
+cudaError_t check_element_nodes(const int *d_en, long long cnt, int N, long long *first_bad, cudaStream_t st);
 int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const double *d_cx, int nv,
                  bool want_union, bool want_csr, CanonOut &out, int *d_flags, cudaStream_t st,
                  std::string &err);

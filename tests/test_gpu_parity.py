@@ -165,12 +165,16 @@ def test_bad_indices_rejected(ctx):
         ctx.run(p, src_node=bad)
     assert e.value.status == 5
     en = p.mesh.element_node.copy()
+    en[11] = 0
     en[3] = p.mesh.node_num + 5
     q = small_problem("Q4", n=8, step=10, pml=2)
     q.mesh.element_node = en
     with pytest.raises(SfgError) as e:
         ctx.setup(q)
     assert e.value.status == 5
+    assert "out of range at 3" in str(e.value)      # the first bad entry
+    ctx.setup(p)                                    # the context stays usable
+    assert ctx.run(p)["status"] == 0
 
 
 def test_zero_area_rejected(ctx):
