@@ -202,8 +202,10 @@ sfg_ctx *sfg_create(int device)
 {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return nullptr;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return nullptr;
+    // one attribute, not the whole property set (which takes milliseconds)
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess || major < 10)
+        return nullptr;
     if (cudaSetDevice(device) != cudaSuccess) return nullptr;
     sfg_ctx *c = new sfg_ctx();
     c->device = device;

@@ -667,20 +667,23 @@ __global__ void canon_pass2(int N, int nv, long long nnz, const int *__restrict_
     }
 }
 
-// Nonzeros of each stream: block s sums cnt_v[s][0 .. N).
-__global__ void __launch_bounds__(256) count_totals(int N, const int *__restrict__ cnt_v, long long *__restrict__ tot)
+// Nonzeros of each stream: blocks (b, s) stride over cnt_v[s][0 .. N) and
+// add their sums to tot[s] (zeroed by the caller).
+__global__ void __launch_bounds__(256) count_totals(int N, const int *__restrict__ cnt_v,
+                                                    unsigned long long *__restrict__ tot)
 {
     __shared__ long long red[8];
-    const int s = blockIdx.x;
+    const int s = blockIdx.y;
     long long c = 0;
-    for (int r = threadIdx.x; r < N; r += blockDim.x) c += cnt_v[(long long)s * N + r];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x)
+        c += cnt_v[(long long)s * N + r];
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
         long long t = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
-        tot[s] = t;
+        atomicAdd(&tot[s], (unsigned long long)t);
     }
 }
 
@@ -800,7 +803,10 @@ int canonicalize(int N, long long nnz, const int *d_ci, const int *d_cj, const d
     long long *d_tot = nullptr;
     if (sums && !want_csr) {
         SFG_TRY(tmp_alloc((void **)&d_tot, sizeof(long long) * 8, st));
-        count_totals<<<nv, 256, 0, st>>>(N, cv, d_tot);
+        SFG_TRY(cudaMemsetAsync(d_tot, 0, sizeof(long long) * 8, st));
+        if (N > 0)
+            count_totals<<<dim3((unsigned)std::min((N + 255) / 256, 128), nv), 256, 0, st>>>(
+                N, cv, reinterpret_cast<unsigned long long *>(d_tot));
         SFG_TRY(cudaGetLastError());
         SFG_TRY(cudaMemcpyAsync(out.nnz_v, d_tot, sizeof(long long) * nv, cudaMemcpyDeviceToHost, st));
     }
