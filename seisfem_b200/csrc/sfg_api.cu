@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -703,24 +704,41 @@ Step2 step2_args(const DevProblem &P, const LoopPlan &pl, const StepCommon &c, c
     return a;
 }
 
-// Queue the whole time loop of one batch on `st` (captured into a graph by
-// the caller).  Returns the number of kernels queued, or -1 on a launch error.
+// Snapshot row that the first step at or after `it` writes next: row 0 is
+// the initial state, and step it writes row srow after its update when
+// (it + 1) % snap_every == 0 and srow < nsnap.
+int snapshot_row_before(int it, int snap_every, int nsnap)
+{
+    if (nsnap <= 0 || snap_every <= 0) return 1;
+    int taken = 0;
+    for (int k = 2; k < it; k++)
+        if ((k + 1) % snap_every == 0) taken++;
+    return std::min(1 + taken, nsnap);
+}
+
+// Queue the time loop of one batch on `st`: steps [it_begin, it_end) of the
+// loop over it = 2 .. 2 + steps_to_run (it_end < 0: to the end), then the
+// receiver row of the last state when the range reaches the end.  Captured
+// into a graph by the caller, or queued directly.  Returns the number of
+// kernels queued, or -1 on a launch error.
 int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b, int snap_every,
-               int nsnap, int steps_to_run, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr)
+               int nsnap, int steps_to_run, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr,
+               int it_begin = 2, int it_end = -1)
 {
     const DevProblem &P = ctx->P;
     const int N = P.node_num, S = pl.S, R = run->rec_num, rows = run->step - 2;
     int launches = 0;
     StepCommon c = step_common(P, pl, run, b);
     (void)R; (void)rows;
-    int cur = 0, srow = 1;
     const int last = 2 + steps_to_run;   // exclusive
+    if (it_end < 0 || it_end > last) it_end = last;
+    int cur = (it_begin - 2) & 1, srow = snapshot_row_before(it_begin, snap_every, nsnap);
     if (pl.kind == SFG_FP32_PLAIN_PATH) {
         Plain32 a;
         a.c = c;
         for (int k = 0; k < 7; k++) a.m[k] = {P.csr[k].p, P.csr[k].j, ctx->plain_x[k]};
         a.coef = P.coef32; a.st = b.pst; a.eq = b.peq; a.rhs = b.prhs; a.anew = b.panew;
-        for (int it = 2; it < last; it++) {
+        for (int it = it_begin; it < it_end; it++) {
             a.c.it = it;
             a.c.seis_row = it - 2;
             if (launch_plain_step(a, 256, st, &launches) != cudaSuccess) return -1;
@@ -732,7 +750,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
         }
         return launches;
     }
-    for (int it = 2; it < last; it++) {
+    for (int it = it_begin; it < it_end; it++) {
         c.it = it;
         c.seis_row = it >= 3 ? it - 3 : -1;
         const int nxt = cur ^ 1;
@@ -784,6 +802,7 @@ int queue_loop(sfg_ctx *ctx, const LoopPlan &pl, const sfg_run_desc *run, BatchB
             srow++;
         }
     }
+    if (it_end < last) return launches;
     // the last state's receiver row
     c.it = last - 1;
     c.seis_row = last - 3;
@@ -1008,6 +1027,8 @@ int ensure_plain_matrices(sfg_ctx *ctx)
 // A prepared run: device buffers of one batch, every batch's sources staged on
 // the device, and the whole time loop of a batch (state reset included)
 // captured once into a CUDA graph.
+constexpr int kChunkSlots = 4;   // two that alternate, the first chunk, the last chunk
+
 struct sfg_plan {
     sfg_ctx *ctx = nullptr;
     LoopPlan pl;
@@ -1019,6 +1040,10 @@ struct sfg_plan {
     float *d_cmm_all = nullptr, *d_sig_all = nullptr;   // one model per shot: [batch][N][6][S], [batch][S]
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // directly queued plans: executable graphs of loop chunks (plan_launch),
+    // each with an event recorded after its last launch
+    cudaGraphExec_t chunk_exec[kChunkSlots] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t chunk_done[kChunkSlots] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -1026,6 +1051,11 @@ namespace {
 void plan_free(sfg_plan *p)
 {
     if (!p) return;
+    for (int k = 0; k < kChunkSlots; k++) {
+        if (p->chunk_done[k]) cudaEventSynchronize(p->chunk_done[k]);
+        if (p->chunk_exec[k]) cudaGraphExecDestroy(p->chunk_exec[k]);
+        if (p->chunk_done[k]) cudaEventDestroy(p->chunk_done[k]);
+    }
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     free_bufs(p->ctx, p->b);
@@ -1200,7 +1230,14 @@ int plan_create(sfg_ctx *ctx, const sfg_run_desc *run, sfg_plan **out, bool capt
     return SFG_OK;
 }
 
-int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr)
+// Queue batch `batch` of a plan on `st`.  With `snap_done` (directly queued
+// plans), snapshot row r's event is recorded once the row is written, and
+// `on_row(r)`, when given, is called for every row in order after its event
+// is recorded: for the chunked loop one chunk behind the last launched one,
+// so that a caller whose copy of the row to pageable host memory blocks until
+// the copy is done waits for a chunk that is finishing while the next runs.
+int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaEvent_t> *snap_done = nullptr,
+                const std::function<int(int)> *on_row = nullptr)
 {
     sfg_ctx *ctx = p->ctx;
     if (batch < 0 || batch >= p->nbatch) return fail(ctx, SFG_ERR_ARG, "batch out of range");
@@ -1222,11 +1259,97 @@ int plan_launch(sfg_plan *p, int batch, cudaStream_t st, const std::vector<cudaE
     if (queue_reset(p->pl, N, p->run.step, p->nsnap, p->b, st) != cudaSuccess)
         return fail(ctx, SFG_ERR_CUDA, "state reset failed");
     // snapshot row 0 (the initial, zero state) is final once the reset ran
-    if (snap_done && !snap_done->empty()) CK(cudaEventRecord((*snap_done)[0], st));
-    const int n = queue_loop(ctx, p->pl, &p->run, p->b, p->run.snap_every, p->nsnap, p->run.step - 2, st, snap_done);
+    const bool rows = snap_done && (int)snap_done->size() >= p->nsnap && p->nsnap > 0;
+    if (rows) CK(cudaEventRecord((*snap_done)[0], st));
+    int handed = 0;   // rows given to on_row
+    auto hand_over = [&](int upto) {
+        for (; rows && on_row && handed < upto; handed++) {
+            const int rc = (*on_row)(handed);
+            if (rc != SFG_OK) return fail(ctx, rc, "snapshot copies failed");
+        }
+        return (int)SFG_OK;
+    };
+    const LoopPlan &pl = p->pl;
+    const int se = p->run.snap_every, ns = p->nsnap, steps = p->run.step - 2, last = p->run.step;
+    const bool chunked = pl.kind == SFG_FP32 || pl.kind == SFG_FP32_KAHAN || pl.kind == SFG_FP64;
+    if (!chunked) {
+        const int n = queue_loop(ctx, pl, &p->run, p->b, se, ns, steps, st, rows ? snap_done : nullptr);
+        if (n < 0) return fail(ctx, SFG_ERR_CUDA, "launch of the time loop failed");
+        p->launches = n;
+        return hand_over(ns);
+    }
+    // The first kHeadSteps steps go to the stream directly (the GPU starts at
+    // once); the rest as graphs of up to kChunkSteps steps that end after a
+    // snapshot step, each captured while the earlier ones run (a graph's
+    // steps follow one another with less device-side overhead than stream
+    // launches joined by events).  Chunks of one length share their
+    // topology: two executable graphs alternate, each updated in place
+    // (cudaGraphExecUpdate) once its previous launch has finished, so that
+    // nothing is instantiated or destroyed per chunk; a chunk of another
+    // length (the first, the last) has a slot of its own.
+    constexpr int kHeadSteps = 16, kChunkSteps = 256;
+    const int head = std::min(last, 2 + kHeadSteps);
+    int n = queue_loop(ctx, pl, &p->run, p->b, se, ns, steps, st, rows ? snap_done : nullptr, 2, head);
     if (n < 0) return fail(ctx, SFG_ERR_CUDA, "launch of the time loop failed");
+    int recorded = rows ? snapshot_row_before(head, se, ns) : 0;   // rows whose events are recorded
+    int turn = 0;
+    for (int it = head; it < last;) {
+        int end = std::min(last, it + kChunkSteps);
+        for (int k = it; ns > 0 && se > 0 && k < end; k++)
+            if ((k + 1) % se == 0) { end = k + 1; break; }
+        // slot: 0 and 1 alternate for the chunks after the first, 2 holds the
+        // first chunk, 3 the last
+        int slot = it == head ? 2 : (end == last ? 3 : -1);
+        if (slot < 0) {
+            slot = turn;
+            turn ^= 1;
+        }
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return fail(ctx, SFG_ERR_CUDA, "capture of a loop chunk failed");
+        const int nk = queue_loop(ctx, pl, &p->run, p->b, se, ns, steps, st, nullptr, it, end);
+        const cudaError_t ec = cudaStreamEndCapture(st, &g);
+        if (nk < 0 || ec != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(ctx, SFG_ERR_CUDA, "capture of a loop chunk failed");
+        }
+        cudaGraphExec_t &x = p->chunk_exec[slot];
+        cudaEvent_t &done = p->chunk_done[slot];
+        bool ready = false;
+        if (x) {
+            // the slot's previous chunk has finished before its graph changes
+            if (cudaEventSynchronize(done) != cudaSuccess) { cudaGraphDestroy(g); return fail(ctx, SFG_ERR_CUDA, "loop chunk"); }
+            cudaGraphExecUpdateResultInfo info;
+            ready = cudaGraphExecUpdate(x, g, &info) == cudaSuccess;
+            if (!ready) {
+                (void)cudaGetLastError();
+                cudaGraphExecDestroy(x);
+                x = nullptr;
+            }
+        }
+        if (!ready) {
+            const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+            if (ei != cudaSuccess) {
+                x = nullptr;
+                cudaGraphDestroy(g);
+                return fail(ctx, SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+            }
+        }
+        cudaGraphDestroy(g);
+        if (!done) CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        CK(cudaGraphLaunch(x, st));
+        CK(cudaEventRecord(done, st));
+        n += nk;
+        // the rows of the earlier chunks to the caller, then this chunk's events
+        const int rc = hand_over(recorded);
+        if (rc != SFG_OK) return rc;
+        if (rows)
+            for (const int upto = snapshot_row_before(end, se, ns); recorded < upto; recorded++)
+                CK(cudaEventRecord((*snap_done)[recorded], st));
+        it = end;
+    }
     p->launches = n;
-    return SFG_OK;
+    return hand_over(ns);
 }
 
 // Wait for a launched batch, copy its outputs to the caller (host or device
@@ -1305,25 +1428,28 @@ int run_all(sfg_ctx *ctx, const sfg_run_desc *run, double *seis_u, double *seis_
     }
     const bool streamed = overlap && (int)snap_done.size() == p->nsnap;
     for (int bidx = 0; bidx < p->nbatch; bidx++) {
+        const int S = p->pl.S, N = ctx->N, s0 = bidx * S, ns = std::min(S, run->src_num - s0);
+        // snapshot row k of every shot of the batch to the caller, on the
+        // copy stream once the row is written
+        const std::function<int(int)> copy_row = [&](int k) {
+            if (cudaStreamWaitEvent(ctx->stream3, snap_done[k], 0) != cudaSuccess) return (int)SFG_ERR_CUDA;
+            for (int sh = 0; sh < ns; sh++) {
+                const size_t src = ((size_t)sh * p->nsnap + k) * N, dst = ((size_t)(s0 + sh) * p->nsnap + k) * N;
+                if (cudaMemcpyAsync(snap_u + dst, p->b.snap_u + src, sizeof(double) * N, cudaMemcpyDefault,
+                                    ctx->stream3) != cudaSuccess ||
+                    cudaMemcpyAsync(snap_w + dst, p->b.snap_w + src, sizeof(double) * N, cudaMemcpyDefault,
+                                    ctx->stream3) != cudaSuccess)
+                    return (int)SFG_ERR_CUDA;
+            }
+            return (int)SFG_OK;
+        };
         cudaEventRecord(e0, st);
-        rc = plan_launch(p, bidx, st, streamed ? &snap_done : nullptr);
+        rc = plan_launch(p, bidx, st, streamed ? &snap_done : nullptr, streamed ? &copy_row : nullptr);
         cudaEventRecord(e1, st);
         if (rc) { status = rc; break; }
-        if (streamed) {
-            const int S = p->pl.S, N = ctx->N, s0 = bidx * S, ns = std::min(S, run->src_num - s0);
-            for (int k = 0; k < p->nsnap && rc == SFG_OK; k++) {
-                if (cudaStreamWaitEvent(ctx->stream3, snap_done[k], 0) != cudaSuccess) { rc = SFG_ERR_CUDA; break; }
-                for (int sh = 0; sh < ns && rc == SFG_OK; sh++) {
-                    const size_t src = ((size_t)sh * p->nsnap + k) * N, dst = ((size_t)(s0 + sh) * p->nsnap + k) * N;
-                    if (cudaMemcpyAsync(snap_u + dst, p->b.snap_u + src, sizeof(double) * N, cudaMemcpyDefault,
-                                        ctx->stream3) != cudaSuccess ||
-                        cudaMemcpyAsync(snap_w + dst, p->b.snap_w + src, sizeof(double) * N, cudaMemcpyDefault,
-                                        ctx->stream3) != cudaSuccess)
-                        rc = SFG_ERR_CUDA;
-                }
-            }
-            if (cudaStreamSynchronize(ctx->stream3) != cudaSuccess) rc = SFG_ERR_CUDA;
-            if (rc) { status = fail(ctx, rc, "snapshot copies failed"); break; }
+        if (streamed && cudaStreamSynchronize(ctx->stream3) != cudaSuccess) {
+            status = fail(ctx, SFG_ERR_CUDA, "snapshot copies failed");
+            break;
         }
         tr.mark("run: launch + loop");
         rc = plan_finish(p, bidx, seis_u, seis_w, streamed ? nullptr : snap_u, streamed ? nullptr : snap_w, st, kind);

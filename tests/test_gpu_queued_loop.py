@@ -1,10 +1,12 @@
 """The time loop of large runs (sfg_run on meshes whose node count times the
-batch's shot count reaches 2^18) is queued on the stream step by step, with
-each snapshot row copied to the caller on a copy stream once it is written
-(an event per row, row 0 after the state reset).  A plan
-(sfg_plan_*) captures the same loop as one graph and copies the rows at the
-end.  The two give the same outputs bit for bit (snapshots every 25 steps,
-so that rows fall on both parities of the ping-pong state buffers)."""
+batch's shot count reaches 2^18) is queued as 16 direct steps and then as
+graphs of up to 256 steps that end after snapshot steps, two executable
+graphs updated in place in turn; snapshot rows go to the caller on a copy
+stream one chunk behind (an event per row, row 0 after the state reset).  A
+plan (sfg_plan_*) captures the same loop as one graph and copies the rows at
+the end.  The two give the same outputs bit for bit (snapshots every 25
+steps, so that chunks start on both parities of the ping-pong state
+buffers)."""
 import numpy as np
 import pytest
 
@@ -35,13 +37,13 @@ def _run_both(prob, precision, spb):
 @pytest.mark.parametrize("precision", ["fp32k", "fp64"])
 def test_one_shot_queued_loop_equals_one_graph(precision):
     prob = small_problem("Q4", n=512, step=122, pml=10, seed=3)
-    assert prob.mesh.node_num >= 1 << 18           # sfg_run queues the loop step by step
+    assert prob.mesh.node_num >= 1 << 18           # sfg_run queues the loop in chunks
     run, one, launches, stats = _run_both(prob, precision, 1)
     assert run["status"] == 0 and one["status"] == 0
     for k in KEYS:
         assert np.array_equal(run[k], one[k]), k
     assert np.linalg.norm(one["snap_u"][0, -1]) > 0     # the wave reached the snapshots
-    assert stats["kernel_launches"] == launches        # the same kernels as the plan's graph
+    assert stats["kernel_launches"] == launches        # the chunks queue the plan's kernels
 
 
 def test_batched_queued_loop_equals_one_graph():
