@@ -124,6 +124,11 @@ const char *sfg_last_error(const sfg_ctx *ctx);
  * flags, and build the device step data.  Replaces elastic_wave.c:136-313. */
 int sfg_setup(sfg_ctx *ctx, const sfg_mesh *mesh, const sfg_model *model);
 
+/* The canonical CSR of matrix 0..6 (M, K1..K6; coo2csr_lib.f90's output:
+ * p [node_num+1], j and x [nnz], 0-based).  sfg_setup keeps the union of the
+ * seven patterns with their values; the first sfg_csr_copy of a set-up forms
+ * every matrix's CSR from it (its nonzero union entries in column order, the
+ * same arrays) and keeps them on the device. */
 int sfg_csr_nnz(sfg_ctx *ctx, int matrix, int *nnz);
 int sfg_csr_copy(sfg_ctx *ctx, int matrix, int *p, int *j, double *x);
 int sfg_lumped_mass_copy(sfg_ctx *ctx, double *mass_lump);         /* [node_num] */

@@ -54,3 +54,28 @@ def test_batched_queued_loop_equals_one_graph():
     for k in KEYS:
         assert np.array_equal(run[k], one[k]), k
     assert stats["kernel_launches"] == launches
+
+
+def test_two_batches_reuse_the_chunk_graphs():
+    """96 shots in batches of 64: the second (ragged) batch's chunks update
+    the graphs the first batch's chunks left in the plan."""
+    from seisfem_b200.api import Context, Plan
+    prob = small_problem("Q4", n=64, step=122, pml=6, shots=96, seed=12)
+    assert prob.mesh.node_num * 64 >= 1 << 18
+    ctx = Context(0)
+    try:
+        ctx.setup(prob)
+        run = ctx.run(prob, precision="fp32k", shots_per_batch=64, snap_every=25)
+        plan = Plan(ctx, prob, precision="fp32k", snap_every=25, shots_per_batch=64)
+        assert plan.batches == 2
+        outs = []
+        for b in range(2):
+            plan.launch(b)
+            outs.append(plan.finish(b))
+        plan.close()
+    finally:
+        ctx.close()
+    assert run["status"] == 0
+    for k in KEYS:
+        one = np.concatenate([outs[0][k][:64], outs[1][k][64:]])   # each batch at its shots' offset
+        assert np.array_equal(run[k], one), k
