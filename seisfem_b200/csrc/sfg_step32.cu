@@ -327,7 +327,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
         if (DICT) {
             DictSlots ss;
             if (!STG) ss.init(a.sellAd + (size_t)s0 * 32 + lane, s1 - s0);
-#pragma unroll 2
+#pragma unroll 3
             for (int g = s0; g < s1; ++g) {
                 const int2 cv = STG ? stg[(g - slb) * 32 + lane] : ss.next();
                 const float4 t0 = stab[cv.y], t1 = stab[cv.y + 1];
@@ -442,7 +442,7 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
             }
         };
         if (full) {
-#pragma unroll 2
+#pragma unroll 1
             for (int g = s0; g < s1; ++g) {
                 int j;
                 float vm, kv[6];
@@ -467,7 +467,7 @@ __device__ __forceinline__ void stepZ_body(const Step2 &a, int bid, const float4
                 m[16] += vm * q1.z; m[17] += vm * q1.w; m[18] += vm * q2.x; m[19] += vm * q2.y;
             }
         } else {
-#pragma unroll 2
+#pragma unroll 1
             for (int g = s0; g < s1; ++g) {
                 int j;
                 float vm, kv[4];
