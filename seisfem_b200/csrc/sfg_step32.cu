@@ -265,6 +265,34 @@ struct DictSlots {
     }
 };
 
+// The same with three slot rows in flight: the class-A loop (unrolled by
+// three) keeps one more slot load outstanding per thread, which its
+// register budget allows and class Z's does not.
+struct DictSlots3 {
+    const int2 *p;
+    int left;
+    int2 s0, s1, s2;
+    __device__ __forceinline__ void init(const int2 *base, int n)
+    {
+        p = base;
+        left = n;
+        s0 = n > 0 ? __ldcs(p) : make_int2(0, 0);
+        s1 = n > 1 ? __ldcs(p + 32) : make_int2(0, 0);
+        s2 = n > 2 ? __ldcs(p + 64) : make_int2(0, 0);
+        p += 96;
+    }
+    __device__ __forceinline__ int2 next()
+    {
+        const int2 r = s0;
+        s0 = s1;
+        s1 = s2;
+        s2 = left > 3 ? __ldcs(p) : make_int2(0, 0);
+        p += 32;
+        left--;
+        return r;
+    }
+};
+
 // the dictionary's tuples into shared memory (2 float4 each)
 template <int THREADS>
 __device__ __forceinline__ void load_dict(const Step2 &a, float4 *stab)
@@ -325,7 +353,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
             mL[4] += vm * q1.z; mL[5] += vm * q1.w; mL[6] += vm * q2.x; mL[7] += vm * q2.y;
         };
         if (DICT) {
-            DictSlots ss;
+            DictSlots3 ss;
             if (!STG) ss.init(a.sellAd + (size_t)s0 * 32 + lane, s1 - s0);
 #pragma unroll 3
             for (int g = s0; g < s1; ++g) {
