@@ -367,7 +367,7 @@ __device__ __forceinline__ void stepA_body(const Step2 &a, int bid, const float4
             for (int k = 0; k < 8; k++) mL[k] *= rho;
         } else {
             const float *sd = a.sellA + (size_t)s0 * 192 + lane;
-#pragma unroll 2
+#pragma unroll 3
             for (int g = s0; g < s1; ++g, sd += 192) {
                 float kv[4];
 #pragma unroll
