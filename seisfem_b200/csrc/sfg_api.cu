@@ -913,8 +913,9 @@ cudaError_t queue_reset(const LoopPlan &pl, int N, int step, int nsnap, BatchBuf
 
 // Time a few steps of each candidate launch shape and keep the fastest:
 // first one shape for both class kernels, then the class-Z kernel's shape with
-// the class-A shape fixed (the two run concurrently, so the step time is the
-// objective).  The caller resets the state afterwards.
+// the class-A shape fixed, then the class-A shape with that class-Z shape (the
+// two run concurrently, so the step time is the objective).  The caller
+// resets the state afterwards.
 int autotune(sfg_ctx *ctx, LoopPlan &pl, const sfg_run_desc *run, BatchBufs &b)
 {
     if (fp64(pl) || pl.kind == SFG_FP32_PLAIN_PATH) { pl.threads = 128; return SFG_OK; }
